@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Throughput of the Matjes LLG hot path on B200: spin-updates/s and HBM roofline.
+
+Workload (default): the 1024x1024 periodic triangular monolayer with exchange
+shells J1..J3 = 1.0, -0.1, -0.05 meV, interfacial D1 = 0.2 meV, K = 0.05 meV
+easy axis, Bz = 1 T, SIB integrator, alpha = 0.1, dt = 0.1 fs, T = 10 K with
+Philox thermal noise (seed 1), initial state: +z ferromagnet with 20 reversed
+disks of radius 8.  One bench step = one full LLG time step over the lattice
+(both SIB passes, with the total energy of the incoming state fused into the
+first pass).  Synthetic data of the stated shapes; nothing is read from disk.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs one process per GPU (torchrun); the path does not shard, so every
+rank runs its own replica (Philox stream = rank) and the value is the sum over
+ranks with the time the max over ranks ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+UNIT = "spin-updates/s"
+FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
+
+
+def metric_name() -> str:
+    try:
+        with open(os.path.join(ROOT, "BASELINE.json")) as f:
+            return json.load(f)["metric"]
+    except Exception:
+        return "LLG spin-updates/s & HBM GB/s"
+
+
+def peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def workload_config(name, deck, dyn, extra=None) -> dict:
+    cfg = {
+        "workload": name,
+        "lattice": f"{deck.L[0]}x{deck.L[1]}x{deck.L[2]} triangular, periodic in-plane" if "triangular" in name
+        else f"{deck.L[0]}x{deck.L[1]}x{deck.L[2]}",
+        "terms": "J1,J2,J3 + D1 (hollow-site mediators) + uniaxial K + Zeeman",
+        "integrator": dyn["integrator"],
+        "timestep_fs": dyn["timestep"],
+        "alpha": dyn["alpha"],
+        "temperature_K": dyn["temperature"],
+        "noise": dyn.get("noise", "off"),
+        "sites": int(deck.nsites),
+        "l2": "flushed between timed steps (256 MiB write), fields 2 x 25 MB",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ----------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            if line.startswith("index") or not line.strip():
+                continue
+            parts = [p.strip() for p in line.split(",")]
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+            except Exception:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """dram bytes per launch from a committed ncu summary (profiles/<kernel>_<workload>.md),
+    per site so that it scales to the bench lattice; None if there is none."""
+    fn = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    if not os.path.exists(fn):
+        return None
+    m = re.search(r"dram_bytes_per_site:\s*([0-9.eE+-]+)", open(fn).read())
+    return float(m.group(1)) if m else None
+
+
+# ----------------------------------------------------------------------
+def cpu_oracle_rate(wname, seconds=10.0, side=512):
+    """The oracle (C restatement, OpenMP over all host threads) on a bounded
+    sample of the same workload: the same couplings and dynamics on a
+    side x side lattice."""
+    from matjes_b200.deck import workload
+    from oracle import oracle as O
+
+    w = workload(wname, scale=1024 // side)
+    dyn = dict(w["dyn"])
+    dyn.pop("steps")
+    M = O.Model(w["deck"])
+    m = w["m0"].copy()
+    t = time.perf_counter()
+    M.run(m, 2, **dyn)
+    per = (time.perf_counter() - t) / 2
+    nst = int(max(3, min(400, seconds / max(per, 1e-6))))
+    t = time.perf_counter()
+    M.run(m, nst, step0=2, **dyn)
+    el = time.perf_counter() - t
+    return {"value": w["deck"].nsites * nst / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle SIB+Philox on {side}x{side} triangular (same couplings), {nst} steps, {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle port (the reference cannot be compiled here:
+    no Fortran compiler) on the full workload, all host threads."""
+    if rank != 0:
+        return
+    from matjes_b200.deck import workload
+    from oracle import oracle as O
+
+    w = workload(args.workload)
+    dyn = dict(w["dyn"])
+    dyn.pop("steps")
+    M = O.Model(w["deck"])
+    m = w["m0"].copy()
+    M.run(m, args.warmup, **dyn)
+    t = time.perf_counter()
+    E = M.run(m, args.steps, step0=args.warmup, energies=True, **dyn)
+    el = time.perf_counter() - t
+    N = w["deck"].nsites
+    value = N * args.steps / el
+    line = {
+        "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": workload_config(args.workload, w["deck"], w["dyn"], {"energy_per_step": "after each step"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"full {w['deck'].L[0]}x{w['deck'].L[1]} lattice, {args.steps} SIB steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "final_energy_eV": float(E[-1]),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------
+def run_gpu(args, rank, world):
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import workload
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+
+    w = workload(args.workload)
+    deck, dyn = w["deck"], dict(w["dyn"])
+    dyn.pop("steps")
+    N = deck.nsites
+    ham = mj.Hamiltonian(deck, device=dev)
+    sd = mj.SpinDynamics(ham, stream_id=rank, **dyn)
+    p = sd.p
+    p.energy_mode = _abi.MJ_ENERGY_BEFORE
+    m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
+    K, W = args.steps, args.warmup
+    E = torch.zeros(W + 2 * K + 8, dtype=torch.float64, device=m.device)
+    flush = torch.empty(FLUSH_BYTES // 8, dtype=torch.float64, device=m.device)
+    stream = torch.cuda.current_stream().cuda_stream
+    lib = _abi.lib
+
+    def step(k):
+        p.step0 = k
+        _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, E[k:].data_ptr(), stream))
+
+    for k in range(W):
+        flush.zero_()
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record()
+        step(W + k)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    ck = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    # per-kernel live timing on a second pass of the same K steps
+    _abi.check(lib.mj_profile_enable(ham.plan, 1))
+    for k in range(K):
+        flush.zero_()
+        step(W + K + k)
+    prof = _abi.profile_read(ham.plan)
+    _abi.check(lib.mj_profile_enable(ham.plan, 0))
+    t = torch.tensor([ms], dtype=torch.float64, device=m.device)
+    if dist:
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = N * K * world / (ms_max / 1e3)
+
+    # end to end through the reference-facing C ABI with host buffers (pinned)
+    st = mj.SpinState(ham)
+    host = torch.empty((N, 3), dtype=torch.float64, pin_memory=True)
+    host.copy_(torch.from_numpy(w["m0"]))
+    ke = max(3, min(K, 20))
+    Eh = torch.empty(1, dtype=torch.float64, pin_memory=True)
+    times = []
+    for k in range(ke + 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _abi.check(lib.mj_state_upload(st.handle, host.data_ptr(), stream))
+        p.step0 = 10_000 + k
+        _abi.check(lib.mj_step(ham.plan, st.handle, _abi.C.byref(p), 1, E[-4:].data_ptr(), stream))
+        _abi.check(lib.mj_state_download(st.handle, host.data_ptr(), stream))
+        Eh.copy_(E[-4:-3])
+        _ = float(Eh.item())
+        if k >= 2:
+            times.append(time.perf_counter() - t0)
+    te = torch.tensor([sum(times)], dtype=torch.float64, device=m.device)
+    if dist:
+        td.all_reduce(te, op=td.ReduceOp.MAX)
+    e2e = N * len(times) * world / float(te.item())
+
+    if rank != 0:
+        return
+    pk = peaks()
+    bytes_site = {"k_sib1": 48.0, "k_sib2": 72.0}
+    kernels = {}
+    for name, (tot, cnt) in prof.items():
+        avg = tot / max(cnt, 1)
+        b = bytes_site.get(name, 0.0) * N
+        kernels[name] = {"launches": cnt, "avg_us": 1e3 * avg, "alg_bytes": b,
+                         "achieved_gbs": (b / (avg / 1e3) / 1e9) if b else None}
+    dom = max((k for k in kernels if k in bytes_site), key=lambda k: kernels[k]["avg_us"])
+    ach = kernels[dom]["achieved_gbs"]
+    tr = ncu_traffic(dom, args.workload)
+    cpu = cpu_oracle_rate(args.workload) if (world == 1 and not args.no_cpu_baseline) else None
+    line = {
+        "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args.workload, deck, w["dyn"],
+                                                       {"parallelism": f"replicas x{world}" if world > 1 else "single",
+                                                        "energy_per_step": "fused into pass 1"}),
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
+                     "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},
+        "step_roofline": {"alg_bytes_per_site": 120.0,
+                          "achieved_gbs": 120.0 * N / (ms_max / K / 1e3) / 1e9,
+                          "frac": 120.0 * N / (ms_max / K / 1e3) / 1e9 / pk["hbm_gbs"]},
+        "kernels": kernels,
+        "clocks": ck,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 24 * N + 8,
+                "path": "mj_state_upload (pinned AoS) + mj_step + mj_state_download + energy read"},
+        "gpu_launches": 2 * K,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="triangular1024_thermal")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_gpu(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as td
+
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

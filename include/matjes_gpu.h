@@ -1,0 +1,205 @@
+/*
+ * matjes_gpu.h -- C ABI of the B200-native Matjes spin-dynamics hot path.
+ *
+ * Plain C: pointers, fixed-width integers and doubles only; no CUDA or torch
+ * types in any signature (a stream is passed as `void*` holding a
+ * cudaStream_t, NULL = legacy default stream).  Every call returns an
+ * mj_status; mj_last_error() gives the message of the last failure on the
+ * calling thread.  Nothing aborts.
+ *
+ * Physical conventions are Matjes' own (src/ paths of the Matjes tree):
+ *   energies and fields in eV (B_eff = -dE/dm), applied field in Tesla,
+ *   time in fs, lengths in nm, hbar = 0.658211928 eV fs
+ *   (fixed-parameters/constant.f90:28), the Landau-Lifshitz form of
+ *   solvers/propagator.f90:13-58.
+ *
+ * Host arrays use the reference layout (AoS, m[3*site+comp], site =
+ * cell*Nmag + imag, cell = x + Lx*(y + Ly*z));  device arrays are SoA
+ * (x[N], y[N], z[N] with one base pointer of 3N doubles).
+ */
+#ifndef MATJES_GPU_H
+#define MATJES_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t mj_status;
+enum {
+    MJ_OK = 0,
+    MJ_ERR_ARG = 1,         /* bad argument / size */
+    MJ_ERR_OOM = 2,         /* device or host allocation failed */
+    MJ_ERR_CUDA = 3,        /* CUDA runtime / cuFFT error */
+    MJ_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    MJ_ERR_NAN = 5,         /* non-finite value detected in the state */
+    MJ_ERR_UNSUPPORTED = 6, /* input outside what the kernels implement */
+    MJ_ERR_GEOMETRY = 7     /* shell / DMI geometry could not be built */
+};
+
+enum { MJ_EULER = 1, MJ_HEUN_MATJES = 2, MJ_SIB = 3 };
+enum { MJ_NOISE_OFF = 0, MJ_NOISE_PHILOX = 1, MJ_NOISE_INJECT = 2 };
+
+#define MJ_MAX_ATOMS 16
+
+/* Lattice and cell: IO-input/rw_lattice.f90:28-80 (Periodic_log, alat,
+ * lattice, Nsize) and IO-input/rw_cell.f90:5-31 (atomtypes / atoms). */
+typedef struct {
+    int32_t L[3];            /* Nsize */
+    int32_t periodic[3];     /* Periodic_log */
+    double areal[3][3];      /* lattice vectors as rows, in nm (alat applied) */
+    int32_t natom;
+    double frac[MJ_MAX_ATOMS][3];  /* fractional atom positions */
+    int32_t attype[MJ_MAX_ATOMS];  /* atom type id (1-based) */
+    double moment[MJ_MAX_ATOMS];   /* magnetic moment in mu_B, > 0 = magnetic */
+} mj_lattice_desc;
+
+/* magnetic_J  t1 t2 shell J  (Energy/exchange_Heisenberg_J.f90:18-130) */
+typedef struct { int32_t t1, t2, shell; double value; } mj_exchange_term;
+/* magnetic_D  t1 t2 mediator shell D  (Energy/exchange_Heisenberg_D.f90:11-144) */
+typedef struct { int32_t t1, t2, tmed, shell; double value; } mj_dmi_term;
+/* magnetic_anisotropy  type  ex ey ez  K  (Energy/anisotropy_heisenberg.f90:148-292) */
+typedef struct { int32_t type; double axis[3]; double value; } mj_aniso_term;
+
+typedef struct {
+    int32_t nJ; const mj_exchange_term* J;
+    int32_t nD; const mj_dmi_term* D;
+    int32_t nK; const mj_aniso_term* K;
+    double c_H_J, c_H_D, c_H_ani, c_zeeman; /* reference defaults: -1, -1, +1, -1 */
+    double B_ext[3];                        /* H_ext (Tesla) */
+    int32_t zeeman_on;                      /* enable_H; also on when |H_ext| >= 1e-8 */
+    int32_t dip_on;                         /* mag_dip_use (FFT route) */
+    int32_t dip_period_cut[3];              /* mag_dip_period_cut, default 1 1 1 */
+} mj_hamiltonian_desc;
+
+typedef struct {
+    int32_t integrator;   /* MJ_EULER, MJ_HEUN_MATJES, MJ_SIB */
+    double timestep;      /* fs (the deck's `timestep`) */
+    double alpha;         /* damping */
+    double temperature;   /* K */
+    int32_t noise;        /* MJ_NOISE_* */
+    uint64_t seed;        /* Philox key */
+    uint32_t stream_id;   /* replica id folded into the Philox counter */
+    uint32_t step0;       /* global index of the first step (Philox counter / inject slot) */
+    const double* inject; /* device N(0,1) buffer, layout [nbuf][3][N] (MJ_NOISE_INJECT) */
+    int32_t inject_nbuf;
+    int32_t energy_mode;  /* MJ_ENERGY_AFTER (reference: E after each step, one extra
+                             field pass per call) or MJ_ENERGY_BEFORE (E of the state
+                             entering each step, fused into the first pass, no extra pass) */
+} mj_dyn_params;
+
+enum { MJ_ENERGY_AFTER = 0, MJ_ENERGY_BEFORE = 1 };
+
+typedef struct mj_plan mj_plan;
+typedef struct mj_state mj_state;
+
+/* ---- errors ---------------------------------------------------------- */
+/* Message of the last failing call on this thread (never NULL). */
+const char* mj_last_error(void);
+/* Library version string. */
+const char* mj_version(void);
+
+/* ---- plans (Hamiltonian + lattice, device resident) ------------------- */
+/* Replaces the Hamiltonian set-up path setup/setup-simu.f90:104-110 ->
+ * Energy/set_Hamiltonians.f90:9-180 -> Hamiltonian_type/ham_cusparse.f90:134-153
+ * -> cuda_H_init (Hamiltonian_type/cuda_H.cu:45-133), and for the dipolar term
+ * Energy/set_fft_Hamiltonians.f90:8-79 -> cuda_fft_init / set_cuda_fft_plan /
+ * cuda_fft_set_operator (Hamiltonian_type/cuda_fft.cpp:10-143).  Shells are
+ * rebuilt on the host exactly like setup/neighbor_type.f90:78-330; single-atom
+ * cells become a fused stencil, multi-atom cells an ELL matrix. */
+mj_status mj_plan_create(const mj_lattice_desc* lat, const mj_hamiltonian_desc* ham,
+                         int32_t device, mj_plan** out);
+/* Replaces cuda_H_init (Hamiltonian_type/cuda_H.cu:45-133) for a Hamiltonian
+ * handed over as COO triplets (the reference passes 1-based rows/cols,
+ * Hamiltonian_type/ham_coo.f90:158-196; `base` is 0 or 1).  The triplets are
+ * the combined "MM" matrix H (3N x 3N); zeeman[s] is the "BM" coefficient
+ * mu0*muB*c_zeeman*mu_s of site s and b_cell the applied field per cell.  The
+ * field is B = -(H + H^T) m - zeeman*b. */
+mj_status mj_plan_from_coo(int64_t nsites, int64_t nnz, const int64_t* rows, const int64_t* cols,
+                           const double* vals, int32_t base, const double* zeeman,
+                           const double* b_cell, int32_t device, mj_plan** out);
+/* Replaces cuda_H_destroy / cuda_fft destroy (cuda_H.cu:315-344, cuda_fft.cpp:145-180). */
+mj_status mj_plan_destroy(mj_plan* plan);
+/* Number of spin sites N (= Ncell * Nmag). */
+mj_status mj_plan_nsites(const mj_plan* plan, int64_t* n);
+/* Stencil introspection: number of neighbour offsets (0 for ELL plans). */
+mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n);
+/* Per-site applied field map (Tesla, host AoS 3*Ncell; NULL = uniform H_ext):
+ * the Bfield_init.dat input read by initialization/orders_initialize.f90:28. */
+mj_status mj_plan_set_bfield(mj_plan* plan, const double* b_cell_host);
+/* Same, from a device SoA buffer (3*Ncell doubles, copied). */
+mj_status mj_plan_set_bfield_device(mj_plan* plan, const double* b_cell_dev_soa, void* stream);
+
+/* Host-only (touches no GPU): the fused stencil a single-atom deck compiles to,
+ * i.e. the couplings Energy/set_Hamiltonians.f90:9-180 would hand to
+ * cuda_H_init, folded per neighbour offset: B_i = sum_o W_o m_{i+o} + W0 m_i
+ * + zc b_i with W_o = -(T_o + T_{-o}^T).  offsets: 3*cap ints, W: 9*cap doubles
+ * (row-major), W0: 9 doubles.  MJ_ERR_UNSUPPORTED for multi-atom cells. */
+mj_status mj_stencil_describe(const mj_lattice_desc* lat, const mj_hamiltonian_desc* ham, int32_t cap,
+                              int32_t* n_off, int32_t* offsets, double* W, double* W0, double* zc);
+
+/* ---- states (spin field, device resident SoA) ------------------------- */
+/* Replaces cuda_fvec_init / cuda_fvec_alloccopy (cuda_H_vec.cu:11-43). */
+mj_status mj_state_create(const mj_plan* plan, mj_state** out);
+mj_status mj_state_destroy(mj_state* st);
+/* Host AoS -> device SoA (cuda_fvec_set, cuda_H_vec.cu:60-73). */
+mj_status mj_state_upload(mj_state* st, const double* m_host_aos, void* stream);
+/* Device SoA -> host AoS (cuda_fvec_get, cuda_H_vec.cu:75-88). */
+mj_status mj_state_download(const mj_state* st, double* m_host_aos, void* stream);
+/* Device pointer of the SoA spin field (3N doubles: x block, y block, z block). */
+mj_status mj_state_device_ptr(const mj_state* st, double** m_dev_soa);
+
+/* ---- field and energy ------------------------------------------------- */
+/* B_eff = -dE/dm: hamiltonian%get_eff_field (Hamiltonian_type/hamiltonian_collection.f90:433-454,
+ * reached from dynamics/spindynamics.f90:298).  Device SoA output (3N); e_site
+ * (device, N, may be NULL) is the per-site energy of energy_distrib
+ * (hamiltonian_collection.f90:332-363). */
+mj_status mj_field(mj_plan* plan, const mj_state* st, double* B_dev_soa, double* e_site_dev, void* stream);
+/* Same on caller-owned device SoA spins (torch tensors). */
+mj_status mj_field_dev(mj_plan* plan, const double* m_dev_soa, double* B_dev_soa, double* e_site_dev, void* stream);
+/* hamiltonian%energy (hamiltonian_collection.f90:390-400): total energy in eV,
+ * synchronous, written to *E_host. */
+mj_status mj_energy(mj_plan* plan, const mj_state* st, double* E_host);
+/* Host-array convenience form of get_eff_field (reference AoS layout); it
+ * uploads m, evaluates, downloads B and e_site (may be NULL); synchronous. */
+mj_status mj_field_host(mj_plan* plan, const double* m_host_aos, double* B_host_aos, double* e_site_host);
+
+/* ---- dynamics ----------------------------------------------------------- */
+/* nsteps LLG time steps in place: the loop body dynamics/spindynamics.f90:260-323
+ * (stage loop 282-313, thermal field 268-272, energy 323).  E_dev (device,
+ * nsteps doubles, may be NULL) receives H%energy after each step. */
+mj_status mj_step(mj_plan* plan, mj_state* st, const mj_dyn_params* p, int32_t nsteps,
+                  double* E_dev, void* stream);
+/* Same on caller-owned device SoA spins. */
+mj_status mj_step_dev(mj_plan* plan, double* m_dev_soa, const mj_dyn_params* p, int32_t nsteps,
+                      double* E_dev, void* stream);
+/* Host-array convenience: upload m, run nsteps, download m and E (host, may be NULL). */
+mj_status mj_step_host(mj_plan* plan, double* m_host_aos, const mj_dyn_params* p, int32_t nsteps,
+                       double* E_host);
+/* The step loop captured once as a CUDA graph of `nsteps` steps and replayed
+ * `nreplay` times (steps advance p->step0 by nsteps per replay). */
+mj_status mj_graph_run(mj_plan* plan, mj_state* st, const mj_dyn_params* p, int32_t nsteps,
+                       int32_t nreplay, double* E_dev, void* stream);
+
+/* Per-kernel device timing of a plan (CUDA events around every kernel the plan
+ * launches), the evidence behind the achieved-bandwidth figures; no
+ * counterpart in the reference, which only times the whole dynamics with
+ * cpu_time (dynamics/spindynamics.f90:118,456-457).  enable != 0 clears the
+ * accumulators and starts recording; mj_profile_read synchronises and returns
+ * up to `cap` kernels: names (32 chars each), total ms and launch counts. */
+mj_status mj_profile_enable(mj_plan* plan, int32_t enable);
+mj_status mj_profile_read(mj_plan* plan, int32_t cap, char* names, double* total_ms, int64_t* launches,
+                          int32_t* n);
+
+/* Thermal helpers: reference temperature estimator T = sum|m x B|^2 / (2 kB sum m.B)
+ * (dynamics/measure_temp.f90:21-43), synchronous. */
+mj_status mj_measure_temperature(mj_plan* plan, const mj_state* st, double* T_host);
+/* Philox N(0,1) triples exactly as the thermal kernels draw them (device SoA [3][n]). */
+mj_status mj_philox_normals(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n,
+                            double* out_dev_soa, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MATJES_GPU_H */

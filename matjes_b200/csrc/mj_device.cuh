@@ -1,0 +1,202 @@
+// Device helpers shared by the field, step, batch and adjoint kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mj_internal.hpp"
+
+namespace mj {
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11) and Box-Muller normals.  Counter = (site, step, stream,
+// call), key = the 64-bit seed.  Two calls give two Box-Muller pairs of 53-bit
+// uniforms: (r1 cos t1, r1 sin t1, r2 cos t2).
+__device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += W0;
+            k1 += W1;
+        }
+        const uint32_t lo0 = M0 * c[0], hi0 = __umulhi(M0, c[0]);
+        const uint32_t lo1 = M1 * c[2], hi1 = __umulhi(M1, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ k0;
+        const uint32_t n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+    }
+}
+
+__device__ __forceinline__ double u53_open(uint32_t a, uint32_t b) {
+    const uint64_t k = (static_cast<uint64_t>(a >> 5) << 26) | static_cast<uint64_t>(b >> 6);
+    return static_cast<double>(k + 1) * (1.0 / 9007199254740992.0);
+}
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    const uint64_t k = (static_cast<uint64_t>(a >> 5) << 26) | static_cast<uint64_t>(b >> 6);
+    return static_cast<double>(k) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site) {
+    const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+    uint32_t c[4] = {site, step, stream, 0u};
+    philox10(c, k0, k1);
+    uint32_t d[4] = {site, step, stream, 1u};
+    philox10(d, k0, k1);
+    const double r1 = sqrt(-2.0 * log(u53_open(c[0], c[1])));
+    const double r2 = sqrt(-2.0 * log(u53_open(d[0], d[1])));
+    double s1, c1;
+    sincos(6.283185307179586 * u53(c[2], c[3]), &s1, &c1);
+    const double c2 = cos(6.283185307179586 * u53(d[2], d[3]));
+    return make_double3(r1 * c1, r1 * s1, r2 * c2);
+}
+
+// Thermal field b = sigma * N(0,1) (dynamics/spindynamics.f90:268-272): Philox
+// in-kernel, or read from an injected N(0,1) buffer laid out [nbuf][3][N].
+__device__ __forceinline__ double3 thermal_field(const DynCoef& C, uint32_t step, int64_t i, int64_t N) {
+    if (C.step_base) step += *C.step_base;
+    if (C.noise == MJ_NOISE_PHILOX) {
+        const double3 z = philox_normals(C.seed, step, C.stream_id, static_cast<uint32_t>(i));
+        return make_double3(C.sigma * z.x, C.sigma * z.y, C.sigma * z.z);
+    }
+    const double* buf = C.inject + static_cast<int64_t>(step % static_cast<uint32_t>(C.inject_nbuf)) * 3 * N;
+    return make_double3(C.sigma * __ldg(buf + i), C.sigma * __ldg(buf + N + i), C.sigma * __ldg(buf + 2 * N + i));
+}
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double3 cross(double3 a, double3 b) {
+    return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double dot(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+__device__ __forceinline__ double3 ld3(const double* __restrict__ m, int64_t i, int64_t N) {
+    return make_double3(__ldg(m + i), __ldg(m + N + i), __ldg(m + 2 * N + i));
+}
+__device__ __forceinline__ void st3(double* m, int64_t i, int64_t N, double3 v) {
+    m[i] = v.x;
+    m[N + i] = v.y;
+    m[2 * N + i] = v.z;
+}
+
+__device__ __forceinline__ double3 ld_dip(const DipView& v, int x, int y, int z) {
+    const int64_t q = x + static_cast<int64_t>(v.px) * (y + static_cast<int64_t>(v.py) * z);
+    return make_double3(__ldg(v.h + q), __ldg(v.h + v.nk + q), __ldg(v.h + 2 * v.nk + q));
+}
+
+// Matjes LLG right-hand side (solvers/propagator.f90:13-58):
+// D = -[m^ x B + alpha m^ x (m^ x B)] / (1 + alpha^2), m^ = m/|m| when |m| > 1e-8.
+__device__ __forceinline__ double3 llg_rhs(double3 B, double3 m, double alpha, double inv_den) {
+    const double n2 = dot(m, m);
+    double3 mn = m;
+    if (n2 > 1e-16) {
+        const double inv = 1.0 / sqrt(n2);
+        mn = make_double3(m.x * inv, m.y * inv, m.z * inv);
+    }
+    const double3 t = cross(mn, B);
+    const double3 l = make_double3(B.x + alpha * t.x, B.y + alpha * t.y, B.z + alpha * t.z);
+    const double3 o = cross(mn, l);
+    return make_double3(-o.x * inv_den, -o.y * inv_den, -o.z * inv_den);
+}
+
+// Projection onto the old norm (solvers/solver.f90:113-116), |t| > 1e-8 guard.
+__device__ __forceinline__ double3 project(double3 t, double3 m) {
+    const double nt = sqrt(dot(t, t));
+    if (!(nt > 1e-8)) return m;
+    const double s = sqrt(dot(m, m)) / nt;
+    return make_double3(t.x * s, t.y * s, t.z * s);
+}
+
+// SIB stage (Mentink et al., J. Phys.: Condens. Matter 22, 176001 (2010)):
+// y = m + ((m + y)/2) x a,  h = a/2 = hc (H + alpha p^ x H), hc = -dt/(2 hbar (1+alpha^2)).
+// Closed form: y = (d - h x d + (h.d) h) / (1 + |h|^2), d = m + m x h  (|y| = |m|).
+__device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, double alpha, double hc) {
+    const double np2 = dot(p, p);
+    double3 pn = p;
+    if (np2 > 1e-16) {
+        const double inv = 1.0 / sqrt(np2);
+        pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
+    }
+    const double3 pxh = cross(pn, H);
+    const double3 h = make_double3(hc * (H.x + alpha * pxh.x), hc * (H.y + alpha * pxh.y), hc * (H.z + alpha * pxh.z));
+    const double3 mxh = cross(m, h);
+    const double3 d = make_double3(m.x + mxh.x, m.y + mxh.y, m.z + mxh.z);
+    const double3 hxd = cross(h, d);
+    const double hd = dot(h, d);
+    const double inv = 1.0 / (1.0 + dot(h, h));
+    return make_double3((d.x - hxd.x + hd * h.x) * inv, (d.y - hxd.y + hd * h.y) * inv, (d.z - hxd.z + hd * h.z) * inv);
+}
+
+// ---------------------------------------------------------------------------
+struct FieldOut {
+    double3 B;     // real-space field (MM + Zeeman)
+    double3 Bzee;  // Zeeman part
+};
+
+// Per-site energy (energy_distrib, left-assigned; hamiltonian_collection.f90:332-363):
+// E_i = m.(H m)_i + E_zee,i with (H m)_i = -B_mm/2 for the symmetric combined MM
+// matrix, and the dipolar term doubled as in fft_ham_base.f90:247-256.
+__device__ __forceinline__ double site_energy(const FieldOut& f, double3 m, double3 Hd) {
+    const double3 Bmm = make_double3(f.B.x - f.Bzee.x, f.B.y - f.Bzee.y, f.B.z - f.Bzee.z);
+    return -0.5 * dot(m, Bmm) - dot(m, f.Bzee) + 2.0 * dot(m, Hd);
+}
+// Contribution of one site to H%energy (dipolar counted once, fft_ham_base.f90:258-267).
+__device__ __forceinline__ double total_energy_part(const FieldOut& f, double3 m, double3 Hd) {
+    const double3 Bmm = make_double3(f.B.x - f.Bzee.x, f.B.y - f.Bzee.y, f.B.z - f.Bzee.z);
+    return -0.5 * dot(m, Bmm) - dot(m, f.Bzee) + dot(m, Hd);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic grid reduction of NV doubles for blocks of 256 threads:
+// per-block partials in block order, summed by the last block to finish;
+// the ticket counter is re-armed by that block.
+template <int NV>
+__device__ void grid_reduce(double (&v)[NV], double* partials, unsigned int* counter, double* out, int nblocks) {
+    __shared__ double wsum[NV][8];
+    __shared__ bool last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double e = v[q];
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+        if (lane == 0) wsum[q][wid] = e;
+    }
+    __syncthreads();
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < nthr / 32; ++w) s += wsum[q][w];
+            partials[static_cast<int64_t>(q) * nblocks + bid] = s;
+        }
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == static_cast<unsigned int>(nblocks - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0.0;
+        for (int b = tid; b < nblocks; b += nthr) s += __ldcg(partials + static_cast<int64_t>(q) * nblocks + b);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        __syncthreads();
+        if (lane == 0) wsum[q][wid] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < nthr / 32; ++w) t += wsum[q][w];
+            out[q] = t;
+        }
+    }
+    if (tid == 0) *counter = 0u;
+}
+
+}  // namespace mj

@@ -1,0 +1,173 @@
+// Internal declarations shared by the host builder, the kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/matjes_gpu.h"
+
+namespace mj {
+
+// fixed-parameters/constant.f90:11-32
+constexpr double kHbar = 0.658211928;         // eV fs
+constexpr double kKB = 0.000086173324;        // eV / K
+constexpr double kMuB = 0.0000578838180661;   // eV / T
+constexpr double kDipPref = 6.745817653234234066975e-7;  // Energy/dipolar_magnetic.f90:41
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+constexpr int kMaxOff = 48;  // neighbour offsets held in the launch parameters
+
+// One 3x3 coupling block of the "MM" Hamiltonian: rows = components of
+// magnetic atom a in cell c, cols = components of magnetic atom b in cell c+o.
+struct Block {
+    int a, b;
+    int o[3];
+    double T[9];  // row-major
+};
+
+struct Geometry {
+    mj_lattice_desc d;
+    double pos[MJ_MAX_ATOMS][3];  // nm
+    int magidx[MJ_MAX_ATOMS];
+    int magatom[MJ_MAX_ATOMS];
+    int nmag = 0;
+};
+
+// Host builder (mj_lattice.cpp).  Returns false with `err` set on failure.
+bool build_geometry(const mj_lattice_desc& lat, Geometry& g, std::string& err);
+bool build_blocks(const Geometry& g, const mj_hamiltonian_desc& ham, std::vector<Block>& blocks,
+                  std::vector<double>& onsite /* 9*nmag*nmag, per (a,b) pair at o=0 */, std::string& err);
+// Real-space dipolar K on the N_rep grid (Nmag = 1): K[k*9 + 3r + c].
+bool build_dipolar_kernel(const Geometry& g, const mj_hamiltonian_desc& ham, int nrep[3],
+                          std::vector<double>& K, std::string& err);
+
+// Launch-parameter image of a single-atom stencil.  Passed by value
+// (__grid_constant__) so that every plan can run without global state.
+struct StencilParams {
+    int L[3];
+    int periodic[3];
+    int n_off;
+    int has_onsite;
+    int off[kMaxOff][3];
+    int iso[kMaxOff];         // 1 when W == w*I (pure exchange offset)
+    double W[kMaxOff][9];     // B_i += W_o m_{i+o},  W_o = -(T_o + T_{-o}^T)
+    double W0[9];             // on-site: -(T_0 + T_0^T)
+    double zc;                // B_i += zc * b_cell,  zc = -(mu0 muB c_zeeman mu_s)
+    double bext[3];
+    int zee_on;
+};
+
+// Dipolar H on the padded FFT grid (the unpack is fused into the consumers):
+// component c of site (x,y,z) is h[c*nk + x + px*(y + py*z)].
+struct DipView {
+    const double* h;
+    int64_t nk;
+    int px, py;
+};
+
+// Dynamics coefficients computed once per call on the host.
+struct DynCoef {
+    int integrator;
+    int thermal;
+    int noise;
+    double h_over_hbar;   // stage dt / hbar (Euler, Heun)
+    double inv_den;       // 1/(1+alpha^2)
+    double alpha;
+    double sib_hc;        // -0.5 (dt/hbar)/(1+alpha^2)
+    double sigma;         // sqrt(alpha kT hbar / dt_noise)
+    uint64_t seed;
+    uint32_t stream_id;
+    const double* inject;
+    int inject_nbuf;
+    // graph replay: the thermal step index is *step_base + step (null = step)
+    const uint32_t* step_base;
+};
+
+}  // namespace mj
+
+struct mj_plan {
+    int device = 0;
+    int64_t N = 0;        // spin sites
+    int64_t ncell = 0;
+    int nmag = 1;
+    bool is_stencil = true;
+    mj::StencilParams sp{};
+    // ELL form (multi-atom cells, COO input): width entries per site
+    int ell_width = 0;
+    int* d_ell_col = nullptr;        // [width][N], -1 = empty
+    double* d_ell_val = nullptr;     // [width][9][N]
+    double* d_zee = nullptr;         // per-site Zeeman coefficient zc (ELL)
+    // applied field map (SoA per cell) or null for uniform
+    double* d_bmap = nullptr;
+    std::vector<double> bext_cell;   // ELL uniform field
+    // dipolar
+    bool dip_on = false;
+    int nrep[3] = {0, 0, 0};
+    void* dip = nullptr;             // DipolarPlan (mj_dipolar.cu)
+    // scratch
+    double* d_mid = nullptr;         // 3N
+    double* d_aux = nullptr;         // 3N (Heun D1)
+    double* d_aux2 = nullptr;        // 3N (Heun DT)
+    double* d_field = nullptr;       // 3N (field scratch)
+    double* d_partials = nullptr;    // per-block energy partials
+    unsigned int* d_counter = nullptr;
+    double* d_scalar = nullptr;      // 8 doubles of device scratch
+    int64_t partial_cap = 0;
+    // host-array convenience calls (allocated on first use)
+    double* d_stage = nullptr;       // 3N AoS staging
+    double* d_tmp_m = nullptr;       // 3N
+    double* d_tmp_b = nullptr;       // 3N
+    double* d_tmp_e = nullptr;       // N + 8
+    // CUDA graph of a step loop (mj_graph_run), cached with the key it was captured for
+    uint32_t* d_stepctr = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::string graph_key;
+    // per-kernel event timing (mj_profile_enable / mj_profile_read)
+    bool prof_on = false;
+    struct ProfRec {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof;
+    std::vector<std::string> prof_names;
+    std::vector<mj::Block> blocks;   // kept for the adjoint / introspection
+};
+
+struct mj_state {
+    const mj_plan* plan = nullptr;
+    double* d_m = nullptr;  // SoA 3N
+};
+
+namespace mj {
+// error reporting (mj_abi.cpp)
+mj_status set_error(mj_status st, const std::string& msg);
+mj_status cuda_status(cudaError_t e, const char* where);
+
+// per-kernel timing records (mj_abi.cpp); prof_begin returns -1 when not recording
+int prof_begin(mj_plan* p, const char* name, cudaStream_t s);
+void prof_end(mj_plan* p, int rec, cudaStream_t s);
+
+// kernel launchers (mj_kernels.cu)
+mj_status launch_field(mj_plan* p, const double* m, double* B, double* e_site, double* E_out, cudaStream_t s);
+// one time step; Euler writes m_out, the two-pass schemes update m in place
+mj_status launch_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uint32_t step, double* E_prev_out,
+                      cudaStream_t s);
+mj_status launch_energy(mj_plan* p, const double* m, double* E_out, cudaStream_t s);
+mj_status launch_philox(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n, double* out, cudaStream_t s);
+mj_status launch_temperature(mj_plan* p, const double* m, double* out2 /* device: [sum|mxB|^2, sum m.B] */, cudaStream_t s);
+mj_status step_counter(uint32_t* ctr, uint32_t value, bool add, cudaStream_t s);
+mj_status aos_to_soa(const double* src_aos, double* dst_soa, int64_t n, cudaStream_t s);
+mj_status soa_to_aos(const double* src_soa, double* dst_aos, int64_t n, cudaStream_t s);
+int64_t energy_blocks(const mj_plan* p);
+
+// dipolar (mj_dipolar.cu)
+mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t s);
+void dipolar_destroy(mj_plan* p);
+// H = K * m on the padded grid; consumers read it through dipolar_view and fold B -= 2H.
+mj_status dipolar_apply(mj_plan* p, const double* m, double* H_unused, cudaStream_t s);
+DipView dipolar_view(const mj_plan* p);
+}  // namespace mj

@@ -1,0 +1,532 @@
+// Fused field + LLG kernels for the Matjes hot path (sm_100a, FP64).
+//
+// Every pass reads the spin field once (SoA, coalesced along x), evaluates the
+// effective field of all real-space terms, and fuses the LLG torque and the
+// integrator update into the same pass:
+//   Euler        1 pass   : m' = P(m + (D + DT) h/hbar)            (solvers/solver.f90:97-118)
+//   Heun-Matjes  2 passes : predictor m~, corrector from m~         (dynamics/spindynamics.f90:282-313)
+//   SIB          2 passes : Cayley predictor -> midpoint, corrector (Mentink et al. 2010)
+// The total energy of the incoming state (dynamics/spindynamics.f90:323) is
+// reduced in the first pass at no extra DRAM traffic, deterministically
+// (per-block partials summed in block order by the last block to finish).
+//
+// The passes are templates over a field provider: StencilField (single-atom
+// cells; neighbour offsets and 3x3 tensors in the launch parameters) or
+// EllField (multi-atom cells and COO input; per-site tensor lists).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mj_device.cuh"
+#include "mj_internal.hpp"
+
+namespace mj {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Field providers
+struct StencilField {
+    StencilParams P;
+    const double* bmap;  // per-cell applied field, SoA (null = uniform)
+
+    static constexpr int BX = 32, BY = 8;
+    __device__ __forceinline__ int64_t nsites() const { return static_cast<int64_t>(P.L[0]) * P.L[1] * P.L[2]; }
+    __device__ __forceinline__ bool site(int64_t& i, int& x, int& y, int& z) const {
+        x = blockIdx.x * BX + threadIdx.x;
+        y = blockIdx.y * BY + threadIdx.y;
+        z = blockIdx.z;
+        const bool a = x < P.L[0] && y < P.L[1];
+        i = a ? x + static_cast<int64_t>(P.L[0]) * (y + static_cast<int64_t>(P.L[1]) * z) : 0;
+        return a;
+    }
+    __device__ __forceinline__ FieldOut field(const double* __restrict__ m, int64_t i, int x, int y, int z, double3 m0) const {
+        const int64_t N = nsites();
+        const double* __restrict__ mx = m;
+        const double* __restrict__ my = m + N;
+        const double* __restrict__ mz = m + 2 * N;
+        double bx = 0.0, by = 0.0, bz = 0.0;
+        const int Lx = P.L[0], Ly = P.L[1], Lz = P.L[2];
+        for (int k = 0; k < P.n_off; ++k) {
+            int nx = x + P.off[k][0], ny = y + P.off[k][1], nz = z + P.off[k][2];
+            if (nx < 0 || nx >= Lx) {
+                if (!P.periodic[0]) continue;
+                nx = ((nx % Lx) + Lx) % Lx;
+            }
+            if (ny < 0 || ny >= Ly) {
+                if (!P.periodic[1]) continue;
+                ny = ((ny % Ly) + Ly) % Ly;
+            }
+            if (nz < 0 || nz >= Lz) {
+                if (!P.periodic[2]) continue;
+                nz = ((nz % Lz) + Lz) % Lz;
+            }
+            const int64_t j = nx + static_cast<int64_t>(Lx) * (ny + static_cast<int64_t>(Ly) * nz);
+            const double ax = __ldg(mx + j), ay = __ldg(my + j), az = __ldg(mz + j);
+            const double* W = P.W[k];
+            if (P.iso[k]) {
+                const double w = W[0];
+                bx = fma(w, ax, bx);
+                by = fma(w, ay, by);
+                bz = fma(w, az, bz);
+            } else {
+                bx = fma(W[0], ax, fma(W[1], ay, fma(W[2], az, bx)));
+                by = fma(W[3], ax, fma(W[4], ay, fma(W[5], az, by)));
+                bz = fma(W[6], ax, fma(W[7], ay, fma(W[8], az, bz)));
+            }
+        }
+        if (P.has_onsite) {
+            const double* W = P.W0;
+            bx = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, bx)));
+            by = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, by)));
+            bz = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, bz)));
+        }
+        FieldOut f;
+        f.Bzee = make_double3(0.0, 0.0, 0.0);
+        if (P.zee_on) {
+            double3 b;
+            if (bmap) b = make_double3(__ldg(bmap + i), __ldg(bmap + N + i), __ldg(bmap + 2 * N + i));
+            else b = make_double3(P.bext[0], P.bext[1], P.bext[2]);
+            f.Bzee = make_double3(P.zc * b.x, P.zc * b.y, P.zc * b.z);
+        }
+        f.B = make_double3(bx + f.Bzee.x, by + f.Bzee.y, bz + f.Bzee.z);
+        return f;
+    }
+};
+
+struct EllField {
+    int64_t N;
+    int64_t ncell;
+    int nmag;
+    int width;
+    const int* col;      // [width][N]
+    const double* val;   // [width][9][N]
+    const double* zc;    // [N]
+    const double* bmap;  // per-cell SoA (null = uniform bext)
+    double bext[3];
+    int zee_on;
+
+    static constexpr int BX = 256, BY = 1;
+    __device__ __forceinline__ int64_t nsites() const { return N; }
+    __device__ __forceinline__ bool site(int64_t& i, int& x, int& y, int& z) const {
+        i = blockIdx.x * static_cast<int64_t>(BX) + threadIdx.x;
+        x = y = z = 0;
+        const bool a = i < N;
+        if (!a) i = 0;
+        return a;
+    }
+    __device__ __forceinline__ FieldOut field(const double* __restrict__ m, int64_t i, int, int, int, double3) const {
+        double bx = 0.0, by = 0.0, bz = 0.0;
+        for (int k = 0; k < width; ++k) {
+            const int j = __ldg(col + static_cast<int64_t>(k) * N + i);
+            if (j < 0) continue;
+            const double ax = __ldg(m + j), ay = __ldg(m + N + j), az = __ldg(m + 2 * N + j);
+            const double* W = val + static_cast<int64_t>(k) * 9 * N + i;
+            bx = fma(__ldg(W + 0 * N), ax, fma(__ldg(W + 1 * N), ay, fma(__ldg(W + 2 * N), az, bx)));
+            by = fma(__ldg(W + 3 * N), ax, fma(__ldg(W + 4 * N), ay, fma(__ldg(W + 5 * N), az, by)));
+            bz = fma(__ldg(W + 6 * N), ax, fma(__ldg(W + 7 * N), ay, fma(__ldg(W + 8 * N), az, bz)));
+        }
+        FieldOut f;
+        f.Bzee = make_double3(0.0, 0.0, 0.0);
+        if (zee_on) {
+            const int64_t c = i / nmag;
+            double3 b;
+            if (bmap) b = make_double3(__ldg(bmap + c), __ldg(bmap + ncell + c), __ldg(bmap + 2 * ncell + c));
+            else b = make_double3(bext[0], bext[1], bext[2]);
+            const double z = __ldg(zc + i);
+            f.Bzee = make_double3(z * b.x, z * b.y, z * b.z);
+        }
+        f.B = make_double3(bx + f.Bzee.x, by + f.Bzee.y, bz + f.Bzee.z);
+        return f;
+    }
+};
+
+struct Reduce {
+    double* partials;
+    unsigned int* counter;
+    double* out;  // null = no energy wanted
+    int nblocks;
+};
+
+__device__ __forceinline__ double3 minus2(double3 B, double3 hd) {
+    return make_double3(B.x - 2.0 * hd.x, B.y - 2.0 * hd.y, B.z - 2.0 * hd.z);
+}
+
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(256) k_field(const __grid_constant__ F fp, const double* __restrict__ m,
+                                               const DipView Hd, double* __restrict__ B,
+                                               double* __restrict__ e_site, Reduce R) {
+    int64_t i;
+    int x, y, z;
+    const bool act = fp.site(i, x, y, z);
+    const int64_t N = fp.nsites();
+    double e = 0.0;
+    if (act) {
+        const double3 m0 = ld3(m, i, N);
+        const FieldOut f = fp.field(m, i, x, y, z, m0);
+        const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+        if (B) st3(B, i, N, minus2(f.B, hd));
+        if (e_site) e_site[i] = site_energy(f, m0, hd);
+        e = total_energy_part(f, m0, hd);
+    }
+    if (R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, R.partials, R.counter, R.out, R.nblocks);
+    }
+}
+
+// Euler: one fused pass m -> mout.
+template <class F>
+__global__ void __launch_bounds__(256) k_euler(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
+                                               const double* __restrict__ m, double* __restrict__ mout,
+                                               const DipView Hd, Reduce R) {
+    int64_t i;
+    int x, y, z;
+    const bool act = fp.site(i, x, y, z);
+    const int64_t N = fp.nsites();
+    double e = 0.0;
+    if (act) {
+        const double3 m0 = ld3(m, i, N);
+        const FieldOut f = fp.field(m, i, x, y, z, m0);
+        const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+        e = total_energy_part(f, m0, hd);
+        const double3 D = llg_rhs(minus2(f.B, hd), m0, C.alpha, C.inv_den);
+        const double c = C.h_over_hbar;
+        double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
+        if (C.thermal) {
+            const double3 DT = llg_rhs(thermal_field(C, step, i, N), m0, C.alpha, C.inv_den);
+            t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
+        }
+        st3(mout, i, N, project(t, m0));
+    }
+    if (R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, R.partials, R.counter, R.out, R.nblocks);
+    }
+}
+
+// Heun-Matjes pass 1: predictor m~ = P(m + D1 h/hbar); keeps D1 and DT for pass 2.
+template <class F>
+__global__ void __launch_bounds__(256) k_heun1(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
+                                               const double* __restrict__ m, double* __restrict__ mid,
+                                               double* __restrict__ D1, double* __restrict__ DTo,
+                                               const DipView Hd, Reduce R) {
+    int64_t i;
+    int x, y, z;
+    const bool act = fp.site(i, x, y, z);
+    const int64_t N = fp.nsites();
+    double e = 0.0;
+    if (act) {
+        const double3 m0 = ld3(m, i, N);
+        const FieldOut f = fp.field(m, i, x, y, z, m0);
+        const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+        e = total_energy_part(f, m0, hd);
+        const double3 D = llg_rhs(minus2(f.B, hd), m0, C.alpha, C.inv_den);
+        const double c = C.h_over_hbar;
+        const double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
+        st3(mid, i, N, project(t, m0));
+        st3(D1, i, N, D);
+        if (C.thermal) st3(DTo, i, N, llg_rhs(thermal_field(C, step, i, N), m0, C.alpha, C.inv_den));
+    }
+    if (R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, R.partials, R.counter, R.out, R.nblocks);
+    }
+}
+
+// Heun-Matjes pass 2: corrector restarted from the predictor.
+template <class F>
+__global__ void __launch_bounds__(256) k_heun2(const __grid_constant__ F fp, const DynCoef C,
+                                               const double* __restrict__ mid, const double* __restrict__ D1,
+                                               const double* __restrict__ DTi, double* __restrict__ mout,
+                                               const DipView Hd) {
+    int64_t i;
+    int x, y, z;
+    if (!fp.site(i, x, y, z)) return;
+    const int64_t N = fp.nsites();
+    const double3 mt = ld3(mid, i, N);
+    const FieldOut f = fp.field(mid, i, x, y, z, mt);
+    const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+    const double3 D2 = llg_rhs(minus2(f.B, hd), mt, C.alpha, C.inv_den);
+    const double3 d1 = ld3(D1, i, N);
+    const double3 Di = make_double3(0.5 * d1.x + 0.5 * D2.x, 0.5 * d1.y + 0.5 * D2.y, 0.5 * d1.z + 0.5 * D2.z);
+    const double c = C.h_over_hbar;
+    double3 t = make_double3(mt.x + Di.x * c, mt.y + Di.y * c, mt.z + Di.z * c);
+    if (C.thermal) {
+        const double3 DT = ld3(DTi, i, N);
+        t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
+    }
+    st3(mout, i, N, project(t, mt));
+}
+
+// SIB pass 1: Cayley predictor from m_n with A(m_n); writes the midpoint (m_n + m~)/2.
+template <class F>
+__global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
+                                              const double* __restrict__ m, double* __restrict__ mid,
+                                              const DipView Hd, Reduce R) {
+    int64_t i;
+    int x, y, z;
+    const bool act = fp.site(i, x, y, z);
+    const int64_t N = fp.nsites();
+    double e = 0.0;
+    if (act) {
+        const double3 m0 = ld3(m, i, N);
+        const FieldOut f = fp.field(m, i, x, y, z, m0);
+        const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+        e = total_energy_part(f, m0, hd);
+        double3 H = minus2(f.B, hd);
+        if (C.thermal) {
+            const double3 b = thermal_field(C, step, i, N);
+            H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
+        }
+        const double3 yv = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
+        st3(mid, i, N, make_double3(0.5 * (m0.x + yv.x), 0.5 * (m0.y + yv.y), 0.5 * (m0.z + yv.z)));
+    }
+    if (R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, R.partials, R.counter, R.out, R.nblocks);
+    }
+}
+
+// SIB pass 2: corrector from m_n with A(midpoint); in place (only the own site of m is read).
+template <class F>
+__global__ void __launch_bounds__(256) k_sib2(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
+                                              const double* __restrict__ mid, double* m, const DipView Hd) {
+    int64_t i;
+    int x, y, z;
+    if (!fp.site(i, x, y, z)) return;
+    const int64_t N = fp.nsites();
+    const double3 mb = ld3(mid, i, N);
+    const FieldOut f = fp.field(mid, i, x, y, z, mb);
+    const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+    double3 H = minus2(f.B, hd);
+    if (C.thermal) {
+        const double3 b = thermal_field(C, step, i, N);
+        H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
+    }
+    const double3 m0 = make_double3(m[i], m[N + i], m[2 * N + i]);
+    st3(m, i, N, sib_solve(m0, mb, H, C.alpha, C.sib_hc));
+}
+
+// Reference temperature estimator (dynamics/measure_temp.f90:21-43): sum |m x B|^2, sum m.B.
+template <class F>
+__global__ void __launch_bounds__(256) k_temperature(const __grid_constant__ F fp, const double* __restrict__ m,
+                                                     const DipView Hd, Reduce R) {
+    int64_t i;
+    int x, y, z;
+    const bool act = fp.site(i, x, y, z);
+    const int64_t N = fp.nsites();
+    double v[2] = {0.0, 0.0};
+    if (act) {
+        const double3 m0 = ld3(m, i, N);
+        const FieldOut f = fp.field(m, i, x, y, z, m0);
+        const double3 hd = Hd.h ? ld_dip(Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+        const double3 Bt = minus2(f.B, hd);
+        const double3 c = cross(m0, Bt);
+        v[0] = dot(c, c);
+        v[1] = dot(m0, Bt);
+    }
+    grid_reduce<2>(v, R.partials, R.counter, R.out, R.nblocks);
+}
+
+__global__ void k_philox(uint64_t seed, uint32_t step, uint32_t stream, int64_t n, double* out) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const double3 z = philox_normals(seed, step, stream, static_cast<uint32_t>(i));
+    out[i] = z.x;
+    out[n + i] = z.y;
+    out[2 * n + i] = z.z;
+}
+
+__global__ void k_step_counter(uint32_t* ctr, uint32_t value, int add) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *ctr = add ? *ctr + value : value;
+}
+
+__global__ void k_aos_to_soa(const double* __restrict__ a, double* __restrict__ s, int64_t n) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    s[i] = a[3 * i];
+    s[n + i] = a[3 * i + 1];
+    s[2 * n + i] = a[3 * i + 2];
+}
+__global__ void k_soa_to_aos(const double* __restrict__ s, double* __restrict__ a, int64_t n) {
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    a[3 * i] = s[i];
+    a[3 * i + 1] = s[n + i];
+    a[3 * i + 2] = s[2 * n + i];
+}
+
+// ---------------------------------------------------------------------------
+StencilField stencil_of(const mj_plan* p) {
+    StencilField f;
+    f.P = p->sp;
+    f.bmap = p->d_bmap;
+    return f;
+}
+EllField ell_of(const mj_plan* p) {
+    EllField f;
+    f.N = p->N;
+    f.ncell = p->ncell;
+    f.nmag = p->nmag;
+    f.width = p->ell_width;
+    f.col = p->d_ell_col;
+    f.val = p->d_ell_val;
+    f.zc = p->d_zee;
+    f.bmap = p->d_bmap;
+    for (int k = 0; k < 3; ++k) f.bext[k] = p->bext_cell.size() == 3 ? p->bext_cell[k] : 0.0;
+    f.zee_on = p->d_zee != nullptr;
+    return f;
+}
+dim3 grid_stencil(const StencilParams& P) {
+    return dim3((P.L[0] + StencilField::BX - 1) / StencilField::BX, (P.L[1] + StencilField::BY - 1) / StencilField::BY, P.L[2]);
+}
+dim3 grid_ell(int64_t N) { return dim3(static_cast<unsigned>((N + EllField::BX - 1) / EllField::BX), 1, 1); }
+
+template <class F>
+struct Launch {
+    F fp;
+    dim3 grid, block;
+};
+
+Reduce make_reduce(mj_plan* p, double* out) {
+    Reduce r;
+    r.partials = p->d_partials;
+    r.counter = p->d_counter;
+    r.out = out;
+    r.nblocks = static_cast<int>(energy_blocks(p));
+    return r;
+}
+
+DipView dip_field(mj_plan* p, const double* m, cudaStream_t s, mj_status& st) {
+    st = MJ_OK;
+    if (p->dip_on) {
+        const int r = prof_begin(p, "dipolar_fft", s);
+        st = dipolar_apply(p, m, nullptr, s);
+        prof_end(p, r, s);
+    }
+    return dipolar_view(p);
+}
+
+#define MJ_LAUNCH(name, kern, ...)                                  \
+    do {                                                            \
+        const int rec_ = prof_begin(p, name, s);                    \
+        kern<<<L.grid, L.block, 0, s>>>(__VA_ARGS__);               \
+        prof_end(p, rec_, s);                                       \
+        if ((st = cuda_status(cudaGetLastError(), name)) != MJ_OK) return st; \
+    } while (0)
+
+template <class F>
+mj_status field_impl(mj_plan* p, const Launch<F>& L, const double* m, double* B, double* e_site, double* E_out,
+                     cudaStream_t s) {
+    mj_status st;
+    DipView Hd = dip_field(p, m, s, st);
+    if (st != MJ_OK) return st;
+    MJ_LAUNCH("k_field", k_field<F>, L.fp, m, Hd, B, e_site, make_reduce(p, E_out));
+    return MJ_OK;
+}
+
+// One time step.  Euler writes m_out (ping-pong owned by the caller); the
+// two-pass schemes update m in place through the plan's midpoint buffer.
+template <class F>
+mj_status step_impl(mj_plan* p, const Launch<F>& L, double* m, double* m_out, const DynCoef& c, uint32_t step,
+                    double* E_prev, cudaStream_t s) {
+    mj_status st;
+    switch (c.integrator) {
+        case MJ_EULER: {
+            DipView Hd = dip_field(p, m, s, st);
+            if (st != MJ_OK) return st;
+            MJ_LAUNCH("k_euler", k_euler<F>, L.fp, c, step, m, m_out, Hd, make_reduce(p, E_prev));
+            return MJ_OK;
+        }
+        case MJ_HEUN_MATJES: {
+            DipView Hd = dip_field(p, m, s, st);
+            if (st != MJ_OK) return st;
+            MJ_LAUNCH("k_heun1", k_heun1<F>, L.fp, c, step, m, p->d_mid, p->d_aux, p->d_aux2, Hd, make_reduce(p, E_prev));
+            Hd = dip_field(p, p->d_mid, s, st);
+            if (st != MJ_OK) return st;
+            MJ_LAUNCH("k_heun2", k_heun2<F>, L.fp, c, p->d_mid, p->d_aux, p->d_aux2, m, Hd);
+            return MJ_OK;
+        }
+        case MJ_SIB: {
+            DipView Hd = dip_field(p, m, s, st);
+            if (st != MJ_OK) return st;
+            MJ_LAUNCH("k_sib1", k_sib1<F>, L.fp, c, step, m, p->d_mid, Hd, make_reduce(p, E_prev));
+            Hd = dip_field(p, p->d_mid, s, st);
+            if (st != MJ_OK) return st;
+            MJ_LAUNCH("k_sib2", k_sib2<F>, L.fp, c, step, p->d_mid, m, Hd);
+            return MJ_OK;
+        }
+        default:
+            return set_error(MJ_ERR_ARG, "unknown integrator");
+    }
+}
+
+template <class F>
+mj_status temperature_impl(mj_plan* p, const Launch<F>& L, const double* m, double* out2, cudaStream_t s) {
+    mj_status st;
+    DipView Hd = dip_field(p, m, s, st);
+    if (st != MJ_OK) return st;
+    k_temperature<F><<<L.grid, L.block, 0, s>>>(L.fp, m, Hd, make_reduce(p, out2));
+    return cuda_status(cudaGetLastError(), "k_temperature");
+}
+
+Launch<StencilField> stencil_launch(const mj_plan* p) {
+    return Launch<StencilField>{stencil_of(p), grid_stencil(p->sp), dim3(StencilField::BX, StencilField::BY)};
+}
+Launch<EllField> ell_launch(const mj_plan* p) {
+    return Launch<EllField>{ell_of(p), grid_ell(p->N), dim3(EllField::BX, 1)};
+}
+
+}  // namespace
+
+int64_t energy_blocks(const mj_plan* p) {
+    if (p->is_stencil) {
+        const dim3 g = grid_stencil(p->sp);
+        return static_cast<int64_t>(g.x) * g.y * g.z;
+    }
+    return grid_ell(p->N).x;
+}
+
+mj_status launch_field(mj_plan* p, const double* m, double* B, double* e_site, double* E_out, cudaStream_t s) {
+    if (p->is_stencil) return field_impl(p, stencil_launch(p), m, B, e_site, E_out, s);
+    return field_impl(p, ell_launch(p), m, B, e_site, E_out, s);
+}
+
+mj_status launch_energy(mj_plan* p, const double* m, double* E_out, cudaStream_t s) {
+    return launch_field(p, m, nullptr, nullptr, E_out, s);
+}
+
+mj_status launch_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uint32_t step, double* E_prev_out,
+                      cudaStream_t s) {
+    if (p->is_stencil) return step_impl(p, stencil_launch(p), m, m_out, c, step, E_prev_out, s);
+    return step_impl(p, ell_launch(p), m, m_out, c, step, E_prev_out, s);
+}
+
+mj_status launch_temperature(mj_plan* p, const double* m, double* out2, cudaStream_t s) {
+    if (p->is_stencil) return temperature_impl(p, stencil_launch(p), m, out2, s);
+    return temperature_impl(p, ell_launch(p), m, out2, s);
+}
+
+mj_status launch_philox(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n, double* out, cudaStream_t s) {
+    if (n <= 0) return MJ_OK;
+    k_philox<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(seed, step, stream_id, n, out);
+    return cuda_status(cudaGetLastError(), "k_philox");
+}
+
+mj_status step_counter(uint32_t* ctr, uint32_t value, bool add, cudaStream_t s) {
+    k_step_counter<<<1, 32, 0, s>>>(ctr, value, add ? 1 : 0);
+    return cuda_status(cudaGetLastError(), "k_step_counter");
+}
+
+mj_status aos_to_soa(const double* a, double* so, int64_t n, cudaStream_t s) {
+    if (n <= 0) return MJ_OK;
+    k_aos_to_soa<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(a, so, n);
+    return cuda_status(cudaGetLastError(), "aos_to_soa");
+}
+mj_status soa_to_aos(const double* so, double* a, int64_t n, cudaStream_t s) {
+    if (n <= 0) return MJ_OK;
+    k_soa_to_aos<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(so, a, n);
+    return cuda_status(cudaGetLastError(), "soa_to_aos");
+}
+
+}  // namespace mj

@@ -1,0 +1,229 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline / reference legs may use
+it; the product (matjes_b200) never imports it.  See matjes_oracle.h for the
+reference routines it restates and for its pinning status.
+
+Decks are duck-typed: any object with the attributes of matjes_b200.deck.Deck
+(L, periodic, areal, atoms, J, D, K, B_ext, zeeman_on, dip, dip_cut, c_H_*).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+MAXAT = 16
+MAXTERM = 32
+KB = 0.000086173324
+MUB = 0.0000578838180661
+HBAR = 0.658211928
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+class _Lat(C.Structure):
+    _fields_ = [("L", C.c_int * 3), ("periodic", C.c_int * 3), ("areal", (C.c_double * 3) * 3), ("natom", C.c_int),
+                ("frac", (C.c_double * 3) * MAXAT), ("attype", C.c_int * MAXAT), ("moment", C.c_double * MAXAT)]
+
+
+class _J(C.Structure):
+    _fields_ = [("t1", C.c_int), ("t2", C.c_int), ("shell", C.c_int), ("J", C.c_double)]
+
+
+class _D(C.Structure):
+    _fields_ = [("t1", C.c_int), ("t2", C.c_int), ("tmed", C.c_int), ("shell", C.c_int), ("D", C.c_double)]
+
+
+class _K(C.Structure):
+    _fields_ = [("type", C.c_int), ("axis", C.c_double * 3), ("K", C.c_double)]
+
+
+class _Input(C.Structure):
+    _fields_ = [("lat", _Lat), ("nJ", C.c_int), ("J", _J * MAXTERM), ("nD", C.c_int), ("D", _D * MAXTERM),
+                ("nK", C.c_int), ("K", _K * MAXTERM), ("c_H_J", C.c_double), ("c_H_D", C.c_double),
+                ("c_H_ani", C.c_double), ("c_zeeman", C.c_double), ("B_ext", C.c_double * 3), ("zeeman_on", C.c_int),
+                ("dip_on", C.c_int), ("dip_period_cut", C.c_int * 3)]
+
+
+class _Dyn(C.Structure):
+    _fields_ = [("integrator", C.c_int), ("timestep", C.c_double), ("alpha", C.c_double),
+                ("temperature", C.c_double), ("noise", C.c_int), ("seed", C.c_uint64), ("stream", C.c_uint32),
+                ("step0", C.c_uint32), ("inject", C.c_void_p), ("inject_nbuf", C.c_int)]
+
+
+INTEGRATORS = {"euler": 1, "heun": 2, "heun_matjes": 2, "sib": 3}
+NOISES = {"off": 0, "philox": 1, "inject": 2}
+
+
+def _lib():
+    if not os.path.exists(LIB):
+        build()
+    lib = C.CDLL(LIB)
+    P, DP = C.c_void_p, C.POINTER(C.c_double)
+    lib.orc_input_defaults.argtypes = [C.POINTER(_Input)]
+    lib.orc_model_build.argtypes = [C.POINTER(_Input), C.POINTER(P)]
+    lib.orc_model_build.restype = C.c_int
+    lib.orc_model_free.argtypes = [P]
+    lib.orc_nsites.argtypes = [P]
+    lib.orc_nsites.restype = C.c_int64
+    lib.orc_mm_nnz.argtypes = [P]
+    lib.orc_mm_nnz.restype = C.c_int64
+    lib.orc_mm_coo.argtypes = [P, C.c_int64, P, P, P]
+    lib.orc_set_bfield.argtypes = [P, P]
+    lib.orc_dip_nrep.argtypes = [P, C.c_int * 3]
+    lib.orc_field.argtypes = [P, P, P, P]
+    lib.orc_field_terms.argtypes = [P, P, P, P, P]
+    lib.orc_energy.argtypes = [P, P]
+    lib.orc_energy.restype = C.c_double
+    lib.orc_dipolar_explicit_field.argtypes = [P, P, P]
+    lib.orc_philox_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, C.c_int64, P]
+    lib.orc_philox4x32.argtypes = [P, P, P]
+    lib.orc_run.argtypes = [P, C.POINTER(_Dyn), P, C.c_int, P]
+    lib.orc_run.restype = C.c_int
+    lib.orc_llg_torque.argtypes = [P, C.c_double, P, P, C.c_int64]
+    return lib
+
+
+lib = _lib()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Model:
+    """The reference Hamiltonian of a deck, assembled as the reference does."""
+
+    def __init__(self, deck):
+        inp = _Input()
+        lib.orc_input_defaults(C.byref(inp))
+        for d in range(3):
+            inp.lat.L[d] = int(deck.L[d])
+            inp.lat.periodic[d] = int(bool(deck.periodic[d]))
+            for k in range(3):
+                inp.lat.areal[d][k] = float(deck.areal[d][k])
+        inp.lat.natom = len(deck.atoms)
+        for a, (frac, t, mom) in enumerate(deck.atoms):
+            for k in range(3):
+                inp.lat.frac[a][k] = float(frac[k])
+            inp.lat.attype[a] = int(t)
+            inp.lat.moment[a] = float(mom)
+        inp.nJ = len(deck.J)
+        for i, (t1, t2, s, v) in enumerate(deck.J):
+            inp.J[i] = _J(t1, t2, s, v)
+        inp.nD = len(deck.D)
+        for i, (t1, t2, tm, s, v) in enumerate(deck.D):
+            inp.D[i] = _D(t1, t2, tm, s, v)
+        inp.nK = len(deck.K)
+        for i, (t, ax, v) in enumerate(deck.K):
+            inp.K[i].type = t
+            for k in range(3):
+                inp.K[i].axis[k] = ax[k]
+            inp.K[i].K = v
+        inp.c_H_J, inp.c_H_D, inp.c_H_ani, inp.c_zeeman = deck.c_H_J, deck.c_H_D, deck.c_H_ani, deck.c_zeeman
+        for k in range(3):
+            inp.B_ext[k] = float(deck.B_ext[k])
+            inp.dip_period_cut[k] = int(deck.dip_cut[k])
+        inp.zeeman_on = int(bool(deck.zeeman_on))
+        inp.dip_on = int(bool(deck.dip))
+        h = C.c_void_p()
+        rc = lib.orc_model_build(C.byref(inp), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"oracle model build failed ({rc})")
+        self.h = h
+        self.N = int(lib.orc_nsites(h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.orc_model_free(self.h)
+            self.h = None
+
+    def set_bfield(self, b_cell):
+        self._b = None if b_cell is None else np.ascontiguousarray(b_cell, np.float64)
+        lib.orc_set_bfield(self.h, _p(self._b))
+
+    def field(self, m):
+        m = np.ascontiguousarray(m, np.float64)
+        B = np.empty_like(m)
+        e = np.empty(self.N)
+        lib.orc_field(self.h, _p(m), _p(B), _p(e))
+        return B, e
+
+    def field_terms(self, m):
+        m = np.ascontiguousarray(m, np.float64)
+        out = [np.empty_like(m) for _ in range(3)]
+        lib.orc_field_terms(self.h, _p(m), *[_p(o) for o in out])
+        return out
+
+    def energy(self, m) -> float:
+        return float(lib.orc_energy(self.h, _p(np.ascontiguousarray(m, np.float64))))
+
+    def dipolar_explicit(self, m):
+        m = np.ascontiguousarray(m, np.float64)
+        B = np.empty_like(m)
+        lib.orc_dipolar_explicit_field(self.h, _p(m), _p(B))
+        return B
+
+    def nrep(self):
+        a = (C.c_int * 3)()
+        lib.orc_dip_nrep(self.h, a)
+        return tuple(a)
+
+    def coo(self):
+        n = int(lib.orc_mm_nnz(self.h))
+        r = np.empty(n, np.int64)
+        c = np.empty(n, np.int64)
+        v = np.empty(n)
+        lib.orc_mm_coo(self.h, n, _p(r), _p(c), _p(v))
+        return r, c, v
+
+    def run(self, m, nsteps, integrator="sib", timestep=0.1, alpha=0.1, temperature=0.0, noise="off", seed=0,
+            stream=0, step0=0, inject=None, energies=False, **_ignored):
+        """Advance m (N,3) in place; inject is a host array [nbuf][3][N]."""
+        assert m.dtype == np.float64 and m.flags.c_contiguous
+        d = _Dyn()
+        d.integrator = INTEGRATORS[integrator]
+        d.timestep, d.alpha, d.temperature = timestep, alpha, temperature
+        d.noise = NOISES[noise]
+        d.seed, d.stream, d.step0 = seed, stream, step0
+        keep = None
+        if inject is not None:
+            keep = np.ascontiguousarray(inject, np.float64)
+            d.inject = keep.ctypes.data
+            d.inject_nbuf = keep.shape[0]
+        E = np.empty(nsteps) if energies else None
+        rc = lib.orc_run(self.h, C.byref(d), _p(m), int(nsteps), _p(E))
+        if rc != 0:
+            raise RuntimeError("oracle run failed")
+        return E
+
+
+def philox_normals(seed, step, stream, site0, n):
+    out = np.empty((n, 3))
+    lib.orc_philox_normals(seed, step, stream, site0, n, _p(out))
+    return out
+
+
+def philox4x32(ctr, key):
+    c = np.asarray(ctr, np.uint32)
+    k = np.asarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib.orc_philox4x32(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return [int(x) for x in out]
+
+
+def llg_torque(B, alpha, m):
+    B = np.ascontiguousarray(B, np.float64)
+    m = np.ascontiguousarray(m, np.float64)
+    D = np.empty_like(m)
+    lib.orc_llg_torque(_p(B), alpha, _p(m), _p(D), m.shape[0])
+    return D
