@@ -72,53 +72,60 @@ def workload_config(name, deck, dyn, extra=None) -> dict:
 
 # ----------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons polled through NVML every
+    0.5 ms while the timed region runs (read-only queries)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+    def __init__(self, cuda_index: int):
+        self.samples, self.reasons, self.err = [], set(), None
+        self.handle = None
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(cuda_index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        except Exception as e:  # noqa: BLE001
+            self.err = f"nvml unavailable: {e}"
+
+    def _poll(self):
+        nv = self.nvml
+        while not self._stop:
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)))
+                r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception as e:  # noqa: BLE001
+                self.err = str(e)
+                return
+            time.sleep(0.0005)
 
     def start(self):
-        try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv",
-                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+        import threading
+
+        if self.handle is None:
+            return
+        self._stop = False
+        self.th = threading.Thread(target=self._poll, daemon=True)
+        self.th.start()
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.f.close()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            if line.startswith("index") or not line.strip():
-                continue
-            parts = [p.strip() for p in line.split(",")]
-            try:
-                sm.append(float(parts[1].split()[0]))
-                smax.append(float(parts[2].split()[0]))
-            except Exception:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.handle is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no nvml"]}
+        self._stop = True
+        self.th.join()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [self.err or "no samples"]}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples), "source": "nvml"}
 
 
 def ncu_traffic(kernel: str, workload: str):
@@ -220,6 +227,11 @@ def run_gpu(args, rank, world):
         p.step0 = k
         _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, E[k:].data_ptr(), stream))
 
+    # the library's autotuner picks the kernel variant (tile shape) for this lattice
+    best = _abi.C.c_int32()
+    tune = np.zeros(5)
+    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 10, _abi.C.byref(best), tune.ctypes.data))
+
     for k in range(W):
         flush.zero_()
         step(k)
@@ -295,7 +307,10 @@ def run_gpu(args, rank, world):
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(args.workload, deck, w["dyn"],
                                                        {"parallelism": f"replicas x{world}" if world > 1 else "single",
-                                                        "energy_per_step": "fused into pass 1"}),
+                                                        "energy_per_step": "fused into pass 1",
+                                                        "kernel_variant": int(best.value),
+                                                        "autotune_ms_per_step": {str(v): round(float(t), 5) for v, t
+                                                                                 in zip(range(-1, 4), tune)}}),
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
                      "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},
@@ -315,7 +330,7 @@ def run_gpu(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")

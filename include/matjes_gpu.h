@@ -125,6 +125,20 @@ mj_status mj_plan_destroy(mj_plan* plan);
 mj_status mj_plan_nsites(const mj_plan* plan, int64_t* n);
 /* Stencil introspection: number of neighbour offsets (0 for ELL plans). */
 mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n);
+/* Kernel variant of a stencil plan: -1 = generic per-offset kernel; 0..3 =
+ * shared-memory tiled kernel with 32 x (threads-in-y * sites-per-thread)
+ * tiles of 4x8, 8x4, 4x4, 2x8.  Tiled variants exist for the square (NN,
+ * NN+NNN) and triangular (NN, three shells) offset sets; MJ_ERR_UNSUPPORTED
+ * otherwise.  No counterpart in the reference (its SpMV has no tiling). */
+mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant);
+/* Current variant (-1 generic) and the matched compile-time shape id (0 none). */
+mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape);
+/* Autotuner: times `steps` steps of `p` for every variant of the plan on a
+ * scratch copy of the device spins m_dev_soa (left untouched), keeps the
+ * fastest and returns it in *best; ms_per_step (5 doubles, variants -1..3, may
+ * be NULL) receives the timings (negative = variant unavailable).  Synchronous. */
+mj_status mj_plan_autotune(mj_plan* plan, const double* m_dev_soa, const mj_dyn_params* p, int32_t steps,
+                           int32_t* best, double* ms_per_step);
 /* Per-site applied field map (Tesla, host AoS 3*Ncell; NULL = uniform H_ext):
  * the Bfield_init.dat input read by initialization/orders_initialize.f90:28. */
 mj_status mj_plan_set_bfield(mj_plan* plan, const double* b_cell_host);

@@ -8,8 +8,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmatjes_b200.so")
-SOURCES = ["mj_kernels.cu", "mj_dipolar.cu", "mj_lattice.cpp", "mj_abi.cpp"]
-HEADERS = ["mj_internal.hpp", "mj_device.cuh", os.path.join("..", "..", "include", "matjes_gpu.h")]
+SOURCES = ["mj_kernels.cu", "mj_tiled.cu", "mj_dipolar.cu", "mj_lattice.cpp", "mj_abi.cpp"]
+HEADERS = ["mj_internal.hpp", "mj_device.cuh", "mj_shapes.hpp", os.path.join("..", "..", "include", "matjes_gpu.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

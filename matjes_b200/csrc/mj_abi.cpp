@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "mj_internal.hpp"
+#include "mj_shapes.hpp"
 
 namespace mj {
 
@@ -22,6 +23,8 @@ mj_status cuda_status(cudaError_t e, const char* where) {
     const mj_status st = (e == cudaErrorMemoryAllocation) ? MJ_ERR_OOM : MJ_ERR_CUDA;
     return set_error(st, std::string(where) + ": " + cudaGetErrorString(e));
 }
+
+void match_shape(StencilParams& sp);
 
 int prof_begin(mj_plan* p, const char* name, cudaStream_t s) {
     if (!p->prof_on) return -1;
@@ -130,6 +133,30 @@ bool make_stencil(const std::vector<Block>& blocks, const std::vector<double>& o
     return true;
 }
 
+// Reorder a stencil into the offset order of a compile-time shape, if its
+// offset set is the shape's (in-plane only) and every offset the shape treats
+// as isotropic is isotropic here.
+template <class S>
+bool try_shape(StencilParams& sp) {
+    if (sp.n_off != S::K) return false;
+    int perm[kMaxOff];
+    for (int k = 0; k < S::K; ++k) {
+        int j = -1;
+        for (int q = 0; q < sp.n_off; ++q)
+            if (sp.off[q][0] == S::DX[k] && sp.off[q][1] == S::DY[k] && sp.off[q][2] == 0) j = q;
+        if (j < 0 || (S::ISO[k] && !sp.iso[j])) return false;
+        perm[k] = j;
+    }
+    StencilParams o = sp;
+    for (int k = 0; k < S::K; ++k) {
+        for (int d = 0; d < 3; ++d) sp.off[k][d] = o.off[perm[k]][d];
+        for (int q = 0; q < 9; ++q) sp.W[k][q] = o.W[perm[k]][q];
+        sp.iso[k] = o.iso[perm[k]];
+    }
+    sp.shape = S::id;
+    return true;
+}
+
 struct Entry {
     int64_t row, col;
     double W[9];
@@ -230,7 +257,9 @@ mj_status alloc_scratch(mj_plan* p) {
     if ((st = dalloc(&p->d_mid, 3 * N, "mid")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_aux, 3 * N, "aux")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_aux2, 3 * N, "aux2")) != MJ_OK) return st;
-    p->partial_cap = 2 * energy_blocks(p);
+    // generic grid, or the smallest tile of the tiled kernels (32 x 16), whichever has more blocks
+    const int64_t tiled_max = p->is_stencil ? static_cast<int64_t>((p->sp.L[0] + 31) / 32) * ((p->sp.L[1] + 15) / 16) * p->sp.L[2] : 0;
+    p->partial_cap = 2 * std::max(energy_blocks(p), tiled_max) + 64;
     if ((st = dalloc(&p->d_partials, static_cast<size_t>(p->partial_cap), "partials")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_counter, 4, "counter")) != MJ_OK) return st;
     if ((st = cuda_status(cudaMemset(p->d_counter, 0, 4 * sizeof(unsigned int)), "counter init")) != MJ_OK) return st;
@@ -328,6 +357,18 @@ mj_status step_sequence(mj_plan* p, double* m, const DynCoef& c, int energy_mode
     return MJ_OK;
 }
 
+}  // namespace
+
+void match_shape(StencilParams& sp) {
+    sp.shape = kShapeGeneric;
+    if (try_shape<ShapeTri3>(sp)) return;
+    if (try_shape<ShapeTriNN>(sp)) return;
+    if (try_shape<ShapeSquareNN>(sp)) return;
+    try_shape<ShapeSquare2>(sp);
+}
+
+namespace {
+
 mj_status run_steps(mj_plan* p, double* m, const mj_dyn_params* prm, int32_t nsteps, double* E_dev, cudaStream_t s) {
     if (nsteps < 0) return set_error(MJ_ERR_ARG, "nsteps must be >= 0");
     DynCoef c;
@@ -378,6 +419,10 @@ mj_status mj_plan_create(const mj_lattice_desc* lat, const mj_hamiltonian_desc* 
     for (int k = 0; k < 3; ++k) sp.bext[k] = ham->B_ext[k];
     p->bext_cell.assign(ham->B_ext, ham->B_ext + 3);
     p->is_stencil = g.nmag == 1 && make_stencil(blocks, onsite, sp);
+    if (p->is_stencil) {
+        match_shape(sp);
+        p->tiled_shape = sp.shape;
+    }
     if (p->is_stencil) {
         sp.zc = -((1.0 * kMuB * ham->c_zeeman) * lat->moment[g.magatom[0]]);
     } else {
@@ -535,6 +580,82 @@ mj_status mj_plan_nsites(const mj_plan* plan, int64_t* n) {
 mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n) {
     if (!plan || !n) return set_error(MJ_ERR_ARG, "null argument");
     *n = plan->is_stencil ? plan->sp.n_off : 0;
+    return MJ_OK;
+}
+
+mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    if (variant < -1 || variant > 3) return set_error(MJ_ERR_ARG, "variant must be -1..3");
+    if (variant >= 0 && !(plan->is_stencil && plan->tiled_shape != 0))
+        return set_error(MJ_ERR_UNSUPPORTED, "no tiled kernel for this plan's offsets");
+    if (variant < 0) {
+        plan->sp.shape = 0;
+    } else {
+        plan->sp.shape = plan->tiled_shape;
+        plan->tile_variant = variant;
+    }
+    if (plan->graph_exec) {  // the captured graph holds the old kernels
+        cudaGraphExecDestroy(plan->graph_exec);
+        plan->graph_exec = nullptr;
+        plan->graph_key.clear();
+    }
+    return MJ_OK;
+}
+
+mj_status mj_plan_autotune(mj_plan* plan, const double* m, const mj_dyn_params* prm, int32_t steps, int32_t* best,
+                           double* ms_per_step) {
+    if (!plan || !m || !prm || !best || steps < 1) return set_error(MJ_ERR_ARG, "bad autotune arguments");
+    cudaSetDevice(plan->device);
+    mj_status st = ensure_host_scratch(plan);
+    if (st != MJ_OK) return st;
+    DynCoef c;
+    if ((st = dyn_coef(prm, plan->N, c)) != MJ_OK) return st;
+    const int32_t v0 = (plan->is_stencil && plan->sp.shape != 0) ? plan->tile_variant : -1;
+    const bool has_tiled = plan->is_stencil && plan->tiled_shape != 0;
+    cudaEvent_t a, b;
+    if ((st = cuda_status(cudaEventCreate(&a), "event")) != MJ_OK) return st;
+    if ((st = cuda_status(cudaEventCreate(&b), "event")) != MJ_OK) {
+        cudaEventDestroy(a);
+        return st;
+    }
+    double best_ms = 1e300;
+    int32_t best_v = v0;
+    for (int32_t v = -1; v <= 3; ++v) {
+        double ms = -1.0;
+        if ((v >= 0 && !has_tiled) || (v == -1 && !plan->is_stencil)) {
+            if (ms_per_step) ms_per_step[v + 1] = ms;
+            continue;
+        }
+        if (plan->is_stencil && (st = mj_plan_set_variant(plan, v)) != MJ_OK) break;
+        if ((st = cuda_status(cudaMemcpy(plan->d_tmp_m, m, sizeof(double) * 3 * plan->N, cudaMemcpyDeviceToDevice),
+                              "autotune copy")) != MJ_OK)
+            break;
+        if ((st = step_sequence(plan, plan->d_tmp_m, c, MJ_ENERGY_BEFORE, prm->step0, 1, nullptr, 0)) != MJ_OK) break;
+        cudaEventRecord(a, 0);
+        if ((st = step_sequence(plan, plan->d_tmp_m, c, MJ_ENERGY_BEFORE, prm->step0, steps, nullptr, 0)) != MJ_OK) break;
+        cudaEventRecord(b, 0);
+        if ((st = cuda_status(cudaEventSynchronize(b), "autotune sync")) != MJ_OK) break;
+        float f = 0.0f;
+        cudaEventElapsedTime(&f, a, b);
+        ms = f / steps;
+        if (ms_per_step) ms_per_step[v + 1] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (st != MJ_OK) return st;
+    if (plan->is_stencil && (st = mj_plan_set_variant(plan, best_v)) != MJ_OK) return st;
+    *best = best_v;
+    return MJ_OK;
+}
+
+mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape) {
+    if (!plan || !variant || !shape) return set_error(MJ_ERR_ARG, "null argument");
+    *variant = (plan->is_stencil && plan->sp.shape != 0) ? plan->tile_variant : -1;
+    *shape = plan->tiled_shape;
     return MJ_OK;
 }
 

@@ -49,9 +49,10 @@ __device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, 
     philox10(d, k0, k1);
     const double r1 = sqrt(-2.0 * log(u53_open(c[0], c[1])));
     const double r2 = sqrt(-2.0 * log(u53_open(d[0], d[1])));
+    // angle 2 pi u through sinpi/cospi of 2u (exact argument, no range reduction)
     double s1, c1;
-    sincos(6.283185307179586 * u53(c[2], c[3]), &s1, &c1);
-    const double c2 = cos(6.283185307179586 * u53(d[2], d[3]));
+    sincospi(2.0 * u53(c[2], c[3]), &s1, &c1);
+    const double c2 = cospi(2.0 * u53(d[2], d[3]));
     return make_double3(r1 * c1, r1 * s1, r2 * c2);
 }
 
@@ -93,7 +94,7 @@ __device__ __forceinline__ double3 llg_rhs(double3 B, double3 m, double alpha, d
     const double n2 = dot(m, m);
     double3 mn = m;
     if (n2 > 1e-16) {
-        const double inv = 1.0 / sqrt(n2);
+        const double inv = rsqrt(n2);
         mn = make_double3(m.x * inv, m.y * inv, m.z * inv);
     }
     const double3 t = cross(mn, B);
@@ -117,7 +118,7 @@ __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, do
     const double np2 = dot(p, p);
     double3 pn = p;
     if (np2 > 1e-16) {
-        const double inv = 1.0 / sqrt(np2);
+        const double inv = rsqrt(np2);
         pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
     }
     const double3 pxh = cross(pn, H);

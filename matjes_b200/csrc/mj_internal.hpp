@@ -58,6 +58,7 @@ struct StencilParams {
     double zc;                // B_i += zc * b_cell,  zc = -(mu0 muB c_zeeman mu_s)
     double bext[3];
     int zee_on;
+    int shape;                // mj_shapes.hpp ShapeId; W is then in the shape's offset order
 };
 
 // Dipolar H on the padded FFT grid (the unpack is fused into the consumers):
@@ -95,6 +96,8 @@ struct mj_plan {
     int nmag = 1;
     bool is_stencil = true;
     mj::StencilParams sp{};
+    int tile_variant = 0;            // tiled-kernel shape (threads in y x sites per thread), see mj_tiled.cu
+    int tiled_shape = 0;             // matched compile-time shape (sp.shape is 0 while the generic path is forced)
     // ELL form (multi-atom cells, COO input): width entries per site
     int ell_width = 0;
     int* d_ell_col = nullptr;        // [width][N], -1 = empty
@@ -163,6 +166,14 @@ mj_status step_counter(uint32_t* ctr, uint32_t value, bool add, cudaStream_t s);
 mj_status aos_to_soa(const double* src_aos, double* dst_soa, int64_t n, cudaStream_t s);
 mj_status soa_to_aos(const double* src_soa, double* dst_aos, int64_t n, cudaStream_t s);
 int64_t energy_blocks(const mj_plan* p);
+
+// tiled kernels for compile-time stencil shapes (mj_tiled.cu)
+// pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
+mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
+                       double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s);
+int64_t tiled_energy_blocks(const mj_plan* p);
+// match a single-atom stencil to a compile-time shape and reorder its tensors (mj_abi.cpp)
+void match_shape(mj::StencilParams& sp);
 
 // dipolar (mj_dipolar.cu)
 mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t s);

@@ -487,7 +487,58 @@ int64_t energy_blocks(const mj_plan* p) {
     return grid_ell(p->N).x;
 }
 
+namespace {
+
+bool tiled(const mj_plan* p) { return p->is_stencil && p->sp.shape != 0; }
+
+mj_status tiled_call(mj_plan* p, const char* name, int pass, const DynCoef& c, const double* ms, const double* mn,
+                     double* out, double* aux, double* aux2, DipView Hd, double* E, uint32_t step, cudaStream_t s) {
+    const int rec = prof_begin(p, name, s);
+    mj_status st = launch_tiled(p, pass, c, ms, mn, out, aux, aux2, Hd, E, step, s);
+    prof_end(p, rec, s);
+    return st;
+}
+
+mj_status tiled_field(mj_plan* p, const double* m, double* B, double* e_site, double* E_out, cudaStream_t s) {
+    mj_status st;
+    DipView Hd = dip_field(p, m, s, st);
+    if (st != MJ_OK) return st;
+    DynCoef c{};
+    return tiled_call(p, "k_field", 0, c, m, nullptr, B, e_site, nullptr, Hd, E_out, 0u, s);
+}
+
+mj_status tiled_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uint32_t step, double* E_prev,
+                     cudaStream_t s) {
+    mj_status st;
+    DipView Hd = dip_field(p, m, s, st);
+    if (st != MJ_OK) return st;
+    switch (c.integrator) {
+        case MJ_EULER:
+            return tiled_call(p, "k_euler", 1, c, m, nullptr, m_out, nullptr, nullptr, Hd, E_prev, step, s);
+        case MJ_HEUN_MATJES:
+            if ((st = tiled_call(p, "k_heun1", 2, c, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, Hd, E_prev, step, s)) != MJ_OK)
+                return st;
+            Hd = dip_field(p, p->d_mid, s, st);
+            if (st != MJ_OK) return st;
+            return tiled_call(p, "k_heun2", 3, c, p->d_mid, nullptr, m, p->d_aux, p->d_aux2, Hd, nullptr, step, s);
+        case MJ_SIB: {
+            // Philox draws are made once per step in pass 1 and kept for the corrector
+            double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX) ? p->d_aux : nullptr;
+            if ((st = tiled_call(p, "k_sib1", 4, c, m, nullptr, p->d_mid, bstore, nullptr, Hd, E_prev, step, s)) != MJ_OK)
+                return st;
+            Hd = dip_field(p, p->d_mid, s, st);
+            if (st != MJ_OK) return st;
+            return tiled_call(p, "k_sib2", 5, c, p->d_mid, m, m, bstore, nullptr, Hd, nullptr, step, s);
+        }
+        default:
+            return set_error(MJ_ERR_ARG, "unknown integrator");
+    }
+}
+
+}  // namespace
+
 mj_status launch_field(mj_plan* p, const double* m, double* B, double* e_site, double* E_out, cudaStream_t s) {
+    if (tiled(p)) return tiled_field(p, m, B, e_site, E_out, s);
     if (p->is_stencil) return field_impl(p, stencil_launch(p), m, B, e_site, E_out, s);
     return field_impl(p, ell_launch(p), m, B, e_site, E_out, s);
 }
@@ -498,6 +549,7 @@ mj_status launch_energy(mj_plan* p, const double* m, double* E_out, cudaStream_t
 
 mj_status launch_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uint32_t step, double* E_prev_out,
                       cudaStream_t s) {
+    if (tiled(p)) return tiled_step(p, m, m_out, c, step, E_prev_out, s);
     if (p->is_stencil) return step_impl(p, stencil_launch(p), m, m_out, c, step, E_prev_out, s);
     return step_impl(p, ell_launch(p), m, m_out, c, step, E_prev_out, s);
 }

@@ -32,10 +32,32 @@ def test_zero_temperature_trajectory_1000_steps(integrator):
     Eo = O.Model(deck).run(mo, 1000, energies=True, **dyn)
     assert np.abs(m - mo).max() < 1e-9
     assert np.abs(E - Eo).max() < 1e-12 * np.abs(Eo).max()
+    drift = np.abs(np.linalg.norm(m, axis=1) - 1).max()
     if integrator == "sib":
-        assert np.abs(np.linalg.norm(m, axis=1) - 1).max() < 1e-13
+        assert drift < 1e-13
     else:
-        assert np.abs(np.linalg.norm(m, axis=1) - 1).max() < 1e-13
+        # Euler/Heun project onto the old norm (solvers/solver.f90:113-116); the
+        # rounding of that projection random-walks |m| by ~1e-13 per 1000 steps in
+        # the reference formula itself (the oracle drifts 1.1e-13 for Heun here)
+        drift_ref = np.abs(np.linalg.norm(mo, axis=1) - 1).max()
+        assert drift < max(3 * drift_ref, 1e-13)
+
+
+@pytest.mark.parametrize("variant", [-1, 1, 2, 3])
+def test_tiled_variants_trajectory(variant):
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    deck = mj.triangular((40, 36))
+    m0 = mj.reversed_disks(deck, 4, 5.0, 6)
+    dyn = dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=5)
+    ham = mj.Hamiltonian(deck)
+    _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, variant))
+    m = m0.copy()
+    mj.SpinDynamics(ham, **dyn).run(m, 300)
+    mo = m0.copy()
+    O.Model(deck).run(mo, 300, **dyn)
+    assert np.abs(m - mo).max() < 1e-9
 
 
 @pytest.mark.parametrize("integrator", ["sib", "heun", "euler"])

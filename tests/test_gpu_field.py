@@ -37,6 +37,21 @@ DECK_NAMES = ["square64_cfg", "triangular64_3shells", "film16x16x6_open_z", "odd
               "chain_open", "open_square_9x6", "tilted_axis_inplane_B", "two_atom_cell_ell"]
 
 
+def variants(ham):
+    """Kernel variants of a plan: -1 generic, 0..3 tiled (when a shape matched)."""
+    from matjes_b200 import _abi
+
+    v, s = _abi.C.c_int32(), _abi.C.c_int32()
+    _abi.check(_abi.lib.mj_plan_get_variant(ham.plan, _abi.C.byref(v), _abi.C.byref(s)))
+    return [-1, 0, 1, 2, 3] if s.value else [-1]
+
+
+def set_variant(ham, v):
+    from matjes_b200 import _abi
+
+    _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, v))
+
+
 @pytest.mark.parametrize("name", DECK_NAMES)
 def test_field_energy_match_oracle(name):
     import matjes_b200 as mj
@@ -45,12 +60,47 @@ def test_field_energy_match_oracle(name):
     ham = mj.Hamiltonian(deck)
     M = O.Model(deck)
     m = mj.random_sphere(deck.nsites, 11)
-    B, e = ham.get_eff_field(m, with_energy=True)
     Bo, eo = M.field(m)
-    assert site_rel_err(B, Bo) < TOL
-    assert scalar_rel_err(e, eo) < TOL
-    E, Eo = ham.energy(m), M.energy(m)
-    assert abs(E - Eo) <= TOL * abs(Eo)
+    Eo = M.energy(m)
+    for v in variants(ham):
+        if ham.noffsets:
+            set_variant(ham, v)
+        B, e = ham.get_eff_field(m, with_energy=True)
+        assert site_rel_err(B, Bo) < TOL, v
+        assert scalar_rel_err(e, eo) < TOL, v
+        assert abs(ham.energy(m) - Eo) <= TOL * abs(Eo), v
+
+
+def test_shapes_are_matched():
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    def shape(deck):
+        v, s = _abi.C.c_int32(), _abi.C.c_int32()
+        _abi.check(_abi.lib.mj_plan_get_variant(mj.Hamiltonian(deck).plan, _abi.C.byref(v), _abi.C.byref(s)))
+        return s.value
+
+    assert shape(mj.square_film((16, 16, 1))) == 1
+    assert shape(mj.triangular((16, 16), J=(1e-3,))) == 2
+    assert shape(mj.triangular((16, 16))) == 3
+    sq2 = mj.square_film((16, 16, 1))
+    sq2.J.append((1, 1, 2, -0.1e-3))
+    assert shape(sq2) == 4
+    assert shape(mj.square_film((8, 8, 4), med_z=-0.3)) == 0  # z couplings: generic kernel
+
+
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3])
+def test_square_nnn_variants(variant):
+    import matjes_b200 as mj
+
+    deck = mj.square_film((40, 24, 1))
+    deck.J.append((1, 1, 2, -0.1e-3))
+    ham = mj.Hamiltonian(deck)
+    set_variant(ham, variant)
+    m = mj.random_sphere(deck.nsites, 12)
+    Bo, eo = O.Model(deck).field(m)
+    B, e = ham.get_eff_field(m, with_energy=True)
+    assert site_rel_err(B, Bo) < TOL and scalar_rel_err(e, eo) < TOL
 
 
 def test_per_site_bfield_map():
