@@ -228,9 +228,10 @@ def run_gpu(args, rank, world):
         _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, E[k:].data_ptr(), stream))
 
     # the library's autotuner picks the kernel variant (tile shape) for this lattice
-    best = _abi.C.c_int32()
-    tune = np.zeros(5)
-    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 10, _abi.C.byref(best), tune.ctypes.data))
+    best, best_tma = _abi.C.c_int32(), _abi.C.c_int32()
+    tune = np.zeros(13)
+    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 10, _abi.C.byref(best),
+                                    _abi.C.byref(best_tma), tune.ctypes.data))
 
     for k in range(W):
         flush.zero_()
@@ -309,8 +310,11 @@ def run_gpu(args, rank, world):
                                                        {"parallelism": f"replicas x{world}" if world > 1 else "single",
                                                         "energy_per_step": "fused into pass 1",
                                                         "kernel_variant": int(best.value),
-                                                        "autotune_ms_per_step": {str(v): round(float(t), 5) for v, t
-                                                                                 in zip(range(-1, 4), tune)}}),
+                                                        "tma_halo": bool(best_tma.value),
+                                                        "autotune_ms_per_step": {
+                                                            name: round(float(t), 5) for name, t in zip(
+                                                                ["generic"] + [f"tile{v}" for v in range(6)]
+                                                                + [f"tile{v}_tma" for v in range(6)], tune)}}),
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
                      "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},

@@ -125,20 +125,30 @@ mj_status mj_plan_destroy(mj_plan* plan);
 mj_status mj_plan_nsites(const mj_plan* plan, int64_t* n);
 /* Stencil introspection: number of neighbour offsets (0 for ELL plans). */
 mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n);
-/* Kernel variant of a stencil plan: -1 = generic per-offset kernel; 0..3 =
+/* Kernel variant of a stencil plan: -1 = generic per-offset kernel; 0..5 =
  * shared-memory tiled kernel with 32 x (threads-in-y * sites-per-thread)
- * tiles of 4x8, 8x4, 4x4, 2x8.  Tiled variants exist for the square (NN,
+ * tiles of 4x4, 8x4, 8x2, then 4x4, 8x2, 4x2 compiled for 6, 4, 8 resident
+ * blocks per SM (fewer registers).  Tiled variants exist for the square (NN,
  * NN+NNN) and triangular (NN, three shells) offset sets; MJ_ERR_UNSUPPORTED
  * otherwise.  No counterpart in the reference (its SpMV has no tiling). */
 mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant);
 /* Current variant (-1 generic) and the matched compile-time shape id (0 none). */
 mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape);
-/* Autotuner: times `steps` steps of `p` for every variant of the plan on a
- * scratch copy of the device spins m_dev_soa (left untouched), keeps the
- * fastest and returns it in *best; ms_per_step (5 doubles, variants -1..3, may
- * be NULL) receives the timings (negative = variant unavailable).  Synchronous. */
+/* Halo staging of the tiled kernels: enable = 1 (default) uses TMA bulk-tensor
+ * copies in persistent, double-buffered blocks (tiles whose halo wraps a
+ * periodic edge fall back to plain loads); 0 = plain loads, one tile per block. */
+mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable);
+/* Autotuner: times `steps` steps of `p` for every kernel configuration of the
+ * plan on a scratch copy of the device spins m_dev_soa (left untouched), keeps
+ * the fastest and returns its variant in *best (and its staging in *best_tma,
+ * may be NULL).  ms_per_step (13 doubles, may be NULL): [0] generic kernel,
+ * [1+v] tiled variant v with plain loads, [7+v] with TMA; negative = not
+ * available.  Synchronous. */
 mj_status mj_plan_autotune(mj_plan* plan, const double* m_dev_soa, const mj_dyn_params* p, int32_t steps,
-                           int32_t* best, double* ms_per_step);
+                           int32_t* best, int32_t* best_tma, double* ms_per_step);
+/* Device status word of the plan's kernels (synchronises, then clears it):
+ * MJ_ERR_TIMEOUT when a bounded device wait gave up since the last check. */
+mj_status mj_plan_check_status(mj_plan* plan);
 /* Per-site applied field map (Tesla, host AoS 3*Ncell; NULL = uniform H_ext):
  * the Bfield_init.dat input read by initialization/orders_initialize.f90:28. */
 mj_status mj_plan_set_bfield(mj_plan* plan, const double* b_cell_host);

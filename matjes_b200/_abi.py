@@ -114,7 +114,10 @@ SIGNATURES = {
     "mj_plan_noffsets": (C.c_int32, [P, C.POINTER(C.c_int32)]),
     "mj_plan_set_variant": (C.c_int32, [P, C.c_int32]),
     "mj_plan_get_variant": (C.c_int32, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
-    "mj_plan_autotune": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32), P]),
+    "mj_plan_autotune": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), P]),
+    "mj_plan_set_tma": (C.c_int32, [P, C.c_int32]),
+    "mj_plan_check_status": (C.c_int32, [P]),
     "mj_plan_set_bfield": (C.c_int32, [P, P]),
     "mj_plan_set_bfield_device": (C.c_int32, [P, P, P]),
     "mj_state_create": (C.c_int32, [P, C.POINTER(P)]),

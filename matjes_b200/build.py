@@ -1,15 +1,23 @@
-"""Build the CUDA library in-tree for sm_100a (``python -m matjes_b200.build``)."""
+"""Build the CUDA library in-tree for sm_100a (``python matjes_b200/build.py``).
+
+Every translation unit is compiled to an object in parallel (the tiled kernels
+are one unit per lattice shape), then linked into libmatjes_b200.so.
+"""
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmatjes_b200.so")
-SOURCES = ["mj_kernels.cu", "mj_tiled.cu", "mj_dipolar.cu", "mj_lattice.cpp", "mj_abi.cpp"]
-HEADERS = ["mj_internal.hpp", "mj_device.cuh", "mj_shapes.hpp", os.path.join("..", "..", "include", "matjes_gpu.h")]
+OBJDIR = os.path.join(os.path.dirname(HERE), "_build", "obj")
+SOURCES = ["mj_kernels.cu", "mj_tiled.cu", "mj_tiled_square_nn.cu", "mj_tiled_square2.cu", "mj_tiled_tri_nn.cu",
+           "mj_tiled_tri3.cu", "mj_dipolar.cu", "mj_lattice.cpp", "mj_abi.cpp"]
+HEADERS = ["mj_internal.hpp", "mj_device.cuh", "mj_shapes.hpp", "mj_tiled_impl.cuh",
+           os.path.join("..", "..", "include", "matjes_gpu.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
@@ -35,20 +43,39 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources() if os.path.exists(s))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def _compile(src: str):
+    obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+    cmd = [_nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    return src, obj, res
+
+
+def build(force: bool = False, verbose: bool = False, jobs: int = 0) -> str:
     if not force and up_to_date():
         return OUT
+    os.makedirs(OBJDIR, exist_ok=True)
+    jobs = jobs or max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        results = list(ex.map(_compile, SOURCES))
+    report = []
+    for src, obj, res in results:
+        report.append(f"=== {src}\n{res.stderr}")
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError(f"nvcc failed on {src}")
     tmp = OUT + ".tmp"
-    cmd = [_nvcc(), *NVCC_FLAGS, "-shared", "-o", tmp, *[os.path.join(CSRC, s) for s in SOURCES], "-lcufft"]
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    link = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp,
+            *[obj for _, obj, _ in results], "-lcufft"]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc build of libmatjes_b200.so failed")
-    if verbose:
-        sys.stderr.write(res.stderr)
+        raise RuntimeError("link of libmatjes_b200.so failed")
     os.replace(tmp, OUT)
+    text = "\n".join(report)
+    if verbose:
+        sys.stderr.write(text)
     with open(os.path.join(HERE, "ptxas_report.txt"), "w") as f:
-        f.write(res.stderr)
+        f.write(text)
     return OUT
 
 

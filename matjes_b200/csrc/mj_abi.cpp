@@ -257,14 +257,20 @@ mj_status alloc_scratch(mj_plan* p) {
     if ((st = dalloc(&p->d_mid, 3 * N, "mid")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_aux, 3 * N, "aux")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_aux2, 3 * N, "aux2")) != MJ_OK) return st;
-    // generic grid, or the smallest tile of the tiled kernels (32 x 16), whichever has more blocks
-    const int64_t tiled_max = p->is_stencil ? static_cast<int64_t>((p->sp.L[0] + 31) / 32) * ((p->sp.L[1] + 15) / 16) * p->sp.L[2] : 0;
+    // generic grid, or the smallest tile of the tiled kernels (32 x 8), whichever has more blocks
+    const int64_t tiled_max = p->is_stencil ? static_cast<int64_t>((p->sp.L[0] + 31) / 32) * ((p->sp.L[1] + 7) / 8) * p->sp.L[2] : 0;
     p->partial_cap = 2 * std::max(energy_blocks(p), tiled_max) + 64;
     if ((st = dalloc(&p->d_partials, static_cast<size_t>(p->partial_cap), "partials")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_counter, 4, "counter")) != MJ_OK) return st;
     if ((st = cuda_status(cudaMemset(p->d_counter, 0, 4 * sizeof(unsigned int)), "counter init")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_scalar, 8, "scalar")) != MJ_OK) return st;
-    return MJ_OK;
+    if ((st = dalloc(&p->d_status, 4, "status")) != MJ_OK) return st;
+    if ((st = cuda_status(cudaMemset(p->d_status, 0, 4 * sizeof(int)), "status init")) != MJ_OK) return st;
+    cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
+    double tab[768];
+    build_noise_tables(tab);
+    if ((st = dalloc(&p->d_noise_tab, 768, "noise tables")) != MJ_OK) return st;
+    return cuda_status(cudaMemcpy(p->d_noise_tab, tab, sizeof(tab), cudaMemcpyHostToDevice), "noise tables");
 }
 
 void free_plan(mj_plan* p) {
@@ -285,6 +291,8 @@ void free_plan(mj_plan* p) {
     cudaFree(p->d_partials);
     cudaFree(p->d_counter);
     cudaFree(p->d_scalar);
+    cudaFree(p->d_status);
+    cudaFree(p->d_noise_tab);
     cudaFree(p->d_stage);
     cudaFree(p->d_tmp_m);
     cudaFree(p->d_tmp_b);
@@ -302,7 +310,7 @@ mj_status ensure_host_scratch(mj_plan* p) {
     return MJ_OK;
 }
 
-mj_status dyn_coef(const mj_dyn_params* d, int64_t N, DynCoef& c) {
+mj_status dyn_coef(const mj_dyn_params* d, const mj_plan* plan, DynCoef& c) {
     if (!d) return set_error(MJ_ERR_ARG, "null dynamics parameters");
     if (d->integrator != MJ_EULER && d->integrator != MJ_HEUN_MATJES && d->integrator != MJ_SIB)
         return set_error(MJ_ERR_ARG, "integrator must be MJ_EULER, MJ_HEUN_MATJES or MJ_SIB");
@@ -325,9 +333,16 @@ mj_status dyn_coef(const mj_dyn_params* d, int64_t N, DynCoef& c) {
     c.inject = d->inject;
     c.inject_nbuf = d->inject_nbuf;
     c.step_base = nullptr;
+    uint32_t k0 = static_cast<uint32_t>(d->seed), k1 = static_cast<uint32_t>(d->seed >> 32);
+    for (int r = 0; r < 10; ++r) {  // Philox4x32 key schedule (Weyl increments)
+        c.keys[2 * r] = k0;
+        c.keys[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    c.noise_tab = plan->d_noise_tab;
     if (c.thermal && d->noise == MJ_NOISE_INJECT && (!d->inject || d->inject_nbuf < 1))
         return set_error(MJ_ERR_ARG, "MJ_NOISE_INJECT needs a device buffer and inject_nbuf >= 1");
-    (void)N;
     return MJ_OK;
 }
 
@@ -372,7 +387,7 @@ namespace {
 mj_status run_steps(mj_plan* p, double* m, const mj_dyn_params* prm, int32_t nsteps, double* E_dev, cudaStream_t s) {
     if (nsteps < 0) return set_error(MJ_ERR_ARG, "nsteps must be >= 0");
     DynCoef c;
-    mj_status st = dyn_coef(prm, p->N, c);
+    mj_status st = dyn_coef(prm, p, c);
     if (st != MJ_OK) return st;
     return step_sequence(p, m, c, prm->energy_mode, prm->step0, nsteps, E_dev, s);
 }
@@ -585,7 +600,7 @@ mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n) {
 
 mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant) {
     if (!plan) return set_error(MJ_ERR_ARG, "null plan");
-    if (variant < -1 || variant > 3) return set_error(MJ_ERR_ARG, "variant must be -1..3");
+    if (variant < -1 || variant >= kTiledVariants) return set_error(MJ_ERR_ARG, "variant must be -1..5");
     if (variant >= 0 && !(plan->is_stencil && plan->tiled_shape != 0))
         return set_error(MJ_ERR_UNSUPPORTED, "no tiled kernel for this plan's offsets");
     if (variant < 0) {
@@ -603,13 +618,13 @@ mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant) {
 }
 
 mj_status mj_plan_autotune(mj_plan* plan, const double* m, const mj_dyn_params* prm, int32_t steps, int32_t* best,
-                           double* ms_per_step) {
+                           int32_t* best_tma, double* ms_per_step) {
     if (!plan || !m || !prm || !best || steps < 1) return set_error(MJ_ERR_ARG, "bad autotune arguments");
     cudaSetDevice(plan->device);
     mj_status st = ensure_host_scratch(plan);
     if (st != MJ_OK) return st;
     DynCoef c;
-    if ((st = dyn_coef(prm, plan->N, c)) != MJ_OK) return st;
+    if ((st = dyn_coef(prm, plan, c)) != MJ_OK) return st;
     const int32_t v0 = (plan->is_stencil && plan->sp.shape != 0) ? plan->tile_variant : -1;
     const bool has_tiled = plan->is_stencil && plan->tiled_shape != 0;
     cudaEvent_t a, b;
@@ -620,12 +635,17 @@ mj_status mj_plan_autotune(mj_plan* plan, const double* m, const mj_dyn_params* 
     }
     double best_ms = 1e300;
     int32_t best_v = v0;
-    for (int32_t v = -1; v <= 3; ++v) {
+    bool best_t = plan->use_tma;
+    // configurations: 0 generic, 1..6 tiled variants 0..5 with plain loads, 7..12 with TMA
+    for (int cfg = 0; cfg < 1 + 2 * kTiledVariants; ++cfg) {
+        const int32_t v = cfg == 0 ? -1 : (cfg - 1) % kTiledVariants;
+        const bool tma = cfg > kTiledVariants;
         double ms = -1.0;
         if ((v >= 0 && !has_tiled) || (v == -1 && !plan->is_stencil)) {
-            if (ms_per_step) ms_per_step[v + 1] = ms;
+            if (ms_per_step) ms_per_step[cfg] = ms;
             continue;
         }
+        plan->use_tma = tma;
         if (plan->is_stencil && (st = mj_plan_set_variant(plan, v)) != MJ_OK) break;
         if ((st = cuda_status(cudaMemcpy(plan->d_tmp_m, m, sizeof(double) * 3 * plan->N, cudaMemcpyDeviceToDevice),
                               "autotune copy")) != MJ_OK)
@@ -638,18 +658,48 @@ mj_status mj_plan_autotune(mj_plan* plan, const double* m, const mj_dyn_params* 
         float f = 0.0f;
         cudaEventElapsedTime(&f, a, b);
         ms = f / steps;
-        if (ms_per_step) ms_per_step[v + 1] = ms;
+        if (ms_per_step) ms_per_step[cfg] = ms;
         if (ms < best_ms) {
             best_ms = ms;
             best_v = v;
+            best_t = tma;
         }
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (st != MJ_OK) return st;
+    plan->use_tma = best_t;
     if (plan->is_stencil && (st = mj_plan_set_variant(plan, best_v)) != MJ_OK) return st;
+    if ((st = mj_plan_check_status(plan)) != MJ_OK) return st;
     *best = best_v;
+    if (best_tma) *best_tma = best_t ? 1 : 0;
     return MJ_OK;
+}
+
+mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    plan->use_tma = enable != 0;
+    if (plan->graph_exec) {
+        cudaGraphExecDestroy(plan->graph_exec);
+        plan->graph_exec = nullptr;
+        plan->graph_key.clear();
+    }
+    return MJ_OK;
+}
+
+mj_status mj_plan_check_status(mj_plan* plan) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    cudaSetDevice(plan->device);
+    int word = 0;
+    mj_status st = cuda_status(cudaDeviceSynchronize(), "status sync");
+    if (st != MJ_OK) return st;
+    if ((st = cuda_status(cudaMemcpy(&word, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status read")) != MJ_OK)
+        return st;
+    if (word == 0) return MJ_OK;
+    // a timed-out block skipped the energy reduction: re-arm its ticket counter too
+    cudaMemset(plan->d_status, 0, sizeof(int));
+    cudaMemset(plan->d_counter, 0, 4 * sizeof(unsigned int));
+    return set_error(MJ_ERR_TIMEOUT, "a bounded device wait (TMA mbarrier) gave up; results of that launch are invalid");
 }
 
 mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape) {
@@ -815,7 +865,7 @@ mj_status mj_graph_run(mj_plan* plan, mj_state* s, const mj_dyn_params* prm, int
     if (!plan || !s || !prm || nsteps < 1 || nreplay < 0) return set_error(MJ_ERR_ARG, "bad graph arguments");
     cudaSetDevice(plan->device);
     DynCoef c;
-    mj_status st = dyn_coef(prm, plan->N, c);
+    mj_status st = dyn_coef(prm, plan, c);
     if (st != MJ_OK) return st;
     if (!plan->d_stepctr && (st = dalloc(&plan->d_stepctr, 4, "step counter")) != MJ_OK) return st;
     if (!plan->cap_stream &&

@@ -41,19 +41,96 @@ __device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
     return static_cast<double>(k) * (1.0 / 9007199254740992.0);
 }
 
-__device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site) {
-    const uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+// Philox4x32-10 with the ten round keys precomputed (keys[2r], keys[2r+1]).
+__device__ __forceinline__ void philox10k(uint32_t c[4], const uint32_t* keys) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = M0 * c[0], hi0 = __umulhi(M0, c[0]);
+        const uint32_t lo1 = M1 * c[2], hi1 = __umulhi(M1, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ keys[2 * r];
+        const uint32_t n2 = hi0 ^ c[3] ^ keys[2 * r + 1];
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+    }
+}
+
+// Table-driven FP64 log and sin/cos of 2 pi u (our own evaluation, the same
+// arithmetic as the oracle's): tab[0..511] = (sin, cos)(2 pi i/256) pairs,
+// tab[512..767] = (1/F, ln F) pairs for F = (j + 96)/128 (j = 0..96 used).
+//   ln u = e ln2 + ln F + ln(1 + r), mantissa m in [0.75, 1.5), F the nearest
+//   multiple of 1/128, r = (m - F)/F, |r| <= 1/192, series to r^7;
+//   2 pi u = 2 pi i/256 + x, |x| < pi/128, Taylor sin to x^7 and cos to x^8.
+constexpr double kLn2 = 0.6931471805599453;        // ln 2
+constexpr double kPiOver128 = 0.02454369260617026;  // pi / 128
+
+__device__ __forceinline__ double tab_log(double u, const double* __restrict__ tab) {
+    const long long b = __double_as_longlong(u);
+    int e = static_cast<int>((b >> 52) & 0x7ff) - 1023;
+    double m = __longlong_as_double((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+    if (m >= 1.5) {  // centre the mantissa in [0.75, 1.5): no cancellation against e ln2 near u = 1
+        m *= 0.5;
+        e += 1;
+    }
+    const int j = static_cast<int>(m * 128.0 + 0.5);  // nearest F = j/128, j = 96..192
+    const double F = static_cast<double>(j) * (1.0 / 128.0);
+    const double2 t = __ldg(reinterpret_cast<const double2*>(tab + 512) + (j - 96));
+    const double r = (m - F) * t.x;
+    double p = fma(r, 1.0 / 7.0, -1.0 / 6.0);
+    p = fma(p, r, 1.0 / 5.0);
+    p = fma(p, r, -0.25);
+    p = fma(p, r, 1.0 / 3.0);
+    p = fma(p, r, -0.5);
+    const double l1p = fma(r * r, p, r);
+    return fma(static_cast<double>(e), kLn2, t.y + l1p);
+}
+
+__device__ __forceinline__ void tab_sincos2pi(double u, const double* __restrict__ tab, double* s, double* c) {
+    const double t = u * 256.0;
+    const int i = static_cast<int>(t);
+    const double x = (t - static_cast<double>(i)) * kPiOver128;
+    const double x2 = x * x;
+    double ps = fma(x2, -1.0 / 5040.0, 1.0 / 120.0);
+    ps = fma(ps, x2, -1.0 / 6.0);
+    const double sx = fma(x * x2, ps, x);
+    double pc = fma(x2, 1.0 / 40320.0, -1.0 / 720.0);
+    pc = fma(pc, x2, 1.0 / 24.0);
+    pc = fma(pc, x2, -0.5);
+    const double cm = x2 * pc;
+    const double2 sc = __ldg(reinterpret_cast<const double2*>(tab) + i);
+    *s = sc.x + fma(sc.x, cm, sc.y * sx);
+    *c = sc.y + fma(sc.y, cm, -(sc.x * sx));
+}
+
+// N(0,1) triple of one site and step: two Box-Muller pairs from two Philox
+// blocks, counter = (site, step, stream, call), 53-bit uniforms.
+__device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, const double* __restrict__ tab,
+                                                      uint32_t step, uint32_t stream, uint32_t site) {
     uint32_t c[4] = {site, step, stream, 0u};
-    philox10(c, k0, k1);
+    philox10k(c, keys);
     uint32_t d[4] = {site, step, stream, 1u};
-    philox10(d, k0, k1);
-    const double r1 = sqrt(-2.0 * log(u53_open(c[0], c[1])));
-    const double r2 = sqrt(-2.0 * log(u53_open(d[0], d[1])));
-    // angle 2 pi u through sinpi/cospi of 2u (exact argument, no range reduction)
-    double s1, c1;
-    sincospi(2.0 * u53(c[2], c[3]), &s1, &c1);
-    const double c2 = cospi(2.0 * u53(d[2], d[3]));
+    philox10k(d, keys);
+    const double r1 = sqrt(-2.0 * tab_log(u53_open(c[0], c[1]), tab));
+    const double r2 = sqrt(-2.0 * tab_log(u53_open(d[0], d[1]), tab));
+    double s1, c1, s2, c2;
+    tab_sincos2pi(u53(c[2], c[3]), tab, &s1, &c1);
+    tab_sincos2pi(u53(d[2], d[3]), tab, &s2, &c2);
     return make_double3(r1 * c1, r1 * s1, r2 * c2);
+}
+
+__device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site,
+                                                  const double* __restrict__ tab) {
+    uint32_t keys[20];
+    uint32_t k0 = static_cast<uint32_t>(seed), k1 = static_cast<uint32_t>(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        keys[2 * r] = k0;
+        keys[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return philox_normals_tab(keys, tab, step, stream, site);
 }
 
 // Thermal field b = sigma * N(0,1) (dynamics/spindynamics.f90:268-272): Philox
@@ -61,7 +138,7 @@ __device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, 
 __device__ __forceinline__ double3 thermal_field(const DynCoef& C, uint32_t step, int64_t i, int64_t N) {
     if (C.step_base) step += *C.step_base;
     if (C.noise == MJ_NOISE_PHILOX) {
-        const double3 z = philox_normals(C.seed, step, C.stream_id, static_cast<uint32_t>(i));
+        const double3 z = philox_normals_tab(C.keys, C.noise_tab, step, C.stream_id, static_cast<uint32_t>(i));
         return make_double3(C.sigma * z.x, C.sigma * z.y, C.sigma * z.z);
     }
     const double* buf = C.inject + static_cast<int64_t>(step % static_cast<uint32_t>(C.inject_nbuf)) * 3 * N;

@@ -85,7 +85,13 @@ struct DynCoef {
     int inject_nbuf;
     // graph replay: the thermal step index is *step_base + step (null = step)
     const uint32_t* step_base;
+    uint32_t keys[20];          // Philox round keys of `seed`
+    const double* noise_tab;    // device tables of the Box-Muller evaluation (768 doubles)
 };
+
+// Box-Muller tables (host-built, identical to the oracle's): 256 (sin, cos) pairs
+// of 2 pi i/256 followed by 128 (1/F, ln F) pairs of F = 1 + j/128.
+void build_noise_tables(double* tab768);
 
 }  // namespace mj
 
@@ -98,6 +104,10 @@ struct mj_plan {
     mj::StencilParams sp{};
     int tile_variant = 0;            // tiled-kernel shape (threads in y x sites per thread), see mj_tiled.cu
     int tiled_shape = 0;             // matched compile-time shape (sp.shape is 0 while the generic path is forced)
+    bool use_tma = true;             // tiled kernels stage halos with TMA (persistent, double-buffered)
+    int tma_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // persistent grid per tile variant (occupancy x SMs)
+    int num_sms = 148;
+    int* d_status = nullptr;         // device status word: bit 0 = bounded wait timed out
     // ELL form (multi-atom cells, COO input): width entries per site
     int ell_width = 0;
     int* d_ell_col = nullptr;        // [width][N], -1 = empty
@@ -118,6 +128,7 @@ struct mj_plan {
     double* d_partials = nullptr;    // per-block energy partials
     unsigned int* d_counter = nullptr;
     double* d_scalar = nullptr;      // 8 doubles of device scratch
+    double* d_noise_tab = nullptr;   // Box-Muller tables (768 doubles)
     int64_t partial_cap = 0;
     // host-array convenience calls (allocated on first use)
     double* d_stage = nullptr;       // 3N AoS staging
@@ -167,10 +178,22 @@ mj_status aos_to_soa(const double* src_aos, double* dst_soa, int64_t n, cudaStre
 mj_status soa_to_aos(const double* src_soa, double* dst_aos, int64_t n, cudaStream_t s);
 int64_t energy_blocks(const mj_plan* p);
 
-// tiled kernels for compile-time stencil shapes (mj_tiled.cu)
+// tiled kernels for compile-time stencil shapes (mj_tiled.cu dispatches to one
+// translation unit per shape, mj_tiled_<shape>.cu)
 // pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
+constexpr int kTiledVariants = 6;
+constexpr int kTiledVariantTY[kTiledVariants] = {16, 32, 16, 16, 16, 8};  // tile height per variant
+static_assert(kTiledVariants <= static_cast<int>(sizeof(mj_plan::tma_blocks) / sizeof(int)),
+              "mj_plan::tma_blocks holds one persistent grid size per tiled variant");
 mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
                        double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s);
+#define MJ_TILED_SHAPE_DECL(fn)                                                                                   \
+    mj_status fn(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,         \
+                 double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s);
+MJ_TILED_SHAPE_DECL(launch_tiled_square_nn)
+MJ_TILED_SHAPE_DECL(launch_tiled_square2)
+MJ_TILED_SHAPE_DECL(launch_tiled_tri_nn)
+MJ_TILED_SHAPE_DECL(launch_tiled_tri3)
 int64_t tiled_energy_blocks(const mj_plan* p);
 // match a single-atom stencil to a compile-time shape and reorder its tensors (mj_abi.cpp)
 void match_shape(mj::StencilParams& sp);

@@ -328,10 +328,10 @@ __global__ void __launch_bounds__(256) k_temperature(const __grid_constant__ F f
     grid_reduce<2>(v, R.partials, R.counter, R.out, R.nblocks);
 }
 
-__global__ void k_philox(uint64_t seed, uint32_t step, uint32_t stream, int64_t n, double* out) {
+__global__ void k_philox(uint64_t seed, uint32_t step, uint32_t stream, int64_t n, double* out, const double* tab) {
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    const double3 z = philox_normals(seed, step, stream, static_cast<uint32_t>(i));
+    const double3 z = philox_normals(seed, step, stream, static_cast<uint32_t>(i), tab);
     out[i] = z.x;
     out[n + i] = z.y;
     out[2 * n + i] = z.z;
@@ -561,7 +561,20 @@ mj_status launch_temperature(mj_plan* p, const double* m, double* out2, cudaStre
 
 mj_status launch_philox(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n, double* out, cudaStream_t s) {
     if (n <= 0) return MJ_OK;
-    k_philox<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(seed, step, stream_id, n, out);
+    // Box-Muller tables of the current device, built once per device
+    static double* tabs[64] = {nullptr};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return set_error(MJ_ERR_ARG, "device index out of range");
+    if (!tabs[dev]) {
+        double h[768];
+        build_noise_tables(h);
+        mj_status st = cuda_status(cudaMalloc(&tabs[dev], sizeof(h)), "philox tables");
+        if (st != MJ_OK) return st;
+        if ((st = cuda_status(cudaMemcpy(tabs[dev], h, sizeof(h), cudaMemcpyHostToDevice), "philox tables")) != MJ_OK)
+            return st;
+    }
+    k_philox<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(seed, step, stream_id, n, out, tabs[dev]);
     return cuda_status(cudaGetLastError(), "k_philox");
 }
 

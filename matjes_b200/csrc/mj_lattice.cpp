@@ -314,6 +314,21 @@ bool build_blocks(const Geometry& g, const mj_hamiltonian_desc& h, std::vector<B
     return true;
 }
 
+void build_noise_tables(double* tab) {
+    // evaluated in extended precision, then rounded once to double
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int i = 0; i < 256; ++i) {
+        const long double a = two_pi * static_cast<long double>(i) / 256.0L;
+        tab[2 * i] = static_cast<double>(sinl(a));
+        tab[2 * i + 1] = static_cast<double>(cosl(a));
+    }
+    for (int j = 0; j < 128; ++j) {
+        const long double F = static_cast<long double>(j + 96) / 128.0L;  // used for j + 96 = 96..192
+        tab[512 + 2 * j] = static_cast<double>(1.0L / F);
+        tab[512 + 2 * j + 1] = static_cast<double>(logl(F));
+    }
+}
+
 bool build_dipolar_kernel(const Geometry& g, const mj_hamiltonian_desc& h, int nrep[3], std::vector<double>& K,
                           std::string& err) {
     if (g.nmag != 1) {

@@ -1,0 +1,599 @@
+// Shared-memory tiled stencil passes for the lattices with compile-time offset
+// tables (mj_shapes.hpp): square NN / NN+NNN, triangular NN / three shells.
+//
+// A block of 32 x BYT threads owns a 32 x (BYT*RY) tile of one z-layer; each
+// thread owns RY sites stacked along y.  The tile plus its halo is staged in
+// shared memory (SoA), then each thread walks the stencil column by column: a
+// value of column dx is loaded once and accumulated into every one of the
+// thread's RY sites that sees it.  Offsets and tensor slots are compile-time
+// constants; the coupling values come from the launch parameters.
+//
+// Two kernels share that compute:
+//   k_tiled : one tile per block, halo staged with plain loads (periodic wrap
+//             resolved per element);
+//   k_tma   : persistent blocks walking a strided tile list with two shared
+//             buffers; the halo box of the next tile is fetched by one
+//             cp.async.bulk.tensor (TMA, 4D: x, y, z, component) completing on
+//             an mbarrier while the current tile computes.  Tiles whose halo
+//             wraps around a periodic edge take the plain-load path; on open
+//             axes the TMA zero fill of out-of-range cells is the open boundary.
+// The halo along x is rounded up to an even width so that every TMA box starts
+// on a 16-byte boundary.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <utility>
+
+#include "mj_device.cuh"
+#include "mj_internal.hpp"
+#include "mj_shapes.hpp"
+
+namespace mj {
+namespace {
+
+enum { PASS_FIELD = 0, PASS_EULER = 1, PASS_HEUN1 = 2, PASS_HEUN2 = 3, PASS_SIB1 = 4, PASS_SIB2 = 5 };
+
+struct TReduce {
+    double* partials;
+    unsigned int* counter;
+    double* out;
+    int nblocks;
+};
+
+struct TiledArgs {
+    const double* ms;   // spins the stencil runs on (m, or the midpoint in pass 2)
+    const double* mn;   // m_n (own site) for the SIB corrector
+    double* out;        // field B / next state / midpoint
+    double* aux;        // Heun D1, SIB Philox draw, or per-site energy (field pass)
+    double* aux2;       // Heun DT
+    const double* bmap; // per-cell applied field (SoA) or null
+    DipView Hd;
+    TReduce R;
+    uint32_t step;
+    int* status;        // device status word (bounded-wait timeouts)
+};
+
+template <class S, int BYT, int RY>
+struct TileGeom {
+    static constexpr int R = S::R;               // halo along y
+    static constexpr int RX = (S::R + 1) & ~1;   // halo along x, even (16-byte TMA boxes)
+    static constexpr int TX = 32, TY = BYT * RY;
+    static constexpr int PX = TX + 2 * RX;
+    static constexpr int PY = TY + 2 * R;
+    static constexpr int NS = PX * PY;
+    static constexpr size_t buf_bytes = sizeof(double) * 3 * NS;        // one TMA box
+    static constexpr size_t buf_stride = (buf_bytes + 127) / 128 * 128;  // 128-byte aligned buffers
+    static constexpr size_t buf_stride_d = buf_stride / sizeof(double);
+};
+
+// ---------------------------------------------------------------------------
+// stencil accumulation, fully unrolled over compile-time offsets
+template <class S, int RY, int DX, int YY, int... Kk>
+__device__ __forceinline__ void row_accumulate(const StencilParams& P, double vx, double vy, double vz, double* bx,
+                                               double* by, double* bz, std::integer_sequence<int, Kk...>) {
+    (
+        [&] {
+            constexpr int k = Kk;
+            if constexpr (S::DX[k] == DX) {
+                constexpr int r = YY - S::DY[k];
+                if constexpr (r >= 0 && r < RY) {
+                    const double* W = P.W[k];
+                    if constexpr (S::ISO[k] != 0) {
+                        const double w = W[0];
+                        bx[r] = fma(w, vx, bx[r]);
+                        by[r] = fma(w, vy, by[r]);
+                        bz[r] = fma(w, vz, bz[r]);
+                    } else {
+                        bx[r] = fma(W[0], vx, fma(W[1], vy, fma(W[2], vz, bx[r])));
+                        by[r] = fma(W[3], vx, fma(W[4], vy, fma(W[5], vz, by[r])));
+                        bz[r] = fma(W[6], vx, fma(W[7], vy, fma(W[8], vz, bz[r])));
+                    }
+                }
+            }
+        }(),
+        ...);
+}
+
+template <class S, int BYT, int RY, int DX, int... Y>
+__device__ __forceinline__ void column_rows(const StencilParams& P, const double* sm, int base, double* bx, double* by,
+                                            double* bz, std::integer_sequence<int, Y...>) {
+    using G = TileGeom<S, BYT, RY>;
+    constexpr int ylo = shape_col_ymin<S>(DX);
+    (
+        [&] {
+            constexpr int yy = ylo + Y;
+            const int s = base + (yy + G::R) * G::PX + DX + G::RX;
+            row_accumulate<S, RY, DX, yy>(P, sm[s], sm[G::NS + s], sm[2 * G::NS + s], bx, by, bz,
+                                          std::make_integer_sequence<int, S::K>{});
+        }(),
+        ...);
+}
+
+template <class S, int BYT, int RY, int... C>
+__device__ __forceinline__ void all_columns(const StencilParams& P, const double* sm, int base, double* bx, double* by,
+                                            double* bz, std::integer_sequence<int, C...>) {
+    (
+        [&] {
+            constexpr int dx = C - S::R;
+            constexpr int ylo = shape_col_ymin<S>(dx), yhi = shape_col_ymax<S>(dx);
+            if constexpr (ylo <= yhi) {
+                column_rows<S, BYT, RY, dx>(P, sm, base, bx, by, bz,
+                                            std::make_integer_sequence<int, RY + yhi - ylo>{});
+            }
+        }(),
+        ...);
+}
+
+// per-site epilogue inputs that live in global memory, loaded before the
+// stencil so that their latency overlaps it
+struct Pre {
+    double3 a;  // SIB2: m_n;  HEUN2: D1
+    double3 b;  // SIB2: stored Philox draw;  HEUN2: DT
+};
+
+template <int PASS>
+__device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N) {
+    Pre p;
+    p.a = make_double3(0.0, 0.0, 0.0);
+    p.b = p.a;
+    if constexpr (PASS == PASS_SIB2) {
+        p.a = make_double3(A.mn[i], A.mn[N + i], A.mn[2 * N + i]);
+        if (C.thermal && A.aux) p.b = ld3(A.aux, i, N);
+    } else if constexpr (PASS == PASS_HEUN2) {
+        p.a = ld3(A.aux, i, N);
+        if (C.thermal) p.b = ld3(A.aux2, i, N);
+    }
+    return p;
+}
+
+template <int PASS>
+__device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N, double3 m0,
+                                           const FieldOut& f, double3 hd, const Pre& pre) {
+    const double3 B = make_double3(f.B.x - 2.0 * hd.x, f.B.y - 2.0 * hd.y, f.B.z - 2.0 * hd.z);
+    if constexpr (PASS == PASS_FIELD) {
+        if (A.out) st3(A.out, i, N, B);
+        if (A.aux) A.aux[i] = site_energy(f, m0, hd);
+        return total_energy_part(f, m0, hd);
+    } else if constexpr (PASS == PASS_EULER) {
+        const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
+        const double c = C.h_over_hbar;
+        double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
+        if (C.thermal) {
+            const double3 DT = llg_rhs(thermal_field(C, A.step, i, N), m0, C.alpha, C.inv_den);
+            t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
+        }
+        st3(A.out, i, N, project(t, m0));
+        return total_energy_part(f, m0, hd);
+    } else if constexpr (PASS == PASS_HEUN1) {
+        const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
+        const double c = C.h_over_hbar;
+        const double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
+        st3(A.out, i, N, project(t, m0));
+        st3(A.aux, i, N, D);
+        if (C.thermal) st3(A.aux2, i, N, llg_rhs(thermal_field(C, A.step, i, N), m0, C.alpha, C.inv_den));
+        return total_energy_part(f, m0, hd);
+    } else if constexpr (PASS == PASS_HEUN2) {
+        const double3 D2 = llg_rhs(B, m0, C.alpha, C.inv_den);
+        const double3 d1 = pre.a;
+        const double3 Di = make_double3(0.5 * d1.x + 0.5 * D2.x, 0.5 * d1.y + 0.5 * D2.y, 0.5 * d1.z + 0.5 * D2.z);
+        const double c = C.h_over_hbar;
+        double3 t = make_double3(m0.x + Di.x * c, m0.y + Di.y * c, m0.z + Di.z * c);
+        if (C.thermal) {
+            const double3 DT = pre.b;
+            t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
+        }
+        st3(A.out, i, N, project(t, m0));
+        return 0.0;
+    } else if constexpr (PASS == PASS_SIB1) {
+        double3 H = B;
+        if (C.thermal) {
+            const double3 b = thermal_field(C, A.step, i, N);
+            if (A.aux) st3(A.aux, i, N, b);  // the corrector reuses this step's draw
+            H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
+        }
+        const double3 y = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
+        st3(A.out, i, N, make_double3(0.5 * (m0.x + y.x), 0.5 * (m0.y + y.y), 0.5 * (m0.z + y.z)));
+        return total_energy_part(f, m0, hd);
+    } else {  // PASS_SIB2: m0 is the midpoint, the corrector starts from m_n
+        double3 H = B;
+        if (C.thermal) {
+            const double3 b = A.aux ? pre.b : thermal_field(C, A.step, i, N);
+            H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
+        }
+        st3(A.out, i, N, sib_solve(pre.a, m0, H, C.alpha, C.sib_hc));
+        return 0.0;
+    }
+}
+
+// plain staging of tile + halo; periodic wrap per element, zeros off open edges
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void load_tile(const StencilParams& P, const double* ms, int x0, int y0, int z, double* sm) {
+    using G = TileGeom<S, BYT, RY>;
+    const int Lx = P.L[0], Ly = P.L[1];
+    const int64_t layer = static_cast<int64_t>(Lx) * Ly;
+    const int64_t N = layer * P.L[2];
+    const double* mx = ms + layer * z;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    for (int idx = tid; idx < G::NS; idx += 32 * BYT) {
+        const int ly = idx / G::PX;
+        const int lx = idx - ly * G::PX;
+        int gx = x0 + lx - G::RX, gy = y0 + ly - G::R;
+        bool ok = true;
+        if (gx < 0 || gx >= Lx) {
+            if (P.periodic[0]) gx = ((gx % Lx) + Lx) % Lx;
+            else ok = false;
+        }
+        if (gy < 0 || gy >= Ly) {
+            if (P.periodic[1]) gy = ((gy % Ly) + Ly) % Ly;
+            else ok = false;
+        }
+        double vx = 0.0, vy = 0.0, vz = 0.0;
+        if (ok) {
+            const int64_t j = gx + static_cast<int64_t>(Lx) * gy;
+            vx = __ldg(mx + j);
+            vy = __ldg(mx + N + j);
+            vz = __ldg(mx + 2 * N + j);
+        }
+        sm[idx] = vx;
+        sm[G::NS + idx] = vy;
+        sm[2 * G::NS + idx] = vz;
+    }
+}
+
+// stencil + epilogue of one staged tile; returns the energy of its sites
+template <class S, int BYT, int RY, int PASS>
+__device__ __forceinline__ double compute_tile(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
+                                               const double* sm, int x0, int y0, int z) {
+    using G = TileGeom<S, BYT, RY>;
+    const int Lx = P.L[0], Ly = P.L[1];
+    const int64_t layer = static_cast<int64_t>(Lx) * Ly;
+    const int64_t N = layer * P.L[2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = x0 + tx;
+    Pre pre[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int y = y0 + ty * RY + r;
+        if (x < Lx && y < Ly) pre[r] = prefetch<PASS>(C, A, layer * z + x + static_cast<int64_t>(Lx) * y, N);
+    }
+    double bx[RY], by[RY], bz[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
+    const int base = (ty * RY) * G::PX + tx;
+    all_columns<S, BYT, RY>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
+    double e = 0.0;
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int y = y0 + ty * RY + r;
+        const int c = base + (r + G::R) * G::PX + G::RX;
+        const double3 m0 = make_double3(sm[c], sm[G::NS + c], sm[2 * G::NS + c]);
+        if (x < Lx && y < Ly) {
+            const int64_t i = layer * z + x + static_cast<int64_t>(Lx) * y;
+            double b0 = bx[r], b1 = by[r], b2 = bz[r];
+            if (P.has_onsite) {
+                const double* W = P.W0;
+                b0 = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, b0)));
+                b1 = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, b1)));
+                b2 = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, b2)));
+            }
+            FieldOut f;
+            f.Bzee = make_double3(0.0, 0.0, 0.0);
+            if (P.zee_on) {
+                double3 b;
+                if (A.bmap) b = make_double3(__ldg(A.bmap + i), __ldg(A.bmap + N + i), __ldg(A.bmap + 2 * N + i));
+                else b = make_double3(P.bext[0], P.bext[1], P.bext[2]);
+                f.Bzee = make_double3(P.zc * b.x, P.zc * b.y, P.zc * b.z);
+            }
+            f.B = make_double3(b0 + f.Bzee.x, b1 + f.Bzee.y, b2 + f.Bzee.z);
+            const double3 hd = A.Hd.h ? ld_dip(A.Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
+            e += epilogue<PASS>(C, A, i, N, m0, f, hd, pre[r]);
+        }
+    }
+    return e;
+}
+
+template <class S, int BYT, int RY, int PASS, int MINB>
+__global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant__ StencilParams P, const DynCoef C,
+                                                     const TiledArgs A) {
+    using G = TileGeom<S, BYT, RY>;
+    extern __shared__ __align__(128) double smem_t[];
+    const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY, z = blockIdx.z;
+    load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
+    __syncthreads();
+    const double e = compute_tile<S, BYT, RY, PASS>(P, C, A, smem_t, x0, y0, z);
+    if (A.R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// TMA + mbarrier helpers (single CTA, no cluster multicast)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait: false after ~limit polls (the caller records a timeout)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y, int z,
+                                            int c) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(c), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct TileList {
+    int ntx, nty, nz;
+    __device__ __forceinline__ int count() const { return ntx * nty * nz; }
+};
+
+template <class G>
+__device__ __forceinline__ bool tma_ok(const StencilParams& P, int x0, int y0) {
+    // a halo crossing a periodic edge needs wrap-around: plain loads
+    if (P.periodic[0] && (x0 - G::RX < 0 || x0 + G::TX + G::RX > P.L[0])) return false;
+    if (P.periodic[1] && (y0 - G::R < 0 || y0 + G::TY + G::R > P.L[1])) return false;
+    return true;
+}
+
+template <class S, int BYT, int RY, int PASS, int MINB>
+__global__ void __launch_bounds__(32 * BYT, MINB) k_tma(const __grid_constant__ CUtensorMap tmap,
+                                                   const __grid_constant__ StencilParams P, const DynCoef C,
+                                                   const TiledArgs A, const TileList T) {
+    using G = TileGeom<S, BYT, RY>;
+    extern __shared__ __align__(128) double smem_t[];
+    __shared__ __align__(8) uint64_t bar[2];
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int ntile = T.count();
+    auto origin = [&](int t, int& x0, int& y0, int& z) {
+        const int ix = t % T.ntx;
+        const int r = t / T.ntx;
+        x0 = ix * G::TX;
+        y0 = (r % T.nty) * G::TY;
+        z = r / T.nty;
+    };
+    auto issue = [&](int t, int b) {
+        int x0, y0, z;
+        origin(t, x0, y0, z);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[b], static_cast<uint32_t>(G::buf_bytes));
+        tma_load_4d(&tmap, &bar[b], smem_t + static_cast<size_t>(b) * G::buf_stride_d, x0 - G::RX, y0 - G::R, z, 0);
+    };
+    uint32_t phase[2] = {0u, 0u};
+    double e = 0.0;
+    bool failed = false;
+    int t = blockIdx.x;
+    bool cur_tma = false;
+    if (t < ntile) {
+        int x0, y0, z;
+        origin(t, x0, y0, z);
+        cur_tma = tma_ok<G>(P, x0, y0);
+        if (tid == 0 && cur_tma) issue(t, 0);
+    }
+    for (int it = 0; t < ntile; ++it, t += gridDim.x) {
+        const int b = it & 1;
+        const int tn = t + gridDim.x;
+        bool next_tma = false;
+        if (tn < ntile) {
+            int x1, y1, z1;
+            origin(tn, x1, y1, z1);
+            next_tma = tma_ok<G>(P, x1, y1);
+            if (tid == 0 && next_tma) issue(tn, b ^ 1);  // that buffer was released at the end of it-1
+        }
+        int x0, y0, z;
+        origin(t, x0, y0, z);
+        double* sm = smem_t + static_cast<size_t>(b) * G::buf_stride_d;
+        if (cur_tma) {
+            const bool ok = mbar_wait_bounded(&bar[b], phase[b], 1u << 22);
+            if (__syncthreads_or(!ok)) {  // the whole block agrees before leaving the loop
+                failed = true;
+                if (tid == 0 && A.status) atomicOr(A.status, 1);
+                break;
+            }
+            phase[b] ^= 1u;
+        } else {
+            load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, sm);
+            __syncthreads();
+        }
+        e += compute_tile<S, BYT, RY, PASS>(P, C, A, sm, x0, y0, z);
+        __syncthreads();
+        cur_tma = next_tma;
+    }
+    if (failed) {
+        // let copies still in flight land before the block exits (bounded)
+        for (int b = 0; b < 2; ++b) mbar_wait_bounded(&bar[b], phase[b], 1u << 16);
+        return;
+    }
+    if (A.R.out) {
+        double v[1] = {e};
+        grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
+    }
+}
+
+// ---------------------------------------------------------------------------
+template <class S, int BYT, int RY, int MINB>
+struct TiledLauncher {
+    using G = TileGeom<S, BYT, RY>;
+    using Shape = S;
+    static constexpr int BYT_ = BYT, RY_ = RY, MINB_ = MINB;
+    static dim3 grid(const StencilParams& P) {
+        return dim3((P.L[0] + G::TX - 1) / G::TX, (P.L[1] + G::TY - 1) / G::TY, P.L[2]);
+    }
+    template <int PASS>
+    static mj_status launch(const StencilParams& P, const DynCoef& C, const TiledArgs& A, cudaStream_t s) {
+        auto kern = k_tiled<S, BYT, RY, PASS, MINB>;
+        kern<<<grid(P), dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
+        return cuda_status(cudaGetLastError(), "k_tiled");
+    }
+    template <int PASS>
+    static mj_status launch_tma(const CUtensorMap& map, const StencilParams& P, const DynCoef& C, TiledArgs A,
+                                int nblocks, cudaStream_t s) {
+        auto kern = k_tma<S, BYT, RY, PASS, MINB>;
+        const size_t smem = 2 * G::buf_stride;
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            attr = true;
+        }
+        const dim3 g = grid(P);
+        TileList T{static_cast<int>(g.x), static_cast<int>(g.y), static_cast<int>(g.z)};
+        A.R.nblocks = nblocks;
+        kern<<<nblocks, dim3(32, BYT), smem, s>>>(map, P, C, A, T);
+        return cuda_status(cudaGetLastError(), "k_tma");
+    }
+    static int persistent_blocks(int sms) {
+        int per = 0;
+        auto kern = k_tma<S, BYT, RY, PASS_SIB1, MINB>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(2 * G::buf_stride));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * BYT, 2 * G::buf_stride);
+        return sms * (per > 0 ? per : 1);
+    }
+};
+
+template <class S, int BYT, int RY, int MINB>
+mj_status tiled_pass(int pass, const StencilParams& P, const DynCoef& C, const TiledArgs& A, const CUtensorMap* map,
+                     int nblocks, cudaStream_t s) {
+    using L = TiledLauncher<S, BYT, RY, MINB>;
+    if (map) {
+        switch (pass) {
+            case PASS_FIELD: return L::template launch_tma<PASS_FIELD>(*map, P, C, A, nblocks, s);
+            case PASS_EULER: return L::template launch_tma<PASS_EULER>(*map, P, C, A, nblocks, s);
+            case PASS_HEUN1: return L::template launch_tma<PASS_HEUN1>(*map, P, C, A, nblocks, s);
+            case PASS_HEUN2: return L::template launch_tma<PASS_HEUN2>(*map, P, C, A, nblocks, s);
+            case PASS_SIB1: return L::template launch_tma<PASS_SIB1>(*map, P, C, A, nblocks, s);
+            default: return L::template launch_tma<PASS_SIB2>(*map, P, C, A, nblocks, s);
+        }
+    }
+    switch (pass) {
+        case PASS_FIELD: return L::template launch<PASS_FIELD>(P, C, A, s);
+        case PASS_EULER: return L::template launch<PASS_EULER>(P, C, A, s);
+        case PASS_HEUN1: return L::template launch<PASS_HEUN1>(P, C, A, s);
+        case PASS_HEUN2: return L::template launch<PASS_HEUN2>(P, C, A, s);
+        case PASS_SIB1: return L::template launch<PASS_SIB1>(P, C, A, s);
+        default: return L::template launch<PASS_SIB2>(P, C, A, s);
+    }
+}
+
+// tile variants: (threads in y, sites per thread, min resident blocks per SM);
+// the tile heights are kTiledVariantTY (mj_internal.hpp)
+template <class S, class F>
+auto with_variant(int variant, F&& f) {
+    switch (variant) {
+        case 1: return f(TiledLauncher<S, 8, 4, 1>{});
+        case 2: return f(TiledLauncher<S, 8, 2, 1>{});
+        case 3: return f(TiledLauncher<S, 4, 4, 6>{});
+        case 4: return f(TiledLauncher<S, 8, 2, 4>{});
+        case 5: return f(TiledLauncher<S, 4, 2, 8>{});
+        default: return f(TiledLauncher<S, 4, 4, 1>{});
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tensor maps (driver entry point fetched through the runtime, no -lcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 4D map over the SoA spins: (x, y, z, component), box = tile + halo of one layer, 3 components
+bool make_map(CUtensorMap* map, const double* base, const StencilParams& P, int box_x, int box_y) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (P.L[0] & 1) != 0) return false;
+    const cuuint64_t dims[4] = {static_cast<cuuint64_t>(P.L[0]), static_cast<cuuint64_t>(P.L[1]),
+                                static_cast<cuuint64_t>(P.L[2]), 3};
+    const cuuint64_t layer = static_cast<cuuint64_t>(P.L[0]) * P.L[1];
+    const cuuint64_t strides[3] = {static_cast<cuuint64_t>(P.L[0]) * 8, layer * 8, layer * P.L[2] * 8};
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(box_x), static_cast<cuuint32_t>(box_y), 1, 3};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// All passes of one compile-time shape (one translation unit per shape keeps
+// the build parallel).  pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
+template <class S>
+mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
+                             double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s) {
+    TiledArgs A;
+    A.ms = ms;
+    A.mn = mn;
+    A.out = out;
+    A.aux = aux;
+    A.aux2 = aux2;
+    A.bmap = p->d_bmap;
+    A.Hd = Hd;
+    A.R.partials = p->d_partials;
+    A.R.counter = p->d_counter;
+    A.R.out = E_out;
+    A.R.nblocks = static_cast<int>(tiled_energy_blocks(p));
+    A.step = step;
+    A.status = p->d_status;
+    return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
+        using Launcher = decltype(L);
+        using G = typename Launcher::G;
+        if (p->use_tma) {
+            CUtensorMap map;
+            if (make_map(&map, ms, p->sp, G::PX, G::PY)) {
+                if (p->tma_blocks[p->tile_variant] <= 0)
+                    p->tma_blocks[p->tile_variant] = Launcher::persistent_blocks(p->num_sms);
+                const int nb = static_cast<int>(std::min<int64_t>(p->tma_blocks[p->tile_variant], tiled_energy_blocks(p)));
+                return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, &map,
+                                                                                           nb, s);
+            }
+        }
+        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, nullptr, 0, s);
+    });
+}
+
+}  // namespace
+}  // namespace mj

@@ -713,26 +713,106 @@ static double u53(uint32_t a, uint32_t b) {
     uint64_t k = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
     return (double)k * (1.0 / 9007199254740992.0);
 }
+/* Box-Muller with table-driven FP64 log and sin/cos of 2 pi u (the same
+ * evaluation as the product's, explicit fma, no contraction):
+ *   tab[0..511]   (sin, cos)(2 pi i/256), i = 0..255
+ *   tab[512..767] (1/F, ln F), F = (j + 96)/128, j = 0..127 (96..192 used)
+ *   ln u = e ln2 + ln F + ln(1 + r), m in [0.75, 1.5), F the nearest j/128,
+ *   r = (m - F)/F, |r| <= 1/192, series to r^7
+ *   sin/cos(2 pi i/256 + x), |x| < pi/128, Taylor to x^7 / x^8. */
+static double g_tab[768];
+static int g_tab_ready = 0;
+#define LN2_D 0.6931471805599453
+#define PI_OVER_128 0.02454369260617026
+
+static void noise_tables(void) {
+    if (g_tab_ready) return;
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int i = 0; i < 256; i++) {
+        long double a = two_pi * (long double)i / 256.0L;
+        g_tab[2 * i] = (double)sinl(a);
+        g_tab[2 * i + 1] = (double)cosl(a);
+    }
+    for (int j = 0; j < 128; j++) {
+        long double F = (long double)(j + 96) / 128.0L; /* used for j + 96 = 96..192 */
+        g_tab[512 + 2 * j] = (double)(1.0L / F);
+        g_tab[512 + 2 * j + 1] = (double)logl(F);
+    }
+    g_tab_ready = 1;
+}
+
+static double tab_log(double u) {
+    uint64_t b;
+    memcpy(&b, &u, 8);
+    int e = (int)((b >> 52) & 0x7ff) - 1023;
+    uint64_t mb = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+    double m;
+    memcpy(&m, &mb, 8);
+    if (m >= 1.5) { /* centre the mantissa in [0.75, 1.5): no cancellation against e ln2 near u = 1 */
+        m *= 0.5;
+        e += 1;
+    }
+    int j = (int)(m * 128.0 + 0.5); /* nearest F_j = j/128, j = 96..192 */
+    double F = (double)j * (1.0 / 128.0);
+    j -= 96;
+    double r = (m - F) * g_tab[512 + 2 * j];
+    double p = fma(r, 1.0 / 7.0, -1.0 / 6.0);
+    p = fma(p, r, 1.0 / 5.0);
+    p = fma(p, r, -0.25);
+    p = fma(p, r, 1.0 / 3.0);
+    p = fma(p, r, -0.5);
+    double l1p = fma(r * r, p, r);
+    return fma((double)e, LN2_D, g_tab[512 + 2 * j + 1] + l1p);
+}
+
+static void tab_sincos2pi(double u, double* s, double* c) {
+    double t = u * 256.0;
+    int i = (int)t;
+    double x = (t - (double)i) * PI_OVER_128;
+    double x2 = x * x;
+    double ps = fma(x2, -1.0 / 5040.0, 1.0 / 120.0);
+    ps = fma(ps, x2, -1.0 / 6.0);
+    double sx = fma(x * x2, ps, x);
+    double pc = fma(x2, 1.0 / 40320.0, -1.0 / 720.0);
+    pc = fma(pc, x2, 1.0 / 24.0);
+    pc = fma(pc, x2, -0.5);
+    double cm = x2 * pc;
+    double S = g_tab[2 * i], Cc = g_tab[2 * i + 1];
+    *s = S + fma(S, cm, Cc * sx);
+    *c = Cc + fma(Cc, cm, -(S * sx));
+}
+
 static void philox_site(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site, double out[3]) {
     uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
     uint32_t c[4] = {site, step, stream, 0u};
     philox4x32_10(c, k0, k1);
-    double r = sqrt(-2.0 * log(u53_open(c[0], c[1])));
-    double th = 6.283185307179586 * u53(c[2], c[3]);
-    out[0] = r * cos(th);
-    out[1] = r * sin(th);
     uint32_t d[4] = {site, step, stream, 1u};
     philox4x32_10(d, k0, k1);
-    double r2 = sqrt(-2.0 * log(u53_open(d[0], d[1])));
-    double th2 = 6.283185307179586 * u53(d[2], d[3]);
-    out[2] = r2 * cos(th2);
+    double r1 = sqrt(-2.0 * tab_log(u53_open(c[0], c[1])));
+    double r2 = sqrt(-2.0 * tab_log(u53_open(d[0], d[1])));
+    double s1, c1, s2, c2;
+    tab_sincos2pi(u53(c[2], c[3]), &s1, &c1);
+    tab_sincos2pi(u53(d[2], d[3]), &s2, &c2);
+    (void)s2;
+    out[0] = r1 * c1;
+    out[1] = r1 * s1;
+    out[2] = r2 * c2;
 }
+void orc_tab_eval(const double* u, int64_t n, double* lg, double* s, double* c) {
+    noise_tables();
+    for (int64_t i = 0; i < n; i++) {
+        lg[i] = u[i] > 0.0 ? tab_log(u[i]) : 0.0;
+        tab_sincos2pi(u[i] < 1.0 ? u[i] : 0.0, s + i, c + i);
+    }
+}
+
 void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
     philox4x32_10(c, key[0], key[1]);
     memcpy(out, c, sizeof c);
 }
 void orc_philox_normals(uint64_t seed, uint32_t step, uint32_t stream, int64_t site0, int64_t n, double* out) {
+    noise_tables();
     for (int64_t i = 0; i < n; i++) philox_site(seed, step, stream, (uint32_t)(site0 + i), out + 3 * i);
 }
 
@@ -802,6 +882,7 @@ static void sib_stage(const double* m, const double* p, const double* B, const d
 static void draw_noise(const orc_model* M, const orc_dyn* d, uint32_t step, double sigma, double* b) {
     int64_t N = M->nsite;
     if (d->noise == ORC_NOISE_PHILOX) {
+        noise_tables();
 #pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; i++) {
             double z[3];

@@ -87,6 +87,7 @@ def _lib():
     lib.orc_dipolar_explicit_field.argtypes = [P, P, P]
     lib.orc_philox_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, C.c_int64, P]
     lib.orc_philox4x32.argtypes = [P, P, P]
+    lib.orc_tab_eval.argtypes = [P, C.c_int64, P, P, P]
     lib.orc_run.argtypes = [P, C.POINTER(_Dyn), P, C.c_int, P]
     lib.orc_run.restype = C.c_int
     lib.orc_llg_torque.argtypes = [P, C.c_double, P, P, C.c_int64]
@@ -219,6 +220,14 @@ def philox4x32(ctr, key):
     out = np.zeros(4, np.uint32)
     lib.orc_philox4x32(c.ctypes.data, k.ctypes.data, out.ctypes.data)
     return [int(x) for x in out]
+
+
+def tab_eval(u):
+    """(log u, sin 2 pi u, cos 2 pi u) through the Box-Muller tables."""
+    u = np.ascontiguousarray(u, np.float64)
+    lg, s, c = np.empty_like(u), np.empty_like(u), np.empty_like(u)
+    lib.orc_tab_eval(u.ctypes.data, u.size, lg.ctypes.data, s.ctypes.data, c.ctypes.data)
+    return lg, s, c
 
 
 def llg_torque(B, alpha, m):

@@ -43,21 +43,40 @@ def test_zero_temperature_trajectory_1000_steps(integrator):
         assert drift < max(3 * drift_ref, 1e-13)
 
 
-@pytest.mark.parametrize("variant", [-1, 1, 2, 3])
-def test_tiled_variants_trajectory(variant):
+@pytest.mark.parametrize("variant,tma", [(-1, 0), (0, 0), (1, 1), (2, 1), (3, 1), (1, 0)])
+@pytest.mark.parametrize("L", [(40, 36), (96, 80)])
+def test_tiled_variants_trajectory(variant, tma, L):
     import matjes_b200 as mj
     from matjes_b200 import _abi
 
-    deck = mj.triangular((40, 36))
+    deck = mj.triangular(L)
     m0 = mj.reversed_disks(deck, 4, 5.0, 6)
     dyn = dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=5)
     ham = mj.Hamiltonian(deck)
     _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, variant))
+    _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, tma))
     m = m0.copy()
-    mj.SpinDynamics(ham, **dyn).run(m, 300)
+    mj.SpinDynamics(ham, **dyn).run(m, 200)
+    _abi.check(_abi.lib.mj_plan_check_status(ham.plan))
     mo = m0.copy()
-    O.Model(deck).run(mo, 300, **dyn)
+    O.Model(deck).run(mo, 200, **dyn)
     assert np.abs(m - mo).max() < 1e-9
+
+
+def test_open_boundary_tma_zero_fill():
+    """Open in-plane axes: the TMA boxes reaching past the edge read zeros."""
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    deck = mj.square_film((96, 64, 1), periodic=(0, 0, 0))
+    ham = mj.Hamiltonian(deck)
+    m = mj.random_sphere(deck.nsites, 4)
+    Bo = O.Model(deck).field(m)[0]
+    for tma in (0, 1):
+        _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, tma))
+        B = ham.get_eff_field(m)
+        assert np.abs(B - Bo).max() <= 1e-12 * np.abs(Bo).max()
+    _abi.check(_abi.lib.mj_plan_check_status(ham.plan))
 
 
 @pytest.mark.parametrize("integrator", ["sib", "heun", "euler"])

@@ -62,13 +62,18 @@ def test_field_energy_match_oracle(name):
     m = mj.random_sphere(deck.nsites, 11)
     Bo, eo = M.field(m)
     Eo = M.energy(m)
+    from matjes_b200 import _abi
+
     for v in variants(ham):
-        if ham.noffsets:
-            set_variant(ham, v)
-        B, e = ham.get_eff_field(m, with_energy=True)
-        assert site_rel_err(B, Bo) < TOL, v
-        assert scalar_rel_err(e, eo) < TOL, v
-        assert abs(ham.energy(m) - Eo) <= TOL * abs(Eo), v
+        for tma in ((0, 1) if v >= 0 else (0,)):
+            if ham.noffsets:
+                set_variant(ham, v)
+                _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, tma))
+            B, e = ham.get_eff_field(m, with_energy=True)
+            assert site_rel_err(B, Bo) < TOL, (v, tma)
+            assert scalar_rel_err(e, eo) < TOL, (v, tma)
+            assert abs(ham.energy(m) - Eo) <= TOL * abs(Eo), (v, tma)
+            _abi.check(_abi.lib.mj_plan_check_status(ham.plan))
 
 
 def test_shapes_are_matched():

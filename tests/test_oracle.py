@@ -147,6 +147,21 @@ def test_philox_known_answers():
         0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
 
 
+def test_box_muller_tables_are_accurate():
+    """The table-driven log and sin/cos(2 pi u) agree with libm to a few ulp."""
+    rng = np.random.default_rng(0)
+    u = np.concatenate([rng.random(200000), 2.0 ** -rng.uniform(0, 53, 20000), 1 - 2.0 ** -rng.uniform(1, 53, 20000),
+                        [1.0 - 2 ** -53, 2 ** -53, 0.5, 0.75]])
+    lg, s, c = O.tab_eval(u)
+    ref = np.log(u)
+    assert (np.abs(lg - ref) / np.spacing(np.abs(ref))).max() <= 2.0  # within 2 ulp of libm
+    assert O.tab_eval(np.array([1.0]))[0][0] == 0.0
+    uu = u[u < 1.0]
+    _, s, c = O.tab_eval(uu)
+    ang = 2 * np.pi * uu
+    assert np.abs(s - np.sin(ang)).max() < 8e-16 and np.abs(c - np.cos(ang)).max() < 8e-16
+
+
 def test_philox_normals_statistics():
     z = O.philox_normals(seed=7, step=3, stream=0, site0=0, n=200000).ravel()
     assert abs(z.mean()) < 5 * 1 / np.sqrt(z.size)
