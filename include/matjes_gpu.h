@@ -185,6 +185,23 @@ mj_status mj_field_dev(mj_plan* plan, const double* m_dev_soa, double* B_dev_soa
 /* hamiltonian%energy (hamiltonian_collection.f90:390-400): total energy in eV,
  * synchronous, written to *E_host. */
 mj_status mj_energy(mj_plan* plan, const mj_state* st, double* E_host);
+/* Total energy (as mj_energy) of device spins m_dev_soa (3N doubles, SoA) into
+ * *E_dev (one device double), on `stream`, without allocating anything.  No
+ * counterpart in the reference.  It is meant for callers that cannot call
+ * cudaMalloc when they evaluate the energy: a host code whose GPU memory is
+ * handed out by its own pool or capped by its job scheduler once set up, or a
+ * driver that must not allocate inside its time loop.  Its scratch (one
+ * partial sum per thread block and a ticket counter) is a fixed static device
+ * array of MJ_NOALLOC_MAX_BLOCKS doubles (512 KiB) that every GPU loading the
+ * library holds until the process exits; lattices needing more blocks than
+ * that (more than 2^24 sites) are rejected with MJ_ERR_ARG, and plans with the
+ * FFT dipolar term with MJ_ERR_UNSUPPORTED.  The first call on a device looks
+ * up the array's device address: make that first call before any stream
+ * capture.  All calls share the one array and each leaves its partial sums in
+ * it: calls that overlap on the GPU (different streams or host threads) race,
+ * so serialise them. */
+#define MJ_NOALLOC_MAX_BLOCKS 65536
+mj_status mj_energy_noalloc(const mj_plan* plan, const double* m_dev_soa, double* E_dev, void* stream);
 /* Host-array convenience form of get_eff_field (reference AoS layout); it
  * uploads m, evaluates, downloads B and e_site (may be NULL); synchronous. */
 mj_status mj_field_host(mj_plan* plan, const double* m_host_aos, double* B_host_aos, double* e_site_host);

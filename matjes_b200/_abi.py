@@ -129,6 +129,7 @@ SIGNATURES = {
     "mj_field_dev": (C.c_int32, [P, P, P, P, P]),
     "mj_energy": (C.c_int32, [P, P, DP]),
     "mj_field_host": (C.c_int32, [P, P, P, P]),
+    "mj_energy_noalloc": (C.c_int32, [P, P, P, P]),
     "mj_step": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, P, P]),
     "mj_step_dev": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, P, P]),
     "mj_step_host": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, P]),

@@ -16,6 +16,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <string>
+
 #include "mj_device.cuh"
 #include "mj_internal.hpp"
 
@@ -594,4 +597,78 @@ mj_status soa_to_aos(const double* so, double* a, int64_t n, cudaStream_t s) {
     return cuda_status(cudaGetLastError(), "soa_to_aos");
 }
 
+// ---------------------------------------------------------------------------
+// Energy with no allocation (mj_energy_noalloc).  The reduction scratch is this
+// fixed array: MJ_NOALLOC_MAX_BLOCKS per-block partial sums, then the ticket
+// counter in the first 4 bytes of the slot after them.  Every GPU that loads
+// the library holds it until exit; all calls on a device share it.
+static __device__ __align__(256) double g_noalloc_scratch[MJ_NOALLOC_MAX_BLOCKS + 32];
+
+namespace {
+
+__global__ void k_noalloc_arm(unsigned int* counter) {
+    if (threadIdx.x == 0) *counter = 0u;  // a previous call may have stopped before re-arming it
+}
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once per
+// device (host code cannot use the symbol's name as a device pointer).
+mj_status noalloc_scratch(double** out) {
+    int dev = -1;
+    mj_status st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != MJ_OK) return st;
+    if (dev < 0 || dev >= 64) return set_error(MJ_ERR_ARG, "device index out of range for the no-allocation scratch");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if ((st = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-allocation scratch)")) !=
+            MJ_OK)
+            return st;
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return MJ_OK;
+}
+
+}  // namespace
+
 }  // namespace mj
+
+extern "C" mj_status mj_energy_noalloc(const mj_plan* plan, const double* m, double* E, void* stream) {
+    using namespace mj;
+    if (!plan || !m || !E) return set_error(MJ_ERR_ARG, "null argument");
+    if (plan->dip_on)
+        return set_error(MJ_ERR_UNSUPPORTED, "the FFT dipolar term needs the plan's FFT buffers; use mj_energy");
+    mj_status st = cuda_status(cudaSetDevice(plan->device), "cudaSetDevice");
+    if (st != MJ_OK) return st;
+    const int64_t nblocks = energy_blocks(plan);
+    if (nblocks > MJ_NOALLOC_MAX_BLOCKS)
+        return set_error(MJ_ERR_ARG, "lattice needs " + std::to_string(nblocks) +
+                                         " thread blocks; the no-allocation scratch holds MJ_NOALLOC_MAX_BLOCKS = " +
+                                         std::to_string(MJ_NOALLOC_MAX_BLOCKS) + " (at most 2^24 sites)");
+    double* scratch = nullptr;
+    if ((st = noalloc_scratch(&scratch)) != MJ_OK) return st;
+    unsigned int* counter = reinterpret_cast<unsigned int*>(scratch + MJ_NOALLOC_MAX_BLOCKS);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_noalloc_arm<<<1, 32, 0, s>>>(counter);
+    if ((st = cuda_status(cudaGetLastError(), "k_noalloc_arm")) != MJ_OK) return st;
+    Reduce R;
+    R.partials = scratch;
+    R.counter = counter;
+    R.out = E;
+    R.nblocks = static_cast<int>(nblocks);
+    DipView none;
+    none.h = nullptr;
+    none.nk = 0;
+    none.px = none.py = 0;
+    if (plan->is_stencil) {
+        const Launch<StencilField> L = stencil_launch(plan);
+        k_field<StencilField><<<L.grid, L.block, 0, s>>>(L.fp, m, none, nullptr, nullptr, R);
+    } else {
+        const Launch<EllField> L = ell_launch(plan);
+        k_field<EllField><<<L.grid, L.block, 0, s>>>(L.fp, m, none, nullptr, nullptr, R);
+    }
+    return cuda_status(cudaGetLastError(), "k_field (no allocation)");
+}
