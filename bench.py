@@ -195,6 +195,89 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------------
+def run_batch(dev: int, steps: int = 200) -> dict:
+    """The 256-replica workload (square lattices of sides 32..256, about 5.1M
+    sites, Bz ~ U(0,2) T, T geometric 1..50 K, SIB alpha = 0.5, Philox, a
+    parallel-tempering round every 100 steps): one batch advanced by CUDA
+    graphs of 100 steps against the same replicas run one after another
+    through their own plans (mj_step_dev, and mj_graph_run of 100 steps)."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import square_film, workload
+
+    w = workload("square_replicas256")
+    d = w["dyn"]
+    sizes, B, T = w["sizes"], w["B_ext"], w["temperature"]
+    spg = int(d["swap_every"])
+    nrg = max(1, steps // spg)
+    steps = spg * nrg
+    b = mj.ReplicaBatch(w["cell"], sizes, B, T, device=dev)
+    b.upload(w["m0"])
+    N = b.N
+    p = b.params(timestep=d["timestep"], alpha=d["alpha"], noise="philox", seed=d["seed"])
+    (v, bps), table = b.autotune(p, steps=5)
+    b.graph_run(p, spg, 1, swap_every=spg)  # capture + one warm replay
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    b.graph_run(p, spg, nrg, swap_every=spg)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1)
+    Tn, acc = b.temperatures()
+    b.close()
+
+    # the same replicas, one plan each, run one after another
+    plans = []
+    for r in range(len(sizes)):
+        deck = square_film((int(sizes[r][0]), int(sizes[r][1]), 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=B[r, 2])
+        ham = mj.Hamiltonian(deck, device=dev)
+        sd = mj.SpinDynamics(ham, integrator="sib", timestep=d["timestep"], alpha=d["alpha"], temperature=T[r],
+                             noise="philox", seed=d["seed"], stream_id=r)
+        m = torch.tensor(w["m0"][int(np.sum(sizes[:r, 0].astype(np.int64) * sizes[:r, 1]))
+                                 :int(np.sum(sizes[:r + 1, 0].astype(np.int64) * sizes[:r + 1, 1]))].T.copy(),
+                         device=f"cuda:{dev}")
+        st = mj.SpinState(ham)
+        st.device_tensor().copy_(m)
+        plans.append((ham, sd, m, st))
+    lib = _abi.lib
+
+    def sequential(nsteps, graphs):
+        for ham, sd, m, st in plans:
+            if graphs:
+                _abi.check(lib.mj_graph_run(ham.plan, st.handle, _abi.C.byref(sd.p), spg, nsteps // spg, None, None))
+            else:
+                _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(sd.p), nsteps, None, None))
+            sd.p.step0 += nsteps
+
+    res = {}
+    for graphs in (False, True):
+        sequential(spg, graphs)  # warm-up (and graph capture)
+        torch.cuda.synchronize()
+        e0.record()
+        sequential(steps, graphs)
+        e1.record()
+        torch.cuda.synchronize()
+        res[graphs] = e0.elapsed_time(e1)
+    su_batch = N * steps / (ms_batch / 1e3)
+    return {
+        "workload": "square_replicas256", "replicas": int(len(sizes)), "sites": int(N), "steps": steps,
+        "swap_every": spg, "tile_variant": int(v), "blocks_per_sm": int(bps),
+        "value": su_batch, "unit": UNIT, "ms_per_step": ms_batch / steps,
+        "achieved_gbs": 120.0 * N * steps / (ms_batch / 1e3) / 1e9,
+        "sequential_plain": {"value": N * steps / (res[False] / 1e3), "ms_per_step": res[False] / steps,
+                             "path": "256 plans, mj_step_dev one replica after another"},
+        "sequential_graphs": {"value": N * steps / (res[True] / 1e3), "ms_per_step": res[True] / steps,
+                              "path": "256 plans, mj_graph_run (100-step graphs) one replica after another"},
+        "speedup_vs_sequential_plain": res[False] / ms_batch,
+        "speedup_vs_sequential_graphs": res[True] / ms_batch,
+        "swaps_accepted": int(acc.sum()),
+        "autotune_ms_per_step": np.round(table, 5).tolist(),
+    }
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -303,6 +386,7 @@ def run_gpu(args, rank, world):
     ach = kernels[dom]["achieved_gbs"]
     tr = ncu_traffic(dom, args.workload)
     cpu = cpu_oracle_rate(args.workload) if (world == 1 and not args.no_cpu_baseline) else None
+    batch = run_batch(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -327,6 +411,7 @@ def run_gpu(args, rank, world):
                 "path": "mj_state_upload (pinned AoS) + mj_step + mj_state_download + energy read"},
         "gpu_launches": 2 * K,
         "cpu_baseline": cpu,
+        "batch": batch,
     }
     print(json.dumps(line), flush=True)
 
@@ -339,6 +424,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-replica batch measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

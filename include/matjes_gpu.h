@@ -240,6 +240,60 @@ mj_status mj_measure_temperature(mj_plan* plan, const mj_state* st, double* T_ho
 mj_status mj_philox_normals(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n,
                             double* out_dev_soa, void* stream);
 
+/* ---- batched replicas ---------------------------------------------------- */
+/* Many independent 2D replicas of one single-atom Hamiltonian (the cell, shells
+ * and couplings of `cell`/`ham`), each with its own size L[2r], L[2r+1], applied
+ * field B_ext[3r..3r+2] (T) and temperature[r] (K), advanced by SIB in one
+ * persistent launch per stage.  In the reference every such replica is a
+ * separate run of the dynamics (dynamics/spindynamics.f90:260-323), one per MPI
+ * rank group for parallel tempering (paratemp-MC/parallel_tempering.f90:24-217).
+ * Spins are packed SoA: x[Ntot] | y[Ntot] | z[Ntot], replica r at sites
+ * [off_r, off_r+1) of mj_batch_nsites.  Replica r draws Philox noise on stream
+ * p->stream_id + r with its local site index, so it reproduces a plan of its
+ * own size run with stream_id + r.  The dipolar term is not batched. */
+typedef struct mj_batch mj_batch;
+mj_status mj_batch_create(const mj_lattice_desc* cell, const mj_hamiltonian_desc* ham, int32_t nrep,
+                          const int32_t* L, const double* B_ext, const double* temperature,
+                          int32_t device, mj_batch** out);
+mj_status mj_batch_destroy(mj_batch* b);
+/* Ntot and, if offsets != NULL, nrep+1 packed offsets. */
+mj_status mj_batch_nsites(const mj_batch* b, int64_t* total, int64_t* offsets);
+mj_status mj_batch_device_ptr(const mj_batch* b, double** m_dev_soa);
+/* Host AoS (3, Ntot) in replica order (asynchronous upload, synchronous download). */
+mj_status mj_batch_upload(mj_batch* b, const double* m_host_aos, void* stream);
+mj_status mj_batch_download(const mj_batch* b, double* m_host_aos, void* stream);
+/* nsteps SIB steps of every replica (p->integrator must be MJ_SIB, noise OFF or
+ * PHILOX, p->temperature is ignored: each replica has its own).  With
+ * swap_every > 0, after every step s with (s+1) % swap_every == 0 the replica
+ * energies are evaluated and one parallel-tempering round runs on the ladder of
+ * temperatures: paratemp-MC/paratemp.f90:47-103 (reorder_temperature: pairs
+ * (l, l+1) from l = round % 2 in steps of 2) and :105-119 (accept: delta =
+ * (1/kT_{l+1} - 1/kT_l)(E_{l+1} - E_l), accepted if > 0, else if
+ * exp(max(delta,-200)) > u, u a Philox uniform); only neighbours of equal size
+ * are compared; an accepted swap exchanges the two replicas' temperatures.
+ * E_dev (device, nrep doubles, may be NULL) receives the energies after the
+ * last step. */
+mj_status mj_batch_step(mj_batch* b, const mj_dyn_params* p, int32_t nsteps, int32_t swap_every,
+                        double* E_dev, void* stream);
+/* The same as a CUDA graph of steps_per_graph steps (a multiple of swap_every,
+ * p->step0 too) replayed nreplay times; steps advance p->step0 by
+ * steps_per_graph per replay. */
+mj_status mj_batch_graph_run(mj_batch* b, const mj_dyn_params* p, int32_t steps_per_graph, int32_t nreplay,
+                             int32_t swap_every, double* E_dev, void* stream);
+/* Energies (host, nrep) of the current state; synchronous. */
+mj_status mj_batch_energies(mj_batch* b, double* E_host);
+/* Current temperature of every replica (K) and, if accepted != NULL, the
+ * accepted-swap count of every ladder pair (l, l+1) (reference Nsuccess). */
+mj_status mj_batch_temperatures(const mj_batch* b, double* T_host, int32_t* accepted);
+/* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
+ * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
+mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);
+/* Times `steps` steps of every (variant, blocks per SM in {2,4,8,16,32}) on the
+ * current state (restored afterwards), keeps the fastest; ms_table (15 doubles,
+ * may be NULL) gets ms per step in variant-major order. */
+mj_status mj_batch_autotune(mj_batch* b, const mj_dyn_params* p, int32_t steps, int32_t* best_variant,
+                            int32_t* best_blocks_per_sm, double* ms_table);
+
 #ifdef __cplusplus
 }
 #endif

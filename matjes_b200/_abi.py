@@ -138,6 +138,20 @@ SIGNATURES = {
     "mj_profile_read": (C.c_int32, [P, C.c_int32, P, P, P, C.POINTER(C.c_int32)]),
     "mj_measure_temperature": (C.c_int32, [P, P, DP]),
     "mj_philox_normals": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, P, P]),
+    "mj_batch_create": (C.c_int32, [C.POINTER(LatticeDesc), C.POINTER(HamiltonianDesc), C.c_int32, P, P, P,
+                                    C.c_int32, C.POINTER(P)]),
+    "mj_batch_destroy": (C.c_int32, [P]),
+    "mj_batch_nsites": (C.c_int32, [P, C.POINTER(C.c_int64), P]),
+    "mj_batch_device_ptr": (C.c_int32, [P, C.POINTER(P)]),
+    "mj_batch_upload": (C.c_int32, [P, P, P]),
+    "mj_batch_download": (C.c_int32, [P, P, P]),
+    "mj_batch_step": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.c_int32, P, P]),
+    "mj_batch_graph_run": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.c_int32, C.c_int32, P, P]),
+    "mj_batch_energies": (C.c_int32, [P, P]),
+    "mj_batch_temperatures": (C.c_int32, [P, P, P]),
+    "mj_batch_set_config": (C.c_int32, [P, C.c_int32, C.c_int32]),
+    "mj_batch_autotune": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
+                                      C.POINTER(C.c_int32), P]),
 }
 
 

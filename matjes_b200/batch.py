@@ -1,0 +1,143 @@
+"""Batched replicas with parallel tempering over the C ABI (mj_batch_*).
+
+A ``ReplicaBatch`` holds many independent 2D lattices of one single-atom
+Hamiltonian (the cell, shells and couplings of a ``Deck``), each with its own
+size, applied field and temperature, advanced together by SIB.  In the
+reference every replica is a separate run of dynamics/spindynamics.f90:260-323
+(one per MPI rank group in paratemp-MC/parallel_tempering.f90:24-217); the
+temperature swaps follow paratemp-MC/paratemp.f90:47-119.
+
+Host arrays use the reference AoS layout (Ntot, 3) in replica order; the
+device state is SoA (3, Ntot), replica r at columns offsets[r]:offsets[r+1].
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, lib, ptr
+from .deck import Deck
+
+N_BATCH_VARIANTS = 3
+BATCH_BLOCKS_PER_SM = (2, 4, 8, 16, 32)
+
+
+class ReplicaBatch:
+    def __init__(self, cell: Deck, sizes: Sequence[Sequence[int]], B_ext: np.ndarray, temperature: Sequence[float],
+                 device: int = 0):
+        """cell: the deck whose cell and couplings every replica shares (its L and
+        B_ext are ignored); sizes: (nrep, 2) lattice sides; B_ext: (nrep, 3) T;
+        temperature: (nrep,) K."""
+        self.cell = cell
+        self.device = device
+        L = np.ascontiguousarray(sizes, np.int32).reshape(-1, 2)
+        self.nrep = L.shape[0]
+        B = np.ascontiguousarray(B_ext, np.float64).reshape(self.nrep, 3)
+        T = np.ascontiguousarray(temperature, np.float64).reshape(self.nrep)
+        lat, h, keep = cell.c_structs()
+        b = C.c_void_p()
+        check(lib.mj_batch_create(C.byref(lat), C.byref(h), self.nrep, ptr(L), ptr(B), ptr(T), device, C.byref(b)))
+        self._keep = keep
+        self.handle = b
+        self.sizes = L.copy()
+        self.B_ext = B.copy()
+        self.T0 = T.copy()
+        tot = C.c_int64()
+        off = np.zeros(self.nrep + 1, np.int64)
+        check(lib.mj_batch_nsites(b, C.byref(tot), ptr(off)))
+        self.N = int(tot.value)
+        self.offsets = off
+
+    # -- state ------------------------------------------------------------
+    def upload(self, m: np.ndarray) -> None:
+        mh = np.ascontiguousarray(m, np.float64)
+        assert mh.shape == (self.N, 3)
+        check(lib.mj_batch_upload(self.handle, ptr(mh), None))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.N, 3))
+        check(lib.mj_batch_download(self.handle, ptr(out), None))
+        return out
+
+    def replica(self, m: np.ndarray, r: int) -> np.ndarray:
+        """Rows of replica r in a (Ntot, 3) array."""
+        return m[self.offsets[r]:self.offsets[r + 1]]
+
+    def device_tensor(self):
+        """torch view (3, Ntot) of the batch's device spins (no copy)."""
+        from .hamiltonian import _wrap_device
+
+        p = C.c_void_p()
+        check(lib.mj_batch_device_ptr(self.handle, C.byref(p)))
+        return _wrap_device(p.value, (3, self.N), self.device)
+
+    # -- dynamics ---------------------------------------------------------
+    @staticmethod
+    def params(timestep: float = 0.1, alpha: float = 0.5, noise: str = "philox", seed: int = 0, stream_id: int = 0,
+               step0: int = 0) -> _abi.DynParams:
+        p = _abi.DynParams()
+        p.integrator = _abi.MJ_SIB
+        p.timestep = float(timestep)
+        p.alpha = float(alpha)
+        p.noise = _abi.NOISES[noise]
+        p.seed = int(seed)
+        p.stream_id = int(stream_id)
+        p.step0 = int(step0)
+        return p
+
+    def step(self, p: _abi.DynParams, nsteps: int, swap_every: int = 0, energies: bool = False, stream=None):
+        """nsteps SIB steps (p.step0 advances); a parallel-tempering round after
+        every step s with (s+1) % swap_every == 0.  Returns the replica energies
+        after the last step (a device tensor) when asked."""
+        E = None
+        if energies:
+            import torch
+
+            E = torch.empty(self.nrep, dtype=torch.float64, device=f"cuda:{self.device}")
+        check(lib.mj_batch_step(self.handle, C.byref(p), int(nsteps), int(swap_every), ptr(E), stream))
+        p.step0 += int(nsteps)
+        return E
+
+    def graph_run(self, p: _abi.DynParams, steps_per_graph: int, nreplay: int, swap_every: int = 0, stream=None):
+        """The same steps as one CUDA graph of steps_per_graph steps replayed nreplay times."""
+        check(lib.mj_batch_graph_run(self.handle, C.byref(p), int(steps_per_graph), int(nreplay), int(swap_every),
+                                     None, stream))
+        p.step0 += int(steps_per_graph) * int(nreplay)
+
+    def energies(self) -> np.ndarray:
+        out = np.empty(self.nrep)
+        check(lib.mj_batch_energies(self.handle, ptr(out)))
+        return out
+
+    def temperatures(self):
+        """(temperature of every replica in K, accepted swaps of every ladder pair)."""
+        T = np.empty(self.nrep)
+        acc = np.zeros(self.nrep, np.int32)
+        check(lib.mj_batch_temperatures(self.handle, ptr(T), ptr(acc)))
+        return T, acc
+
+    def set_config(self, variant: int, blocks_per_sm: int) -> None:
+        check(lib.mj_batch_set_config(self.handle, int(variant), int(blocks_per_sm)))
+
+    def autotune(self, p: _abi.DynParams, steps: int = 5):
+        """Pick the fastest (tile variant, blocks per SM); returns it and the ms/step table."""
+        v = C.c_int32()
+        bps = C.c_int32()
+        table = np.full(N_BATCH_VARIANTS * len(BATCH_BLOCKS_PER_SM), np.nan)
+        check(lib.mj_batch_autotune(self.handle, C.byref(p), int(steps), C.byref(v), C.byref(bps), ptr(table)))
+        return (int(v.value), int(bps.value)), table.reshape(N_BATCH_VARIANTS, len(BATCH_BLOCKS_PER_SM))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.mj_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -374,6 +374,10 @@ mj_status step_sequence(mj_plan* p, double* m, const DynCoef& c, int energy_mode
 
 }  // namespace
 
+bool stencil_from_blocks(const std::vector<Block>& blocks, const std::vector<double>& onsite, StencilParams& sp) {
+    return make_stencil(blocks, onsite, sp);
+}
+
 void match_shape(StencilParams& sp) {
     sp.shape = kShapeGeneric;
     if (try_shape<ShapeTri3>(sp)) return;

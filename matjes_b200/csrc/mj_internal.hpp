@@ -197,6 +197,8 @@ MJ_TILED_SHAPE_DECL(launch_tiled_tri3)
 int64_t tiled_energy_blocks(const mj_plan* p);
 // match a single-atom stencil to a compile-time shape and reorder its tensors (mj_abi.cpp)
 void match_shape(mj::StencilParams& sp);
+// single-atom stencil tensors W_o from coupling blocks; false past kMaxOff offsets (mj_abi.cpp)
+bool stencil_from_blocks(const std::vector<Block>& blocks, const std::vector<double>& onsite, StencilParams& sp);
 
 // dipolar (mj_dipolar.cu)
 mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t s);

@@ -211,4 +211,22 @@ def workload(name: str, scale: int = 1) -> dict:
         return dict(deck=deck, m0=random_sphere(deck.nsites, 4),
                     dyn=dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=5.0, noise="philox", seed=4,
                              steps=2000))
+    if name == "square_replicas256":
+        # 256 square replicas, sides drawn from {32..256} (seed 2), Bz ~ U(0, 2) T,
+        # temperatures geometric 1 -> 50 K; `scale` divides the sides and the count
+        rng = np.random.default_rng(2)
+        nrep = max(4, 256 // scale)
+        sides = np.array([32, 48, 64, 96, 128, 192, 256])
+        Ls = rng.choice(sides, size=256)[:nrep] // scale
+        Ls = np.maximum(Ls, 8)
+        Bz = rng.uniform(0.0, 2.0, size=256)[:nrep]
+        T = 1.0 * (50.0 / 1.0) ** (np.arange(nrep) / max(1, nrep - 1))
+        cell = square_film((8, 8, 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.0)
+        sizes = np.stack([Ls, Ls], axis=1).astype(np.int32)
+        B = np.zeros((nrep, 3))
+        B[:, 2] = Bz
+        ntot = int((Ls.astype(np.int64) ** 2).sum())
+        return dict(cell=cell, sizes=sizes, B_ext=B, temperature=T, m0=random_sphere(ntot, 2),
+                    dyn=dict(integrator="sib", timestep=0.1, alpha=0.5, noise="philox", seed=2, steps=5000,
+                             swap_every=100))
     raise KeyError(name)

@@ -236,3 +236,35 @@ def llg_torque(B, alpha, m):
     D = np.empty_like(m)
     lib.orc_llg_torque(_p(B), alpha, _p(m), _p(D), m.shape[0])
     return D
+
+
+def pt_uniform(seed: int, l: int, round_idx: int) -> float:
+    """The uniform of the swap test of ladder pair (l, l+1) in round round_idx:
+    Philox4x32-10 of counter (l, round, 0x50545357, 2) under key `seed`, the
+    53-bit uniform [0, 1) of its first two words."""
+    w = philox4x32([l & 0xFFFFFFFF, round_idx & 0xFFFFFFFF, 0x50545357, 2],
+                   [seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF])
+    k = ((w[0] >> 5) << 26) | (w[1] >> 6)
+    return k * (1.0 / 9007199254740992.0)
+
+
+def pt_round(kT_slot, image, E, sizes, round_idx: int, seed: int):
+    """One parallel-tempering round (paratemp-MC/paratemp.f90:84-99, accept
+    :105-119): ladder pairs (l, l+1) from l = round % 2 in steps of 2, replicas
+    of equal size only; delta = (1/kT_{l+1} - 1/kT_l)(E_{l+1} - E_l), accepted
+    if delta > 0 or exp(max(delta, -200)) > u.  Returns the new slot -> replica
+    map and the accepted pairs."""
+    image = list(image)
+    accepted = []
+    for l in range(round_idx % 2, len(image) - 1, 2):
+        a, b = image[l], image[l + 1]
+        if tuple(sizes[a]) != tuple(sizes[b]):
+            continue
+        delta = (1.0 / kT_slot[l + 1] - 1.0 / kT_slot[l]) * (E[b] - E[a])
+        acc = delta > 0.0
+        if not acc:
+            acc = np.exp(max(delta, -200.0)) > pt_uniform(seed, l, round_idx)
+        if acc:
+            image[l], image[l + 1] = b, a
+            accepted.append(l)
+    return image, accepted

@@ -186,3 +186,33 @@ def test_thermal_noise_sigma_matches_reference_formula():
     DT = O.llg_torque(b[None], alpha, np.array([[1.0, 0.0, 0.0]]))[0]
     t = np.array([1.0, 0.0, 0.0]) + DT * dt / O.HBAR
     assert np.allclose(m[0], t / np.linalg.norm(t), atol=1e-16)
+
+
+def test_parallel_tempering_rule_known_answers():
+    """paratemp-MC/paratemp.f90:84-119: equal energies always swap (delta = 0,
+    exp(0) = 1 > u), delta > 0 always swaps, unequal sizes never swap, and the
+    starting pair alternates with the round parity."""
+    kT = [1.0, 2.0, 3.0, 4.0, 5.0]
+    sizes = [(8, 8)] * 5
+    E = [0.0] * 5
+    img, acc = O.pt_round(kT, range(5), E, sizes, 0, seed=1)
+    assert img == [1, 0, 3, 2, 4] and acc == [0, 2]
+    img, acc = O.pt_round(kT, range(5), E, sizes, 1, seed=1)
+    assert img == [0, 2, 1, 4, 3] and acc == [1, 3]
+    # colder slot holds the higher energy: (1/kT2 - 1/kT1) < 0, (E2 - E1) < 0, delta > 0
+    img, acc = O.pt_round(kT, range(5), [5.0, 1.0, 5.0, 1.0, 0.0], sizes, 0, seed=1)
+    assert acc == [0, 2]
+    img, acc = O.pt_round(kT, range(5), E, [(8, 8), (9, 8), (8, 8), (8, 8), (8, 9)], 1, seed=1)
+    assert acc == [] and img == [0, 1, 2, 3, 4]
+
+
+def test_parallel_tempering_acceptance_rate():
+    """For delta = -1 the swap is accepted with probability e^-1."""
+    kT = [1.0, 0.5]          # 1/kT2 - 1/kT1 = 1
+    E = [0.0, -1.0]          # E2 - E1 = -1  ->  delta = -1
+    n = 20000
+    hits = sum(len(O.pt_round(kT, [0, 1], E, [(4, 4)] * 2, 2 * r, seed=9)[1]) for r in range(n))
+    p = np.exp(-1.0)
+    assert abs(hits / n - p) < 4 * np.sqrt(p * (1 - p) / n)
+    u = [O.pt_uniform(9, 0, r) for r in range(1000)]
+    assert 0.0 <= min(u) and max(u) < 1.0 and len(set(u)) == 1000
