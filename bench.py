@@ -278,6 +278,70 @@ def run_batch(dev: int, steps: int = 200) -> dict:
     }
 
 
+def run_adjoint(dev: int, reps: int = 3) -> dict:
+    """The 256 x 256 adjoint workload (square lattice, J, D, K + per-site Bz,
+    SIB alpha = 0.2, 500 steps, checkpoints every 50): one forward + backward
+    sweep (gradients for m0, the three coupling terms and the per-site field)
+    against the plain 500-step forward through mj_step_dev."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import workload
+
+    w = workload("square256_adjoint")
+    deck, d = w["deck"], w["dyn"]
+    N = deck.nsites
+    ham = mj.Hamiltonian(deck, device=dev)
+    b = torch.tensor(w["bfield"].T.copy(), device=f"cuda:{dev}")
+    m0 = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
+    target = torch.tensor(mj.random_sphere(N, 7).T.copy(), device=f"cuda:{dev}")
+    traj = mj.SIBTrajectory(ham, d["steps"], checkpoint_every=d["checkpoint_every"], timestep=d["timestep"],
+                            alpha=d["alpha"])
+    traj.set_bfield(b)
+    sd = mj.SpinDynamics(ham, integrator="sib", timestep=d["timestep"], alpha=d["alpha"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def plain():
+        m = m0.clone()
+        sd.run(m, d["steps"], step0=0)
+        return m
+
+    st = mj.SpinState(ham)
+
+    def plain_graph():
+        st.device_tensor().copy_(m0)
+        sd.p.step0 = 0
+        _abi.check(_abi.lib.mj_graph_run(ham.plan, st.handle, _abi.C.byref(sd.p), d["steps"], 1, None, None))
+
+    def adjoint():
+        mT = traj.forward(m0)
+        g = 2.0 * (mT - target) / N
+        return traj.backward(g)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    f = timed(plain)
+    fg = timed(plain_graph)
+    a = timed(adjoint)
+    return {"workload": "square256_adjoint", "sites": N, "steps": d["steps"],
+            "checkpoint_every": d["checkpoint_every"], "forward_ms": f, "forward_graph_ms": fg,
+            "forward_backward_ms": a, "cost_ratio": a / f, "cost_ratio_vs_graph_forward": a / fg,
+            "gradients": "m0 (3N), J, D, K, per-site B (3N)",
+            "launches_per_step": {"forward": 2, "adjoint": 6},
+            "adjoint_path": "forward and backward sweeps replayed as CUDA graphs"}
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -387,6 +451,7 @@ def run_gpu(args, rank, world):
     tr = ncu_traffic(dom, args.workload)
     cpu = cpu_oracle_rate(args.workload) if (world == 1 and not args.no_cpu_baseline) else None
     batch = run_batch(dev) if (world == 1 and not args.no_batch) else None
+    adjoint = run_adjoint(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -412,6 +477,7 @@ def run_gpu(args, rank, world):
         "gpu_launches": 2 * K,
         "cpu_baseline": cpu,
         "batch": batch,
+        "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 
@@ -424,7 +490,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the 256-replica batch measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch and adjoint measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -240,6 +240,35 @@ mj_status mj_measure_temperature(mj_plan* plan, const mj_state* st, double* T_ho
 mj_status mj_philox_normals(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n,
                             double* out_dev_soa, void* stream);
 
+/* ---- reverse mode (adjoint) ---------------------------------------------- */
+/* The reference has no derivative code: these entries have no counterpart in
+ * it.  They differentiate its forward map, the SIB step of the dynamics
+ * (dynamics/spindynamics.f90:282-313 stage loop) with the effective field of
+ * Hamiltonian_type/hamiltonian_collection.f90:433-454, on single-atom stencil
+ * plans without the dipolar term.  The differentiable coupling terms are the
+ * J, D and K terms of the plan's mj_hamiltonian_desc in that order (nJ + nD + nK
+ * values, at most 8); the field is linear in their values. */
+mj_status mj_plan_nterms(const mj_plan* plan, int32_t* nterms);
+/* Re-set the term values (the `value` fields, in the same order) of a stencil plan. */
+mj_status mj_plan_set_terms(mj_plan* plan, const double* values);
+/* VJP of get_eff_field at m (device SoA) for the cotangent v: g_m = (dB/dm)^T v,
+ * g_terms[t] = v . dB/dvalue_t (device, nterms doubles), g_b = (dB/db)^T v per
+ * site (device SoA, the applied-field map); each output may be NULL. */
+mj_status mj_field_vjp(mj_plan* plan, const double* m_dev_soa, const double* v_dev_soa, double* g_m_dev_soa,
+                       double* g_terms_dev, double* g_b_dev_soa, void* stream);
+/* A reverse-mode trajectory of `nsteps` SIB steps, checkpointed every
+ * `checkpoint_every` steps (each segment is recomputed in the backward sweep). */
+typedef struct mj_adjoint mj_adjoint;
+mj_status mj_adjoint_create(mj_plan* plan, int32_t nsteps, int32_t checkpoint_every, mj_adjoint** out);
+mj_status mj_adjoint_destroy(mj_adjoint* a);
+/* m_T from m_0 (device SoA; p: MJ_SIB, any noise mode), keeping the checkpoints. */
+mj_status mj_adjoint_forward(mj_adjoint* a, const mj_dyn_params* p, const double* m0_dev_soa, double* mT_dev_soa,
+                             void* stream);
+/* Given dL/dm_T, the gradients of the last forward: dL/dm_0, dL/dvalue_t
+ * (device, nterms doubles, may be NULL) and dL/db per site (device SoA, may be NULL). */
+mj_status mj_adjoint_backward(mj_adjoint* a, const double* gT_dev_soa, double* g0_dev_soa, double* g_terms_dev,
+                              double* g_b_dev_soa, void* stream);
+
 /* ---- batched replicas ---------------------------------------------------- */
 /* Many independent 2D replicas of one single-atom Hamiltonian (the cell, shells
  * and couplings of `cell`/`ham`), each with its own size L[2r], L[2r+1], applied

@@ -138,6 +138,13 @@ SIGNATURES = {
     "mj_profile_read": (C.c_int32, [P, C.c_int32, P, P, P, C.POINTER(C.c_int32)]),
     "mj_measure_temperature": (C.c_int32, [P, P, DP]),
     "mj_philox_normals": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, P, P]),
+    "mj_plan_nterms": (C.c_int32, [P, C.POINTER(C.c_int32)]),
+    "mj_plan_set_terms": (C.c_int32, [P, P]),
+    "mj_field_vjp": (C.c_int32, [P, P, P, P, P, P, P]),
+    "mj_adjoint_create": (C.c_int32, [P, C.c_int32, C.c_int32, C.POINTER(P)]),
+    "mj_adjoint_destroy": (C.c_int32, [P]),
+    "mj_adjoint_forward": (C.c_int32, [P, C.POINTER(DynParams), P, P, P]),
+    "mj_adjoint_backward": (C.c_int32, [P, P, P, P, P, P]),
     "mj_batch_create": (C.c_int32, [C.POINTER(LatticeDesc), C.POINTER(HamiltonianDesc), C.c_int32, P, P, P,
                                     C.c_int32, C.POINTER(P)]),
     "mj_batch_destroy": (C.c_int32, [P]),
@@ -158,7 +165,7 @@ SIGNATURES = {
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m matjes_b200.build` "
+            f"{LIB_PATH} is missing: build it with `python matjes_b200/build.py` "
             "(the CUDA library is required; there is no CPU fallback)")
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():

@@ -297,6 +297,9 @@ void free_plan(mj_plan* p) {
     cudaFree(p->d_tmp_m);
     cudaFree(p->d_tmp_b);
     cudaFree(p->d_tmp_e);
+    cudaFree(p->d_unit);
+    cudaFree(p->d_vjp_part);
+    cudaFree(p->d_vjp_counter);
     delete p;
 }
 
@@ -378,6 +381,14 @@ bool stencil_from_blocks(const std::vector<Block>& blocks, const std::vector<dou
     return make_stencil(blocks, onsite, sp);
 }
 
+mj_status make_dyn_coef(const mj_dyn_params* d, const mj_plan* plan, DynCoef& c) { return dyn_coef(d, plan, c); }
+
+void drop_graph(mj_plan* p) {
+    if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+    p->graph_exec = nullptr;
+    p->graph_key.clear();
+}
+
 void match_shape(StencilParams& sp) {
     sp.shape = kShapeGeneric;
     if (try_shape<ShapeTri3>(sp)) return;
@@ -426,6 +437,14 @@ mj_status mj_plan_create(const mj_lattice_desc* lat, const mj_hamiltonian_desc* 
     p->ncell = static_cast<int64_t>(lat->L[0]) * lat->L[1] * lat->L[2];
     p->N = p->ncell * g.nmag;
     p->blocks = blocks;
+    p->geom = g;
+    p->ham = *ham;
+    p->ham.J = nullptr;
+    p->ham.D = nullptr;
+    p->ham.K = nullptr;
+    p->termJ.assign(ham->J, ham->J + ham->nJ);
+    p->termD.assign(ham->D, ham->D + ham->nD);
+    p->termK.assign(ham->K, ham->K + ham->nK);
     const bool zee_on = ham->zeeman_on ||
                         std::sqrt(ham->B_ext[0] * ham->B_ext[0] + ham->B_ext[1] * ham->B_ext[1] + ham->B_ext[2] * ham->B_ext[2]) >= 1e-8;
     StencilParams& sp = p->sp;

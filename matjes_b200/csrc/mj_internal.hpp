@@ -149,6 +149,18 @@ struct mj_plan {
     std::vector<ProfRec> prof;
     std::vector<std::string> prof_names;
     std::vector<mj::Block> blocks;   // kept for the adjoint / introspection
+    // differentiable coupling terms (stencil plans): the description the plan was
+    // built from, and per-term unit stencils W_t (W = sum_t value_t W_t), built on
+    // first use: [nterm][n_off + 1][9], on-site tensor last, offsets in sp order
+    mj::Geometry geom;
+    mj_hamiltonian_desc ham{};       // term pointers cleared; the terms are copied below
+    std::vector<mj_exchange_term> termJ;
+    std::vector<mj_dmi_term> termD;
+    std::vector<mj_aniso_term> termK;
+    std::vector<double> unitW;
+    double* d_unit = nullptr;
+    double* d_vjp_part = nullptr;          // term-gradient reduction scratch of mj_field_vjp
+    unsigned int* d_vjp_counter = nullptr;
 };
 
 struct mj_state {
@@ -199,6 +211,10 @@ int64_t tiled_energy_blocks(const mj_plan* p);
 void match_shape(mj::StencilParams& sp);
 // single-atom stencil tensors W_o from coupling blocks; false past kMaxOff offsets (mj_abi.cpp)
 bool stencil_from_blocks(const std::vector<Block>& blocks, const std::vector<double>& onsite, StencilParams& sp);
+// dynamics coefficients of a plan, validated (mj_abi.cpp)
+mj_status make_dyn_coef(const mj_dyn_params* d, const mj_plan* plan, DynCoef& c);
+// drop a plan's captured step graph (after its launch parameters change)
+void drop_graph(mj_plan* p);
 
 // dipolar (mj_dipolar.cu)
 mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t s);

@@ -200,10 +200,21 @@ def workload(name: str, scale: int = 1) -> dict:
                     dyn=dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=1,
                              steps=2000))
     if name == "square256_adjoint":
+        # parameters J, D, K (global) and a per-site Bz = 0.5 + N(0, 0.05) T (seed 3);
+        # the target state comes from J, D, K = 1.1, 0.35, -0.08 meV and
+        # Bz = 0.5 + 0.2 sin(2 pi x / L) T from the same initial state
         L = 256 // scale
         deck = square_film((L, L, 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5)
+        rng = np.random.default_rng(3)
+        bz = 0.5 + 0.05 * rng.standard_normal(deck.nsites)
+        x = np.arange(deck.nsites) % L
+        bz_target = 0.5 + 0.2 * np.sin(2.0 * np.pi * x / L)
         return dict(deck=deck, m0=random_sphere(deck.nsites, 3),
-                    dyn=dict(integrator="sib", timestep=0.1, alpha=0.2, temperature=0.0, steps=500))
+                    bfield=np.stack([np.zeros_like(bz), np.zeros_like(bz), bz], axis=1),
+                    target_terms=np.array([1.1e-3, 0.35e-3, -0.08e-3]),
+                    target_bfield=np.stack([np.zeros_like(bz), np.zeros_like(bz), bz_target], axis=1),
+                    dyn=dict(integrator="sib", timestep=0.1, alpha=0.2, temperature=0.0, steps=500,
+                             checkpoint_every=50))
     if name == "film128x16_dipolar":
         L = 128 // scale
         Lz = max(2, 16 // scale)

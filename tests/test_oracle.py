@@ -216,3 +216,23 @@ def test_parallel_tempering_acceptance_rate():
     assert abs(hits / n - p) < 4 * np.sqrt(p * (1 - p) / n)
     u = [O.pt_uniform(9, 0, r) for r in range(1000)]
     assert 0.0 <= min(u) and max(u) < 1.0 and len(set(u)) == 1000
+
+
+def test_torch_sib_restatement_matches_oracle():
+    """The float64 torch restatement used for the autograd checks follows the
+    oracle's SIB trajectory (same couplings, field map and noise-free dynamics)."""
+    import torch
+
+    from matjes_b200.deck import random_sphere
+    from tests import sib_torch_reference as R
+
+    deck = square_film((8, 6, 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5)
+    n = deck.nsites
+    m0 = random_sphere(n, 3)
+    b = np.tile([0.0, 0.0, 0.5], (n, 1))
+    A = R.unit_matrices(deck)
+    terms = torch.tensor([1e-3, 0.3e-3, -0.1e-3], dtype=torch.float64)
+    mt = R.trajectory(torch.tensor(m0), terms, torch.tensor(b), A, R.zeeman_coefficient(deck), 50, 0.1, 0.2)
+    mo = m0.copy()
+    O.Model(deck).run(mo, 50, integrator="sib", timestep=0.1, alpha=0.2)
+    assert np.abs(mt.numpy() - mo).max() < 1e-12
