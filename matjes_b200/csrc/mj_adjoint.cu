@@ -17,9 +17,12 @@
 //   dL/dm_n = gm2 + gmb/2 + gm1 + gp1 + W gH1
 //   dL/dv_t += gH2 . W_t mb + gH1 . W_t m_n,   dL/db_i += zc (gH1_i + gH2_i)
 // Kernels per backward step: k_adj_ca (the W gH1 of step n+1 fused with the
-// stage-2 transpose of step n) and k_adj_b (W gH2, stage-1 transpose).  The
-// trajectory is checkpointed every `checkpoint_every` steps; each segment is
-// recomputed (m_n and mb stored) before its backward sweep.
+// stage-2 transpose of step n) and k_adj_b (W gH2, stage-1 transpose), each as
+// a tiled kernel over a compile-time stencil shape (both stencil inputs staged
+// in shared memory, every offset unrolled) or, for other lattices, a generic
+// one-site-per-thread kernel.  The trajectory is checkpointed every
+// `checkpoint_every` steps; each segment is recomputed (m_n and mb stored)
+// with the plan's own SIB kernels before its backward sweep.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -28,6 +31,7 @@
 
 #include "mj_device.cuh"
 #include "mj_internal.hpp"
+#include "mj_tiled_impl.cuh"
 
 namespace mj {
 namespace {
@@ -44,20 +48,32 @@ __device__ __forceinline__ bool adj_site(const StencilParams& P, int64_t& i, int
     return a;
 }
 
+// periodic image of a coordinate one offset away (one add in the common case)
+__device__ __forceinline__ int wrap(int v, int L) {
+    if (v < 0) {
+        v += L;
+        if (v < 0) v = ((v % L) + L) % L;
+    } else if (v >= L) {
+        v -= L;
+        if (v >= L) v %= L;
+    }
+    return v;
+}
+
 __device__ __forceinline__ bool neighbour(const StencilParams& P, int x, int y, int z, int k, int64_t& j) {
     int nx = x + P.off[k][0], ny = y + P.off[k][1], nz = z + P.off[k][2];
     const int Lx = P.L[0], Ly = P.L[1], Lz = P.L[2];
     if (nx < 0 || nx >= Lx) {
         if (!P.periodic[0]) return false;
-        nx = ((nx % Lx) + Lx) % Lx;
+        nx = wrap(nx, Lx);
     }
     if (ny < 0 || ny >= Ly) {
         if (!P.periodic[1]) return false;
-        ny = ((ny % Ly) + Ly) % Ly;
+        ny = wrap(ny, Ly);
     }
     if (nz < 0 || nz >= Lz) {
         if (!P.periodic[2]) return false;
-        nz = ((nz % Lz) + Lz) % Lz;
+        nz = wrap(nz, Lz);
     }
     j = nx + static_cast<int64_t>(Lx) * (ny + static_cast<int64_t>(Ly) * nz);
     return true;
@@ -90,12 +106,22 @@ __device__ __forceinline__ double3 w_apply(const StencilParams& P, const double*
     return b;
 }
 
+// Which unit tensors are nonzero / isotropic: bit k of nz[t] (iso[t]) for offset
+// k of term t, bit n_off for the on-site tensor.
+struct TermMasks {
+    unsigned long long nz[kMaxTerms];
+    unsigned long long iso[kMaxTerms];
+    unsigned long long any;  // OR of nz
+    int nterm;
+};
+
 // acc[t] += g . (W_t v)_i for every term t (unit tensors [nterm][n_off+1][9])
-__device__ __forceinline__ void term_grads(const StencilParams& P, const double* __restrict__ unit, int nterm,
+__device__ __forceinline__ void term_grads(const StencilParams& P, const double* __restrict__ unit, const TermMasks& M,
                                            const double* __restrict__ v, int64_t N, int x, int y, int z, double3 v0,
                                            double3 g, double* acc) {
     const int stride = (P.n_off + 1) * 9;
     for (int k = 0; k <= P.n_off; ++k) {
+        if (!((M.any >> k) & 1ull)) continue;
         double3 a;
         if (k < P.n_off) {
             int64_t j;
@@ -104,15 +130,68 @@ __device__ __forceinline__ void term_grads(const StencilParams& P, const double*
         } else {
             a = v0;
         }
+        const double ga = dot(g, a);
 #pragma unroll
         for (int t = 0; t < kMaxTerms; ++t) {
-            if (t < nterm) {
+            if (t < M.nterm && ((M.nz[t] >> k) & 1ull)) {
                 const double* U = unit + t * stride + k * 9;
-                const double3 u = mat3(U, a, make_double3(0.0, 0.0, 0.0));
-                acc[t] = fma(g.x, u.x, fma(g.y, u.y, fma(g.z, u.z, acc[t])));
+                if ((M.iso[t] >> k) & 1ull) {
+                    acc[t] = fma(__ldg(U), ga, acc[t]);
+                } else {
+                    const double3 u = mat3(U, a, make_double3(0.0, 0.0, 0.0));
+                    acc[t] = fma(g.x, u.x, fma(g.y, u.y, fma(g.z, u.z, acc[t])));
+                }
             }
         }
     }
+}
+
+// Deterministic grid reduction of the first nq of kMaxTerms values (blocks of
+// 256 threads): per-block partials, summed in block order by the last block.
+__device__ void term_reduce(const double* acc, int nq, double* partials, unsigned int* counter, double* out,
+                            int nblocks) {
+    __shared__ double wsum[kMaxTerms][8];
+    __shared__ bool last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+#pragma unroll
+    for (int q = 0; q < kMaxTerms; ++q) {
+        if (q < nq) {
+            double e = acc[q];
+            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+            if (lane == 0) wsum[q][wid] = e;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int q = 0; q < nq; ++q) {
+            double sum = 0.0;
+            for (int w = 0; w < nthr / 32; ++w) sum += wsum[q][w];
+            partials[static_cast<int64_t>(q) * nblocks + bid] = sum;
+        }
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        last = (t == static_cast<unsigned int>(nblocks - 1));
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int q = 0; q < nq; ++q) {
+        double sum = 0.0;
+        for (int b = tid; b < nblocks; b += nthr) sum += __ldcg(partials + static_cast<int64_t>(q) * nblocks + b);
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+        __syncthreads();
+        if (lane == 0) wsum[0][wid] = sum;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < nthr / 32; ++w) t += wsum[0][w];
+            out[q] = t;
+        }
+    }
+    if (tid == 0) *counter = 0u;
 }
 
 __device__ __forceinline__ double3 zeeman(const StencilParams& P, const double* __restrict__ bmap, int64_t i,
@@ -210,7 +289,7 @@ __global__ void __launch_bounds__(256) k_adj_f2(const __grid_constant__ StencilP
 // gH1 is null), then, unless mb is null, the stage-2 transpose of step n.
 __global__ void __launch_bounds__(256) k_adj_ca(const __grid_constant__ StencilParams P, const DynCoef C, uint32_t step,
                                                 const double* __restrict__ bmap, const double* __restrict__ unit,
-                                                int nterm, const double* __restrict__ gH1,
+                                                const TermMasks M, const double* __restrict__ gH1,
                                                 const double* __restrict__ mpart, const double* __restrict__ m,
                                                 const double* __restrict__ mb, double* __restrict__ g_out,
                                                 double* __restrict__ gH2, double* __restrict__ gp2,
@@ -235,16 +314,16 @@ __global__ void __launch_bounds__(256) k_adj_ca(const __grid_constant__ StencilP
             st3(gH2, i, N, s.gH);
             st3(gp2, i, N, s.gp);
             st3(gm2, i, N, s.gm);
-            if (nterm > 0) term_grads(P, unit, nterm, mb, N, x, y, z, b0, s.gH, acc);
+            if (M.nterm > 0) term_grads(P, unit, M, mb, N, x, y, z, b0, s.gH, acc);
         }
     }
-    if (mb && nterm > 0) grid_reduce<kMaxTerms>(acc, R.partials, R.counter, R.slot, R.nblocks);
+    if (mb && M.nterm > 0) term_reduce(acc, M.nterm, R.partials, R.counter, R.slot, R.nblocks);
 }
 
 // backward, stage 1 of step n: gmb = gp2 + W gH2, stage-1 transpose, field gradient
 __global__ void __launch_bounds__(256) k_adj_b(const __grid_constant__ StencilParams P, const DynCoef C, uint32_t step,
                                                const double* __restrict__ bmap, const double* __restrict__ unit,
-                                               int nterm, const double* __restrict__ gH2,
+                                               const TermMasks M, const double* __restrict__ gH2,
                                                const double* __restrict__ gp2, const double* __restrict__ gm2,
                                                const double* __restrict__ m, double* __restrict__ gH1,
                                                double* __restrict__ mpart, double* __restrict__ gb, AdjReduce R) {
@@ -268,9 +347,9 @@ __global__ void __launch_bounds__(256) k_adj_b(const __grid_constant__ StencilPa
             const double3 prev = ld3(gb, i, N);
             st3(gb, i, N, add3(prev, scl3(P.zc, add3(s.gH, h2))));
         }
-        if (nterm > 0) term_grads(P, unit, nterm, m, N, x, y, z, m0, s.gH, acc);
+        if (M.nterm > 0) term_grads(P, unit, M, m, N, x, y, z, m0, s.gH, acc);
     }
-    if (nterm > 0) grid_reduce<kMaxTerms>(acc, R.partials, R.counter, R.slot, R.nblocks);
+    if (M.nterm > 0) term_reduce(acc, M.nterm, R.partials, R.counter, R.slot, R.nblocks);
 }
 
 // sum of the per-launch term gradients in launch order
@@ -284,7 +363,7 @@ __global__ void k_adj_sum(const double* __restrict__ slots, int nslot, int nterm
 
 // VJP of the field: g_m = W v, g_terms[t] = v . W_t m, g_b = zc v (per site)
 __global__ void __launch_bounds__(256) k_field_vjp(const __grid_constant__ StencilParams P,
-                                                   const double* __restrict__ unit, int nterm,
+                                                   const double* __restrict__ unit, const TermMasks M,
                                                    const double* __restrict__ m, const double* __restrict__ v,
                                                    double* __restrict__ gm, double* __restrict__ gb, AdjReduce R) {
     int64_t i;
@@ -298,9 +377,316 @@ __global__ void __launch_bounds__(256) k_field_vjp(const __grid_constant__ Stenc
         const double3 v0 = ld3(v, i, N);
         if (gm) st3(gm, i, N, w_apply(P, v, N, x, y, z, v0));
         if (gb) st3(gb, i, N, P.zee_on ? scl3(P.zc, v0) : make_double3(0.0, 0.0, 0.0));
-        if (nterm > 0) term_grads(P, unit, nterm, m, N, x, y, z, ld3(m, i, N), v0, acc);
+        if (M.nterm > 0) term_grads(P, unit, M, m, N, x, y, z, ld3(m, i, N), v0, acc);
     }
-    if (nterm > 0 && R.slot) grid_reduce<kMaxTerms>(acc, R.partials, R.counter, R.slot, R.nblocks);
+    if (M.nterm > 0 && R.slot) term_reduce(acc, M.nterm, R.partials, R.counter, R.slot, R.nblocks);
+}
+
+
+// ---------------------------------------------------------------------------
+// Tiled backward kernels for the compile-time shapes (mj_shapes.hpp).  A block
+// of 32 x BYT threads owns a 32 x BYT*RY tile; the two stencil inputs of the
+// kernel are staged with their halo in shared memory (TileGeom layout), the
+// unit tensors of the terms follow them.  W v reuses the forward column walk
+// (all_columns); the per-term stencils W_t v walk the same tile with the unit
+// tensors read from shared memory, skipping zero tensors and taking one load
+// for isotropic ones.
+template <class S, int RY, int DX, int YY, int... Kk>
+__device__ __forceinline__ void unit_row(const double* U, unsigned long long nz, unsigned long long iso, double vx,
+                                         double vy, double vz, double* bx, double* by, double* bz,
+                                         std::integer_sequence<int, Kk...>) {
+    (
+        [&] {
+            constexpr int k = Kk;
+            if constexpr (S::DX[k] == DX) {
+                constexpr int r = YY - S::DY[k];
+                if constexpr (r >= 0 && r < RY) {
+                    if ((nz >> k) & 1ull) {
+                        const double* W = U + 9 * k;
+                        if ((iso >> k) & 1ull) {
+                            const double w = W[0];
+                            bx[r] = fma(w, vx, bx[r]);
+                            by[r] = fma(w, vy, by[r]);
+                            bz[r] = fma(w, vz, bz[r]);
+                        } else {
+                            bx[r] = fma(W[0], vx, fma(W[1], vy, fma(W[2], vz, bx[r])));
+                            by[r] = fma(W[3], vx, fma(W[4], vy, fma(W[5], vz, by[r])));
+                            bz[r] = fma(W[6], vx, fma(W[7], vy, fma(W[8], vz, bz[r])));
+                        }
+                    }
+                }
+            }
+        }(),
+        ...);
+}
+
+template <class S, int BYT, int RY, int DX, int... Y>
+__device__ __forceinline__ void unit_column(const double* U, unsigned long long nz, unsigned long long iso,
+                                            const double* sm, int base, double* bx, double* by, double* bz,
+                                            std::integer_sequence<int, Y...>) {
+    using G = TileGeom<S, BYT, RY>;
+    constexpr int ylo = shape_col_ymin<S>(DX);
+    (
+        [&] {
+            constexpr int yy = ylo + Y;
+            const int s = base + (yy + G::R) * G::PX + DX + G::RX;
+            unit_row<S, RY, DX, yy>(U, nz, iso, sm[s], sm[G::NS + s], sm[2 * G::NS + s], bx, by, bz,
+                                    std::make_integer_sequence<int, S::K>{});
+        }(),
+        ...);
+}
+
+template <class S, int BYT, int RY, int... Cc>
+__device__ __forceinline__ void unit_columns(const double* U, unsigned long long nz, unsigned long long iso,
+                                             const double* sm, int base, double* bx, double* by, double* bz,
+                                             std::integer_sequence<int, Cc...>) {
+    (
+        [&] {
+            constexpr int dx = Cc - S::R;
+            constexpr int ylo = shape_col_ymin<S>(dx), yhi = shape_col_ymax<S>(dx);
+            if constexpr (ylo <= yhi) {
+                unit_column<S, BYT, RY, dx>(U, nz, iso, sm, base, bx, by, bz,
+                                            std::make_integer_sequence<int, RY + yhi - ylo>{});
+            }
+        }(),
+        ...);
+}
+
+// acc[t] += g_r . (W_t v)_r over the thread's RY sites, v staged in `tile`
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void tiled_term_grads(const double* Us, const TermMasks& M, const double* tile, int base,
+                                                 const double3* g, const bool* act, double* acc) {
+    using G = TileGeom<S, BYT, RY>;
+#pragma unroll
+    for (int t = 0; t < kMaxTerms; ++t) {
+        if (t < M.nterm) {
+            const double* U = Us + t * (S::K + 1) * 9;
+            double ux[RY], uy[RY], uz[RY];
+#pragma unroll
+            for (int r = 0; r < RY; ++r) ux[r] = uy[r] = uz[r] = 0.0;
+            unit_columns<S, BYT, RY>(U, M.nz[t], M.iso[t], tile, base, ux, uy, uz,
+                                     std::make_integer_sequence<int, 2 * S::R + 1>{});
+            const bool onsite = (M.nz[t] >> S::K) & 1ull;
+            const double* U0 = U + 9 * S::K;
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                if (!act[r]) continue;
+                double3 u = make_double3(ux[r], uy[r], uz[r]);
+                if (onsite) {
+                    const int c = base + (r + G::R) * G::PX + G::RX;
+                    u = mat3(U0, make_double3(tile[c], tile[G::NS + c], tile[2 * G::NS + c]), u);
+                }
+                acc[t] = fma(g[r].x, u.x, fma(g[r].y, u.y, fma(g[r].z, u.z, acc[t])));
+            }
+        }
+    }
+}
+
+// W v at the thread's RY sites (main stencil + on-site tensor), v staged in `tile`
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void tiled_apply(const StencilParams& P, const double* tile, int base, double3* out) {
+    using G = TileGeom<S, BYT, RY>;
+    double bx[RY], by[RY], bz[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
+    all_columns<S, BYT, RY>(P, tile, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        out[r] = make_double3(bx[r], by[r], bz[r]);
+        if (P.has_onsite) {
+            const int c = base + (r + G::R) * G::PX + G::RX;
+            out[r] = mat3(P.W0, make_double3(tile[c], tile[G::NS + c], tile[2 * G::NS + c]), out[r]);
+        }
+    }
+}
+
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void stage_units(const double* __restrict__ unit, const TermMasks& M, double* Us) {
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const int nu = M.nterm * (S::K + 1) * 9;
+    for (int q = tid; q < nu; q += 32 * BYT) Us[q] = __ldg(unit + q);
+}
+
+template <class S, int BYT, int RY>
+__global__ void __launch_bounds__(32 * BYT) k_tadj_ca(const __grid_constant__ StencilParams P, const DynCoef C,
+                                                      uint32_t step, const double* __restrict__ bmap,
+                                                      const double* __restrict__ unit, const TermMasks M,
+                                                      const double* __restrict__ gH1, const double* __restrict__ mpart,
+                                                      const double* __restrict__ m, const double* __restrict__ mb,
+                                                      double* __restrict__ g_out, double* __restrict__ gH2,
+                                                      double* __restrict__ gp2, double* __restrict__ gm2,
+                                                      AdjReduce R) {
+    using G = TileGeom<S, BYT, RY>;
+    extern __shared__ __align__(128) double smem_a[];
+    double* tA = smem_a;               // gH1
+    double* tB = smem_a + 3 * G::NS;   // mb
+    double* Us = smem_a + 6 * G::NS;   // unit tensors
+    const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY;
+    const int64_t N = static_cast<int64_t>(P.L[0]) * P.L[1];
+    if (gH1) load_tile<S, BYT, RY>(P, gH1, x0, y0, 0, tA);
+    if (mb) load_tile<S, BYT, RY>(P, mb, x0, y0, 0, tB);
+    if (mb) stage_units<S, BYT, RY>(unit, M, Us);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int base = (ty * RY) * G::PX + tx;
+    const int x = x0 + tx;
+    double3 g[RY], wg[RY];
+    bool act[RY];
+    int64_t idx[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int y = y0 + ty * RY + r;
+        act[r] = x < P.L[0] && y < P.L[1];
+        idx[r] = act[r] ? x + static_cast<int64_t>(P.L[0]) * y : 0;
+        g[r] = act[r] ? ld3(mpart, idx[r], N) : make_double3(0.0, 0.0, 0.0);
+    }
+    if (gH1) {
+        tiled_apply<S, BYT, RY>(P, tA, base, wg);
+#pragma unroll
+        for (int r = 0; r < RY; ++r) g[r] = add3(g[r], wg[r]);
+    }
+    double acc[kMaxTerms];
+#pragma unroll
+    for (int t = 0; t < kMaxTerms; ++t) acc[t] = 0.0;
+    if (!mb) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r)
+            if (act[r]) st3(g_out, idx[r], N, g[r]);
+        return;
+    }
+    double3 H[RY];
+    tiled_apply<S, BYT, RY>(P, tB, base, H);
+    double3 gh[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        gh[r] = make_double3(0.0, 0.0, 0.0);
+        if (!act[r]) continue;
+        const int c = base + (r + G::R) * G::PX + G::RX;
+        const double3 b0 = make_double3(tB[c], tB[G::NS + c], tB[2 * G::NS + c]);
+        const double3 H2 = add3(add3(H[r], zeeman(P, bmap, idx[r], N)), noise(C, step, idx[r], N));
+        const SibGrad sg = sib_vjp(ld3(m, idx[r], N), b0, H2, C.alpha, C.sib_hc, g[r]);
+        st3(gH2, idx[r], N, sg.gH);
+        st3(gp2, idx[r], N, sg.gp);
+        st3(gm2, idx[r], N, sg.gm);
+        gh[r] = sg.gH;
+    }
+    if (M.nterm > 0) {
+        tiled_term_grads<S, BYT, RY>(Us, M, tB, base, gh, act, acc);
+        term_reduce(acc, M.nterm, R.partials, R.counter, R.slot, R.nblocks);
+    }
+}
+
+template <class S, int BYT, int RY>
+__global__ void __launch_bounds__(32 * BYT) k_tadj_b(const __grid_constant__ StencilParams P, const DynCoef C,
+                                                     uint32_t step, const double* __restrict__ bmap,
+                                                     const double* __restrict__ unit, const TermMasks M,
+                                                     const double* __restrict__ gH2, const double* __restrict__ gp2,
+                                                     const double* __restrict__ gm2, const double* __restrict__ m,
+                                                     double* __restrict__ gH1, double* __restrict__ mpart,
+                                                     double* __restrict__ gb, AdjReduce R) {
+    using G = TileGeom<S, BYT, RY>;
+    extern __shared__ __align__(128) double smem_b[];
+    double* tA = smem_b;               // gH2
+    double* tB = smem_b + 3 * G::NS;   // m_n
+    double* Us = smem_b + 6 * G::NS;
+    const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY;
+    const int64_t N = static_cast<int64_t>(P.L[0]) * P.L[1];
+    load_tile<S, BYT, RY>(P, gH2, x0, y0, 0, tA);
+    load_tile<S, BYT, RY>(P, m, x0, y0, 0, tB);
+    stage_units<S, BYT, RY>(unit, M, Us);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int base = (ty * RY) * G::PX + tx;
+    const int x = x0 + tx;
+    double3 wg[RY], H[RY], gh[RY];
+    bool act[RY];
+    int64_t idx[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int y = y0 + ty * RY + r;
+        act[r] = x < P.L[0] && y < P.L[1];
+        idx[r] = act[r] ? x + static_cast<int64_t>(P.L[0]) * y : 0;
+    }
+    tiled_apply<S, BYT, RY>(P, tA, base, wg);
+    tiled_apply<S, BYT, RY>(P, tB, base, H);
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        gh[r] = make_double3(0.0, 0.0, 0.0);
+        if (!act[r]) continue;
+        const int c = base + (r + G::R) * G::PX + G::RX;
+        const double3 h2 = make_double3(tA[c], tA[G::NS + c], tA[2 * G::NS + c]);
+        const double3 m0 = make_double3(tB[c], tB[G::NS + c], tB[2 * G::NS + c]);
+        const double3 gmb = add3(ld3(gp2, idx[r], N), wg[r]);
+        const double3 gy1 = scl3(0.5, gmb);
+        const double3 H1 = add3(add3(H[r], zeeman(P, bmap, idx[r], N)), noise(C, step, idx[r], N));
+        const SibGrad sg = sib_vjp(m0, m0, H1, C.alpha, C.sib_hc, gy1);
+        st3(gH1, idx[r], N, sg.gH);
+        st3(mpart, idx[r], N, add3(add3(ld3(gm2, idx[r], N), gy1), add3(sg.gm, sg.gp)));
+        if (gb && P.zee_on) st3(gb, idx[r], N, add3(ld3(gb, idx[r], N), scl3(P.zc, add3(sg.gH, h2))));
+        gh[r] = sg.gH;
+    }
+    if (M.nterm > 0) {
+        double acc[kMaxTerms];
+#pragma unroll
+        for (int t = 0; t < kMaxTerms; ++t) acc[t] = 0.0;
+        tiled_term_grads<S, BYT, RY>(Us, M, tB, base, gh, act, acc);
+        term_reduce(acc, M.nterm, R.partials, R.counter, R.slot, R.nblocks);
+    }
+}
+
+// tile shape of the tiled backward: 32 x 8 sites, one per thread
+constexpr int kTBYT = 8, kTRY = 1;
+
+template <class S>
+size_t tadj_smem(int nterm) {
+    using G = TileGeom<S, kTBYT, kTRY>;
+    return sizeof(double) * (6 * G::NS + static_cast<size_t>(nterm) * (S::K + 1) * 9);
+}
+
+template <class S>
+dim3 tadj_grid(const StencilParams& P) {
+    using G = TileGeom<S, kTBYT, kTRY>;
+    return dim3((P.L[0] + G::TX - 1) / G::TX, (P.L[1] + G::TY - 1) / G::TY, 1);
+}
+
+struct CaArgs {
+    uint32_t step;
+    const double *gH1, *mpart, *m, *mb;
+    double *g_out, *gH2, *gp2, *gm2;
+    AdjReduce R;
+};
+struct BArgs {
+    uint32_t step;
+    const double *gH2, *gp2, *gm2, *m;
+    double *gH1, *mpart, *gb;
+    AdjReduce R;
+};
+
+template <class S>
+void tadj_launch(const mj_plan* plan, const DynCoef& c, const TermMasks& M, const CaArgs* ca, const BArgs* b,
+                 cudaStream_t s) {
+    const size_t sm = tadj_smem<S>(M.nterm);
+    const dim3 grid = tadj_grid<S>(plan->sp), blk(32, kTBYT);
+    if (ca)
+        k_tadj_ca<S, kTBYT, kTRY><<<grid, blk, sm, s>>>(plan->sp, c, ca->step, plan->d_bmap, plan->d_unit, M, ca->gH1,
+                                                       ca->mpart, ca->m, ca->mb, ca->g_out, ca->gH2, ca->gp2, ca->gm2,
+                                                       ca->R);
+    if (b)
+        k_tadj_b<S, kTBYT, kTRY><<<grid, blk, sm, s>>>(plan->sp, c, b->step, plan->d_bmap, plan->d_unit, M, b->gH2,
+                                                      b->gp2, b->gm2, b->m, b->gH1, b->mpart, b->gb, b->R);
+}
+
+// the tiled backward kernels of the plan's shape; false when none applies
+bool tadj_dispatch(const mj_plan* plan, const DynCoef& c, const TermMasks& M, const CaArgs* ca, const BArgs* b,
+                   cudaStream_t s) {
+    if (plan->sp.L[2] != 1) return false;
+    switch (plan->sp.shape) {
+        case kShapeSquareNN: tadj_launch<ShapeSquareNN>(plan, c, M, ca, b, s); return true;
+        case kShapeSquare2: tadj_launch<ShapeSquare2>(plan, c, M, ca, b, s); return true;
+        case kShapeTriNN: tadj_launch<ShapeTriNN>(plan, c, M, ca, b, s); return true;
+        case kShapeTri3: tadj_launch<ShapeTri3>(plan, c, M, ca, b, s); return true;
+        default: return false;
+    }
 }
 
 dim3 adj_grid(const StencilParams& P) {
@@ -309,6 +695,27 @@ dim3 adj_grid(const StencilParams& P) {
 
 int plan_nterm(const mj_plan* p) {
     return static_cast<int>(p->termJ.size() + p->termD.size() + p->termK.size());
+}
+
+// nonzero / isotropic masks of the unit tensors (nterm = 0 gives an empty set)
+TermMasks term_masks(const mj_plan* p, int nterm) {
+    TermMasks M;
+    std::memset(&M, 0, sizeof(M));
+    M.nterm = nterm;
+    const int n_off = p->sp.n_off;
+    for (int t = 0; t < nterm; ++t)
+        for (int k = 0; k <= n_off; ++k) {
+            const double* U = p->unitW.data() + (static_cast<size_t>(t) * (n_off + 1) + k) * 9;
+            bool nz = false, iso = U[0] == U[4] && U[0] == U[8];
+            for (int q = 0; q < 9; ++q) {
+                nz = nz || U[q] != 0.0;
+                if (q != 0 && q != 4 && q != 8 && U[q] != 0.0) iso = false;
+            }
+            if (nz) M.nz[t] |= 1ull << k;
+            if (nz && iso) M.iso[t] |= 1ull << k;
+            if (nz) M.any |= 1ull << k;
+        }
+    return M;
 }
 
 // per-term unit stencils in the plan's offset order
@@ -453,11 +860,30 @@ mj_status adj_coef(mj_adjoint* a, const mj_dyn_params* p, DynCoef& c) {
 
 double* ckpt(const mj_adjoint* a, int k) { return a->d_ckpt + static_cast<int64_t>(k) * 3 * a->N; }
 
+// One SIB stage of the forward map with explicit buffers: the plan's tiled
+// kernels when a compile-time shape is active (the same arithmetic as
+// mj_step), the generic stencil kernels otherwise.  The thermal draw is
+// recomputed in the second stage.
+void stage1(mj_plan* plan, const DynCoef& c, uint32_t step, const double* m, double* mb, cudaStream_t s) {
+    if (plan->sp.shape != 0) {
+        launch_tiled(plan, 4, c, m, nullptr, mb, nullptr, nullptr, DipView{nullptr, 0, 0, 0}, nullptr, step, s);
+        return;
+    }
+    k_adj_f1<<<adj_grid(plan->sp), dim3(kABX, kABY), 0, s>>>(plan->sp, c, step, plan->d_bmap, m, mb);
+}
+void stage2(mj_plan* plan, const DynCoef& c, uint32_t step, const double* m, const double* mb, double* out,
+            cudaStream_t s) {
+    if (plan->sp.shape != 0) {
+        launch_tiled(plan, 5, c, mb, m, out, nullptr, nullptr, DipView{nullptr, 0, 0, 0}, nullptr, step, s);
+        return;
+    }
+    k_adj_f2<<<adj_grid(plan->sp), dim3(kABX, kABY), 0, s>>>(plan->sp, c, step, plan->d_bmap, m, mb, out);
+}
+
 // forward sweep from checkpoint 0 (already holding m_0) to checkpoint nseg
 void forward_launches(mj_adjoint* a, const DynCoef& c, uint32_t step0, cudaStream_t s) {
-    const mj_plan* plan = a->plan;
+    mj_plan* plan = a->plan;
     const int64_t n3 = 3 * a->N;
-    const dim3 grid = adj_grid(plan->sp), blk(kABX, kABY);
     double* mid = a->d_work + 2 * n3;
     const int E = a->every;
     for (int32_t k = 0; k < a->nsteps; ++k) {
@@ -465,16 +891,17 @@ void forward_launches(mj_adjoint* a, const DynCoef& c, uint32_t step0, cudaStrea
         const bool bound = ((k + 1) % E == 0) || (k + 1 == a->nsteps);
         double* dst = bound ? ckpt(a, (k + E) / E) : a->d_work + ((k + 1) % 2) * n3;
         const uint32_t step = step0 + static_cast<uint32_t>(k);
-        k_adj_f1<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, src, mid);
-        k_adj_f2<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, src, mid, dst);
+        stage1(plan, c, step, src, mid, s);
+        stage2(plan, c, step, src, mid, dst, s);
     }
 }
 
 // backward sweep from d_gin (dL/dm_T) to d_g0, d_gterms and, if want_b, d_gb
 void backward_launches(mj_adjoint* a, const DynCoef& c, uint32_t step0, bool want_b, cudaStream_t s) {
-    const mj_plan* plan = a->plan;
+    mj_plan* plan = a->plan;
     const int64_t n3 = 3 * a->N;
     const int nt = plan_nterm(plan);
+    const TermMasks M = term_masks(plan, nt);
     const dim3 grid = adj_grid(plan->sp), blk(kABX, kABY);
     double* gb = want_b ? a->d_gb : nullptr;
     if (gb) cudaMemsetAsync(gb, 0, sizeof(double) * n3, s);
@@ -488,26 +915,32 @@ void backward_launches(mj_adjoint* a, const DynCoef& c, uint32_t step0, bool wan
         auto segm = [&](int k) -> double* { return k == 0 ? ckpt(a, seg) : a->d_segm + k * n3; };
         for (int k = 0; k < len; ++k) {
             const uint32_t step = step0 + static_cast<uint32_t>(s0 + k);
-            k_adj_f1<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, segm(k), a->d_segb + k * n3);
-            if (k + 1 < len)
-                k_adj_f2<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, segm(k), a->d_segb + k * n3, segm(k + 1));
+            stage1(plan, c, step, segm(k), a->d_segb + k * n3, s);
+            if (k + 1 < len) stage2(plan, c, step, segm(k), a->d_segb + k * n3, segm(k + 1), s);
         }
         for (int k = len - 1; k >= 0; --k) {
             const uint32_t step = step0 + static_cast<uint32_t>(s0 + k);
             AdjReduce Ra{a->d_partials, a->d_counter, a->d_slots + static_cast<int64_t>(slot++) * kMaxTerms, a->nblocks};
-            k_adj_ca<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, plan->d_unit, nt, first ? nullptr : a->d_gH1,
-                                          first ? a->d_gin : a->d_mpart, segm(k), a->d_segb + k * n3, nullptr, a->d_gH2,
-                                          a->d_gp2, a->d_gm2, Ra);
+            const CaArgs ca{step, first ? nullptr : a->d_gH1, first ? a->d_gin : a->d_mpart, segm(k),
+                            a->d_segb + k * n3, nullptr, a->d_gH2, a->d_gp2, a->d_gm2, Ra};
+            if (!tadj_dispatch(plan, c, M, &ca, nullptr, s))
+                k_adj_ca<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, plan->d_unit, M, ca.gH1, ca.mpart, ca.m,
+                                              ca.mb, nullptr, a->d_gH2, a->d_gp2, a->d_gm2, Ra);
             first = false;
             AdjReduce Rb{a->d_partials, a->d_counter, a->d_slots + static_cast<int64_t>(slot++) * kMaxTerms, a->nblocks};
-            k_adj_b<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, plan->d_unit, nt, a->d_gH2, a->d_gp2, a->d_gm2,
-                                         segm(k), a->d_gH1, a->d_mpart, gb, Rb);
+            const BArgs bb{step, a->d_gH2, a->d_gp2, a->d_gm2, segm(k), a->d_gH1, a->d_mpart, gb, Rb};
+            if (!tadj_dispatch(plan, c, M, nullptr, &bb, s))
+                k_adj_b<<<grid, blk, 0, s>>>(plan->sp, c, step, plan->d_bmap, plan->d_unit, M, a->d_gH2, a->d_gp2,
+                                             a->d_gm2, segm(k), a->d_gH1, a->d_mpart, gb, Rb);
         }
     }
     // dL/dm_0 = mpart + W gH1 of step 0
     AdjReduce R0{nullptr, nullptr, nullptr, 0};
-    k_adj_ca<<<grid, blk, 0, s>>>(plan->sp, c, 0u, plan->d_bmap, plan->d_unit, 0, a->d_gH1, a->d_mpart, nullptr, nullptr,
-                                  a->d_g0, nullptr, nullptr, nullptr, R0);
+    const TermMasks M0 = term_masks(plan, 0);
+    const CaArgs c0{0u, a->d_gH1, a->d_mpart, nullptr, nullptr, a->d_g0, nullptr, nullptr, nullptr, R0};
+    if (!tadj_dispatch(plan, c, M0, &c0, nullptr, s))
+        k_adj_ca<<<grid, blk, 0, s>>>(plan->sp, c, 0u, plan->d_bmap, plan->d_unit, M0, a->d_gH1, a->d_mpart, nullptr,
+                                      nullptr, a->d_g0, nullptr, nullptr, nullptr, R0);
     if (nt > 0) k_adj_sum<<<1, kMaxTerms, 0, s>>>(a->d_slots, slot, nt, a->d_gterms);
 }
 
@@ -635,7 +1068,8 @@ mj_status mj_field_vjp(mj_plan* plan, const double* m, const double* v, double* 
             return st;
     }
     AdjReduce R{plan->d_vjp_part, plan->d_vjp_counter, nt > 0 ? g_terms : nullptr, nb};
-    k_field_vjp<<<grid, dim3(kABX, kABY), 0, static_cast<cudaStream_t>(stream)>>>(plan->sp, plan->d_unit, nt, m, v, g_m,
+    k_field_vjp<<<grid, dim3(kABX, kABY), 0, static_cast<cudaStream_t>(stream)>>>(plan->sp, plan->d_unit,
+                                                                                  term_masks(plan, nt), m, v, g_m,
                                                                                   g_b, R);
     return cuda_status(cudaGetLastError(), "k_field_vjp");
 }

@@ -4,10 +4,20 @@
         --integrator sib --variant 2 --steps 3
 
 --variant: -1 generic kernel, 0..3 tiled tile shapes, "auto" = the autotuner's pick.
+
+    python -m matjes_b200.profile_run --adjoint --L 256 --steps 20 --every 10
+
+runs one forward + backward sweep of the reverse-mode SIB trajectory instead;
+
+    python -m matjes_b200.profile_run --batch --steps 3
+
+steps the 256-replica batch workload.
 """
 from __future__ import annotations
 
 import argparse
+
+import numpy as np
 
 
 def main(argv=None):
@@ -20,7 +30,14 @@ def main(argv=None):
     ap.add_argument("--variant", default="auto")
     ap.add_argument("--tma", type=int, default=1, help="halo staging of the tiled kernels: 1 TMA, 0 plain loads")
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--adjoint", action="store_true", help="one forward + backward sweep of the SIB adjoint")
+    ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
+    ap.add_argument("--batch", action="store_true", help="step the 256-replica batch workload")
     a = ap.parse_args(argv)
+    if a.adjoint:
+        return adjoint(a)
+    if a.batch:
+        return batch(a)
 
     import torch
 
@@ -54,6 +71,40 @@ def main(argv=None):
         _abi.check(_abi.lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(sd.p), 1, E[k:].data_ptr(), stream))
     torch.cuda.synchronize()
     print("ok", E[: a.steps].tolist())
+
+
+def adjoint(a):
+    import torch
+
+    import matjes_b200 as mj
+
+    deck = mj.square_film((a.L, a.L, 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5)
+    ham = mj.Hamiltonian(deck)
+    traj = mj.SIBTrajectory(ham, a.steps, checkpoint_every=a.every, timestep=0.1, alpha=0.2)
+    rng = np.random.default_rng(3)
+    b = torch.tensor(np.stack([np.zeros(deck.nsites), np.zeros(deck.nsites),
+                               0.5 + 0.05 * rng.standard_normal(deck.nsites)]), device="cuda")
+    traj.set_bfield(b)
+    m0 = torch.tensor(mj.random_sphere(deck.nsites, 3).T.copy(), device="cuda")
+    mT = traj.forward(m0)
+    g0, gt, gb = traj.backward(mT - m0)
+    torch.cuda.synchronize()
+    print("ok", gt.tolist(), float(g0.abs().sum()), float(gb.abs().sum()))
+
+
+def batch(a):
+    import torch
+
+    import matjes_b200 as mj
+
+    w = mj.workload("square_replicas256")
+    bt = mj.ReplicaBatch(w["cell"], w["sizes"], w["B_ext"], w["temperature"])
+    bt.upload(w["m0"])
+    d = w["dyn"]
+    p = bt.params(timestep=d["timestep"], alpha=d["alpha"], noise="philox", seed=d["seed"])
+    bt.step(p, a.steps)
+    torch.cuda.synchronize()
+    print("ok", bt.energies()[:4].tolist())
 
 
 if __name__ == "__main__":

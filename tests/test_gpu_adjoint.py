@@ -110,10 +110,22 @@ def _gpu_grads(deck, m0, terms, b, target, nsteps, dyn, every, **noise):
             mT.detach().cpu().numpy().T)
 
 
-def test_adjoint_matches_torch_autograd_16x16():
+def _adj_decks():
     import matjes_b200 as mj
 
-    deck = _deck()
+    return {
+        "square_16x16": _deck(),                                        # tiled kernels, square NN shape
+        "triangular_3_shells": mj.triangular((12, 10), Bz=0.5),         # tiled kernels, three-shell shape
+        "cubic_film_open_z": mj.square_film((6, 6, 3), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5, a=0.25,
+                                            med_z=-0.3),                # generic kernels
+    }
+
+
+@pytest.mark.parametrize("name", ["square_16x16", "triangular_3_shells", "cubic_film_open_z"])
+def test_adjoint_matches_torch_autograd(name):
+    import matjes_b200 as mj
+
+    deck = _adj_decks()[name]
     n = deck.nsites
     rng = np.random.default_rng(6)
     m0 = mj.random_sphere(n, 6)
@@ -230,3 +242,23 @@ def test_full_size_gradients_against_finite_differences():
             fd = (loss(m0, terms, b + h * delta) - loss(m0, terms, b - h * delta)) / (2 * h)
         ad = float((g * delta).sum())
         assert abs(fd - ad) <= GRAD_TOL * abs(ad), (which, fd, ad)
+
+
+@pytest.mark.parametrize("thermal", [False, True])
+def test_adjoint_forward_is_the_plain_forward(thermal):
+    """The adjoint's forward sweep runs the plan's own SIB kernels: its m_T is
+    the state mj_step_dev reaches, bit for bit."""
+    import torch
+
+    import matjes_b200 as mj
+
+    deck = _deck((64, 48))
+    ham = mj.Hamiltonian(deck)
+    noise = dict(temperature=20.0, noise="philox", seed=3, stream_id=1) if thermal else {}
+    traj = mj.SIBTrajectory(ham, 40, checkpoint_every=9, timestep=0.1, alpha=0.2, **noise)
+    m0 = torch.tensor(mj.random_sphere(deck.nsites, 15).T.copy(), device="cuda")
+    mT = traj.forward(m0)
+    m = m0.clone()
+    mj.SpinDynamics(ham, integrator="sib", timestep=0.1, alpha=0.2, **noise).run(m, 40)
+    torch.cuda.synchronize()
+    assert torch.equal(mT, m)
