@@ -128,14 +128,39 @@ class Clocks:
                 "samples": len(self.samples), "source": "nvml"}
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """dram bytes per launch from a committed ncu summary (profiles/<kernel>_<workload>.md),
-    per site so that it scales to the bench lattice; None if there is none."""
-    fn = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+def ncu_traffic(kernel: str, summary: str = "k_tiled_sib_triangular2048.md"):
+    """DRAM bytes (read + write) per site of one launch of `kernel`, from the committed
+    ncu summary of the same kernels on a 2048^2 lattice; None if there is none.  The
+    passes stream their fields once, so the traffic scales with the site count."""
+    fn = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(fn):
         return None
-    m = re.search(r"dram_bytes_per_site:\s*([0-9.eE+-]+)", open(fn).read())
+    m = re.search(r"dram_bytes_per_site %s:\s*([0-9.eE+-]+)" % re.escape(kernel), open(fn).read())
     return float(m.group(1)) if m else None
+
+
+# ----------------------------------------------------------------------
+# replicas-only multi-GPU: every rank advances its own replica of the workload
+def replica_stream(rank: int) -> int:
+    """Philox stream of a rank's replica: replicas draw independent noise."""
+    return int(rank)
+
+
+def max_over_ranks(x: float, device, dist: bool) -> float:
+    """The maximum of a per-rank figure (the job's time is its slowest rank's)."""
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist:
+        import torch.distributed as td
+
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(sites: int, steps: int, world: int, seconds: float) -> float:
+    """Whole-job spin-updates/s: every rank advanced `sites` x `steps`."""
+    return sites * steps * world / seconds
 
 
 # ----------------------------------------------------------------------
@@ -342,6 +367,64 @@ def run_adjoint(dev: int, reps: int = 3) -> dict:
             "adjoint_path": "forward and backward sweeps replayed as CUDA graphs"}
 
 
+def run_dipolar(dev: int, steps: int = 50) -> dict:
+    """The dipolar film (128 x 128 x 16 simple cubic, a = 0.25 nm, periodic in-plane,
+    open along z, J + D + K + Zeeman + FFT dipolar on the 128 x 128 x 32 grid, SIB
+    alpha = 0.1, T = 5 K Philox): one system, and 8 systems with their own initial
+    states (seeds 4..11) advanced concurrently on 8 CUDA streams."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import workload
+
+    w = workload("film128x16_dipolar")
+    deck, d = w["deck"], dict(w["dyn"])
+    d.pop("steps")
+    N = deck.nsites
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    systems = []
+    for k in range(8):
+        ham = mj.Hamiltonian(deck, device=dev)
+        sd = mj.SpinDynamics(ham, stream_id=k, **d)
+        m = torch.tensor(mj.random_sphere(N, 4 + k).T.copy(), device=f"cuda:{dev}")
+        systems.append((ham, sd, m, torch.cuda.Stream(device=dev)))
+    lib = _abi.lib
+
+    def run(sys_list, nsteps, concurrent):
+        for ham, sd, m, st in sys_list:
+            s = st.cuda_stream if concurrent else torch.cuda.current_stream().cuda_stream
+            _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(sd.p), nsteps, None, s))
+            sd.p.step0 += nsteps
+
+    def timed(sys_list, concurrent):
+        run(sys_list, 3, concurrent)
+        torch.cuda.synchronize()
+        e0.record()
+        for _, _, _, st in sys_list:
+            st.wait_event(e0)
+        run(sys_list, steps, concurrent)
+        for _, _, _, st in sys_list:
+            torch.cuda.current_stream().wait_stream(st)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    one = timed(systems[:1], False)
+    ham0 = systems[0][0]
+    _abi.check(lib.mj_profile_enable(ham0.plan, 1))
+    run(systems[:1], 5, False)
+    prof = _abi.profile_read(ham0.plan)
+    _abi.check(lib.mj_profile_enable(ham0.plan, 0))
+    eight = timed(systems, True)
+    tot = sum(t for t, _ in prof.values())
+    return {"workload": "film128x16_dipolar", "sites": N, "steps": steps, "fft_grid": [128, 128, 32],
+            "value": N * steps / (one / 1e3), "unit": UNIT, "ms_per_step": one / steps,
+            "batch8": {"value": 8 * N * steps / (eight / 1e3), "ms_per_step": eight / steps,
+                       "path": "8 plans, mj_step_dev on 8 CUDA streams"},
+            "kernel_share": {k: round(t / tot, 4) for k, (t, _) in prof.items()}}
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -360,7 +443,7 @@ def run_gpu(args, rank, world):
     dyn.pop("steps")
     N = deck.nsites
     ham = mj.Hamiltonian(deck, device=dev)
-    sd = mj.SpinDynamics(ham, stream_id=rank, **dyn)
+    sd = mj.SpinDynamics(ham, stream_id=replica_stream(rank), **dyn)
     p = sd.p
     p.energy_mode = _abi.MJ_ENERGY_BEFORE
     m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
@@ -407,11 +490,8 @@ def run_gpu(args, rank, world):
         step(W + K + k)
     prof = _abi.profile_read(ham.plan)
     _abi.check(lib.mj_profile_enable(ham.plan, 0))
-    t = torch.tensor([ms], dtype=torch.float64, device=m.device)
-    if dist:
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = N * K * world / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, m.device, dist)
+    value = job_rate(N, K, world, ms_max / 1e3)
 
     # end to end through the reference-facing C ABI with host buffers (pinned)
     st = mj.SpinState(ham)
@@ -431,10 +511,7 @@ def run_gpu(args, rank, world):
         _ = float(Eh.item())
         if k >= 2:
             times.append(time.perf_counter() - t0)
-    te = torch.tensor([sum(times)], dtype=torch.float64, device=m.device)
-    if dist:
-        td.all_reduce(te, op=td.ReduceOp.MAX)
-    e2e = N * len(times) * world / float(te.item())
+    e2e = job_rate(N, len(times), world, max_over_ranks(sum(times), m.device, dist))
 
     if rank != 0:
         return
@@ -448,10 +525,11 @@ def run_gpu(args, rank, world):
                          "achieved_gbs": (b / (avg / 1e3) / 1e9) if b else None}
     dom = max((k for k in kernels if k in bytes_site), key=lambda k: kernels[k]["avg_us"])
     ach = kernels[dom]["achieved_gbs"]
-    tr = ncu_traffic(dom, args.workload)
+    tr = ncu_traffic(dom)
     cpu = cpu_oracle_rate(args.workload) if (world == 1 and not args.no_cpu_baseline) else None
     batch = run_batch(dev) if (world == 1 and not args.no_batch) else None
     adjoint = run_adjoint(dev) if (world == 1 and not args.no_batch) else None
+    dipolar = run_dipolar(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -478,6 +556,7 @@ def run_gpu(args, rank, world):
         "cpu_baseline": cpu,
         "batch": batch,
         "adjoint": adjoint,
+        "dipolar": dipolar,
     }
     print(json.dumps(line), flush=True)
 
@@ -490,7 +569,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batch and adjoint measurements")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch, adjoint and dipolar measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
