@@ -218,27 +218,23 @@ __device__ __forceinline__ SibGrad sib_vjp(double3 m, double3 p, double3 H, doub
     }
     const double3 pxh = cross(pn, H);
     const double3 h = scl3(hc, make_double3(H.x + alpha * pxh.x, H.y + alpha * pxh.y, H.z + alpha * pxh.z));
-    const double3 d = add3(m, cross(m, h));
-    const double3 hxd = cross(h, d);
-    const double hd = dot(h, d);
-    const double inv = 1.0 / (1.0 + dot(h, h));
-    const double3 y = scl3(inv, make_double3(d.x - hxd.x + hd * h.x, d.y - hxd.y + hd * h.y, d.z - hxd.z + hd * h.z));
-    // y = q/s, s = 1 + h.h
-    const double3 gq = scl3(inv, gy);
-    const double gs = -dot(gy, y) * inv;
-    double3 gh = scl3(2.0 * gs, h);
-    // q = d - h x d + (h.d) h
-    const double hgq = dot(h, gq);
-    const double3 gd = add3(add3(gq, cross(h, gq)), scl3(hgq, h));
-    gh = add3(gh, add3(add3(cross(gq, d), scl3(hd, gq)), scl3(hgq, d)));
-    // d = m + m x h
+    // y = m + c (u + w), u = m x h, w = u x h, c = 2/(1 + h.h)
+    const double3 u = cross(m, h);
+    const double3 w = cross(u, h);
+    const double c = 2.0 / (1.0 + dot(h, h));
     SibGrad r;
-    r.gm = add3(gd, cross(h, gd));
-    gh = add3(gh, cross(gd, m));
+    r.gm = gy;
+    const double gc = dot(gy, add3(u, w));
+    const double3 gw = scl3(c, gy);
+    double3 gu = add3(scl3(c, gy), cross(h, gw));  // w = u x h: u gets h x gw
+    double3 gh = cross(gw, u);                      //            h gets gw x u
+    r.gm = add3(r.gm, cross(h, gu));                // u = m x h: m gets h x gu
+    gh = add3(gh, cross(gu, m));                    //            h gets gu x m
+    gh = add3(gh, scl3(-gc * c * c, h));            // c = 2/s: dc/dh = -c^2 h
     // h = hc (H + alpha p^ x H)
-    const double3 u = scl3(hc * alpha, gh);
-    r.gH = add3(scl3(hc, gh), cross(u, pn));
-    const double3 gpn = cross(H, u);
+    const double3 uu = scl3(hc * alpha, gh);
+    r.gH = add3(scl3(hc, gh), cross(uu, pn));
+    const double3 gpn = cross(H, uu);
     r.gp = norm ? scl3(invn, make_double3(gpn.x - dot(pn, gpn) * pn.x, gpn.y - dot(pn, gpn) * pn.y,
                                           gpn.z - dot(pn, gpn) * pn.z))
                 : gpn;

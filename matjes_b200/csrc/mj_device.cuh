@@ -190,7 +190,8 @@ __device__ __forceinline__ double3 project(double3 t, double3 m) {
 
 // SIB stage (Mentink et al., J. Phys.: Condens. Matter 22, 176001 (2010)):
 // y = m + ((m + y)/2) x a,  h = a/2 = hc (H + alpha p^ x H), hc = -dt/(2 hbar (1+alpha^2)).
-// Closed form: y = (d - h x d + (h.d) h) / (1 + |h|^2), d = m + m x h  (|y| = |m|).
+// Closed form (the Cayley transform of the rotation): y = m + 2/(1+|h|^2) (u + u x h),
+// u = m x h  (|y| = |m|).
 __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, double alpha, double hc) {
     const double np2 = dot(p, p);
     double3 pn = p;
@@ -200,12 +201,10 @@ __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, do
     }
     const double3 pxh = cross(pn, H);
     const double3 h = make_double3(hc * (H.x + alpha * pxh.x), hc * (H.y + alpha * pxh.y), hc * (H.z + alpha * pxh.z));
-    const double3 mxh = cross(m, h);
-    const double3 d = make_double3(m.x + mxh.x, m.y + mxh.y, m.z + mxh.z);
-    const double3 hxd = cross(h, d);
-    const double hd = dot(h, d);
-    const double inv = 1.0 / (1.0 + dot(h, h));
-    return make_double3((d.x - hxd.x + hd * h.x) * inv, (d.y - hxd.y + hd * h.y) * inv, (d.z - hxd.z + hd * h.z) * inv);
+    const double3 u = cross(m, h);
+    const double3 w = cross(u, h);
+    const double c = 2.0 / (1.0 + dot(h, h));
+    return make_double3(fma(c, u.x + w.x, m.x), fma(c, u.y + w.y, m.y), fma(c, u.z + w.z, m.z));
 }
 
 // ---------------------------------------------------------------------------
@@ -228,31 +227,64 @@ __device__ __forceinline__ double total_energy_part(const FieldOut& f, double3 m
 }
 
 // ---------------------------------------------------------------------------
-// Deterministic grid reduction of NV doubles for blocks of 256 threads:
-// per-block partials in block order, summed by the last block to finish;
-// the ticket counter is re-armed by that block.
+// Deterministic grid reduction of NV doubles, in two halves that a caller may
+// also use apart: block_partials writes one partial per block (warp sums in
+// lane order, warps in order), ordered_sum adds nblocks partials in a fixed
+// order (thread-strided sums, warp shuffles, warps in order).  grid_reduce does
+// both in one launch: the last block to take a ticket sums the partials and
+// re-arms the ticket counter.  Blocks of at most 256 threads.
 template <int NV>
-__device__ void grid_reduce(double (&v)[NV], double* partials, unsigned int* counter, double* out, int nblocks) {
-    __shared__ double wsum[NV][8];
-    __shared__ bool last;
+__device__ __forceinline__ void block_partials(double (&v)[NV], double* partials, int nblocks, int bid) {
+    __shared__ double wsum_p[NV][8];
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
     const int nthr = blockDim.x * blockDim.y;
     const int lane = tid & 31, wid = tid >> 5;
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
         double e = v[q];
         for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-        if (lane == 0) wsum[q][wid] = e;
+        if (lane == 0) wsum_p[q][wid] = e;
     }
     __syncthreads();
     if (tid == 0) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
             double s = 0.0;
-            for (int w = 0; w < nthr / 32; ++w) s += wsum[q][w];
+            for (int w = 0; w < nthr / 32; ++w) s += wsum_p[q][w];
             partials[static_cast<int64_t>(q) * nblocks + bid] = s;
         }
+    }
+}
+
+template <int NV>
+__device__ void ordered_sum(const double* partials, int nblocks, double* out) {
+    __shared__ double wsum_o[NV][8];
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0.0;
+        for (int b = tid; b < nblocks; b += nthr) s += __ldcg(partials + static_cast<int64_t>(q) * nblocks + b);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        __syncthreads();
+        if (lane == 0) wsum_o[q][wid] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < nthr / 32; ++w) t += wsum_o[q][w];
+            out[q] = t;
+        }
+    }
+}
+
+template <int NV>
+__device__ void grid_reduce(double (&v)[NV], double* partials, unsigned int* counter, double* out, int nblocks) {
+    __shared__ bool last;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    block_partials<NV>(v, partials, nblocks, bid);
+    if (tid == 0) {
         __threadfence();
         const unsigned int t = atomicAdd(counter, 1u);
         last = (t == static_cast<unsigned int>(nblocks - 1));
@@ -260,20 +292,7 @@ __device__ void grid_reduce(double (&v)[NV], double* partials, unsigned int* cou
     __syncthreads();
     if (!last) return;
     __threadfence();
-#pragma unroll
-    for (int q = 0; q < NV; ++q) {
-        double s = 0.0;
-        for (int b = tid; b < nblocks; b += nthr) s += __ldcg(partials + static_cast<int64_t>(q) * nblocks + b);
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        __syncthreads();
-        if (lane == 0) wsum[q][wid] = s;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < nthr / 32; ++w) t += wsum[q][w];
-            out[q] = t;
-        }
-    }
+    ordered_sum<NV>(partials, nblocks, out);
     if (tid == 0) *counter = 0u;
 }
 

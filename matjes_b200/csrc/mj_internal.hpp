@@ -108,6 +108,7 @@ struct mj_plan {
     int tma_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // persistent grid per tile variant (occupancy x SMs)
     int num_sms = 148;
     int* d_status = nullptr;         // device status word: bit 0 = bounded wait timed out
+    int defer_nblocks = 0;           // energy partials written by the last pass launched with emode 1
     // ELL form (multi-atom cells, COO input): width entries per site
     int ell_width = 0;
     int* d_ell_col = nullptr;        // [width][N], -1 = empty
@@ -197,11 +198,15 @@ constexpr int kTiledVariants = 6;
 constexpr int kTiledVariantTY[kTiledVariants] = {16, 32, 16, 16, 16, 8};  // tile height per variant
 static_assert(kTiledVariants <= static_cast<int>(sizeof(mj_plan::tma_blocks) / sizeof(int)),
               "mj_plan::tma_blocks holds one persistent grid size per tiled variant");
+// emode: energy reduction of the launch (0: into E_out at once; 1: per-block
+// partials only, counted in p->defer_nblocks; 2: block 0 sums the previous
+// pass's partials into E_out)
 mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
-                       double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s);
+                       double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
+                       int emode = 0);
 #define MJ_TILED_SHAPE_DECL(fn)                                                                                   \
     mj_status fn(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,         \
-                 double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s);
+                 double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s, int emode);
 MJ_TILED_SHAPE_DECL(launch_tiled_square_nn)
 MJ_TILED_SHAPE_DECL(launch_tiled_square2)
 MJ_TILED_SHAPE_DECL(launch_tiled_tri_nn)

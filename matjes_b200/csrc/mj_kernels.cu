@@ -495,9 +495,10 @@ namespace {
 bool tiled(const mj_plan* p) { return p->is_stencil && p->sp.shape != 0; }
 
 mj_status tiled_call(mj_plan* p, const char* name, int pass, const DynCoef& c, const double* ms, const double* mn,
-                     double* out, double* aux, double* aux2, DipView Hd, double* E, uint32_t step, cudaStream_t s) {
+                     double* out, double* aux, double* aux2, DipView Hd, double* E, uint32_t step, cudaStream_t s,
+                     int emode = 0) {
     const int rec = prof_begin(p, name, s);
-    mj_status st = launch_tiled(p, pass, c, ms, mn, out, aux, aux2, Hd, E, step, s);
+    mj_status st = launch_tiled(p, pass, c, ms, mn, out, aux, aux2, Hd, E, step, s, emode);
     prof_end(p, rec, s);
     return st;
 }
@@ -518,20 +519,25 @@ mj_status tiled_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uin
     switch (c.integrator) {
         case MJ_EULER:
             return tiled_call(p, "k_euler", 1, c, m, nullptr, m_out, nullptr, nullptr, Hd, E_prev, step, s);
+        // two-pass schemes: pass 1 writes per-block energy partials, the first block
+        // of pass 2 sums them (no ticket or last-block tail in pass 1)
         case MJ_HEUN_MATJES:
-            if ((st = tiled_call(p, "k_heun1", 2, c, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, Hd, E_prev, step, s)) != MJ_OK)
+            if ((st = tiled_call(p, "k_heun1", 2, c, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, Hd, nullptr, step, s,
+                                 E_prev ? 1 : 0)) != MJ_OK)
                 return st;
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            return tiled_call(p, "k_heun2", 3, c, p->d_mid, nullptr, m, p->d_aux, p->d_aux2, Hd, nullptr, step, s);
+            return tiled_call(p, "k_heun2", 3, c, p->d_mid, nullptr, m, p->d_aux, p->d_aux2, Hd, E_prev, step, s,
+                              E_prev ? 2 : 0);
         case MJ_SIB: {
             // Philox draws are made once per step in pass 1 and kept for the corrector
             double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX) ? p->d_aux : nullptr;
-            if ((st = tiled_call(p, "k_sib1", 4, c, m, nullptr, p->d_mid, bstore, nullptr, Hd, E_prev, step, s)) != MJ_OK)
+            if ((st = tiled_call(p, "k_sib1", 4, c, m, nullptr, p->d_mid, bstore, nullptr, Hd, nullptr, step, s,
+                                 E_prev ? 1 : 0)) != MJ_OK)
                 return st;
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            return tiled_call(p, "k_sib2", 5, c, p->d_mid, m, m, bstore, nullptr, Hd, nullptr, step, s);
+            return tiled_call(p, "k_sib2", 5, c, p->d_mid, m, m, bstore, nullptr, Hd, E_prev, step, s, E_prev ? 2 : 0);
         }
         default:
             return set_error(MJ_ERR_ARG, "unknown integrator");

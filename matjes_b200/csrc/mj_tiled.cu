@@ -11,12 +11,13 @@ int64_t tiled_energy_blocks(const mj_plan* p) {
 }
 
 mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
-                       double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s) {
+                       double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
+                       int emode) {
     switch (p->sp.shape) {
-        case kShapeSquareNN: return launch_tiled_square_nn(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s);
-        case kShapeSquare2: return launch_tiled_square2(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s);
-        case kShapeTriNN: return launch_tiled_tri_nn(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s);
-        case kShapeTri3: return launch_tiled_tri3(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s);
+        case kShapeSquareNN: return launch_tiled_square_nn(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode);
+        case kShapeSquare2: return launch_tiled_square2(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode);
+        case kShapeTriNN: return launch_tiled_tri_nn(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode);
+        case kShapeTri3: return launch_tiled_tri3(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode);
         default: return set_error(MJ_ERR_ARG, "no tiled kernel for this stencil shape");
     }
 }

@@ -38,11 +38,15 @@ namespace {
 
 enum { PASS_FIELD = 0, PASS_EULER = 1, PASS_HEUN1 = 2, PASS_HEUN2 = 3, PASS_SIB1 = 4, PASS_SIB2 = 5 };
 
+// Energy reduction of a launch.  mode 0: grid_reduce into `out` (if set);
+// mode 1: write one partial per block, no ticket (the next pass sums them);
+// mode 2: block 0 sums the `nblocks` partials of the previous pass into `out`.
 struct TReduce {
     double* partials;
     unsigned int* counter;
     double* out;
     int nblocks;
+    int mode;
 };
 
 struct TiledArgs {
@@ -136,6 +140,9 @@ struct Pre {
     double3 b;  // SIB2: stored Philox draw;  HEUN2: DT
 };
 
+// The thermal draw of the passes that make one (Euler, Heun predictor, SIB
+// predictor) is part of the prefetch: it depends on neither the tile nor the
+// stencil, so it can run while the tile's halo loads are in flight.
 template <int PASS>
 __device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N) {
     Pre p;
@@ -143,10 +150,12 @@ __device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, in
     p.b = p.a;
     if constexpr (PASS == PASS_SIB2) {
         p.a = make_double3(A.mn[i], A.mn[N + i], A.mn[2 * N + i]);
-        if (C.thermal && A.aux) p.b = ld3(A.aux, i, N);
+        if (C.thermal) p.b = A.aux ? ld3(A.aux, i, N) : thermal_field(C, A.step, i, N);
     } else if constexpr (PASS == PASS_HEUN2) {
         p.a = ld3(A.aux, i, N);
         if (C.thermal) p.b = ld3(A.aux2, i, N);
+    } else if constexpr (PASS == PASS_SIB1 || PASS == PASS_EULER || PASS == PASS_HEUN1) {
+        if (C.thermal) p.b = thermal_field(C, A.step, i, N);
     }
     return p;
 }
@@ -164,7 +173,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         const double c = C.h_over_hbar;
         double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
         if (C.thermal) {
-            const double3 DT = llg_rhs(thermal_field(C, A.step, i, N), m0, C.alpha, C.inv_den);
+            const double3 DT = llg_rhs(pre.b, m0, C.alpha, C.inv_den);
             t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
         }
         st3(A.out, i, N, project(t, m0));
@@ -175,7 +184,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         const double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
         st3(A.out, i, N, project(t, m0));
         st3(A.aux, i, N, D);
-        if (C.thermal) st3(A.aux2, i, N, llg_rhs(thermal_field(C, A.step, i, N), m0, C.alpha, C.inv_den));
+        if (C.thermal) st3(A.aux2, i, N, llg_rhs(pre.b, m0, C.alpha, C.inv_den));
         return total_energy_part(f, m0, hd);
     } else if constexpr (PASS == PASS_HEUN2) {
         const double3 D2 = llg_rhs(B, m0, C.alpha, C.inv_den);
@@ -192,7 +201,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
     } else if constexpr (PASS == PASS_SIB1) {
         double3 H = B;
         if (C.thermal) {
-            const double3 b = thermal_field(C, A.step, i, N);
+            const double3 b = pre.b;
             if (A.aux) st3(A.aux, i, N, b);  // the corrector reuses this step's draw
             H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
         }
@@ -201,10 +210,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         return total_energy_part(f, m0, hd);
     } else {  // PASS_SIB2: m0 is the midpoint, the corrector starts from m_n
         double3 H = B;
-        if (C.thermal) {
-            const double3 b = A.aux ? pre.b : thermal_field(C, A.step, i, N);
-            H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
-        }
+        if (C.thermal) H = make_double3(H.x + pre.b.x, H.y + pre.b.y, H.z + pre.b.z);
         st3(A.out, i, N, sib_solve(pre.a, m0, H, C.alpha, C.sib_hc));
         return 0.0;
     }
@@ -245,10 +251,93 @@ __device__ __forceinline__ void load_tile(const StencilParams& P, const double* 
     }
 }
 
+// The same staging in two halves: the loads into registers, then the stores
+// to shared memory, so that independent work can run while the loads are in
+// flight.  Used when each thread stages at most kMaxStagedPerThread elements.
+constexpr int kMaxStagedPerThread = 3;
+template <class S, int BYT, int RY>
+struct Staged {
+    static constexpr int NT = 32 * BYT;
+    static constexpr int NPT = (TileGeom<S, BYT, RY>::NS + NT - 1) / NT;
+    double v[NPT][3];
+};
+
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void load_tile_issue(const StencilParams& P, const double* ms, int x0, int y0, int z,
+                                                Staged<S, BYT, RY>& st) {
+    using G = TileGeom<S, BYT, RY>;
+    using T = Staged<S, BYT, RY>;
+    const int Lx = P.L[0], Ly = P.L[1];
+    const int64_t layer = static_cast<int64_t>(Lx) * Ly;
+    const int64_t N = layer * P.L[2];
+    const double* mx = ms + layer * z;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < T::NPT; ++k) {
+        const int idx = tid + k * T::NT;
+        double vx = 0.0, vy = 0.0, vz = 0.0;
+        if (idx < G::NS) {
+            const int ly = idx / G::PX;
+            const int lx = idx - ly * G::PX;
+            int gx = x0 + lx - G::RX, gy = y0 + ly - G::R;
+            bool ok = true;
+            if (gx < 0 || gx >= Lx) {
+                if (P.periodic[0]) gx = ((gx % Lx) + Lx) % Lx;
+                else ok = false;
+            }
+            if (gy < 0 || gy >= Ly) {
+                if (P.periodic[1]) gy = ((gy % Ly) + Ly) % Ly;
+                else ok = false;
+            }
+            if (ok) {
+                const int64_t j = gx + static_cast<int64_t>(Lx) * gy;
+                vx = __ldg(mx + j);
+                vy = __ldg(mx + N + j);
+                vz = __ldg(mx + 2 * N + j);
+            }
+        }
+        st.v[k][0] = vx;
+        st.v[k][1] = vy;
+        st.v[k][2] = vz;
+    }
+}
+
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void load_tile_commit(const Staged<S, BYT, RY>& st, double* sm) {
+    using G = TileGeom<S, BYT, RY>;
+    using T = Staged<S, BYT, RY>;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+#pragma unroll
+    for (int k = 0; k < T::NPT; ++k) {
+        const int idx = tid + k * T::NT;
+        if (idx < G::NS) {
+            sm[idx] = st.v[k][0];
+            sm[G::NS + idx] = st.v[k][1];
+            sm[2 * G::NS + idx] = st.v[k][2];
+        }
+    }
+}
+
+// epilogue inputs of the thread's RY sites (see prefetch)
+template <class S, int BYT, int RY, int PASS>
+__device__ __forceinline__ void prefetch_sites(const StencilParams& P, const DynCoef& C, const TiledArgs& A, int x0,
+                                               int y0, int z, Pre* pre) {
+    const int Lx = P.L[0], Ly = P.L[1];
+    const int64_t layer = static_cast<int64_t>(Lx) * Ly;
+    const int64_t N = layer * P.L[2];
+    const int x = x0 + threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+        const int y = y0 + threadIdx.y * RY + r;
+        if (x < Lx && y < Ly) pre[r] = prefetch<PASS>(C, A, layer * z + x + static_cast<int64_t>(Lx) * y, N);
+    }
+}
+
 // stencil + epilogue of one staged tile; returns the energy of its sites
+// (pre_in: the epilogue inputs when the caller prefetched them, else null)
 template <class S, int BYT, int RY, int PASS>
 __device__ __forceinline__ double compute_tile(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
-                                               const double* sm, int x0, int y0, int z) {
+                                               const double* sm, int x0, int y0, int z, const Pre* pre_in = nullptr) {
     using G = TileGeom<S, BYT, RY>;
     const int Lx = P.L[0], Ly = P.L[1];
     const int64_t layer = static_cast<int64_t>(Lx) * Ly;
@@ -256,10 +345,11 @@ __device__ __forceinline__ double compute_tile(const StencilParams& P, const Dyn
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x = x0 + tx;
     Pre pre[RY];
+    if (pre_in) {
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
-        const int y = y0 + ty * RY + r;
-        if (x < Lx && y < Ly) pre[r] = prefetch<PASS>(C, A, layer * z + x + static_cast<int64_t>(Lx) * y, N);
+        for (int r = 0; r < RY; ++r) pre[r] = pre_in[r];
+    } else {
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
     }
     double bx[RY], by[RY], bz[RY];
 #pragma unroll
@@ -303,10 +393,25 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_t[];
     const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY, z = blockIdx.z;
-    load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (A.R.mode == 2 && bid == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
+    Pre pre[RY];
+    if constexpr (Staged<S, BYT, RY>::NPT <= kMaxStagedPerThread) {
+        // halo loads in flight while the epilogue inputs (the thermal draw) are computed
+        Staged<S, BYT, RY> st;
+        load_tile_issue<S, BYT, RY>(P, A.ms, x0, y0, z, st);
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+        load_tile_commit<S, BYT, RY>(st, smem_t);
+    } else {
+        load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+    }
     __syncthreads();
-    const double e = compute_tile<S, BYT, RY, PASS>(P, C, A, smem_t, x0, y0, z);
-    if (A.R.out) {
+    const double e = compute_tile<S, BYT, RY, PASS>(P, C, A, smem_t, x0, y0, z, pre);
+    if (A.R.mode == 1) {
+        double v[1] = {e};
+        block_partials<1>(v, A.R.partials, A.R.nblocks, bid);
+    } else if (A.R.mode == 0 && A.R.out) {
         double v[1] = {e};
         grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
     }
@@ -378,6 +483,7 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tma(const __grid_constant__ 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (A.R.mode == 2 && blockIdx.x == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
     const int ntile = T.count();
     auto origin = [&](int t, int& x0, int& y0, int& z) {
         const int ix = t % T.ntx;
@@ -436,9 +542,16 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tma(const __grid_constant__ 
     if (failed) {
         // let copies still in flight land before the block exits (bounded)
         for (int b = 0; b < 2; ++b) mbar_wait_bounded(&bar[b], phase[b], 1u << 16);
+        if (A.R.mode == 1) {  // keep the partials complete; the status word reports the failure
+            double v[1] = {e};
+            block_partials<1>(v, A.R.partials, A.R.nblocks, blockIdx.x);
+        }
         return;
     }
-    if (A.R.out) {
+    if (A.R.mode == 1) {
+        double v[1] = {e};
+        block_partials<1>(v, A.R.partials, A.R.nblocks, blockIdx.x);
+    } else if (A.R.mode == 0 && A.R.out) {
         double v[1] = {e};
         grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
     }
@@ -471,7 +584,7 @@ struct TiledLauncher {
         }
         const dim3 g = grid(P);
         TileList T{static_cast<int>(g.x), static_cast<int>(g.y), static_cast<int>(g.z)};
-        A.R.nblocks = nblocks;
+        if (A.R.mode != 2) A.R.nblocks = nblocks;  // mode 2 reads the previous pass's partial count
         kern<<<nblocks, dim3(32, BYT), smem, s>>>(map, P, C, A, T);
         return cuda_status(cudaGetLastError(), "k_tma");
     }
@@ -563,7 +676,8 @@ bool make_map(CUtensorMap* map, const double* base, const StencilParams& P, int 
 // the build parallel).  pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
 template <class S>
 mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
-                             double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s) {
+                             double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
+                             int emode) {
     TiledArgs A;
     A.ms = ms;
     A.mn = mn;
@@ -576,6 +690,8 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
     A.R.counter = p->d_counter;
     A.R.out = E_out;
     A.R.nblocks = static_cast<int>(tiled_energy_blocks(p));
+    A.R.mode = emode;
+    if (emode == 2) A.R.nblocks = p->defer_nblocks;  // the partials of the previous pass
     A.step = step;
     A.status = p->d_status;
     return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
@@ -587,10 +703,12 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
                 if (p->tma_blocks[p->tile_variant] <= 0)
                     p->tma_blocks[p->tile_variant] = Launcher::persistent_blocks(p->num_sms);
                 const int nb = static_cast<int>(std::min<int64_t>(p->tma_blocks[p->tile_variant], tiled_energy_blocks(p)));
+                if (emode == 1) p->defer_nblocks = nb;
                 return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, &map,
                                                                                            nb, s);
             }
         }
+        if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
         return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, nullptr, 0, s);
     });
 }

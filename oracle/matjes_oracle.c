@@ -850,7 +850,8 @@ static void euler_update(const double* m, const double* Dint, const double* DT, 
 }
 
 /* SIB stage (Mentink et al. 2010): y = m + ((m + y)/2) x a, a = dt*Omega(p, B+b),
- * Omega = -(H + alpha p^ x H)/((1+alpha^2) hbar).  Closed-form Cayley solve. */
+ * Omega = -(H + alpha p^ x H)/((1+alpha^2) hbar).  Closed-form Cayley solve with
+ * h = a/2: y = m + 2/(1+|h|^2) (u + u x h), u = m x h. */
 static void sib_stage(const double* m, const double* p, const double* B, const double* b,
                       double hc, double alpha, double* y_out, int midpoint, int64_t n) {
 #pragma omp parallel for schedule(static)
@@ -865,15 +866,13 @@ static void sib_stage(const double* m, const double* p, const double* B, const d
         cross3(pn, Ht, pxh);
         double h[3];
         for (int k = 0; k < 3; k++) h[k] = hc * (Ht[k] + alpha * pxh[k]);
-        double mxh[3], d[3], hxd[3];
-        cross3(mi, h, mxh);
-        for (int k = 0; k < 3; k++) d[k] = mi[k] + mxh[k];
-        cross3(h, d, hxd);
-        double hd = h[0] * d[0] + h[1] * d[1] + h[2] * d[2];
+        double u[3], w[3];
+        cross3(mi, h, u);
+        cross3(u, h, w);
         double h2 = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
-        double inv = 1.0 / (1.0 + h2);
+        double c = 2.0 / (1.0 + h2);
         for (int k = 0; k < 3; k++) {
-            double y = (d[k] - hxd[k] + hd * h[k]) * inv;
+            double y = mi[k] + c * (u[k] + w[k]);
             y_out[3 * i + k] = midpoint ? 0.5 * (mi[k] + y) : y;
         }
     }

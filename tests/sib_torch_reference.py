@@ -3,7 +3,7 @@
 Test infrastructure only.  The field is B = -sum_t v_t (H_t + H_t^T) m + zc b,
 with H_t the oracle's coupling matrix (COO, AoS mode index 3 i + c) of a deck
 holding term t alone at value 1; the SIB stage is the closed-form Cayley solve
-of Mentink et al. (2010) as the library evaluates it.
+of Mentink et al. (2010), y = m + 2/(1+|h|^2) (m x h + (m x h) x h).
 """
 from __future__ import annotations
 
@@ -46,10 +46,9 @@ def sib_solve(m, p, H, alpha, hc):
     np2 = (p * p).sum(-1, keepdim=True)
     pn = torch.where(np2 > 1e-16, p / torch.sqrt(np2), p)
     h = hc * (H + alpha * torch.cross(pn, H, dim=-1))
-    d = m + torch.cross(m, h, dim=-1)
-    hd = (h * d).sum(-1, keepdim=True)
-    inv = 1.0 / (1.0 + (h * h).sum(-1, keepdim=True))
-    return (d - torch.cross(h, d, dim=-1) + hd * h) * inv
+    u = torch.cross(m, h, dim=-1)
+    c = 2.0 / (1.0 + (h * h).sum(-1, keepdim=True))
+    return m + c * (u + torch.cross(u, h, dim=-1))
 
 
 def trajectory(m0, terms, b, A, zc, nsteps, timestep, alpha, noise=None):
