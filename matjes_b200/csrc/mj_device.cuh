@@ -161,8 +161,8 @@ __device__ __forceinline__ void st3(double* m, int64_t i, int64_t N, double3 v) 
 }
 
 __device__ __forceinline__ double3 ld_dip(const DipView& v, int x, int y, int z) {
-    const int64_t q = x + static_cast<int64_t>(v.px) * (y + static_cast<int64_t>(v.py) * z);
-    return make_double3(__ldg(v.h + q), __ldg(v.h + v.nk + q), __ldg(v.h + 2 * v.nk + q));
+    const int64_t q = x + static_cast<int64_t>(v.px) * y + v.zs * z;
+    return make_double3(__ldg(v.h + q), __ldg(v.h + v.cs + q), __ldg(v.h + 2 * v.cs + q));
 }
 
 // Matjes LLG right-hand side (solvers/propagator.f90:13-58):

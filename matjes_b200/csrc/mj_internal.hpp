@@ -62,11 +62,12 @@ struct StencilParams {
 };
 
 // Dipolar H on the padded FFT grid (the unpack is fused into the consumers):
-// component c of site (x,y,z) is h[c*nk + x + px*(y + py*z)].
+// component c of site (x,y,z) is h[c*cs + x + px*y + zs*z].
 struct DipView {
     const double* h;
-    int64_t nk;
-    int px, py;
+    int64_t cs;   // component stride
+    int64_t zs;   // z-plane stride
+    int px;       // padded x extent (row stride)
 };
 
 // Dynamics coefficients computed once per call on the host.

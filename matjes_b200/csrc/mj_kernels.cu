@@ -667,8 +667,8 @@ extern "C" mj_status mj_energy_noalloc(const mj_plan* plan, const double* m, dou
     R.nblocks = static_cast<int>(nblocks);
     DipView none;
     none.h = nullptr;
-    none.nk = 0;
-    none.px = none.py = 0;
+    none.cs = none.zs = 0;
+    none.px = 0;
     if (plan->is_stencil) {
         const Launch<StencilField> L = stencil_launch(plan);
         k_field<StencilField><<<L.grid, L.block, 0, s>>>(L.fp, m, none, nullptr, nullptr, R);
