@@ -314,6 +314,19 @@ mj_status mj_batch_energies(mj_batch* b, double* E_host);
 /* Current temperature of every replica (K) and, if accepted != NULL, the
  * accepted-swap count of every ladder pair (l, l+1) (reference Nsuccess). */
 mj_status mj_batch_temperatures(const mj_batch* b, double* T_host, int32_t* accepted);
+/* Field and energy of every replica at the batch's current state: get_eff_field
+ * and H%energy per image as GNEB evaluates them (GNEB/gneb_utils.f90:77-81,
+ * 154-157).  B_dev (device SoA, 3 Ntot, may be NULL) receives the effective
+ * field, with the component along m removed when project != 0 (vec_project,
+ * vector_utils/vector.f90:61-72); E_dev (device, nrep, may be NULL) the energies. */
+mj_status mj_batch_field(mj_batch* b, double* B_dev_soa, double* E_dev, int32_t project, void* stream);
+/* GNEB path tangents of replicas taken as the images of a path (all of one
+ * size), into tau_dev (device SoA, 3 Ntot): mode 0 the energy-weighted tangent
+ * of GNEB/tangent.f90:93-124 from the image energies E_dev (device, nrep), mode 1
+ * the central difference of :163-180; end images take the one-sided
+ * difference; each tangent is projected on the tangent space of its image and
+ * normalised over the image. */
+mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, double* tau_dev_soa, void* stream);
 /* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
  * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);

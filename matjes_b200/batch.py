@@ -107,6 +107,27 @@ class ReplicaBatch:
                                      None, stream))
         p.step0 += int(steps_per_graph) * int(nreplay)
 
+    def field(self, project: bool = False, energies: bool = True):
+        """Effective field of every replica at the current state (device (3, Ntot)),
+        optionally with the component along m removed, and the replica energies."""
+        import torch
+
+        dev = f"cuda:{self.device}"
+        B = torch.empty((3, self.N), dtype=torch.float64, device=dev)
+        E = torch.empty(self.nrep, dtype=torch.float64, device=dev) if energies else None
+        check(lib.mj_batch_field(self.handle, ptr(B), ptr(E), int(bool(project)), None))
+        return B, E
+
+    def gneb_tangent(self, E=None, mode: str = "energy"):
+        """Path tangents with the replicas as the images of a path (device (3, Ntot)):
+        mode 'energy' (energy-weighted, needs the image energies E) or 'central'."""
+        import torch
+
+        tau = torch.empty((3, self.N), dtype=torch.float64, device=f"cuda:{self.device}")
+        m = {"energy": 0, "central": 1}[mode]
+        check(lib.mj_batch_gneb_tangent(self.handle, ptr(E), m, ptr(tau), None))
+        return tau
+
     def energies(self) -> np.ndarray:
         out = np.empty(self.nrep)
         check(lib.mj_batch_energies(self.handle, ptr(out)))

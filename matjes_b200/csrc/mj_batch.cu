@@ -50,9 +50,10 @@ struct BatchArgs {
     double* tile_e;     // per-tile energy, null = none
     uint32_t step;
     double dt;          // SIB timestep (fs); sigma = sqrt(alpha kT hbar / dt) per replica
+    int project;        // field pass: remove the component along m (B - (B.m) m)
 };
 
-enum { BPASS_ENERGY = 0, BPASS_SIB1 = 4, BPASS_SIB2 = 5 };
+enum { BPASS_ENERGY = 0, BPASS_FIELD = 1, BPASS_SIB1 = 4, BPASS_SIB2 = 5 };
 
 template <class S, int BYT, int RY>
 __device__ __forceinline__ void load_tile_b(const StencilParams& P, const BatchRep& R, const double* ms, int64_t Ntot,
@@ -136,6 +137,14 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
             const double3 zero = make_double3(0.0, 0.0, 0.0);
             if constexpr (PASS == BPASS_ENERGY) {
                 e += total_energy_part(f, m0, zero);
+            } else if constexpr (PASS == BPASS_FIELD) {
+                e += total_energy_part(f, m0, zero);
+                double3 Bv = f.B;
+                if (A.project) {
+                    const double d = dot(Bv, m0);
+                    Bv = make_double3(Bv.x - d * m0.x, Bv.y - d * m0.y, Bv.z - d * m0.z);
+                }
+                st3(A.out, i, Nt, Bv);
             } else if constexpr (PASS == BPASS_SIB1) {
                 e += total_energy_part(f, m0, zero);
                 double3 H = f.B;
@@ -232,6 +241,93 @@ __global__ void k_pt_swap(BatchRep* reps, int* image, const double* slot_kT, int
     }
 }
 
+// GNEB path tangents (GNEB/tangent.f90): for image r with neighbours r-1, r+1
+// tau = wp (m_{r+1} - m_r) + wm (m_r - m_{r-1}), projected on the tangent space
+// of m_r (vec_project, vector_utils/vector.f90:61-72) and normalised over the
+// image.  mode 0 (lattice_special, :93-124, doi:10.1016/j.cpc.2015.07.001):
+// the energy-weighted tangent of interior images; mode 1 (lattice_single,
+// :163-180): m_{r+1} - m_{r-1}.  End images take the one-sided difference.
+__device__ __forceinline__ void gneb_weights(const double* E, int r, int nrep, int mode, double& wp, double& wm) {
+    if (r == 0) {
+        wp = 1.0;
+        wm = 0.0;
+        return;
+    }
+    if (r == nrep - 1) {
+        wp = 0.0;
+        wm = 1.0;
+        return;
+    }
+    if (mode == 1) {
+        wp = wm = 1.0;
+        return;
+    }
+    const double u1 = E[r - 1], u2 = E[r], u3 = E[r + 1];
+    if (u3 > u2 && u2 > u1) {
+        wp = 1.0;
+        wm = 0.0;
+    } else if (u1 > u2 && u2 > u3) {
+        wp = 0.0;
+        wm = 1.0;
+    } else {
+        double dmax = fabs(u3 - u2), dmin = fabs(u1 - u2);
+        if (dmax < dmin) {
+            const double t = dmax;
+            dmax = dmin;
+            dmin = t;
+        }
+        if (u3 > u1) {
+            wp = dmax;
+            wm = dmin;
+        } else {
+            wp = dmin;
+            wm = dmax;
+        }
+    }
+}
+
+// unnormalised projected tangents; partial |tau|^2 per (image, block)
+__global__ void __launch_bounds__(256) k_gneb_tau(const double* __restrict__ m, int64_t n, int64_t Ntot, int nrep,
+                                                  const double* __restrict__ E, int mode, double* __restrict__ tau,
+                                                  double* __restrict__ part) {
+    const int r = blockIdx.y;
+    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double wp, wm;
+    gneb_weights(E, r, nrep, mode, wp, wm);
+    double q = 0.0;
+    if (li < n) {
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        const double3 m0 = ld3(m, i, Ntot);
+        const double3 mp = r + 1 < nrep ? ld3(m, i + n, Ntot) : m0;
+        const double3 mm = r > 0 ? ld3(m, i - n, Ntot) : m0;
+        double3 t = make_double3(wp * (mp.x - m0.x) + wm * (m0.x - mm.x), wp * (mp.y - m0.y) + wm * (m0.y - mm.y),
+                                 wp * (mp.z - m0.z) + wm * (m0.z - mm.z));
+        const double d = dot(t, m0);
+        t = make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
+        st3(tau, i, Ntot, t);
+        q = dot(t, t);
+    }
+    double v[1] = {q};
+    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
+}
+
+// per image: the ordered sum of its partials, then tau /= sqrt(sum)
+__global__ void __launch_bounds__(256) k_gneb_norm(double* __restrict__ tau, int64_t n, int64_t Ntot,
+                                                   const double* __restrict__ part, int nblk) {
+    const int r = blockIdx.x;
+    __shared__ double tot;
+    if (threadIdx.x == 0) tot = 0.0;
+    ordered_sum<1>(part + static_cast<int64_t>(r) * nblk, nblk, &tot);
+    __syncthreads();
+    const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+    for (int64_t li = threadIdx.x; li < n; li += blockDim.x) {
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        tau[i] *= inv;
+        tau[Ntot + i] *= inv;
+        tau[2 * Ntot + i] *= inv;
+    }
+}
+
 template <class S, int BYT, int RY>
 struct BatchLauncher {
     using G = TileGeom<S, BYT, RY>;
@@ -246,6 +342,7 @@ struct BatchLauncher {
         switch (ps) {
             case BPASS_SIB1: return launch<BPASS_SIB1>(P, C, A, nblocks, s);
             case BPASS_SIB2: return launch<BPASS_SIB2>(P, C, A, nblocks, s);
+            case BPASS_FIELD: return launch<BPASS_FIELD>(P, C, A, nblocks, s);
             default: return launch<BPASS_ENERGY>(P, C, A, nblocks, s);
         }
     }
@@ -306,6 +403,7 @@ struct mj_batch {
     int* d_accept = nullptr;
     uint32_t* d_stepctr = nullptr;
     double* d_stage = nullptr;
+    double* d_gneb_part = nullptr;    // tangent norms: one partial per (image, block)
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::string graph_key;
@@ -331,6 +429,7 @@ void batch_free(mj_batch* b) {
     cudaFree(b->d_accept);
     cudaFree(b->d_stepctr);
     cudaFree(b->d_stage);
+    cudaFree(b->d_gneb_part);
     delete b;
 }
 
@@ -417,6 +516,7 @@ BatchArgs batch_args(mj_batch* b, uint32_t step, double dt) {
     A.tile_e = nullptr;
     A.step = step;
     A.dt = dt;
+    A.project = 0;
     return A;
 }
 
@@ -702,6 +802,44 @@ mj_status mj_batch_temperatures(const mj_batch* b, double* T_host, int32_t* acce
     if (accepted)
         return cuda_status(cudaMemcpy(accepted, b->d_accept, sizeof(int) * b->nrep, cudaMemcpyDeviceToHost), "accepts");
     return MJ_OK;
+}
+
+mj_status mj_batch_field(mj_batch* b, double* B_dev, double* E_dev, int32_t project, void* stream) {
+    if (!b || (!B_dev && !E_dev)) return set_error(MJ_ERR_ARG, "null argument");
+    cudaSetDevice(b->device);
+    DynCoef c;
+    std::memset(&c, 0, sizeof(c));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    BatchArgs A = batch_args(b, 0, 0.0);
+    A.out = B_dev;
+    A.project = project ? 1 : 0;
+    A.tile_e = b->d_tile_e;
+    mj_status st = batch_pass(b->shape, b->variant, B_dev ? BPASS_FIELD : BPASS_ENERGY, b->sp, c, A, batch_blocks(b), s);
+    if (st != MJ_OK) return st;
+    if (E_dev) {
+        k_batch_energy<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, E_dev);
+        return cuda_status(cudaGetLastError(), "k_batch_energy");
+    }
+    return MJ_OK;
+}
+
+mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, double* tau_dev, void* stream) {
+    if (!b || !tau_dev || (mode == 0 && !E_dev) || mode < 0 || mode > 1) return set_error(MJ_ERR_ARG, "bad tangent arguments");
+    for (int r = 1; r < b->nrep; ++r)
+        if (b->reps[r].Lx != b->reps[0].Lx || b->reps[r].Ly != b->reps[0].Ly)
+            return set_error(MJ_ERR_UNSUPPORTED, "path tangents need images of one size");
+    cudaSetDevice(b->device);
+    const int64_t n = b->Ntot / b->nrep;
+    const int nblk = static_cast<int>((n + 255) / 256);
+    mj_status st;
+    if (!b->d_gneb_part &&
+        (st = cuda_status(cudaMalloc(&b->d_gneb_part, sizeof(double) * nblk * b->nrep), "tangent partials")) != MJ_OK)
+        return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_gneb_tau<<<dim3(nblk, b->nrep), 256, 0, s>>>(b->d_m, n, b->Ntot, b->nrep, E_dev, mode, tau_dev, b->d_gneb_part);
+    if ((st = cuda_status(cudaGetLastError(), "k_gneb_tau")) != MJ_OK) return st;
+    k_gneb_norm<<<b->nrep, 256, 0, s>>>(tau_dev, n, b->Ntot, b->d_gneb_part, nblk);
+    return cuda_status(cudaGetLastError(), "k_gneb_norm");
 }
 
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm) {

@@ -236,3 +236,83 @@ def test_full_replica_workload_properties():
         mj.SpinDynamics(mj.Hamiltonian(deck), integrator="sib", timestep=d["timestep"], alpha=d["alpha"],
                         temperature=T[r], noise="philox", seed=d["seed"], stream_id=r).run(m, 200)
         assert np.abs(batch.replica(out, r) - m).max() <= 1e-13
+
+
+def test_batch_field_and_energies_of_every_replica():
+    """mj_batch_field: each replica's effective field and energy equal its own
+    plan's get_eff_field / energy and the oracle's (the GNEB per-image call,
+    GNEB/gneb_utils.f90:77-81); the projected field is B - (B.m) m."""
+    import matjes_b200 as mj
+
+    cell, B, decks = CASES["square_mixed"]()
+    ms = _initial(decks, 31)
+    batch = mj.ReplicaBatch(cell, [d.L[:2] for d in decks], B, TEMPS["square_mixed"])
+    batch.upload(np.concatenate(ms))
+    Bb, Eb = batch.field(project=False)
+    Bp, _ = batch.field(project=True, energies=False)
+    Bb = Bb.cpu().numpy().T
+    Bp = Bp.cpu().numpy().T
+    Eb = Eb.cpu().numpy()
+    for r, deck in enumerate(decks):
+        ref = mj.Hamiltonian(deck).get_eff_field(ms[r])
+        got = batch.replica(Bb, r)
+        assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
+        Bo, _ = O.Model(deck).field(ms[r])
+        assert np.abs(got - Bo).max() <= 1e-12 * np.abs(Bo).max()
+        Eo = O.Model(deck).energy(ms[r])
+        assert abs(Eb[r] - Eo) <= E_TOL * abs(Eo)
+        proj = got - np.sum(got * ms[r], axis=1, keepdims=True) * ms[r]
+        assert np.abs(batch.replica(Bp, r) - proj).max() <= 1e-15 * np.abs(ref).max()
+
+
+def _tangent_reference(images, E, r, mode):
+    """GNEB/tangent.f90: lattice_special (:93-124) or lattice_single (:163-180),
+    then vec_project on the image and normalisation over the image."""
+    nim = len(images)
+    m = images[r]
+    if r == 0:
+        tau = images[1] - m
+    elif r == nim - 1:
+        tau = m - images[r - 1]
+    elif mode == "central":
+        tau = images[r + 1] - images[r - 1]
+    else:
+        u1, u2, u3 = E[r - 1], E[r], E[r + 1]
+        taup, taum = images[r + 1] - m, m - images[r - 1]
+        if u3 > u2 > u1:
+            tau = taup
+        elif u1 > u2 > u3:
+            tau = taum
+        else:
+            dmax, dmin = abs(u3 - u2), abs(u1 - u2)
+            if dmax < dmin:
+                dmax, dmin = dmin, dmax
+            tau = dmax * taup + dmin * taum if u3 > u1 else dmin * taup + dmax * taum
+    tau = tau - np.sum(tau * m, axis=1, keepdims=True) * m
+    return tau / np.sqrt(np.sum(tau * tau))
+
+
+@pytest.mark.parametrize("mode", ["energy", "central"])
+def test_gneb_tangents_follow_the_reference(mode):
+    import matjes_b200 as mj
+
+    nim, L = 7, (24, 20)
+    cell, B, decks = _square_batch([L] * nim, [0.3] * nim, [0.0] * nim)
+    # a path from +z to a rotated state through random intermediate images
+    rng = np.random.default_rng(41)
+    n = L[0] * L[1]
+    a = np.tile([0.0, 0.0, 1.0], (n, 1))
+    b = mj.random_sphere(n, 42)
+    images = []
+    for k in range(nim):
+        t = k / (nim - 1)
+        v = (1 - t) * a + t * b + 0.05 * rng.standard_normal((n, 3))
+        images.append(v / np.linalg.norm(v, axis=1, keepdims=True))
+    batch = mj.ReplicaBatch(cell, [L] * nim, B, [0.0] * nim)
+    batch.upload(np.concatenate(images))
+    _, E = batch.field()
+    tau = batch.gneb_tangent(E, mode=mode).cpu().numpy().T
+    Eh = E.cpu().numpy()
+    for r in range(nim):
+        ref = _tangent_reference(images, Eh, r, mode)
+        assert np.abs(batch.replica(tau, r) - ref).max() <= 1e-13, r
