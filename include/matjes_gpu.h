@@ -240,6 +240,33 @@ mj_status mj_measure_temperature(mj_plan* plan, const mj_state* st, double* T_ho
 mj_status mj_philox_normals(uint64_t seed, uint32_t step, uint32_t stream_id, int64_t n,
                             double* out_dev_soa, void* stream);
 
+/* ---- energy minimisation (solvers/minimize.F90) --------------------------- */
+/* min_input of IO-input/minimize_io.f90:6-12: `timestep`, `masse`,
+ * `convergence_criteria`; the host looks at the convergence flag every
+ * `check_every` iterations (the reference prints every `min_Efreq`). */
+typedef struct {
+    double timestep;
+    double mass;
+    double conv_torque;
+    int32_t check_every;
+} mj_min_params;
+/* minimize_run (solvers/minimize.F90:57-166) on the device spins, in place:
+ * velocity projection on the damping force F = B - (m.B) m, the first predictor
+ * unnormalised and later moves keeping each spin's norm, as in the reference.
+ * Stops after max_iter iterations or when the largest |F| drops below
+ * conv_torque; returns the iterations run and that torque.  Any plan. */
+mj_status mj_minimize(mj_plan* plan, double* m_dev_soa, const mj_min_params* p, int64_t max_iter,
+                      int64_t* iterations, double* max_torque, void* stream);
+/* minimize_infdamp_run (solvers/minimize.F90:169-258): every spin turned onto
+ * its normalised local field; the sites are visited colour by colour (colours
+ * (x mod cx) + cx((y mod cy) + cy(z mod cz)) returned in colors[3], chosen so
+ * that no coupling joins two sites of one colour) instead of in site order.
+ * The torque is the largest component of m x B^.  Single-atom stencil plans
+ * without the dipolar term; MJ_ERR_ARG when a site's field is below 1e-8 (the
+ * reference stops there). */
+mj_status mj_minimize_infdamp(mj_plan* plan, double* m_dev_soa, const mj_min_params* p, int64_t max_iter,
+                              int64_t* iterations, double* max_torque, int32_t* colors, void* stream);
+
 /* ---- reverse mode (adjoint) ---------------------------------------------- */
 /* The reference has no derivative code: these entries have no counterpart in
  * it.  They differentiate its forward map, the SIB step of the dynamics

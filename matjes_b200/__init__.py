@@ -9,9 +9,9 @@ libmatjes_b200.so (``python matjes_b200/build.py``); there is no CPU fallback.
 """
 from ._abi import MatjesError, lib  # noqa: F401  (loads the CUDA library or raises)
 from .deck import Deck, random_sphere, reversed_disks, square_film, triangular, workload  # noqa: F401
-from .hamiltonian import Hamiltonian, SpinDynamics, SpinState  # noqa: F401
+from .hamiltonian import Hamiltonian, SpinDynamics, SpinState, minimize  # noqa: F401
 from .batch import ReplicaBatch  # noqa: F401
 from .adjoint import SIBTrajectory, deck_terms, field_vjp  # noqa: F401
 
-__all__ = ["Deck", "Hamiltonian", "SpinDynamics", "SpinState", "ReplicaBatch", "SIBTrajectory", "MatjesError", "workload", "square_film",
+__all__ = ["Deck", "Hamiltonian", "SpinDynamics", "SpinState", "ReplicaBatch", "SIBTrajectory", "minimize", "MatjesError", "workload", "square_film",
            "triangular", "random_sphere", "reversed_disks"]

@@ -86,6 +86,11 @@ class DynParams(C.Structure):
     ]
 
 
+class MinParams(C.Structure):
+    _fields_ = [("timestep", C.c_double), ("mass", C.c_double), ("conv_torque", C.c_double),
+                ("check_every", C.c_int32)]
+
+
 MJ_ENERGY_AFTER = 0
 MJ_ENERGY_BEFORE = 1
 
@@ -138,6 +143,10 @@ SIGNATURES = {
     "mj_profile_read": (C.c_int32, [P, C.c_int32, P, P, P, C.POINTER(C.c_int32)]),
     "mj_measure_temperature": (C.c_int32, [P, P, DP]),
     "mj_philox_normals": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, P, P]),
+    "mj_minimize": (C.c_int32, [P, P, C.POINTER(MinParams), C.c_int64, C.POINTER(C.c_int64),
+                                C.POINTER(C.c_double), P]),
+    "mj_minimize_infdamp": (C.c_int32, [P, P, C.POINTER(MinParams), C.c_int64, C.POINTER(C.c_int64),
+                                        C.POINTER(C.c_double), P, P]),
     "mj_plan_nterms": (C.c_int32, [P, C.POINTER(C.c_int32)]),
     "mj_plan_set_terms": (C.c_int32, [P, P]),
     "mj_field_vjp": (C.c_int32, [P, P, P, P, P, P, P]),

@@ -232,3 +232,21 @@ class SpinDynamics:
             check(lib.mj_step_host(self.ham.plan, ptr(m), C.byref(self.p), int(nsteps), ptr(E)))
         self.p.step0 += int(nsteps)
         return E
+
+
+def minimize(ham: Hamiltonian, m, method: str = "vpo", timestep: float = 0.1, mass: float = 1.0,
+             conv_torque: float = 1e-6, max_iter: int = 100000, check_every: int = 100):
+    """Energy minimisation on the device (solvers/minimize.F90): method 'vpo'
+    (minimize_run, velocity projection) or 'infdamp' (minimize_infdamp_run,
+    spins turned onto their local field, colour by colour).  m: a CUDA (3, N)
+    tensor, updated in place.  Returns (iterations, max torque[, colours])."""
+    assert _is_torch(m) and m.is_contiguous() and m.shape == (3, ham.N)
+    p = _abi.MinParams(float(timestep), float(mass), float(conv_torque), int(check_every))
+    it, mt = C.c_int64(), C.c_double()
+    if method == "vpo":
+        check(lib.mj_minimize(ham.plan, ptr(m), C.byref(p), int(max_iter), C.byref(it), C.byref(mt), _stream(m)))
+        return it.value, mt.value
+    colors = np.zeros(3, np.int32)
+    check(lib.mj_minimize_infdamp(ham.plan, ptr(m), C.byref(p), int(max_iter), C.byref(it), C.byref(mt),
+                                  colors.ctypes.data, _stream(m)))
+    return it.value, mt.value, tuple(int(c) for c in colors)

@@ -942,3 +942,114 @@ int orc_run(const orc_model* M, const orc_dyn* d, double* m, int nsteps, double*
     free(B); free(D1); free(D2); free(DT); free(b); free(mt); free(Dint);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Minimisation drivers (solvers/minimize.F90)                          */
+
+/* field of one site from the current spins (the single-site counterpart of
+ * field_impl; no dipolar term): B_s = -(H + H^T) m |_s - zee b */
+static void site_field(const orc_model* M, const double* m, int64_t s, double* B) {
+    int nm = M->nmag;
+    int64_t cell = s / nm;
+    int a = (int)(s % nm);
+    for (int k = 0; k < 3; k++) {
+        int64_t r = 3 * s + k;
+        double hm = 0.0, htm = 0.0;
+        for (int64_t j = M->rowptr[r]; j < M->rowptr[r + 1]; j++) hm += M->val[j] * m[M->col[j]];
+        for (int64_t j = M->trowptr[r]; j < M->trowptr[r + 1]; j++) htm += M->tval[j] * m[M->tcol[j]];
+        double bz = M->in.zeeman_on ? M->zee[a] * M->bfield[3 * cell + k] : 0.0;
+        B[k] = -(bz + (htm + hm));
+    }
+}
+
+/* minimize_run (solvers/minimize.F90:57-166): velocity projection.  The first
+ * predictor (euler_minimization with dt^2 and 2 mass, solvers/solver.f90:129-138)
+ * is not normalised; later steps keep each spin's norm (euler_o2_minimization,
+ * :140-160; a spin whose predictor is shorter than 1e-8 becomes 0).  Returns the
+ * iterations run and the last maximum torque |F_i|. */
+int orc_minimize_vpo(const orc_model* M, double* m, double dt, double mass, double conv_torque, int64_t niter,
+                     int64_t* iters, double* max_torque) {
+    int64_t n3 = M->n3, N = M->nsite;
+    double* B = (double*)malloc(sizeof(double) * n3);
+    double* force = (double*)calloc((size_t)n3, sizeof(double));
+    double* vel = (double*)calloc((size_t)n3, sizeof(double));
+    if (!B || !force || !vel) { free(B); free(force); free(vel); return -1; }
+    orc_field(M, m, B, NULL);
+    for (int64_t i = 0; i < N; i++) {
+        const double* mi = m + 3 * i;
+        double d = mi[0] * B[3 * i] + mi[1] * B[3 * i + 1] + mi[2] * B[3 * i + 2];
+        for (int k = 0; k < 3; k++) force[3 * i + k] = -(mi[k] * d - B[3 * i + k]);   /* damping_2V */
+    }
+    for (int64_t r = 0; r < n3; r++) m[r] = force[r] * (dt * dt) / (mass * 2.0) + m[r];
+    int64_t it = 0;
+    double maxt = 0.0;
+    for (it = 1; it <= niter; it++) {
+        orc_field(M, m, B, NULL);
+        double dumy = 0.0, fnorm = 0.0;
+        for (int64_t i = 0; i < N; i++) {
+            const double* mi = m + 3 * i;
+            double d = mi[0] * B[3 * i] + mi[1] * B[3 * i + 1] + mi[2] * B[3 * i + 2];
+            double F[3], V[3];
+            for (int k = 0; k < 3; k++) F[k] = -(mi[k] * d - B[3 * i + k]);
+            for (int k = 0; k < 3; k++) V[k] = (force[3 * i + k] + F[k]) / 2.0 * dt / mass + vel[3 * i + k];
+            for (int k = 0; k < 3; k++) { force[3 * i + k] = F[k]; vel[3 * i + k] = V[k]; }
+            dumy += V[0] * F[0] + V[1] * F[1] + V[2] * F[2];
+            fnorm += F[0] * F[0] + F[1] * F[1] + F[2] * F[2];
+        }
+        for (int64_t r = 0; r < n3; r++) vel[r] = fabs(dumy) > 1e-8 ? dumy * force[r] / fnorm : 0.0;
+        maxt = 0.0;
+        for (int64_t i = 0; i < N; i++) {
+            double s[3];
+            for (int k = 0; k < 3; k++)
+                s[k] = force[3 * i + k] * (dt * dt) / mass / 2.0 + vel[3 * i + k] * dt + m[3 * i + k];
+            double ni = nrm3(m + 3 * i), nf = nrm3(s);
+            for (int k = 0; k < 3; k++) m[3 * i + k] = nf > 1e-8 ? s[k] / nf * ni : 0.0;
+            double t = nrm3(force + 3 * i);
+            if (t > maxt) maxt = t;
+        }
+        if (conv_torque > maxt) break;
+    }
+    if (iters) *iters = it > niter ? niter : it;
+    if (max_torque) *max_torque = maxt;
+    free(B); free(force); free(vel);
+    return 0;
+}
+
+/* minimize_infdamp_run (solvers/minimize.F90:169-258): every spin is turned onto
+ * its normalised local field, the field recomputed from the current neighbours.
+ * colors[3] = {1,1,1}: the reference's site order; otherwise the sites of colour
+ * (x mod cx) + cx ((y mod cy) + cy (z mod cz)) are visited colour by colour in
+ * site order (the order the GPU sweeps).  Returns -2 on a field shorter than 1e-8. */
+int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int64_t niter, const int colors[3],
+                         int64_t* iters, double* max_torque) {
+    const int cx = colors[0], cy = colors[1], cz = colors[2];
+    const int ncol = cx * cy * cz;
+    const int* L = M->in.lat.L;
+    int nm = M->nmag;
+    int64_t it = 0;
+    double maxt = 0.0;
+    for (it = 1; it <= niter; it++) {
+        maxt = 0.0;
+        for (int col = 0; col < ncol; col++)
+            for (int64_t s = 0; s < M->nsite; s++) {
+                int64_t cell = s / nm;
+                int x = (int)(cell % L[0]), y = (int)((cell / L[0]) % L[1]), z = (int)(cell / ((int64_t)L[0] * L[1]));
+                if ((x % cx) + cx * ((y % cy) + cy * (z % cz)) != col) continue;
+                double B[3];
+                site_field(M, m, s, B);
+                double bn = nrm3(B);
+                if (bn < 1e-8) return -2;
+                for (int k = 0; k < 3; k++) B[k] = B[k] / bn;
+                double t[3];
+                cross3(m + 3 * s, B, t);
+                double tt = fmax(fabs(t[0]), fmax(fabs(t[1]), fabs(t[2])));
+                if (tt > maxt) maxt = tt;
+                if (nrm3(m + 3 * s) > 1e-8)
+                    for (int k = 0; k < 3; k++) m[3 * s + k] = B[k];
+            }
+        if (maxt < conv_torque) break;
+    }
+    if (iters) *iters = it > niter ? niter : it;
+    if (max_torque) *max_torque = maxt;
+    return 0;
+}

@@ -113,6 +113,11 @@ void orc_dip_nrep(const orc_model* m, int nrep[3]);
 void orc_field(const orc_model* m, const double* mvec, double* B, double* e_site);
 /* Total energy H%energy(lat) (eV, not divided by N). */
 double orc_energy(const orc_model* m, const double* mvec);
+/* Minimisation drivers (solvers/minimize.F90:57-166 and :169-258), see matjes_oracle.c. */
+int orc_minimize_vpo(const orc_model* M, double* m, double dt, double mass, double conv_torque, int64_t niter,
+                     int64_t* iters, double* max_torque);
+int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int64_t niter, const int colors[3],
+                         int64_t* iters, double* max_torque);
 /* Field contributions split: MM only, Zeeman only, dipolar only (for tests). */
 void orc_field_terms(const orc_model* m, const double* mvec, double* B_mm, double* B_zee, double* B_dip);
 /* Explicit O(N^2) dipolar field (get_dipolar, mag_dip_fft F). */

@@ -208,6 +208,37 @@ class Model:
         return E
 
 
+def _minimize_bind():
+    lib.orc_minimize_vpo.restype = C.c_int
+    lib.orc_minimize_vpo.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int64,
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    lib.orc_minimize_infdamp.restype = C.c_int
+    lib.orc_minimize_infdamp.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_int64, C.c_void_p,
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+
+
+def minimize_vpo(model, m, dt, mass, conv_torque, niter):
+    """solvers/minimize.F90:57-166 on m (N,3) in place; returns (iterations, max torque)."""
+    _minimize_bind()
+    it, mt = C.c_int64(), C.c_double()
+    rc = lib.orc_minimize_vpo(model.h, _p(m), dt, mass, conv_torque, int(niter), C.byref(it), C.byref(mt))
+    if rc != 0:
+        raise RuntimeError("oracle minimisation failed")
+    return it.value, mt.value
+
+
+def minimize_infdamp(model, m, conv_torque, niter, colors=(1, 1, 1)):
+    """solvers/minimize.F90:169-258 on m (N,3) in place, in site order (colors 1 1 1)
+    or colour by colour; returns (iterations, max torque)."""
+    _minimize_bind()
+    c = np.ascontiguousarray(colors, np.int32)
+    it, mt = C.c_int64(), C.c_double()
+    rc = lib.orc_minimize_infdamp(model.h, _p(m), conv_torque, int(niter), c.ctypes.data, C.byref(it), C.byref(mt))
+    if rc != 0:
+        raise RuntimeError(f"oracle infinite-damping minimisation failed ({rc})")
+    return it.value, mt.value
+
+
 def philox_normals(seed, step, stream, site0, n):
     out = np.empty((n, 3))
     lib.orc_philox_normals(seed, step, stream, site0, n, _p(out))
