@@ -108,3 +108,26 @@ def test_minimisers_reject_what_they_cannot_run():
     assert st == _abi.MJ_ERR_UNSUPPORTED
     p0 = _abi.MinParams(0.1, 0.0, 1e-6, 10)
     assert _abi.lib.mj_minimize(ham.plan, m.data_ptr(), C.byref(p0), 5, C.byref(it), C.byref(mt), None) == _abi.MJ_ERR_ARG
+
+
+def test_run_from_a_reference_input_directory(tmp_path):
+    """An input directory in the reference's format (input deck + magnetic_init.dat)
+    runs on the GPU and writes EM.dat and magnetic_final.dat; the final state is the
+    oracle's SIB trajectory of the same deck."""
+    from matjes_b200 import reference_io as R
+    from matjes_b200.deck import random_sphere
+    from tests.test_reference_io import DECK
+
+    (tmp_path / "input").write_text(DECK)
+    ri = R.parse_input(DECK)
+    m0 = random_sphere(ri.deck.nsites, 17)
+    R.write_order_file(str(tmp_path / "magnetic_init.dat"), m0)
+    mT, lines = R.run_dynamics(str(tmp_path))
+    assert (tmp_path / "EM.dat").exists() and (tmp_path / "magnetic_final.dat").exists()
+    assert len(lines) == 1 + 3   # header + steps 1, 11, 21 (Efreq 10, duration 30)
+    m_init = R.read_order_file(str(tmp_path / "magnetic_init.dat"), ri.deck.nsites)
+    mo = m_init.copy()
+    O.Model(ri.deck).run(mo, 30, integrator="sib", timestep=0.1, alpha=0.3)
+    assert np.abs(mT - mo).max() < 1e-9
+    back = R.read_order_file(str(tmp_path / "magnetic_final.dat"), ri.deck.nsites)
+    assert np.abs(back - mT).max() < 1e-15
