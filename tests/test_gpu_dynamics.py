@@ -231,3 +231,24 @@ def test_bad_arguments_return_status_not_crash():
     with pytest.raises(mj.MatjesError):
         mj.Hamiltonian(mj.Deck(L=(4, 4, 1), periodic=(1, 1, 0), areal=np.eye(3),
                                atoms=[((0, 0, 0), 1, 2.0), ((0.5, 0.5, 0), 1, 1.0)], J=[(1, 1, 1, 1e-3)], dip=True))
+
+
+@pytest.mark.parametrize("integrator", ["sib", "heun"])
+def test_full_size_thermal_trajectory_matches_oracle(integrator):
+    """The bench workload at full size (1024 x 1024 triangular, three shells + D1 +
+    K + Bz, T = 10 K, Philox seed 1, 20 reversed disks): the oracle draws the same
+    Philox stream, so after 60 steps every site agrees with it, energies included."""
+    import matjes_b200 as mj
+
+    w = mj.workload("triangular1024_thermal")
+    deck, dyn = w["deck"], dict(w["dyn"])
+    dyn.pop("steps")
+    dyn["integrator"] = integrator
+    m = w["m0"].copy()
+    E = mj.SpinDynamics(mj.Hamiltonian(deck), **dyn).run(m, 60, energies=True)
+    mo = w["m0"].copy()
+    Eo = O.Model(deck).run(mo, 60, energies=True, **dyn)
+    assert np.abs(m - mo).max() < 1e-9
+    assert np.abs(E - Eo).max() <= 1e-12 * np.abs(Eo).max()
+    drift = np.abs(np.linalg.norm(m, axis=1) - 1.0).max()
+    assert drift < (1e-13 if integrator == "sib" else 3e-13)
