@@ -13,11 +13,12 @@
 // (the planes z >= Lz of that buffer are zero once and never written).  The
 // inverse runs the z transforms and then 2D inverse transforms of the Lz
 // planes the consumers read.  Layouts are z-major, [z][component][y][x], so
-// that one batched plan covers every (plane, component).  K is even
-// (K(-r) = K(r) on the periodic N_rep grid), so K_F is real; the pointwise
-// product then reads 6 real instead of 6 complex values per wave vector (when
-// the transformed K has imaginary parts above 1e-13 of its scale, the complex
-// product is kept).  The unpack is fused into the consumers: the field and
+// that one batched plan covers every (plane, component).  When K is even on
+// the N_rep grid (K(-r) = K(r), e.g. open axes without images) K_F is real and
+// the pointwise product reads 6 real instead of 6 complex values per wave
+// vector; with periodic axes the reference's truncated image sums leave K
+// slightly uneven (imaginary parts of K_F ~1e-7 of its scale), and the complex
+// product is kept whenever they exceed 1e-13.  The unpack is fused into the consumers: the field and
 // step kernels read H on the padded (y, x) grid of the lattice planes.
 #include <cufft.h>
 
