@@ -267,6 +267,45 @@ mj_status mj_minimize(mj_plan* plan, double* m_dev_soa, const mj_min_params* p, 
 mj_status mj_minimize_infdamp(mj_plan* plan, double* m_dev_soa, const mj_min_params* p, int64_t max_iter,
                               int64_t* iterations, double* max_torque, int32_t* colors, void* stream);
 
+/* ---- Metropolis Monte Carlo (Metropolis-MC/MCstep.f90) ------------------- */
+/* Proposals of Metropolis-MC/track_value.f90: sample_sphere (sphereft of
+ * paratemp-MC/sampling.f90:9-62, a uniform direction in the cone about the old
+ * spin), sample_ising (the flip), sample_underrelax / sample_overrelax
+ * (Metropolis-MC/relaxationtype.f90, from the site's effective field).  The
+ * reference's equi_samp draws the same uniform-in-the-cone distribution as
+ * sphereft by rejection; a caller maps it to MJ_MC_CONE. */
+enum { MJ_MC_CONE = 0, MJ_MC_ISING = 1, MJ_MC_UNDERRELAX = 2, MJ_MC_OVERRELAX = 3 };
+typedef struct {
+    double temperature;      /* K */
+    double cone;             /* half-angle of the proposal cone (rad); updated when adapt_cone */
+    int32_t proposal;        /* MJ_MC_* */
+    int32_t adapt_cone;      /* 1: the reference's rate-driven cone update (track_value.f90 cone_update) */
+    uint64_t seed;           /* Philox key */
+    uint32_t stream_id;      /* replica id folded into the Philox counter */
+    uint32_t sweep0;         /* index of the next sweep (advanced by each call) */
+    int64_t accepted_total;  /* running counts of accepted and proposed moves */
+    int64_t proposed_total;
+} mj_mc_params;
+/* nsweeps Metropolis sweeps on the device spins, in place: every site moved
+ * once per sweep, colour by colour in a colouring where no coupling joins two
+ * sites of one colour.  colors[4] returns it: {q, b, c, 1} for the linear
+ * colour (x + b y + c z) mod q, moved k = 0 .. q-1 in turn, or {cx, cy, cz, 0}
+ * for the product colour (x mod cx, y mod cy, z mod cz), moved with x mod cx
+ * fastest; the one with fewer colours is chosen.  Each move makes the proposal
+ * and the acceptance test of
+ * MCstep.f90:75-89 on the single-site energy change.  The reference moves
+ * randomly chosen sites (choose_spin.f90) with a sequential generator; here
+ * the uniforms are Philox draws, counter (site, sweep, stream_id, 0x4D43).
+ * E_dev (nsweeps doubles) and M_dev (3 nsweeps) receive the energy and the
+ * summed spins after each sweep (either may be NULL); *accepted the accepted
+ * moves of the call.  Single-atom stencil plans without the dipolar term
+ * (MJ_ERR_UNSUPPORTED otherwise, and when neither a linear colouring of at
+ * most 16 colours nor a product one of at most 4 x 4 x 4 fits the stencil and
+ * the periodic sizes).  The adaptive cone (sample_sphere) is updated once per
+ * sweep by 1e-4 per move of the sweep from the running acceptance rate. */
+mj_status mj_mc_sweeps(mj_plan* plan, double* m_dev_soa, mj_mc_params* p, int32_t nsweeps, double* E_dev,
+                       double* M_dev, int64_t* accepted, int32_t* colors, void* stream);
+
 /* ---- reverse mode (adjoint) ---------------------------------------------- */
 /* The reference has no derivative code: these entries have no counterpart in
  * it.  They differentiate its forward map, the SIB step of the dynamics

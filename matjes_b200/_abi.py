@@ -91,6 +91,17 @@ class MinParams(C.Structure):
                 ("check_every", C.c_int32)]
 
 
+class McParams(C.Structure):
+    _fields_ = [("temperature", C.c_double), ("cone", C.c_double), ("proposal", C.c_int32),
+                ("adapt_cone", C.c_int32), ("seed", C.c_uint64), ("stream_id", C.c_uint32),
+                ("sweep0", C.c_uint32), ("accepted_total", C.c_int64), ("proposed_total", C.c_int64)]
+
+
+MJ_MC_CONE = 0
+MJ_MC_ISING = 1
+MJ_MC_UNDERRELAX = 2
+MJ_MC_OVERRELAX = 3
+
 MJ_ENERGY_AFTER = 0
 MJ_ENERGY_BEFORE = 1
 
@@ -147,6 +158,8 @@ SIGNATURES = {
                                 C.POINTER(C.c_double), P]),
     "mj_minimize_infdamp": (C.c_int32, [P, P, C.POINTER(MinParams), C.c_int64, C.POINTER(C.c_int64),
                                         C.POINTER(C.c_double), P, P]),
+    "mj_mc_sweeps": (C.c_int32, [P, P, C.POINTER(McParams), C.c_int32, P, P, C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int32), P]),
     "mj_plan_nterms": (C.c_int32, [P, C.POINTER(C.c_int32)]),
     "mj_plan_set_terms": (C.c_int32, [P, P]),
     "mj_field_vjp": (C.c_int32, [P, P, P, P, P, P, P]),

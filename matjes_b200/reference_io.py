@@ -78,7 +78,7 @@ def fortran_e(x: float, w: int, d: int, e: Optional[int] = None) -> str:
     2 when e is not given), right-justified in w characters."""
     if not math.isfinite(x):
         return ("NaN" if math.isnan(x) else ("-Infinity" if x < 0 else "Infinity")).rjust(w)
-    neg = x < 0
+    neg = math.copysign(1.0, x) < 0  # gfortran writes the sign of a negative zero
     a = abs(x)
     if a == 0.0:
         digits, ex = "0" * d, 0

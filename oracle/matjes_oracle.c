@@ -1053,3 +1053,157 @@ int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int6
     if (max_torque) *max_torque = maxt;
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Metropolis Monte Carlo (Metropolis-MC/MCstep.f90)                    */
+
+static double mc_u32(uint32_t w) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
+
+/* sphereft (paratemp-MC/sampling.f90:9-62): cos(theta) uniform in [cos(cone), 1],
+ * phi uniform, the new direction rotated from the z frame onto the old spin */
+static void mc_sphereft(const double* s, double cos_cone, double u1, double u2, double* out) {
+    double ct = u1 + cos_cone * (1.0 - u1);
+    double st = sqrt(1.0 - ct * ct);
+    double phi = 2.0 * ORC_PI * u2;
+    double cti = s[2], rxy2 = s[0] * s[0] + s[1] * s[1], sti = sqrt(rxy2);
+    double cpi = 1.0, spi = 0.0;
+    if (!(rxy2 < 0.00001)) { cpi = s[0] / sqrt(rxy2); spi = s[1] / sqrt(rxy2); }
+    double t = st * sin(phi) * cti + ct * sti;
+    double n[3] = {-st * cos(phi) * spi + t * cpi, st * cos(phi) * cpi + t * spi, -st * sin(phi) * sti + ct * cti};
+    double nn = nrm3(n);
+    for (int k = 0; k < 3; k++) out[k] = n[k] / nn;
+}
+
+/* the proposals of Metropolis-MC/track_value.f90 (sample_sphere, sample_ising,
+ * sample_underrelax, sample_overrelax -> relaxationtype.f90); B = -dE/dm of the site */
+static void mc_propose(int proposal, const double* s, const double* B, double cos_cone, double u1, double u2,
+                       double* out) {
+    if (proposal == 1) { for (int k = 0; k < 3; k++) out[k] = -s[k]; return; }
+    if (proposal == 0) { mc_sphereft(s, cos_cone, u1, u2, out); return; }
+    double sb = s[0] * B[0] + s[1] * B[1] + s[2] * B[2], n[3];
+    if (proposal == 2) for (int k = 0; k < 3; k++) n[k] = s[k] * (1.0 - sb) + B[k];
+    else for (int k = 0; k < 3; k++) n[k] = B[k] - s[k] * (1.0 + sb);
+    double nn = nrm3(n);
+    for (int k = 0; k < 3; k++) out[k] = n[k] / nn;
+}
+
+/* energy change of moving site s to sn: the difference of energy_single
+ * (hamiltonian_collection.f90:402-431, pair terms doubled by mult_M_single),
+ * written as -d.B_s + d^T H_ss d with d = sn - s; B (out) = -dE/dm of the site */
+static double mc_delta_energy(const orc_model* M, const double* m, int64_t s, const double* sn, double* B) {
+    site_field(M, m, s, B);
+    double d[3] = {sn[0] - m[3 * s], sn[1] - m[3 * s + 1], sn[2] - m[3 * s + 2]};
+    double dE = -(d[0] * B[0] + d[1] * B[1] + d[2] * B[2]);
+    for (int k = 0; k < 3; k++) {
+        int64_t r = 3 * s + k;
+        for (int64_t j = M->rowptr[r]; j < M->rowptr[r + 1]; j++) {
+            int64_t c = M->col[j];
+            if (c >= 3 * s && c < 3 * s + 3) dE += d[k] * M->val[j] * d[c - 3 * s];
+        }
+    }
+    return dE;
+}
+
+/* accept (MCstep.f90:75-89) */
+static int mc_accept(double kT, double dE, double u) {
+    if (dE < 0.0) return 1;
+    if (!(kT > 0.0)) return 0;
+    return u < exp(fmax(-dE / kT, -200.0));
+}
+
+/* cone_update (track_value.f90:149-160) */
+static double mc_cone_update(double cone, double rate, double step) {
+    if (rate > 0.5 && cone < ORC_PI) return fmin(ORC_PI, cone + step);
+    if (rate < 0.5 && cone > 0.01) return fmax(0.01, cone - step);
+    return cone;
+}
+
+static void mc_keys(uint64_t seed, uint32_t key[2]) { key[0] = (uint32_t)seed; key[1] = (uint32_t)(seed >> 32); }
+
+static void mc_record(const orc_model* M, const double* m, int k, double* E_out, double* M_out) {
+    if (E_out) E_out[k] = orc_energy(M, m);
+    if (M_out) {
+        double a[3] = {0.0, 0.0, 0.0};
+        for (int64_t i = 0; i < M->nsite; i++) for (int c = 0; c < 3; c++) a[c] += m[3 * i + c];
+        for (int c = 0; c < 3; c++) M_out[3 * k + c] = a[c];
+    }
+}
+
+int orc_mc_sweeps(const orc_model* M, double* m, orc_mc* p, int nsweeps, const int* site_colour, int ncolours,
+                  double* E_out, double* M_out, int64_t* accepted) {
+    if (M->nmag != 1 || M->in.dip_on) return -3;
+    uint32_t key[2];
+    mc_keys(p->seed, key);
+    double kT = p->temperature * ORC_KB;
+    int64_t acc = 0, N = M->nsite;
+    for (int k = 0; k < nsweeps; k++) {
+        uint32_t sweep = p->sweep0 + (uint32_t)k;
+        double cos_cone = cos(p->cone);
+        int64_t acc_sweep = 0;
+        for (int col = 0; col < ncolours; col++)
+            for (int64_t i = 0; i < N; i++) {
+                if (site_colour[i] != col) continue;
+                uint32_t c[4] = {(uint32_t)i, sweep, p->stream_id, 0x4D43u}, w[4];
+                orc_philox4x32(c, key, w);
+                double B[3], sn[3];
+                site_field(M, m, i, B);
+                mc_propose(p->proposal, m + 3 * i, B, cos_cone, mc_u32(w[0]), mc_u32(w[1]), sn);
+                double dE = mc_delta_energy(M, m, i, sn, B);
+                if (mc_accept(kT, dE, mc_u32(w[2]))) {
+                    for (int q = 0; q < 3; q++) m[3 * i + q] = sn[q];
+                    acc_sweep++;
+                }
+            }
+        acc += acc_sweep;
+        p->accepted_total += acc_sweep;
+        p->proposed_total += N;
+        if (p->adapt_cone && p->proposal == 0)
+            p->cone = mc_cone_update(p->cone, (double)p->accepted_total / (double)p->proposed_total, 1e-4 * (double)N);
+        mc_record(M, m, k, E_out, M_out);
+    }
+    p->sweep0 += (uint32_t)nsweeps;
+    if (accepted) *accepted = acc;
+    return 0;
+}
+
+int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double* E_out, double* M_out,
+                  int64_t* accepted) {
+    if (M->in.dip_on) return -3;
+    uint32_t key[2];
+    mc_keys(p->seed, key);
+    double kT = p->temperature * ORC_KB;
+    int64_t N = M->nsite, acc = 0;
+    /* the tracked totals of track_val (init: H%energy and the summed spins),
+     * updated by each accepted move as MCstep.f90:60-68 does */
+    double E = orc_energy(M, m), Mg[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = 0; i < N; i++) for (int c = 0; c < 3; c++) Mg[c] += m[3 * i + c];
+    for (int k = 0; k < nsweeps; k++) {
+        uint32_t sweep = p->sweep0 + (uint32_t)k;
+        for (int64_t t = 0; t < N; t++) {
+            uint32_t c[4] = {(uint32_t)t, sweep, p->stream_id, 0x52534D43u}, w[4];
+            orc_philox4x32(c, key, w);
+            /* choose_spin (choosespin.f90:19-21): iomp = 1 + INT(Choice*(N-1)) */
+            int64_t i = (int64_t)(mc_u32(w[0]) * (double)(N - 1));
+            if (p->proposal == 0 && p->adapt_cone)
+                p->cone = mc_cone_update(p->cone,
+                                         p->proposed_total ? (double)p->accepted_total / (double)p->proposed_total : 0.0,
+                                         1e-4);
+            double B[3], sn[3];
+            site_field(M, m, i, B);
+            mc_propose(p->proposal, m + 3 * i, B, cos(p->cone), mc_u32(w[1]), mc_u32(w[2]), sn);
+            double dE = mc_delta_energy(M, m, i, sn, B);
+            p->proposed_total++;
+            if (mc_accept(kT, dE, mc_u32(w[3]))) {
+                for (int q = 0; q < 3; q++) { Mg[q] += sn[q] - m[3 * i + q]; m[3 * i + q] = sn[q]; }
+                E += dE;
+                acc++;
+                p->accepted_total++;
+            }
+        }
+        if (E_out) E_out[k] = E;
+        if (M_out) for (int q = 0; q < 3; q++) M_out[3 * k + q] = Mg[q];
+    }
+    p->sweep0 += (uint32_t)nsweeps;
+    if (accepted) *accepted = acc;
+    return 0;
+}

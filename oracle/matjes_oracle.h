@@ -26,6 +26,11 @@
  *   - thermal torque (langevin_bath) ............. dynamics/BTeff_sd.f90:18-45
  *   - noise sigma = sqrt(alpha kT hbar / dt) ..... dynamics/spindynamics.f90:268-272
  *   - constants .................................. fixed-parameters/constant.f90:11-32
+ *   - Metropolis move, acceptance ................ Metropolis-MC/MCstep.f90:37-89
+ *   - random site, proposals, cone update ........ Metropolis-MC/choosespin.f90:13-21,
+ *                                                  Metropolis-MC/track_value.f90:90-160,
+ *                                                  Metropolis-MC/relaxationtype.f90:14-78,
+ *                                                  paratemp-MC/sampling.f90:9-62
  *
  * SIB is absent from the reference (solvers/solver_commun.f90:97-108 has it
  * commented out); the SIB here restates the published semi-implicit scheme of
@@ -57,6 +62,7 @@ extern "C" {
 
 /* physical constants, fixed-parameters/constant.f90:11-32 */
 #define ORC_KB 0.000086173324
+#define ORC_PI 3.14159265358979323846
 #define ORC_MUB 0.0000578838180661
 #define ORC_HBAR 0.658211928
 #define ORC_DIP_PREF 6.745817653234234066975e-7 /* Energy/dipolar_magnetic.f90:41 */
@@ -118,6 +124,31 @@ int orc_minimize_vpo(const orc_model* M, double* m, double dt, double mass, doub
                      int64_t* iters, double* max_torque);
 int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int64_t niter, const int colors[3],
                          int64_t* iters, double* max_torque);
+/* Metropolis Monte Carlo.  proposal: 0 sphereft cone, 1 Ising flip,
+ * 2 under-relaxation, 3 over-relaxation.  The uniforms are Philox4x32-10 words
+ * under key `seed`, each turned into (w + 0.5) 2^-32. */
+typedef struct {
+    double temperature, cone;
+    int proposal, adapt_cone;
+    uint64_t seed;
+    uint32_t stream_id, sweep0;
+    int64_t accepted_total, proposed_total;
+} orc_mc;
+/* Sweeps colour by colour (single-atom models): colours 0 .. ncolours-1 in
+ * turn (site_colour[i] the colour of site i), each colour's sites in index
+ * order; site i of sweep t draws counter (i, t, stream, 0x4D43): words 0, 1
+ * the proposal, 2 the test.  After each sweep E_out[k] = H%energy, M_out[3k..]
+ * = summed spins; the cone update of an adaptive cone proposal runs once per
+ * sweep with step 1e-4 N. */
+int orc_mc_sweeps(const orc_model* M, double* m, orc_mc* p, int nsweeps, const int* site_colour, int ncolours,
+                  double* E_out, double* M_out, int64_t* accepted);
+/* The reference's order: N moves per sweep at sites chosen by choose_spin
+ * (1 + INT(u (N-1)), so the last site never moves), move t of sweep k drawing
+ * counter (t, k, stream, 0x52534D43): word 0 the site, 1, 2 the proposal, 3
+ * the test; the cone update before each cone proposal; E_out and M_out the
+ * incrementally tracked totals of track_val after each sweep. */
+int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double* E_out, double* M_out,
+                  int64_t* accepted);
 /* Field contributions split: MM only, Zeeman only, dipolar only (for tests). */
 void orc_field_terms(const orc_model* m, const double* mvec, double* B_mm, double* B_zee, double* B_dip);
 /* Explicit O(N^2) dipolar field (get_dipolar, mag_dip_fft F). */

@@ -239,6 +239,57 @@ def minimize_infdamp(model, m, conv_torque, niter, colors=(1, 1, 1)):
     return it.value, mt.value
 
 
+class MC(C.Structure):
+    """orc_mc: the chain state carried between calls (cone, counts, next sweep)."""
+    _fields_ = [("temperature", C.c_double), ("cone", C.c_double), ("proposal", C.c_int),
+                ("adapt_cone", C.c_int), ("seed", C.c_uint64), ("stream_id", C.c_uint32),
+                ("sweep0", C.c_uint32), ("accepted_total", C.c_int64), ("proposed_total", C.c_int64)]
+
+
+def _mc_bind():
+    lib.orc_mc_sweeps.restype = C.c_int
+    lib.orc_mc_sweeps.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(MC), C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                  C.c_void_p, C.POINTER(C.c_int64)]
+    lib.orc_mc_random.restype = C.c_int
+    lib.orc_mc_random.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(MC), C.c_int, C.c_void_p, C.c_void_p,
+                                  C.POINTER(C.c_int64)]
+
+
+def mc_site_colours(L, colors):
+    """Per-site colour (x fastest) of a colouring {q, b, c, 1} (linear, (x + b y +
+    c z) mod q) or {cx, cy, cz, 0} (product, x mod cx fastest); and the count."""
+    z, y, x = np.meshgrid(np.arange(L[2]), np.arange(L[1]), np.arange(L[0]), indexing="ij")
+    a0, a1, a2, form = (int(v) for v in colors)
+    if form == 1:
+        return np.ascontiguousarray(((x + a1 * y + a2 * z) % a0).ravel(), np.int32), a0
+    return np.ascontiguousarray(((x % a0) + a0 * ((y % a1) + a1 * (z % a2))).ravel(), np.int32), a0 * a1 * a2
+
+
+def mc_sweeps(model, m, st: MC, nsweeps, colors, L):
+    """Metropolis sweeps colour by colour on m (N,3) in place (Metropolis-MC/MCstep.f90
+    moves in the device's site order, `colors` the device's colouring of the
+    lattice of sizes L); returns (E per sweep, summed spins per sweep, accepted)."""
+    _mc_bind()
+    sc, nc = mc_site_colours(L, colors)
+    E, Mg, acc = np.empty(nsweeps), np.empty((nsweeps, 3)), C.c_int64()
+    rc = lib.orc_mc_sweeps(model.h, _p(m), C.byref(st), int(nsweeps), sc.ctypes.data, nc, _p(E), _p(Mg),
+                           C.byref(acc))
+    if rc != 0:
+        raise RuntimeError(f"oracle Monte Carlo failed ({rc})")
+    return E, Mg, acc.value
+
+
+def mc_random(model, m, st: MC, nsweeps):
+    """Metropolis moves at randomly chosen sites as the reference makes them
+    (choose_spin, MCstep), N moves per sweep; returns (tracked E, summed spins, accepted)."""
+    _mc_bind()
+    E, Mg, acc = np.empty(nsweeps), np.empty((nsweeps, 3)), C.c_int64()
+    rc = lib.orc_mc_random(model.h, _p(m), C.byref(st), int(nsweeps), _p(E), _p(Mg), C.byref(acc))
+    if rc != 0:
+        raise RuntimeError(f"oracle Monte Carlo failed ({rc})")
+    return E, Mg, acc.value
+
+
 def philox_normals(seed, step, stream, site0, n):
     out = np.empty((n, 3))
     lib.orc_philox_normals(seed, step, stream, site0, n, _p(out))
