@@ -285,6 +285,8 @@ typedef struct {
     uint32_t sweep0;         /* index of the next sweep (advanced by each call) */
     int64_t accepted_total;  /* running counts of accepted and proposed moves */
     int64_t proposed_total;
+    uint32_t round0;         /* index of the next parallel-tempering round (mj_batch_mc) */
+    uint32_t reserved;
 } mj_mc_params;
 /* nsweeps Metropolis sweeps on the device spins, in place: every site moved
  * once per sweep, colour by colour in a colouring where no coupling joins two
@@ -401,6 +403,25 @@ mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_s
  * may be NULL) gets ms per step in variant-major order. */
 mj_status mj_batch_autotune(mj_batch* b, const mj_dyn_params* p, int32_t steps, int32_t* best_variant,
                             int32_t* best_blocks_per_sm, double* ms_table);
+/* Parallel-tempering Monte Carlo on the replicas: the swap loop of
+ * paratemp-MC/parallel_tempering.f90:143-160.  Each of nrounds rounds runs
+ * sweeps_per_round Metropolis sweeps (mj_mc_sweeps' moves and colouring, one
+ * colouring for every replica) of every replica at the temperature its ladder
+ * slot holds, then measures (measure_add) and, when swap != 0, runs the
+ * parallel-tempering round p->round0 + k of mj_batch_step's rule on those
+ * energies.  Replica r is a chain of its own: Philox stream p->stream_id + r
+ * with its local site index, its own cone and counts (first set from p->cone,
+ * kept across calls; mj_batch_mc_reset sets them again).  p->temperature is
+ * ignored, p->sweep0 and (with swaps) p->round0 advance.  Per round k:
+ * E_dev[k nrep + r] the energy, M_dev[3 (k nrep + r) ..] the summed spins and
+ * slot_dev[k nrep + r] the ladder slot of replica r during the round's sweeps
+ * (each may be NULL); colors[4] as mj_mc_sweeps. */
+mj_status mj_batch_mc(mj_batch* b, mj_mc_params* p, int32_t nrounds, int32_t sweeps_per_round, int32_t swap,
+                      double* E_dev, double* M_dev, int32_t* slot_dev, int32_t* colors, void* stream);
+/* Resets every replica's Monte Carlo chain state: cone, accepted and proposed counts. */
+mj_status mj_batch_mc_reset(mj_batch* b, double cone);
+/* Per-replica cone (rad), accepted and proposed moves (host arrays of nrep, each may be NULL). */
+mj_status mj_batch_mc_state(mj_batch* b, double* cone, int64_t* accepted, int64_t* proposed);
 
 #ifdef __cplusplus
 }

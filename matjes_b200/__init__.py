@@ -12,6 +12,8 @@ from .deck import Deck, random_sphere, reversed_disks, square_film, triangular, 
 from .hamiltonian import Hamiltonian, SpinDynamics, SpinState, minimize  # noqa: F401
 from .batch import ReplicaBatch  # noqa: F401
 from .adjoint import SIBTrajectory, deck_terms, field_vjp  # noqa: F401
+from .montecarlo import MCInput, MetropolisMC, montecarlo_run, parallel_tempering_run  # noqa: F401
 
 __all__ = ["Deck", "Hamiltonian", "SpinDynamics", "SpinState", "ReplicaBatch", "SIBTrajectory", "minimize", "MatjesError", "workload", "square_film",
-           "triangular", "random_sphere", "reversed_disks"]
+           "triangular", "random_sphere", "reversed_disks", "MCInput", "MetropolisMC", "montecarlo_run",
+           "parallel_tempering_run"]

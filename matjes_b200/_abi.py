@@ -94,7 +94,8 @@ class MinParams(C.Structure):
 class McParams(C.Structure):
     _fields_ = [("temperature", C.c_double), ("cone", C.c_double), ("proposal", C.c_int32),
                 ("adapt_cone", C.c_int32), ("seed", C.c_uint64), ("stream_id", C.c_uint32),
-                ("sweep0", C.c_uint32), ("accepted_total", C.c_int64), ("proposed_total", C.c_int64)]
+                ("sweep0", C.c_uint32), ("accepted_total", C.c_int64), ("proposed_total", C.c_int64),
+                ("round0", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 MJ_MC_CONE = 0
@@ -183,6 +184,10 @@ SIGNATURES = {
     "mj_batch_set_config": (C.c_int32, [P, C.c_int32, C.c_int32]),
     "mj_batch_autotune": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
                                       C.POINTER(C.c_int32), P]),
+    "mj_batch_mc": (C.c_int32, [P, C.POINTER(McParams), C.c_int32, C.c_int32, C.c_int32, P, P, P,
+                                C.POINTER(C.c_int32), P]),
+    "mj_batch_mc_reset": (C.c_int32, [P, C.c_double]),
+    "mj_batch_mc_state": (C.c_int32, [P, P, P, P]),
 }
 
 

@@ -140,6 +140,38 @@ class ReplicaBatch:
         check(lib.mj_batch_temperatures(self.handle, ptr(T), ptr(acc)))
         return T, acc
 
+    # -- Monte Carlo -------------------------------------------------------
+    def monte_carlo(self, p: _abi.McParams, nrounds: int, sweeps_per_round: int = 1, swap: bool = True,
+                    record: bool = True, stream=None):
+        """Parallel-tempering Monte Carlo (mj_batch_mc): nrounds rounds of
+        sweeps_per_round Metropolis sweeps of every replica, each round measured
+        and followed by a swap round when `swap`.  p (McParams) carries the
+        proposal, cone, seed, stream base and the advancing sweep and round
+        counters.  Returns (E (nrounds, nrep), summed spins (nrounds, nrep, 3),
+        ladder slots (nrounds, nrep)) as CUDA tensors (None when not recorded)."""
+        import torch
+
+        dev = f"cuda:{self.device}"
+        E = torch.empty((nrounds, self.nrep), dtype=torch.float64, device=dev) if record else None
+        M = torch.empty((nrounds, self.nrep, 3), dtype=torch.float64, device=dev) if record else None
+        S = torch.empty((nrounds, self.nrep), dtype=torch.int32, device=dev) if record else None
+        col = np.zeros(4, np.int32)
+        check(lib.mj_batch_mc(self.handle, C.byref(p), int(nrounds), int(sweeps_per_round), int(bool(swap)), ptr(E),
+                              ptr(M), ptr(S), col.ctypes.data_as(C.POINTER(C.c_int32)), stream))
+        self.mc_colors = tuple(int(c) for c in col)
+        return E, M, S
+
+    def mc_reset(self, cone: float) -> None:
+        check(lib.mj_batch_mc_reset(self.handle, float(cone)))
+
+    def mc_state(self):
+        """(cone, accepted moves, proposed moves) of every replica's chain."""
+        cone = np.empty(self.nrep)
+        acc = np.empty(self.nrep, np.int64)
+        prop = np.empty(self.nrep, np.int64)
+        check(lib.mj_batch_mc_state(self.handle, ptr(cone), ptr(acc), ptr(prop)))
+        return cone, acc, prop
+
     def set_config(self, variant: int, blocks_per_sm: int) -> None:
         check(lib.mj_batch_set_config(self.handle, int(variant), int(blocks_per_sm)))
 

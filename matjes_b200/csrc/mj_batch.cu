@@ -22,6 +22,7 @@
 #include <numeric>
 #include <vector>
 
+#include "mj_mc.cuh"
 #include "mj_tiled_impl.cuh"
 
 namespace mj {
@@ -241,6 +242,96 @@ __global__ void k_pt_swap(BatchRep* reps, int* image, const double* slot_kT, int
     }
 }
 
+// ---------------------------------------------------------------------------
+// Monte Carlo on the replicas (paratemp-MC/parallel_tempering.f90:143-160): each
+// replica is a chain of its own (its own cone and counts, Philox stream
+// stream_id + r, its site index within the replica), moved colour by colour at
+// the temperature its ladder slot holds; the moves are mj_mc.cuh's.  MC tiles
+// are (replica, tx block, ty block) of 32 x 8 threads over a colour class.
+struct BatchMcArgs {
+    const BatchRep* reps;
+    const int4* tiles;          // (replica, x block, y block, -)
+    int64_t Ntot;
+    double* m;
+    const double* cos_cone;     // per replica
+    unsigned long long* acc;    // accepted moves per replica
+    uint32_t keys[20];
+    int proposal;
+    uint32_t sweep;
+    uint32_t stream_id;
+    McClass K;
+};
+
+__global__ void __launch_bounds__(256) k_batch_mc(const __grid_constant__ StencilParams P,
+                                                  const __grid_constant__ BatchMcArgs A) {
+    const int4 tl = A.tiles[blockIdx.x];
+    const BatchRep R = A.reps[tl.x];
+    const McClass& K = A.K;
+    const int y = K.ry + K.sy * (tl.z * 8 + static_cast<int>(threadIdx.y));
+    const int z = K.rz;  // replicas are one layer thick
+    const int x = mc_class_x(K, y, z, tl.y * 32 + static_cast<int>(threadIdx.x));
+    bool acc = false;
+    if (x < R.Lx && y < R.Ly && z == 0) {
+        double* mr = A.m + R.off;
+        const int64_t li = x + static_cast<int64_t>(R.Lx) * y;
+        const double3 s = ld3(mr, li, A.Ntot);
+        const double3 Pf = pair_field(P, mr, A.Ntot, R.Lx, R.Ly, 1, x, y, 0);
+        double3 sn;
+        acc = mc_move(P, A.keys, A.proposal, R.kT, A.cos_cone[tl.x], static_cast<uint32_t>(li), A.sweep,
+                      A.stream_id + R.stream, s, Pf, make_double3(R.zb[0], R.zb[1], R.zb[2]), sn);
+        if (acc) st3(mr, li, A.Ntot, sn);
+    }
+    const int n = __syncthreads_count(acc);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && n) atomicAdd(A.acc + tl.x, static_cast<unsigned long long>(n));
+}
+
+// after a sweep: proposed counts, the cone rule of sample_sphere (track_value.f90
+// cone_update, +-1e-4 per move of the sweep toward a running rate of 0.5, cone in
+// [0.01, pi]) when adapting, and the cosine the next sweep uses
+__global__ void k_batch_mc_cone(const BatchRep* reps, int nrep, const unsigned long long* acc, long long* prop,
+                                double* cone, double* cos_cone, int adapt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    const long long n = static_cast<long long>(reps[r].Lx) * reps[r].Ly;
+    prop[r] += n;
+    if (adapt) {
+        const double rate = static_cast<double>(acc[r]) / static_cast<double>(prop[r]);
+        // product and sum rounded apart (no fused multiply-add), as the host rule rounds them
+        const double step = __dmul_rn(1e-4, static_cast<double>(n));
+        double c = cone[r];
+        if (rate > 0.5 && c < kPi) c = fmin(kPi, __dadd_rn(c, step));
+        else if (rate < 0.5 && c > 0.01) c = fmax(0.01, __dsub_rn(c, step));
+        cone[r] = c;
+    }
+    cos_cone[r] = cos(cone[r]);
+}
+
+__global__ void k_batch_mc_init(int nrep, double cone0, unsigned long long* acc, long long* prop, double* cone,
+                                double* cos_cone) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    acc[r] = 0ull;
+    prop[r] = 0ll;
+    cone[r] = cone0;
+    cos_cone[r] = cos(cone0);
+}
+
+// summed spins of each replica (one block per replica, fixed order) and its slot
+__global__ void __launch_bounds__(256) k_batch_magnet(const BatchRep* reps, const double* m, int64_t Ntot, double* M,
+                                                      int* slot) {
+    const int r = blockIdx.x;
+    const BatchRep R = reps[r];
+    const int64_t n = static_cast<int64_t>(R.Lx) * R.Ly;
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        v[0] += m[R.off + i];
+        v[1] += m[Ntot + R.off + i];
+        v[2] += m[2 * Ntot + R.off + i];
+    }
+    if (M) block_partials<3>(v, M + 3 * static_cast<int64_t>(r), 1, 0);
+    if (slot && threadIdx.x == 0) slot[r] = R.slot;
+}
+
 // GNEB path tangents (GNEB/tangent.f90): for image r with neighbours r-1, r+1
 // tau = wp (m_{r+1} - m_r) + wm (m_r - m_{r-1}), projected on the tangent space
 // of m_r (vec_project, vector_utils/vector.f90:61-72) and normalised over the
@@ -404,6 +495,14 @@ struct mj_batch {
     uint32_t* d_stepctr = nullptr;
     double* d_stage = nullptr;
     double* d_gneb_part = nullptr;    // tangent norms: one partial per (image, block)
+    // Monte Carlo: the colouring, its MC tile list, per-replica chain state
+    int mc_col[4] = {0, 0, 0, 0};
+    int4* d_mc_tiles = nullptr;
+    int mc_ntile = 0;
+    unsigned long long* d_mc_acc = nullptr;
+    long long* d_mc_prop = nullptr;
+    double* d_mc_cone = nullptr;
+    double* d_mc_cos = nullptr;
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::string graph_key;
@@ -430,6 +529,11 @@ void batch_free(mj_batch* b) {
     cudaFree(b->d_stepctr);
     cudaFree(b->d_stage);
     cudaFree(b->d_gneb_part);
+    cudaFree(b->d_mc_tiles);
+    cudaFree(b->d_mc_acc);
+    cudaFree(b->d_mc_prop);
+    cudaFree(b->d_mc_cone);
+    cudaFree(b->d_mc_cos);
     delete b;
 }
 
@@ -903,6 +1007,131 @@ mj_status mj_batch_autotune(mj_batch* b, const mj_dyn_params* p, int32_t steps, 
     *best_variant = bv;
     *best_bps = bb;
     return cuda_status(cudaDeviceSynchronize(), "batch autotune");
+}
+
+// ---- Monte Carlo on the replicas -------------------------------------------
+
+// the colouring of every replica, its MC tile list and the per-replica chain state (first call)
+static mj_status batch_mc_setup(mj_batch* b, double cone0, cudaStream_t s) {
+    if (b->d_mc_tiles) return MJ_OK;
+    std::vector<int> L3(3 * b->nrep);
+    for (int r = 0; r < b->nrep; ++r) {
+        L3[3 * r] = b->reps[r].Lx;
+        L3[3 * r + 1] = b->reps[r].Ly;
+        L3[3 * r + 2] = 1;
+    }
+    if (!mc_colouring(b->sp, L3.data(), b->nrep, b->mc_col))
+        return set_error(MJ_ERR_UNSUPPORTED, "no linear colouring of at most 16 colours and no product colouring of "
+                                             "at most 4 x 4 x 4 fits the stencil and every replica's sizes");
+    const McClass K0 = mc_classes(b->mc_col)[0];
+    std::vector<int4> tiles;
+    for (int r = 0; r < b->nrep; ++r) {
+        const int nx = (b->reps[r].Lx + K0.qx - 1) / K0.qx, ny = (b->reps[r].Ly + K0.sy - 1) / K0.sy;
+        for (int by = 0; by < (ny + 7) / 8; ++by)
+            for (int bx = 0; bx < (nx + 31) / 32; ++bx) tiles.push_back(make_int4(r, bx, by, 0));
+    }
+    b->mc_ntile = static_cast<int>(tiles.size());
+    const int nrep = b->nrep;
+    mj_status st;
+    if ((st = cuda_status(cudaMalloc(&b->d_mc_tiles, sizeof(int4) * tiles.size()), "MC tiles")) != MJ_OK ||
+        (st = cuda_status(cudaMalloc(&b->d_mc_acc, sizeof(unsigned long long) * nrep), "MC state")) != MJ_OK ||
+        (st = cuda_status(cudaMalloc(&b->d_mc_prop, sizeof(long long) * nrep), "MC state")) != MJ_OK ||
+        (st = cuda_status(cudaMalloc(&b->d_mc_cone, sizeof(double) * nrep), "MC state")) != MJ_OK ||
+        (st = cuda_status(cudaMalloc(&b->d_mc_cos, sizeof(double) * nrep), "MC state")) != MJ_OK) {
+        cudaFree(b->d_mc_tiles);
+        b->d_mc_tiles = nullptr;
+        return st;
+    }
+    if ((st = cuda_status(cudaMemcpy(b->d_mc_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice),
+                          "MC tiles")) != MJ_OK)
+        return st;
+    k_batch_mc_init<<<(nrep + 127) / 128, 128, 0, s>>>(nrep, cone0, b->d_mc_acc, b->d_mc_prop, b->d_mc_cone,
+                                                       b->d_mc_cos);
+    return cuda_status(cudaGetLastError(), "k_batch_mc_init");
+}
+
+mj_status mj_batch_mc_reset(mj_batch* b, double cone) {
+    if (!b || !(cone > 0.0)) return set_error(MJ_ERR_ARG, "bad batch Monte Carlo reset");
+    cudaSetDevice(b->device);
+    mj_status st = batch_mc_setup(b, cone, 0);
+    if (st != MJ_OK) return st;
+    k_batch_mc_init<<<(b->nrep + 127) / 128, 128>>>(b->nrep, cone, b->d_mc_acc, b->d_mc_prop, b->d_mc_cone,
+                                                    b->d_mc_cos);
+    if ((st = cuda_status(cudaGetLastError(), "k_batch_mc_init")) != MJ_OK) return st;
+    return cuda_status(cudaDeviceSynchronize(), "batch Monte Carlo reset");
+}
+
+mj_status mj_batch_mc(mj_batch* b, mj_mc_params* p, int32_t nrounds, int32_t sweeps_per_round, int32_t swap,
+                      double* E_dev, double* M_dev, int32_t* slot_dev, int32_t* colors, void* stream) {
+    if (!b || !p || nrounds < 0 || sweeps_per_round < 1) return set_error(MJ_ERR_ARG, "bad batch Monte Carlo arguments");
+    if (p->proposal < MJ_MC_CONE || p->proposal > MJ_MC_OVERRELAX) return set_error(MJ_ERR_ARG, "unknown proposal");
+    if (!(p->cone > 0.0)) return set_error(MJ_ERR_ARG, "cone > 0");
+    cudaSetDevice(b->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    mj_status st = batch_mc_setup(b, p->cone, s);
+    if (st != MJ_OK) return st;
+    if (colors)
+        for (int d = 0; d < 4; ++d) colors[d] = b->mc_col[d];
+    const std::vector<McClass> classes = mc_classes(b->mc_col);
+    BatchMcArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.reps = b->d_reps;
+    A.tiles = b->d_mc_tiles;
+    A.Ntot = b->Ntot;
+    A.m = b->d_m;
+    A.cos_cone = b->d_mc_cos;
+    A.acc = b->d_mc_acc;
+    mc_keys(p->seed, A.keys);
+    A.proposal = p->proposal;
+    A.stream_id = p->stream_id;
+    DynCoef c;  // the swap test's Philox key (no device step counter)
+    std::memset(&c, 0, sizeof(c));
+    mc_keys(p->seed, c.keys);
+    const int adapt = p->adapt_cone && p->proposal == MJ_MC_CONE;
+    const int nrep = b->nrep;
+    for (int32_t k = 0; k < nrounds; ++k) {
+        for (int32_t t = 0; t < sweeps_per_round; ++t) {
+            A.sweep = p->sweep0 + static_cast<uint32_t>(k * sweeps_per_round + t);
+            for (const McClass& K : classes) {
+                A.K = K;
+                k_batch_mc<<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A);
+            }
+            k_batch_mc_cone<<<(nrep + 127) / 128, 128, 0, s>>>(b->d_reps, nrep, b->d_mc_acc, b->d_mc_prop,
+                                                               b->d_mc_cone, b->d_mc_cos, adapt);
+            if ((st = cuda_status(cudaGetLastError(), "k_batch_mc")) != MJ_OK) return st;
+        }
+        // measure (measure_add) before the swap, with the temperatures the sweeps had
+        double* E = E_dev ? E_dev + static_cast<int64_t>(k) * nrep : b->d_E;
+        if ((E_dev || swap) && (st = batch_energy(b, c, E, s)) != MJ_OK) return st;
+        if (M_dev || slot_dev) {
+            k_batch_magnet<<<nrep, 256, 0, s>>>(b->d_reps, b->d_m, b->Ntot,
+                                                M_dev ? M_dev + 3 * static_cast<int64_t>(k) * nrep : nullptr,
+                                                slot_dev ? slot_dev + static_cast<int64_t>(k) * nrep : nullptr);
+            if ((st = cuda_status(cudaGetLastError(), "k_batch_magnet")) != MJ_OK) return st;
+        }
+        if (swap) {
+            k_pt_swap<<<1, 256, 0, s>>>(b->d_reps, b->d_image, b->d_slot_kT, nrep, E, c, p->round0 + static_cast<uint32_t>(k),
+                                        1u, b->d_accept);
+            if ((st = cuda_status(cudaGetLastError(), "k_pt_swap")) != MJ_OK) return st;
+        }
+    }
+    p->sweep0 += static_cast<uint32_t>(nrounds * sweeps_per_round);
+    if (swap) p->round0 += static_cast<uint32_t>(nrounds);
+    return MJ_OK;
+}
+
+mj_status mj_batch_mc_state(mj_batch* b, double* cone, int64_t* accepted, int64_t* proposed) {
+    if (!b) return set_error(MJ_ERR_ARG, "null batch");
+    if (!b->d_mc_tiles) return set_error(MJ_ERR_ARG, "no Monte Carlo has run on this batch");
+    cudaSetDevice(b->device);
+    mj_status st = cuda_status(cudaDeviceSynchronize(), "batch Monte Carlo");
+    const size_t n = static_cast<size_t>(b->nrep);
+    if (st == MJ_OK && cone) st = cuda_status(cudaMemcpy(cone, b->d_mc_cone, sizeof(double) * n, cudaMemcpyDeviceToHost), "MC state");
+    if (st == MJ_OK && accepted)
+        st = cuda_status(cudaMemcpy(accepted, b->d_mc_acc, sizeof(int64_t) * n, cudaMemcpyDeviceToHost), "MC state");
+    if (st == MJ_OK && proposed)
+        st = cuda_status(cudaMemcpy(proposed, b->d_mc_prop, sizeof(int64_t) * n, cudaMemcpyDeviceToHost), "MC state");
+    return st;
 }
 
 }  // extern "C"

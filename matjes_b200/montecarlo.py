@@ -4,7 +4,9 @@
 same names and defaults).  ``MetropolisMC`` stands in for ``track_val`` plus
 ``MCstep`` (Metropolis-MC/track_value.f90, MCstep.f90): it holds the chain
 state that persists across temperatures (cone, accepted and proposed counts)
-and runs sweeps through ``mj_mc_sweeps``.  ``montecarlo_run`` is the
+and runs sweeps through ``mj_mc_sweeps``.  ``parallel_tempering_run`` is the
+replica-exchange loop of paratemp-MC/parallel_tempering.f90 on a batch of
+replicas (``mj_batch_mc``).  ``montecarlo_run`` is the
 temperature loop of Metropolis-MC/MonteCarlo.f90:35-160 (relaxation, then
 Total_MC_Steps measurements T_auto sweeps apart), ``therm_set`` the averages of
 Metropolis-MC/thermo_val.f90:44-77 and ``thermo_print`` the EM.dat rows of
@@ -70,7 +72,7 @@ class MetropolisMC:
             raise ValueError(f"sampling must be one of {sorted(SAMPLING)}")
         self.ham = ham
         self.p = _abi.McParams(0.0, float(cone), SAMPLING[sampling], int(bool(adapt_cone)), int(seed),
-                               int(stream_id), 0, 0, 0)
+                               int(stream_id), 0, 0, 0, 0, 0)
         self.colors = (0, 0, 0, 0)  # {q, b, c, 1} linear or {cx, cy, cz, 0} product, set by sweeps
 
     @property
@@ -170,3 +172,28 @@ def montecarlo_run(ham: Hamiltonian, m, inp: MCInput, temps: Sequence[float], se
         Mg = Mg[every - 1::every].cpu().numpy()
         out.append(therm_set(T, E, Mg, ham.N))
     return out
+
+
+def parallel_tempering_run(batch, inp: MCInput, seed: int = 0, stream_id: int = 0, adapt_cone: bool = True,
+                           return_series: bool = False):
+    """The swap loop of paratemp-MC/parallel_tempering.f90:143-160 on a
+    ReplicaBatch whose replicas (all of one size) hold the temperature ladder:
+    n_sizerelax rounds of T_auto sweeps of every replica, each round measured
+    (measure_add, the measurement following the temperature) and followed by a
+    swap round.  Returns the ThermVal of every ladder temperature, ascending
+    (and, with return_series, the per-round energies, summed spins and ladder
+    slots of every replica).  The reference's temperature-set optimisation (N_Topt > 1,
+    calculate_diffusion) is not run: one pass over the ladder, as N_Topt = 1."""
+    p = _abi.McParams(0.0, float(inp.cone), SAMPLING[inp.sampling], int(bool(adapt_cone)), int(seed), int(stream_id),
+                      0, 0, 0, 0, 0)
+    n = max(1, inp.n_sizerelax)
+    E, M, S = batch.monte_carlo(p, n, max(1, inp.T_auto), swap=True)
+    E, M, S = E.cpu().numpy(), M.cpu().numpy(), S.cpu().numpy()
+    T_rep, _ = batch.temperatures()
+    ladder = np.sort(T_rep)
+    nsite = int(batch.sizes[0, 0] * batch.sizes[0, 1])
+    out = []
+    for l, T in enumerate(ladder):
+        sel = S == l
+        out.append(therm_set(float(T), E[sel], M[sel], nsite))
+    return (out, (E, M, S)) if return_series else out
