@@ -425,6 +425,63 @@ def run_dipolar(dev: int, steps: int = 50) -> dict:
             "kernel_share": {k: round(t / tot, 4) for k, (t, _) in prof.items()}}
 
 
+def run_monte_carlo(dev: int, sweeps: int = 100) -> dict:
+    """Metropolis Monte Carlo: the square film 1024 x 1024 (J + D + K + Bz = 0.5 T,
+    cone proposals, 10 K, 2-colour checkerboard sweeps) on one chain; 256 replicas
+    of 64 x 64 (temperatures geometric 1..50 K) with a parallel-tempering round
+    every 10 sweeps; and, as the CPU baseline, the oracle's random-site chain on one
+    host core (256 x 256, the reference's move order).  Consecutive sweeps keep the 25 MB spin field in
+    L2, as a chain does; the rates are moves per second."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.montecarlo import MetropolisMC
+    from oracle import oracle as O
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    deck = mj.square_film((1024, 1024, 1))
+    ham = mj.Hamiltonian(deck, device=dev)
+    m = torch.tensor(mj.random_sphere(deck.nsites, 1).T.copy(), device=f"cuda:{dev}")
+    ch = MetropolisMC(ham, "sphere", cone=0.5, seed=3, adapt_cone=False)
+    ch.sweeps(m, 5, 10.0, record=False)
+    torch.cuda.synchronize()
+    e0.record()
+    ch.sweeps(m, sweeps, 10.0, record=False)
+    e1.record()
+    torch.cuda.synchronize()
+    one = e0.elapsed_time(e1)
+    n = 256
+    batch = mj.ReplicaBatch(mj.square_film((8, 8, 1)), [(64, 64)] * n, np.zeros((n, 3)),
+                            list(np.geomspace(1.0, 50.0, n)), device=dev)
+    batch.upload(mj.random_sphere(64 * 64 * n, 2))
+    p = _abi.McParams(0.0, 0.5, _abi.MJ_MC_CONE, 1, 5, 0, 0, 0, 0, 0, 0)
+    batch.monte_carlo(p, 2, 10, swap=True, record=False)
+    torch.cuda.synchronize()
+    e0.record()
+    batch.monte_carlo(p, sweeps // 10, 10, swap=True, record=False)
+    e1.record()
+    torch.cuda.synchronize()
+    bt = e0.elapsed_time(e1)
+    cdeck = mj.square_film((256, 256, 1))
+    mo = mj.random_sphere(cdeck.nsites, 1)
+    st = O.MC(temperature=10.0, cone=0.5, proposal=0, adapt_cone=0, seed=3, stream_id=0, sweep0=0)
+    model = O.Model(cdeck)
+    t0 = time.perf_counter()
+    O.mc_random(model, mo, st, 60)
+    ct = time.perf_counter() - t0
+    return {"workload": "square1024_mc", "sites": deck.nsites, "sweeps": sweeps, "colours": list(ch.colors),
+            "value": deck.nsites * sweeps / (one / 1e3), "unit": "moves/s", "us_per_sweep": 1e3 * one / sweeps,
+            "acceptance": ch.rate,
+            "batch": {"workload": "square64_replicas256_ptmc", "sites": batch.N, "swap_every": 10,
+                      "value": batch.N * sweeps / (bt / 1e3), "unit": "moves/s", "us_per_sweep": 1e3 * bt / sweeps},
+            "cpu_baseline": {"value": cdeck.nsites * 60 / ct, "unit": "moves/s", "cores": 1, "kind": "port",
+                             "sample": "256x256 square film, 60 sweeps of random-site moves (orc_mc_random)"}}
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -549,6 +606,7 @@ def run_gpu(args, rank, world):
     batch = run_batch(dev) if (world == 1 and not args.no_batch) else None
     adjoint = run_adjoint(dev) if (world == 1 and not args.no_batch) else None
     dipolar = run_dipolar(dev) if (world == 1 and not args.no_batch) else None
+    monte_carlo = run_monte_carlo(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -575,6 +633,7 @@ def run_gpu(args, rank, world):
         "batch": batch,
         "adjoint": adjoint,
         "dipolar": dipolar,
+        "monte_carlo": monte_carlo,
     }
     print(json.dumps(line), flush=True)
 
@@ -587,7 +646,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batch, adjoint and dipolar measurements")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batch, adjoint, dipolar and Monte Carlo measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -404,7 +404,7 @@ mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_s
 mj_status mj_batch_autotune(mj_batch* b, const mj_dyn_params* p, int32_t steps, int32_t* best_variant,
                             int32_t* best_blocks_per_sm, double* ms_table);
 /* Parallel-tempering Monte Carlo on the replicas: the swap loop of
- * paratemp-MC/parallel_tempering.f90:143-160.  Each of nrounds rounds runs
+ * paratemp-MC/parallel_tempering.f90:163-181.  Each of nrounds rounds runs
  * sweeps_per_round Metropolis sweeps (mj_mc_sweeps' moves and colouring, one
  * colouring for every replica) of every replica at the temperature its ladder
  * slot holds, then measures (measure_add) and, when swap != 0, runs the

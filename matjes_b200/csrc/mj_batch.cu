@@ -243,7 +243,7 @@ __global__ void k_pt_swap(BatchRep* reps, int* image, const double* slot_kT, int
 }
 
 // ---------------------------------------------------------------------------
-// Monte Carlo on the replicas (paratemp-MC/parallel_tempering.f90:143-160): each
+// Monte Carlo on the replicas (paratemp-MC/parallel_tempering.f90:163-181): each
 // replica is a chain of its own (its own cone and counts, Philox stream
 // stream_id + r, its site index within the replica), moved colour by colour at
 // the temperature its ladder slot holds; the moves are mj_mc.cuh's.  MC tiles

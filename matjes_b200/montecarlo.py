@@ -7,7 +7,7 @@ state that persists across temperatures (cone, accepted and proposed counts)
 and runs sweeps through ``mj_mc_sweeps``.  ``parallel_tempering_run`` is the
 replica-exchange loop of paratemp-MC/parallel_tempering.f90 on a batch of
 replicas (``mj_batch_mc``).  ``montecarlo_run`` is the
-temperature loop of Metropolis-MC/MonteCarlo.f90:35-160 (relaxation, then
+temperature loop of Metropolis-MC/MonteCarlo.f90:35-162 (relaxation, then
 Total_MC_Steps measurements T_auto sweeps apart), ``therm_set`` the averages of
 Metropolis-MC/thermo_val.f90:44-77 and ``thermo_print`` the EM.dat rows of
 :102-129.
@@ -156,7 +156,7 @@ def thermo_print(path: str, rows: List[ThermVal]) -> None:
 
 def montecarlo_run(ham: Hamiltonian, m, inp: MCInput, temps: Sequence[float], seed: int = 0,
                    chain: Optional[MetropolisMC] = None) -> List[ThermVal]:
-    """The temperature loop of Metropolis-MC/MonteCarlo.f90:120-150 on m (CUDA
+    """The temperature loop of Metropolis-MC/MonteCarlo.f90:128-160 on m (CUDA
     (3, N), in place): per temperature N_relaxation * T_relax relaxation sweeps,
     then Total_MC_Steps measurements of (E, summed spins), each after T_auto
     sweeps.  The chain (cone, counts) carries over from one temperature to the
@@ -176,7 +176,7 @@ def montecarlo_run(ham: Hamiltonian, m, inp: MCInput, temps: Sequence[float], se
 
 def parallel_tempering_run(batch, inp: MCInput, seed: int = 0, stream_id: int = 0, adapt_cone: bool = True,
                            return_series: bool = False):
-    """The swap loop of paratemp-MC/parallel_tempering.f90:143-160 on a
+    """The swap loop of paratemp-MC/parallel_tempering.f90:163-181 on a
     ReplicaBatch whose replicas (all of one size) hold the temperature ladder:
     n_sizerelax rounds of T_auto sweeps of every replica, each round measured
     (measure_add, the measurement following the temperature) and followed by a

@@ -28,8 +28,8 @@
  *   - constants .................................. fixed-parameters/constant.f90:11-32
  *   - Metropolis move, acceptance ................ Metropolis-MC/MCstep.f90:37-89
  *   - random site, proposals, cone update ........ Metropolis-MC/choosespin.f90:13-21,
- *                                                  Metropolis-MC/track_value.f90:90-160,
- *                                                  Metropolis-MC/relaxationtype.f90:14-78,
+ *                                                  Metropolis-MC/track_value.f90:84-160,
+ *                                                  Metropolis-MC/relaxationtype.f90:15-70,
  *                                                  paratemp-MC/sampling.f90:9-62
  *
  * SIB is absent from the reference (solvers/solver_commun.f90:97-108 has it
