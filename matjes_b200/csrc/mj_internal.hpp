@@ -140,6 +140,9 @@ struct mj_plan {
     // CUDA graph of a step loop (mj_graph_run), cached with the key it was captured for
     uint32_t* d_stepctr = nullptr;
     cudaStream_t cap_stream = nullptr;
+    // streams and events of the striped host-to-host step (mj_step_host)
+    cudaStream_t pipe_stream[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // copies in, out, 4 compute
+    std::vector<cudaEvent_t> pipe_events;
     cudaGraphExec_t graph_exec = nullptr;
     std::string graph_key;
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
@@ -190,6 +193,11 @@ mj_status launch_temperature(mj_plan* p, const double* m, double* out2 /* device
 mj_status step_counter(uint32_t* ctr, uint32_t value, bool add, cudaStream_t s);
 mj_status aos_to_soa(const double* src_aos, double* dst_soa, int64_t n, cudaStream_t s);
 mj_status soa_to_aos(const double* src_soa, double* dst_aos, int64_t n, cudaStream_t s);
+// the transposes restricted to the sites [i0, i0 + cnt) of n
+mj_status aos_to_soa_range(const double* src_aos, double* dst_soa, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s);
+mj_status soa_to_aos_range(const double* src_soa, double* dst_aos, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s);
+// one block of nthreads sums nblocks energy partials in ordered_sum's fixed order
+mj_status launch_ordered_sum(const double* partials, int nblocks, int nthreads, double* out, cudaStream_t s);
 int64_t energy_blocks(const mj_plan* p);
 
 // tiled kernels for compile-time stencil shapes (mj_tiled.cu dispatches to one
@@ -197,22 +205,28 @@ int64_t energy_blocks(const mj_plan* p);
 // pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
 constexpr int kTiledVariants = 6;
 constexpr int kTiledVariantTY[kTiledVariants] = {16, 32, 16, 16, 16, 8};  // tile height per variant
+constexpr int kTiledVariantBYT[kTiledVariants] = {4, 8, 8, 4, 8, 4};     // warps per block per variant
 static_assert(kTiledVariants <= static_cast<int>(sizeof(mj_plan::tma_blocks) / sizeof(int)),
               "mj_plan::tma_blocks holds one persistent grid size per tiled variant");
 // emode: energy reduction of the launch (0: into E_out at once; 1: per-block
 // partials only, counted in p->defer_nblocks; 2: block 0 sums the previous
-// pass's partials into E_out)
+// pass's partials into E_out).  nty >= 0 limits the launch to the tile rows
+// [ty0, ty0 + nty) (plain staging; block ids and energy partials those of the
+// whole-lattice launch, so emode 1 over all row ranges writes the same partials).
 mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
                        double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
-                       int emode = 0);
+                       int emode = 0, int ty0 = 0, int nty = -1);
 #define MJ_TILED_SHAPE_DECL(fn)                                                                                   \
     mj_status fn(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,         \
-                 double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s, int emode);
+                 double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s, int emode,  \
+                 int ty0, int nty);
 MJ_TILED_SHAPE_DECL(launch_tiled_square_nn)
 MJ_TILED_SHAPE_DECL(launch_tiled_square2)
 MJ_TILED_SHAPE_DECL(launch_tiled_tri_nn)
 MJ_TILED_SHAPE_DECL(launch_tiled_tri3)
 int64_t tiled_energy_blocks(const mj_plan* p);
+// tile rows of the tiled kernels (per variant height) over the lattice
+int tiled_tile_rows(const mj_plan* p);
 // match a single-atom stencil to a compile-time shape and reorder its tensors (mj_abi.cpp)
 void match_shape(mj::StencilParams& sp);
 // single-atom stencil tensors W_o from coupling blocks; false past kMaxOff offsets (mj_abi.cpp)

@@ -351,6 +351,28 @@ __global__ void k_aos_to_soa(const double* __restrict__ a, double* __restrict__ 
     s[n + i] = a[3 * i + 1];
     s[2 * n + i] = a[3 * i + 2];
 }
+// the same transposes over the sites [i0, i0 + cnt) of n
+__global__ void k_aos_to_soa_range(const double* __restrict__ a, double* __restrict__ s, int64_t i0, int64_t cnt,
+                                   int64_t n) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t >= cnt) return;
+    const int64_t i = i0 + t;
+    s[i] = a[3 * i];
+    s[n + i] = a[3 * i + 1];
+    s[2 * n + i] = a[3 * i + 2];
+}
+__global__ void k_soa_to_aos_range(const double* __restrict__ s, double* __restrict__ a, int64_t i0, int64_t cnt,
+                                   int64_t n) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (t >= cnt) return;
+    const int64_t i = i0 + t;
+    a[3 * i] = s[i];
+    a[3 * i + 1] = s[n + i];
+    a[3 * i + 2] = s[2 * n + i];
+}
+// energy partials summed in the fixed order of ordered_sum (one block)
+__global__ void k_ordered_sum1(const double* partials, int nblocks, double* out) { ordered_sum<1>(partials, nblocks, out); }
+
 __global__ void k_soa_to_aos(const double* __restrict__ s, double* __restrict__ a, int64_t n) {
     const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
@@ -596,6 +618,20 @@ mj_status aos_to_soa(const double* a, double* so, int64_t n, cudaStream_t s) {
     if (n <= 0) return MJ_OK;
     k_aos_to_soa<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(a, so, n);
     return cuda_status(cudaGetLastError(), "aos_to_soa");
+}
+mj_status aos_to_soa_range(const double* a, double* so, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s) {
+    if (cnt <= 0) return MJ_OK;
+    k_aos_to_soa_range<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(a, so, i0, cnt, n);
+    return cuda_status(cudaGetLastError(), "aos_to_soa_range");
+}
+mj_status soa_to_aos_range(const double* so, double* a, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s) {
+    if (cnt <= 0) return MJ_OK;
+    k_soa_to_aos_range<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(so, a, i0, cnt, n);
+    return cuda_status(cudaGetLastError(), "soa_to_aos_range");
+}
+mj_status launch_ordered_sum(const double* partials, int nblocks, int nthreads, double* out, cudaStream_t s) {
+    k_ordered_sum1<<<1, nthreads, 0, s>>>(partials, nblocks, out);
+    return cuda_status(cudaGetLastError(), "k_ordered_sum1");
 }
 mj_status soa_to_aos(const double* so, double* a, int64_t n, cudaStream_t s) {
     if (n <= 0) return MJ_OK;

@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 #include <utility>
 
@@ -60,6 +61,9 @@ struct TiledArgs {
     TReduce R;
     uint32_t step;
     int* status;        // device status word (bounded-wait timeouts)
+    int ty0;            // first tile row of a launch over a range of tile rows (k_tiled)
+    int nty_all;        // tile rows of the whole lattice (0: the launch covers all of them)
+    int ty_count;       // tile rows of this launch (host side: its grid height)
 };
 
 template <class S, int BYT, int RY>
@@ -392,8 +396,12 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
                                                      const TiledArgs A) {
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_t[];
-    const int x0 = blockIdx.x * G::TX, y0 = blockIdx.y * G::TY, z = blockIdx.z;
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    // a launch may cover the tile rows [ty0, ty0 + gridDim.y) of nty_all; block ids
+    // (energy partials) are those of the launch over the whole lattice
+    const int by = static_cast<int>(blockIdx.y) + A.ty0;
+    const int nty = A.nty_all ? A.nty_all : static_cast<int>(gridDim.y);
+    const int x0 = blockIdx.x * G::TX, y0 = by * G::TY, z = blockIdx.z;
+    const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
     if (A.R.mode == 2 && bid == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
     Pre pre[RY];
     if constexpr (Staged<S, BYT, RY>::NPT <= kMaxStagedPerThread) {
@@ -569,7 +577,9 @@ struct TiledLauncher {
     template <int PASS>
     static mj_status launch(const StencilParams& P, const DynCoef& C, const TiledArgs& A, cudaStream_t s) {
         auto kern = k_tiled<S, BYT, RY, PASS, MINB>;
-        kern<<<grid(P), dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
+        dim3 g = grid(P);
+        if (A.nty_all) g.y = static_cast<unsigned>(A.ty_count);  // a range of tile rows
+        kern<<<g, dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
         return cuda_status(cudaGetLastError(), "k_tiled");
     }
     template <int PASS>
@@ -677,8 +687,9 @@ bool make_map(CUtensorMap* map, const double* base, const StencilParams& P, int 
 template <class S>
 mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
                              double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
-                             int emode) {
+                             int emode, int ty0, int nty) {
     TiledArgs A;
+    std::memset(&A, 0, sizeof(A));
     A.ms = ms;
     A.mn = mn;
     A.out = out;
@@ -697,6 +708,14 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
     return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
         using Launcher = decltype(L);
         using G = typename Launcher::G;
+        if (nty >= 0) {  // tile rows [ty0, ty0 + nty) only, plain staging
+            A.ty0 = ty0;
+            A.nty_all = static_cast<int>(Launcher::grid(p->sp).y);
+            A.ty_count = nty;
+            if (nty == 0) return MJ_OK;
+            if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
+            return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, nullptr, 0, s);
+        }
         if (p->use_tma) {
             CUtensorMap map;
             if (make_map(&map, ms, p->sp, G::PX, G::PY)) {

@@ -4,7 +4,7 @@
 namespace mj {
 mj_status launch_tiled_square_nn(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,
                          double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s,
-                         int emode) {
-    return launch_tiled_shape<ShapeSquareNN>(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode);
+                         int emode, int ty0, int nty) {
+    return launch_tiled_shape<ShapeSquareNN>(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode, ty0, nty);
 }
 }  // namespace mj
