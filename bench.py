@@ -183,8 +183,17 @@ def cpu_oracle_rate(wname, seconds=10.0, side=512):
     t = time.perf_counter()
     M.run(m, nst, step0=2, **dyn)
     el = time.perf_counter() - t
+    # the same on one core (a few seconds)
+    O.set_threads(1)
+    n1 = max(2, nst // max(1, os.cpu_count() or 1) // 2)
+    t = time.perf_counter()
+    M.run(m, n1, step0=2 + nst, **dyn)
+    el1 = time.perf_counter() - t
+    O.set_threads(0)
     return {"value": w["deck"].nsites * nst / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"oracle SIB+Philox on {side}x{side} triangular (same couplings), {nst} steps, {el:.1f} s"}
+            "sample": f"oracle SIB+Philox on {side}x{side} triangular (same couplings), {nst} steps, {el:.1f} s",
+            "single_core": {"value": w["deck"].nsites * n1 / el1, "unit": UNIT, "cores": 1,
+                            "sample": f"the same, {n1} steps, {el1:.1f} s"}}
 
 
 def run_reference(args, rank, world):
@@ -425,6 +434,63 @@ def run_dipolar(dev: int, steps: int = 50) -> dict:
             "kernel_share": {k: round(t / tot, 4) for k, (t, _) in prof.items()}}
 
 
+def run_hbm_resident(dev: int, steps: int = 20) -> dict:
+    """The bench workload at 4096^2 (triangular1024_thermal's couplings and
+    dynamics, 16.8 M sites, 403 MB per field, so every pass streams from HBM with
+    no L2 flush needed): the variant autotuned by the library on this lattice,
+    then `steps` timed SIB steps, with the per-kernel roofline of the two passes."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import workload
+
+    w = workload("triangular4096_thermal")
+    deck, dyn = w["deck"], dict(w["dyn"])
+    dyn.pop("steps")
+    N = deck.nsites
+    ham = mj.Hamiltonian(deck, device=dev)
+    sd = mj.SpinDynamics(ham, **dyn)
+    p = sd.p
+    p.energy_mode = _abi.MJ_ENERGY_BEFORE
+    m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
+    lib = _abi.lib
+    best, best_tma = _abi.C.c_int32(), _abi.C.c_int32()
+    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 3, _abi.C.byref(best),
+                                    _abi.C.byref(best_tma), None))
+    E = torch.zeros(steps + 8, dtype=torch.float64, device=m.device)
+    stream = torch.cuda.current_stream().cuda_stream
+    for k in range(3):
+        p.step0 = k
+        _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, E.data_ptr(), stream))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    p.step0 = 3
+    _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), steps, E.data_ptr(), stream))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    _abi.check(lib.mj_profile_enable(ham.plan, 1))
+    p.step0 = 100
+    _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 5, E.data_ptr(), stream))
+    prof = _abi.profile_read(ham.plan)
+    _abi.check(lib.mj_profile_enable(ham.plan, 0))
+    pk = peaks()
+    kern = {}
+    for name, b in (("k_sib1", 48.0), ("k_sib2", 72.0)):
+        if name in prof:
+            tot, cnt = prof[name]
+            avg = tot / max(cnt, 1)
+            gbs = b * N / (avg / 1e3) / 1e9
+            kern[name] = {"avg_us": 1e3 * avg, "achieved_gbs": gbs, "frac": gbs / pk["hbm_gbs"]}
+    return {"workload": "triangular4096_thermal", "sites": N, "steps": steps, "kernel_variant": int(best.value),
+            "tma_halo": bool(best_tma.value), "value": N / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "step_roofline": {"alg_bytes_per_site": 120.0, "achieved_gbs": 120.0 * N / (ms / 1e3) / 1e9,
+                              "frac": 120.0 * N / (ms / 1e3) / 1e9 / pk["hbm_gbs"]},
+            "kernels": kern}
+
+
 def run_monte_carlo(dev: int, sweeps: int = 100) -> dict:
     """Metropolis Monte Carlo: the square film 1024 x 1024 (J + D + K + Bz = 0.5 T,
     cone proposals, 10 K, 2-colour checkerboard sweeps) on one chain; 256 replicas
@@ -604,6 +670,7 @@ def run_gpu(args, rank, world):
     adjoint = run_adjoint(dev) if (world == 1 and not args.no_batch) else None
     dipolar = run_dipolar(dev) if (world == 1 and not args.no_batch) else None
     monte_carlo = run_monte_carlo(dev) if (world == 1 and not args.no_batch) else None
+    hbm_resident = run_hbm_resident(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -632,6 +699,7 @@ def run_gpu(args, rank, world):
         "adjoint": adjoint,
         "dipolar": dipolar,
         "monte_carlo": monte_carlo,
+        "hbm_resident_4096": hbm_resident,
     }
     print(json.dumps(line), flush=True)
 

@@ -170,14 +170,26 @@ def reversed_disks(deck: Deck, ndisk: int, radius: float, seed: int) -> np.ndarr
     rng = np.random.default_rng(seed)
     cx = rng.integers(0, Lx, ndisk)
     cy = rng.integers(0, Ly, ndisk)
-    y, x = np.meshgrid(np.arange(Ly), np.arange(Lx), indexing="ij")
     a1, a2 = deck.areal[0, :2], deck.areal[1, :2]
     flip = np.zeros((Ly, Lx), bool)
-    for i in range(ndisk):
-        dx = (x - cx[i] + Lx // 2) % Lx - Lx // 2
-        dy = (y - cy[i] + Ly // 2) % Ly - Ly // 2
+    # cell offsets whose distance can be within the radius: |r| >= s_min |(dx, dy)|
+    s_min = np.linalg.svd(np.stack([a1, a2]), compute_uv=False).min()
+    B = int(np.ceil(radius / s_min)) + 1
+    if 2 * B + 2 <= min(Lx, Ly):
+        # the disk's bounding box only (its offsets are the minimum images)
+        dy, dx = np.meshgrid(np.arange(-B, B + 1), np.arange(-B, B + 1), indexing="ij")
         r = dx[..., None] * a1 + dy[..., None] * a2
-        flip |= (r ** 2).sum(-1) <= radius * radius + 1e-9
+        inside = (r ** 2).sum(-1) <= radius * radius + 1e-9
+        ox, oy = dx[inside], dy[inside]
+        for i in range(ndisk):
+            flip[(cy[i] + oy) % Ly, (cx[i] + ox) % Lx] = True
+    else:
+        y, x = np.meshgrid(np.arange(Ly), np.arange(Lx), indexing="ij")
+        for i in range(ndisk):
+            dx = (x - cx[i] + Lx // 2) % Lx - Lx // 2
+            dy = (y - cy[i] + Ly // 2) % Ly - Ly // 2
+            r = dx[..., None] * a1 + dy[..., None] * a2
+            flip |= (r ** 2).sum(-1) <= radius * radius + 1e-9
     m = np.zeros((Ly * Lx, 3))
     m[:, 2] = np.where(flip.ravel(), -1.0, 1.0)
     return np.tile(m, (deck.L[2], 1))
@@ -197,6 +209,14 @@ def workload(name: str, scale: int = 1) -> dict:
         L = 1024 // scale
         deck = triangular((L, L))
         return dict(deck=deck, m0=reversed_disks(deck, 20, 8.0, 1),
+                    dyn=dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=1,
+                             steps=2000))
+    if name == "triangular4096_thermal":
+        # the same couplings and dynamics at 4096^2 (16.8 M sites, 403 MB per field:
+        # every pass streams from HBM), disks at the 1024^2 density
+        L = 4096 // scale
+        deck = triangular((L, L))
+        return dict(deck=deck, m0=reversed_disks(deck, max(1, 20 * (L // 1024) ** 2), 8.0, 1),
                     dyn=dict(integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=1,
                              steps=2000))
     if name == "square256_adjoint":

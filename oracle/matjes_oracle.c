@@ -1207,3 +1207,5 @@ int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double*
     if (accepted) *accepted = acc;
     return 0;
 }
+
+void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }

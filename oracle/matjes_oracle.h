@@ -124,6 +124,8 @@ int orc_minimize_vpo(const orc_model* M, double* m, double dt, double mass, doub
                      int64_t* iters, double* max_torque);
 int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int64_t niter, const int colors[3],
                          int64_t* iters, double* max_torque);
+/* OpenMP threads of the parallel loops (n <= 0: all processors). */
+void orc_set_threads(int n);
 /* Metropolis Monte Carlo.  proposal: 0 sphereft cone, 1 Ising flip,
  * 2 under-relaxation, 3 over-relaxation.  The uniforms are Philox4x32-10 words
  * under key `seed`, each turned into (w + 0.5) 2^-32. */

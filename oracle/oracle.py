@@ -290,6 +290,12 @@ def mc_random(model, m, st: MC, nsweeps):
     return E, Mg, acc.value
 
 
+def set_threads(n: int) -> None:
+    """OpenMP threads of the oracle's parallel loops (n <= 0: all processors)."""
+    lib.orc_set_threads.argtypes = [C.c_int]
+    lib.orc_set_threads(int(n))
+
+
 def philox_normals(seed, step, stream, site0, n):
     out = np.empty((n, 3))
     lib.orc_philox_normals(seed, step, stream, site0, n, _p(out))
