@@ -11,7 +11,11 @@ runs one forward + backward sweep of the reverse-mode SIB trajectory instead;
 
     python -m matjes_b200.profile_run --batch --steps 3
 
-steps the 256-replica batch workload.
+steps the 256-replica batch workload;
+
+    python -m matjes_b200.profile_run --mc --lattice square --L 2048 --steps 3
+
+runs Metropolis sweeps (cone proposals, 10 K) instead of time steps.
 """
 from __future__ import annotations
 
@@ -33,6 +37,7 @@ def main(argv=None):
     ap.add_argument("--adjoint", action="store_true", help="one forward + backward sweep of the SIB adjoint")
     ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
     ap.add_argument("--batch", action="store_true", help="step the 256-replica batch workload")
+    ap.add_argument("--mc", action="store_true", help="Metropolis sweeps (cone proposals) instead of time steps")
     a = ap.parse_args(argv)
     if a.adjoint:
         return adjoint(a)
@@ -55,6 +60,14 @@ def main(argv=None):
         m0 = mj.random_sphere(deck.nsites, 4)
     ham = mj.Hamiltonian(deck)
     m = torch.tensor(m0.T.copy(), device="cuda")
+    if a.mc:
+        from matjes_b200.montecarlo import MetropolisMC
+
+        ch = MetropolisMC(ham, "sphere", cone=0.5, seed=3, adapt_cone=False)
+        E, _, acc = ch.sweeps(m, a.steps, a.T)
+        torch.cuda.synchronize()
+        print("ok", ch.colors, acc, E.tolist())
+        return
     sd = mj.SpinDynamics(ham, integrator=a.integrator, timestep=0.1, alpha=0.1, temperature=a.T, noise="philox", seed=1)
     sd.p.energy_mode = _abi.MJ_ENERGY_BEFORE
     if a.variant == "auto":
