@@ -249,6 +249,7 @@ __global__ void k_pt_swap(BatchRep* reps, int* image, const double* slot_kT, int
 // the temperature its ladder slot holds; the moves are mj_mc.cuh's.  MC tiles
 // are (replica, tx block, ty block) of 32 x 8 threads over a colour class.
 struct BatchMcArgs {
+    const double* tab;          // sin/cos tables
     const BatchRep* reps;
     const int4* tiles;          // (replica, x block, y block, -)
     int64_t Ntot;
@@ -262,6 +263,7 @@ struct BatchMcArgs {
     McClass K;
 };
 
+template <class S>
 __global__ void __launch_bounds__(256) k_batch_mc(const __grid_constant__ StencilParams P,
                                                   const __grid_constant__ BatchMcArgs A) {
     const int4 tl = A.tiles[blockIdx.x];
@@ -275,10 +277,11 @@ __global__ void __launch_bounds__(256) k_batch_mc(const __grid_constant__ Stenci
         double* mr = A.m + R.off;
         const int64_t li = x + static_cast<int64_t>(R.Lx) * y;
         const double3 s = ld3(mr, li, A.Ntot);
-        const double3 Pf = pair_field(P, mr, A.Ntot, R.Lx, R.Ly, 1, x, y, 0);
+        const double3 Pf = pair_field<S>(P, mr, A.Ntot, R.Lx, R.Ly, 1, x, y, 0);
         double3 sn;
-        acc = mc_move(P, A.keys, A.proposal, R.kT, A.cos_cone[tl.x], static_cast<uint32_t>(li), A.sweep,
-                      A.stream_id + R.stream, s, Pf, make_double3(R.zb[0], R.zb[1], R.zb[2]), sn);
+        acc = mc_move(P, A.keys, A.tab, A.proposal, R.kT, R.kT > 0.0 ? 1.0 / R.kT : 0.0, A.cos_cone[tl.x],
+                      static_cast<uint32_t>(li), A.sweep, A.stream_id + R.stream, s, Pf,
+                      make_double3(R.zb[0], R.zb[1], R.zb[2]), sn);
         if (acc) st3(mr, li, A.Ntot, sn);
     }
     const int n = __syncthreads_count(acc);
@@ -1075,6 +1078,7 @@ mj_status mj_batch_mc(mj_batch* b, mj_mc_params* p, int32_t nrounds, int32_t swe
     const std::vector<McClass> classes = mc_classes(b->mc_col);
     BatchMcArgs A;
     std::memset(&A, 0, sizeof(A));
+    A.tab = b->d_noise_tab;
     A.reps = b->d_reps;
     A.tiles = b->d_mc_tiles;
     A.Ntot = b->Ntot;
@@ -1094,7 +1098,13 @@ mj_status mj_batch_mc(mj_batch* b, mj_mc_params* p, int32_t nrounds, int32_t swe
             A.sweep = p->sweep0 + static_cast<uint32_t>(k * sweeps_per_round + t);
             for (const McClass& K : classes) {
                 A.K = K;
-                k_batch_mc<<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A);
+                switch (b->shape) {
+                    case kShapeSquareNN: k_batch_mc<ShapeSquareNN><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
+                    case kShapeSquare2: k_batch_mc<ShapeSquare2><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
+                    case kShapeTriNN: k_batch_mc<ShapeTriNN><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
+                    case kShapeTri3: k_batch_mc<ShapeTri3><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
+                    default: k_batch_mc<void><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A);
+                }
             }
             k_batch_mc_cone<<<(nrep + 127) / 128, 128, 0, s>>>(b->d_reps, nrep, b->d_mc_acc, b->d_mc_prop,
                                                                b->d_mc_cone, b->d_mc_cos, adapt);

@@ -23,13 +23,17 @@ namespace {
 
 struct McCoef {
     double kT;          // eV
+    double inv_kT;      // 1/kT (0 at T = 0)
     double cos_cone;
+    const double* tab;  // sin/cos tables (the plan's thermal-draw tables)
     int proposal;       // MJ_MC_*
     uint32_t keys[20];  // Philox round keys of the seed
     uint32_t sweep;
     uint32_t stream;
 };
 
+// S: the plan's compile-time stencil shape, void for runtime offsets
+template <class S>
 __global__ void __launch_bounds__(256) k_mc_color(const __grid_constant__ StencilParams P, const double* __restrict__ bmap,
                                                   double* m, const McCoef C, const McClass K,
                                                   unsigned long long* accepted) {
@@ -41,10 +45,10 @@ __global__ void __launch_bounds__(256) k_mc_color(const __grid_constant__ Stenci
         const int64_t N = static_cast<int64_t>(P.L[0]) * P.L[1] * P.L[2];
         const int64_t i = x + static_cast<int64_t>(P.L[0]) * (y + static_cast<int64_t>(P.L[1]) * z);
         const double3 s = ld3(m, i, N);
-        const double3 Pf = pair_field(P, m, N, P.L[0], P.L[1], P.L[2], x, y, z);
+        const double3 Pf = pair_field<S>(P, m, N, P.L[0], P.L[1], P.L[2], x, y, z);
         double3 sn;
-        acc = mc_move(P, C.keys, C.proposal, C.kT, C.cos_cone, static_cast<uint32_t>(i), C.sweep, C.stream, s, Pf,
-                      zeeman(P, bmap, i, N), sn);
+        acc = mc_move(P, C.keys, C.tab, C.proposal, C.kT, C.inv_kT, C.cos_cone, static_cast<uint32_t>(i), C.sweep,
+                      C.stream, s, Pf, zeeman(P, bmap, i, N), sn);
         if (acc) st3(m, i, N, sn);
     }
     // accepted moves of the block, added once per block (an integer sum: any order gives the same count)
@@ -107,6 +111,8 @@ mj_status mj_mc_sweeps(mj_plan* plan, double* m, mj_mc_params* p, int32_t nsweep
     McCoef C;
     std::memset(&C, 0, sizeof(C));
     C.kT = p->temperature * kKB;
+    C.inv_kT = C.kT > 0.0 ? 1.0 / C.kT : 0.0;
+    C.tab = plan->d_noise_tab;
     C.proposal = p->proposal;
     C.stream = p->stream_id;
     mc_keys(p->seed, C.keys);
@@ -132,7 +138,24 @@ mj_status mj_mc_sweeps(mj_plan* plan, double* m, mj_mc_params* p, int32_t nsweep
     for (int32_t k = 0; k < nsweeps && st == MJ_OK; ++k) {
         C.sweep = p->sweep0 + static_cast<uint32_t>(k);
         C.cos_cone = std::cos(p->cone);
-        for (const McClass& K : classes) k_mc_color<<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+        for (const McClass& K : classes) {
+            switch (plan->sp.shape) {
+                case kShapeSquareNN:
+                    k_mc_color<ShapeSquareNN><<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+                    break;
+                case kShapeSquare2:
+                    k_mc_color<ShapeSquare2><<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+                    break;
+                case kShapeTriNN:
+                    k_mc_color<ShapeTriNN><<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+                    break;
+                case kShapeTri3:
+                    k_mc_color<ShapeTri3><<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+                    break;
+                default:
+                    k_mc_color<void><<<grid, blk, 0, s>>>(plan->sp, plan->d_bmap, m, C, K, &d_scr->acc);
+            }
+        }
         if ((st = cuda_status(cudaGetLastError(), "k_mc_color")) != MJ_OK) break;
         if (E_dev && (st = launch_energy(plan, m, E_dev + k, s)) != MJ_OK) break;
         if (M_dev) {

@@ -14,8 +14,11 @@
 // (MCstep.f90:75-89).
 #pragma once
 
+#include <type_traits>
+#include <utility>
 #include <vector>
 
+#include "mj_shapes.hpp"
 #include "mj_stencil.cuh"
 
 namespace mj {
@@ -25,24 +28,27 @@ constexpr uint32_t kMcTag = 0x4D43u;  // "MC"
 
 __device__ __forceinline__ double u32_open(uint32_t w) { return (static_cast<double>(w) + 0.5) * (1.0 / 4294967296.0); }
 
-// sphereft: a direction in the cone of half-angle `cone` about s
-__device__ __forceinline__ double3 cone_proposal(double3 s, double cos_cone, double u1, double u2) {
+// sphereft: a direction in the cone of half-angle `cone` about s; sin and cos of
+// phi = 2 pi u2 from the tables of the thermal draw (tab_sincos2pi, <= 8e-16)
+__device__ __forceinline__ double3 cone_proposal(double3 s, double cos_cone, double u1, double u2,
+                                                 const double* __restrict__ tab) {
     const double ct = u1 + cos_cone * (1.0 - u1);
     const double st = sqrt(1.0 - ct * ct);
-    const double phi = 2.0 * kPi * u2;
     const double cti = s.z;
     const double rxy2 = s.x * s.x + s.y * s.y;
     const double sti = sqrt(rxy2);
     double cpi = 1.0, spi = 0.0;
     if (!(rxy2 < 0.00001)) {
-        cpi = s.x / sqrt(rxy2);
-        spi = s.y / sqrt(rxy2);
+        const double inv = 1.0 / sti;
+        cpi = s.x * inv;
+        spi = s.y * inv;
     }
-    const double cph = cos(phi), sph = sin(phi);
+    double sph, cph;
+    tab_sincos2pi(u2, tab, &sph, &cph);
     const double t = st * sph * cti + ct * sti;
     const double3 n = make_double3(-st * cph * spi + t * cpi, st * cph * cpi + t * spi, -st * sph * sti + ct * cti);
-    const double nn = sqrt(dot(n, n));
-    return make_double3(n.x / nn, n.y / nn, n.z / nn);
+    const double inv_n = 1.0 / sqrt(dot(n, n));
+    return make_double3(n.x * inv_n, n.y * inv_n, n.z * inv_n);
 }
 
 // periodic neighbour k of (x, y, z) on a lattice of sizes (Lx, Ly, Lz)
@@ -65,15 +71,53 @@ __device__ __forceinline__ bool neighbour_in(const StencilParams& P, int Lx, int
     return true;
 }
 
+// one compile-time offset k of shape S added to the pair field b
+template <class S, int k>
+__device__ __forceinline__ void pair_term(const StencilParams& P, const double* __restrict__ m, int64_t Ntot, int Lx,
+                                          int Ly, int x, int y, int64_t layer, double3& b) {
+    constexpr int dx = S::DX[k], dy = S::DY[k];
+    int nx = x + dx, ny = y + dy;
+    if (nx < 0 || nx >= Lx) {
+        if (!P.periodic[0]) return;
+        nx = wrap(nx, Lx);
+    }
+    if (ny < 0 || ny >= Ly) {
+        if (!P.periodic[1]) return;
+        ny = wrap(ny, Ly);
+    }
+    const double3 v = ld3(m, layer + nx + static_cast<int64_t>(Lx) * ny, Ntot);
+    if constexpr (S::ISO[k] != 0) {
+        const double w = P.W[k][0];
+        b = make_double3(fma(w, v.x, b.x), fma(w, v.y, b.y), fma(w, v.z, b.z));
+    } else {
+        b = mat3(P.W[k], v, b);
+    }
+}
+
+template <class S, int... Kk>
+__device__ __forceinline__ void pair_terms(const StencilParams& P, const double* __restrict__ m, int64_t Ntot, int Lx,
+                                           int Ly, int x, int y, int64_t layer, double3& b,
+                                           std::integer_sequence<int, Kk...>) {
+    (pair_term<S, Kk>(P, m, Ntot, Lx, Ly, x, y, layer, b), ...);
+}
+
 // pair field P_i = sum_o W_o m_{i+o} (no on-site term) of a lattice whose site 0
-// is packed at `m` (SoA with component stride Ntot)
+// is packed at `m` (SoA with component stride Ntot).  S = void: the plan's
+// runtime offsets; S a compile-time shape (mj_shapes.hpp, in-layer offsets):
+// its offsets unrolled, isotropic shells as one scalar each.
+template <class S>
 __device__ __forceinline__ double3 pair_field(const StencilParams& P, const double* __restrict__ m, int64_t Ntot,
                                               int Lx, int Ly, int Lz, int x, int y, int z) {
     double3 b = make_double3(0.0, 0.0, 0.0);
-    for (int k = 0; k < P.n_off; ++k) {
-        int64_t j;
-        if (!neighbour_in(P, Lx, Ly, Lz, x, y, z, k, j)) continue;
-        b = mat3(P.W[k], ld3(m, j, Ntot), b);
+    if constexpr (std::is_void<S>::value) {
+        for (int k = 0; k < P.n_off; ++k) {
+            int64_t j;
+            if (!neighbour_in(P, Lx, Ly, Lz, x, y, z, k, j)) continue;
+            b = mat3(P.W[k], ld3(m, j, Ntot), b);
+        }
+    } else {
+        pair_terms<S>(P, m, Ntot, Lx, Ly, x, y, static_cast<int64_t>(Lx) * Ly * z, b,
+                      std::make_integer_sequence<int, S::K>{});
     }
     return b;
 }
@@ -85,32 +129,34 @@ __device__ __forceinline__ double onsite_energy(const StencilParams& P, double3 
 
 // the proposal of a move (track_value.f90 sample_*); B the site's effective field
 // -dE/dm (relaxationtype.f90 under- and over-relaxation)
-__device__ __forceinline__ double3 propose(int proposal, double3 s, double3 B, double cos_cone, const uint32_t c[4]) {
+__device__ __forceinline__ double3 propose(int proposal, double3 s, double3 B, double cos_cone, const uint32_t c[4],
+                                           const double* __restrict__ tab) {
     if (proposal == MJ_MC_ISING) return make_double3(-s.x, -s.y, -s.z);
-    if (proposal == MJ_MC_CONE) return cone_proposal(s, cos_cone, u32_open(c[0]), u32_open(c[1]));
+    if (proposal == MJ_MC_CONE) return cone_proposal(s, cos_cone, u32_open(c[0]), u32_open(c[1]), tab);
     const double sb = dot(s, B);
     double3 n;
     if (proposal == MJ_MC_UNDERRELAX) n = make_double3(s.x * (1.0 - sb) + B.x, s.y * (1.0 - sb) + B.y, s.z * (1.0 - sb) + B.z);
     else n = make_double3(B.x - s.x * (1.0 + sb), B.y - s.y * (1.0 + sb), B.z - s.z * (1.0 + sb));
-    const double nn = sqrt(dot(n, n));
-    return make_double3(n.x / nn, n.y / nn, n.z / nn);
+    const double inv_n = 1.0 / sqrt(dot(n, n));
+    return make_double3(n.x * inv_n, n.y * inv_n, n.z * inv_n);
 }
 
 // One Metropolis move of the site holding s (pair field Pf, Zeeman field zb):
 // true and sn the new direction when taken.  `site` is the index of the site
-// within its lattice, the first word of the Philox counter.
-__device__ __forceinline__ bool mc_move(const StencilParams& P, const uint32_t* keys, int proposal, double kT,
-                                        double cos_cone, uint32_t site, uint32_t sweep, uint32_t stream, double3 s,
-                                        double3 Pf, double3 zb, double3& sn) {
+// within its lattice, the first word of the Philox counter; inv_kT = 1/kT.
+__device__ __forceinline__ bool mc_move(const StencilParams& P, const uint32_t* keys, const double* __restrict__ tab,
+                                        int proposal, double kT, double inv_kT, double cos_cone, uint32_t site,
+                                        uint32_t sweep, uint32_t stream, double3 s, double3 Pf, double3 zb,
+                                        double3& sn) {
     uint32_t c[4] = {site, sweep, stream, kMcTag};
     philox10k(c, keys);
     double3 B = add3(Pf, zb);
     if (P.has_onsite) B = mat3(P.W0, s, B);
-    sn = propose(proposal, s, B, cos_cone, c);
+    sn = propose(proposal, s, B, cos_cone, c, tab);
     const double3 d = make_double3(sn.x - s.x, sn.y - s.y, sn.z - s.z);
     const double dE = -dot(d, Pf) + (onsite_energy(P, sn) - onsite_energy(P, s)) - dot(d, zb);
     bool acc = dE < 0.0;
-    if (!acc && kT > 0.0) acc = u32_open(c[2]) < exp(fmax(-dE / kT, -200.0));
+    if (!acc && kT > 0.0) acc = u32_open(c[2]) < exp(fmax(-dE * inv_kT, -200.0));
     return acc;
 }
 

@@ -1060,16 +1060,19 @@ int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int6
 static double mc_u32(uint32_t w) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
 
 /* sphereft (paratemp-MC/sampling.f90:9-62): cos(theta) uniform in [cos(cone), 1],
- * phi uniform, the new direction rotated from the z frame onto the old spin */
+ * phi = 2 pi u2, the new direction rotated from the z frame onto the old spin;
+ * sin and cos of phi from the tables of the thermal draw (tab_sincos2pi) */
 static void mc_sphereft(const double* s, double cos_cone, double u1, double u2, double* out) {
     double ct = u1 + cos_cone * (1.0 - u1);
     double st = sqrt(1.0 - ct * ct);
-    double phi = 2.0 * ORC_PI * u2;
+    double sph, cph;
+    noise_tables();
+    tab_sincos2pi(u2, &sph, &cph);
     double cti = s[2], rxy2 = s[0] * s[0] + s[1] * s[1], sti = sqrt(rxy2);
     double cpi = 1.0, spi = 0.0;
     if (!(rxy2 < 0.00001)) { cpi = s[0] / sqrt(rxy2); spi = s[1] / sqrt(rxy2); }
-    double t = st * sin(phi) * cti + ct * sti;
-    double n[3] = {-st * cos(phi) * spi + t * cpi, st * cos(phi) * cpi + t * spi, -st * sin(phi) * sti + ct * cti};
+    double t = st * sph * cti + ct * sti;
+    double n[3] = {-st * cph * spi + t * cpi, st * cph * cpi + t * spi, -st * sph * sti + ct * cti};
     double nn = nrm3(n);
     for (int k = 0; k < 3; k++) out[k] = n[k] / nn;
 }
