@@ -286,7 +286,9 @@ typedef struct {
     int64_t accepted_total;  /* running counts of accepted and proposed moves */
     int64_t proposed_total;
     uint32_t round0;         /* index of the next parallel-tempering round (mj_batch_mc) */
-    uint32_t reserved;
+    int32_t track_totals;    /* mj_mc_sweeps: 1 = E_dev / M_dev are the totals of the call's start
+                                updated by every accepted move (track_val's E_total and
+                                Magnetization), 0 = recomputed after every sweep */
 } mj_mc_params;
 /* nsweeps Metropolis sweeps on the device spins, in place: every site moved
  * once per sweep, colour by colour in a colouring where no coupling joins two

@@ -95,7 +95,7 @@ class McParams(C.Structure):
     _fields_ = [("temperature", C.c_double), ("cone", C.c_double), ("proposal", C.c_int32),
                 ("adapt_cone", C.c_int32), ("seed", C.c_uint64), ("stream_id", C.c_uint32),
                 ("sweep0", C.c_uint32), ("accepted_total", C.c_int64), ("proposed_total", C.c_int64),
-                ("round0", C.c_uint32), ("reserved", C.c_uint32)]
+                ("round0", C.c_uint32), ("track_totals", C.c_int32)]
 
 
 MJ_MC_CONE = 0

@@ -279,9 +279,10 @@ __global__ void __launch_bounds__(256) k_batch_mc(const __grid_constant__ Stenci
         const double3 s = ld3(mr, li, A.Ntot);
         const double3 Pf = pair_field<S>(P, mr, A.Ntot, R.Lx, R.Ly, 1, x, y, 0);
         double3 sn;
+        double dE;
         acc = mc_move(P, A.keys, A.tab, A.proposal, R.kT, R.kT > 0.0 ? 1.0 / R.kT : 0.0, A.cos_cone[tl.x],
                       static_cast<uint32_t>(li), A.sweep, A.stream_id + R.stream, s, Pf,
-                      make_double3(R.zb[0], R.zb[1], R.zb[2]), sn);
+                      make_double3(R.zb[0], R.zb[1], R.zb[2]), sn, dE);
         if (acc) st3(mr, li, A.Ntot, sn);
     }
     const int n = __syncthreads_count(acc);

@@ -142,19 +142,20 @@ __device__ __forceinline__ double3 propose(int proposal, double3 s, double3 B, d
 }
 
 // One Metropolis move of the site holding s (pair field Pf, Zeeman field zb):
-// true and sn the new direction when taken.  `site` is the index of the site
-// within its lattice, the first word of the Philox counter; inv_kT = 1/kT.
+// true and sn the new direction when taken, dE its energy change.  `site` is the
+// index of the site within its lattice, the first word of the Philox counter;
+// inv_kT = 1/kT.
 __device__ __forceinline__ bool mc_move(const StencilParams& P, const uint32_t* keys, const double* __restrict__ tab,
                                         int proposal, double kT, double inv_kT, double cos_cone, uint32_t site,
                                         uint32_t sweep, uint32_t stream, double3 s, double3 Pf, double3 zb,
-                                        double3& sn) {
+                                        double3& sn, double& dE) {
     uint32_t c[4] = {site, sweep, stream, kMcTag};
     philox10k(c, keys);
     double3 B = add3(Pf, zb);
     if (P.has_onsite) B = mat3(P.W0, s, B);
     sn = propose(proposal, s, B, cos_cone, c, tab);
     const double3 d = make_double3(sn.x - s.x, sn.y - s.y, sn.z - s.z);
-    const double dE = -dot(d, Pf) + (onsite_energy(P, sn) - onsite_energy(P, s)) - dot(d, zb);
+    dE = -dot(d, Pf) + (onsite_energy(P, sn) - onsite_energy(P, s)) - dot(d, zb);
     bool acc = dE < 0.0;
     if (!acc && kT > 0.0) acc = u32_open(c[2]) < exp(fmax(-dE * inv_kT, -200.0));
     return acc;

@@ -67,12 +67,15 @@ class MetropolisMC:
     """The Monte Carlo chain of one spin configuration on the device."""
 
     def __init__(self, ham: Hamiltonian, sampling: str = "sphere", cone: float = math.pi, seed: int = 0,
-                 stream_id: int = 0, adapt_cone: bool = True):
+                 stream_id: int = 0, adapt_cone: bool = True, track_totals: bool = False):
+        """track_totals: the recorded energies and summed spins are the totals of
+        the call's start updated by every accepted move (track_val's E_total and
+        Magnetization, MCstep.f90:60-68) instead of recomputed after every sweep."""
         if sampling not in SAMPLING:
             raise ValueError(f"sampling must be one of {sorted(SAMPLING)}")
         self.ham = ham
         self.p = _abi.McParams(0.0, float(cone), SAMPLING[sampling], int(bool(adapt_cone)), int(seed),
-                               int(stream_id), 0, 0, 0, 0, 0)
+                               int(stream_id), 0, 0, 0, 0, int(bool(track_totals)))
         self.colors = (0, 0, 0, 0)  # {q, b, c, 1} linear or {cx, cy, cz, 0} product, set by sweeps
 
     @property
@@ -159,9 +162,9 @@ def montecarlo_run(ham: Hamiltonian, m, inp: MCInput, temps: Sequence[float], se
     """The temperature loop of Metropolis-MC/MonteCarlo.f90:128-160 on m (CUDA
     (3, N), in place): per temperature N_relaxation * T_relax relaxation sweeps,
     then Total_MC_Steps measurements of (E, summed spins), each after T_auto
-    sweeps.  The chain (cone, counts) carries over from one temperature to the
-    next as track_val does."""
-    chain = chain or MetropolisMC(ham, inp.sampling, inp.cone, seed)
+    sweeps, the totals tracked through the accepted moves as track_val does.
+    The chain (cone, counts) carries over from one temperature to the next."""
+    chain = chain or MetropolisMC(ham, inp.sampling, inp.cone, seed, track_totals=True)
     out = []
     for T in temps:
         chain.sweeps(m, max(1, inp.N_relaxation * max(1, inp.T_relax)), T, record=False)

@@ -76,6 +76,32 @@ def test_chain_equals_the_oracle_move_by_move(name, proposal):
     assert chain.colors == {"square": (2, 1, 0, 1), "cubic": (2, 1, 1, 1), "triangular": (9, 3, 0, 1)}[name]
 
 
+@pytest.mark.parametrize("name", ["square", "triangular", "cubic"])
+def test_tracked_totals_follow_the_recomputed_ones(name):
+    """track_totals: the energy and summed spins of the call's start updated by
+    every accepted move (track_val) equal the recomputed ones to rounding; the
+    moves themselves do not change."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200.montecarlo import MetropolisMC
+
+    deck = _decks()[name]
+    ham = mj.Hamiltonian(deck)
+    m0 = mj.random_sphere(deck.nsites, 5)
+    out = {}
+    for track in (False, True):
+        m = torch.tensor(m0.T.copy(), device="cuda")
+        ch = MetropolisMC(ham, "sphere", cone=0.8, seed=21, stream_id=2, adapt_cone=True, track_totals=track)
+        E1, M1, a1 = ch.sweeps(m, 30, 12.0)
+        E2, M2, a2 = ch.sweeps(m, 20, 40.0)
+        out[track] = (m.cpu().numpy(), torch.cat([E1, E2]).cpu().numpy(), torch.cat([M1, M2]).cpu().numpy(), a1 + a2)
+    (m_a, E_a, M_a, acc_a), (m_b, E_b, M_b, acc_b) = out[False], out[True]
+    assert np.array_equal(m_a, m_b) and acc_a == acc_b
+    assert np.abs(E_b - E_a).max() <= 1e-12 * np.abs(E_a).max()
+    assert np.abs(M_b - M_a).max() <= 1e-10 * deck.nsites
+
+
 def test_zero_temperature_and_unchanged_counter_streams():
     """At T = 0 only moves that lower the energy are taken; replicas on other
     stream ids draw other numbers."""
