@@ -586,9 +586,13 @@ def run_gpu(args, rank, world):
     # the timed loop below (L2 flushed before every step, per-step events); the
     # library's own mj_plan_autotune times back-to-back steps, the right choice
     # when the fields stay in L2 between steps
+    # (--variant skips the sweep: a run under a profiler, whose timing would pick
+    # another variant than a live run)
     configs = [(-1, 0)] + [(v, t) for t in (0, 1) for v in range(6)]
+    if args.variant is not None:
+        configs = [(args.variant, args.tma)]
     tune = np.zeros(len(configs))
-    for ci, (v, t) in enumerate(configs):
+    for ci, (v, t) in enumerate(configs if args.variant is None else []):
         _abi.check(lib.mj_plan_set_variant(ham.plan, v))
         _abi.check(lib.mj_plan_set_tma(ham.plan, t))
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(8)]
@@ -712,6 +716,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="triangular1024_thermal")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="kernel variant (-1 generic, 0..5 tiled) instead of the timed sweep")
+    ap.add_argument("--tma", type=int, default=0, help="halo staging with --variant: 1 TMA, 0 plain loads")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batch, adjoint, dipolar and Monte Carlo measurements")
     args = ap.parse_args()
