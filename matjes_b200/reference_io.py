@@ -24,6 +24,11 @@ Input deck (a subset of the keywords Matjes reads, same meaning):
                  solvers/solver_commun.f90:57)
   minimisation   steps, masse, timestep, min_Efreq, convergence_criteria
                  (IO-input/minimize_io.f90:40-44)
+  Monte Carlo    simulation (metropolis | parallel-tempering), n_Tsteps, Tini, Tfin,
+                 n_relaxation, T_relax, T_auto, Total_MC_Steps, n_sizerelax, cone and
+                 one of the logicals ising, underrelaxation, overrelaxation,
+                 sphere_samp, equi_samp (IO-input/MC_io.f90:92-150); run_montecarlo
+                 writes the Monte Carlo EM.dat (thermo_val.f90 thermo_print)
 Values follow Fortran list-directed input: `1.0d-3` exponents, logicals
 `.T.`/`T`/`.true.`, trailing text after the values ignored.
 
@@ -199,6 +204,31 @@ class ReferenceInput:
     dynamics: DynamicsInput
     minimize: MinimizeInput
     atom_names: List[str] = field(default_factory=list)
+    simulation: str = ""
+    # the Monte Carlo input (IO-input/MC_io.f90 rw_MC), None when the deck sets
+    # no sampling method
+    monte_carlo: Optional[object] = None
+
+
+MC_SAMPLING_KEYS = (("ising", "ising"), ("underrelaxation", "underrelax"), ("overrelaxation", "overrelax"),
+                    ("sphere_samp", "sphere"), ("equi_samp", "equi"))
+
+
+def parse_monte_carlo(inp: "InputDeck"):
+    """rw_MC (IO-input/MC_io.f90:92-150): the counts and the sampling method.
+    A logical keyword needs its value (`ising .T.`), as get_bool reads it; more
+    than one method is an error, none gives None."""
+    from .montecarlo import MCInput
+
+    methods = [name for key, name in MC_SAMPLING_KEYS if inp.values(key, 1, fortran_bool, False)]
+    if len(methods) > 1:
+        raise ValueError(f"more than one Monte Carlo sampling method set: {methods}")
+    if not methods:
+        return None
+    return MCInput(n_Tsteps=inp.values("n_Tsteps", 1, int, 1), n_sizerelax=inp.values("n_sizerelax", 1, int, 1),
+                   N_relaxation=inp.values("n_relaxation", 1, int, 1000), T_relax=inp.values("T_relax", 1, int, 1),
+                   T_auto=inp.values("T_auto", 1, int, 1), Total_MC_Steps=inp.values("Total_MC_Steps", 1, int, 1000),
+                   cone=inp.values("cone", 1, default=math.pi), sampling=methods[0])
 
 
 def _rotation_zxz(angles_pi: Sequence[float]) -> np.ndarray:
@@ -301,7 +331,9 @@ def parse_input(path_or_text: str) -> ReferenceInput:
     mn = MinimizeInput(mass=inp.values("masse", 1, default=1.0), timestep=inp.values("timestep", 1, default=0.1),
                        steps=inp.values("steps", 1, int, 2 ** 62), Efreq=inp.values("min_Efreq", 1, int, 100),
                        conv_torque=inp.values("convergence_criteria", 1, default=1e-6))
-    return ReferenceInput(deck=deck, dynamics=dyn, minimize=mn, atom_names=names)
+    sim = inp.values("simulation", 1, str, "")
+    return ReferenceInput(deck=deck, dynamics=dyn, minimize=mn, atom_names=names, simulation=sim,
+                          monte_carlo=parse_monte_carlo(inp))
 
 
 # ----------------------------------------------------------------------
@@ -416,3 +448,46 @@ def run_dynamics(directory: str, integrator: Optional[str] = None, seed: int = 1
             f.writelines(lines)
         write_order_file(os.path.join(directory, "magnetic_final.dat"), mT)
     return mT, lines
+
+
+def run_montecarlo(directory: str, seed: int = 1, write: bool = True):
+    """The Monte Carlo of an input directory on the GPU: reads `input` and
+    `magnetic_init.dat` when present (else a random state from `seed`), the
+    temperatures of ini_temp (Tini .. Tfin in n_Tsteps steps, geometric when a
+    file `geometric` is in the directory, Metropolis-MC/initialize_temperature.f90),
+    then `simulation metropolis` runs montecarlo_run (Metropolis-MC/MonteCarlo.f90)
+    on one lattice, `simulation parallel-tempering` runs parallel_tempering_run
+    (paratemp-MC/parallel_tempering.f90) on n_Tsteps replicas of the lattice.
+    Writes EM.dat (thermo_print) and returns the ThermVal rows."""
+    import torch
+
+    from . import Hamiltonian
+    from .batch import ReplicaBatch
+    from .deck import random_sphere
+    from .montecarlo import montecarlo_run, parallel_tempering_run, temperatures, thermo_print
+
+    ri = parse_input(os.path.join(directory, "input"))
+    inp = ri.monte_carlo
+    if inp is None:
+        raise ValueError("the input sets no Monte Carlo sampling method (ising, underrelaxation, overrelaxation, "
+                         "sphere_samp or equi_samp)")
+    deck = ri.deck
+    N = deck.nsites
+    init = os.path.join(directory, "magnetic_init.dat")
+    m0 = read_order_file(init, N) if os.path.exists(init) else random_sphere(N, seed)
+    temps = temperatures(ri.dynamics.Tini, ri.dynamics.Tfin, inp.n_Tsteps,
+                         geometric=os.path.exists(os.path.join(directory, "geometric")))
+    if ri.simulation == "parallel-tempering":
+        n = len(temps)
+        batch = ReplicaBatch(deck, [deck.L[:2]] * n, np.tile(np.asarray(deck.B_ext, float), (n, 1)), temps)
+        batch.upload(np.tile(m0, (n, 1)))
+        rows = parallel_tempering_run(batch, inp, seed=seed)
+    elif ri.simulation == "metropolis":
+        ham = Hamiltonian(deck)
+        m = torch.tensor(m0.T.copy(), device="cuda")
+        rows = montecarlo_run(ham, m, inp, temps, seed=seed)
+    else:
+        raise ValueError(f"simulation {ri.simulation!r} is not a Monte Carlo (metropolis, parallel-tempering)")
+    if write:
+        thermo_print(os.path.join(directory, "EM.dat"), rows)
+    return rows

@@ -236,3 +236,57 @@ def test_unsupported_plans_and_bad_arguments():
         MetropolisMC(ham3, "heatbath")
     # nothing moved on the refused calls
     assert torch.equal(m3[2], torch.ones(sq.nsites, dtype=torch.float64, device="cuda"))
+
+
+def test_reference_deck_directory_runs_the_monte_carlo(tmp_path):
+    """run_montecarlo on an input directory: the PTMC deck in the reference's
+    input format as `simulation metropolis` and as `simulation
+    parallel-tempering`; EM.dat has one row per temperature, ascending, and the
+    energies agree with the reference's log at those temperatures."""
+    from matjes_b200 import reference_io as R
+
+    deck_text = _MC_DECK
+    for sim, extra in (("metropolis", ""), ("parallel-tempering", "n_sizerelax 1500\n")):
+        d = tmp_path / sim
+        d.mkdir()
+        (d / "input").write_text(deck_text.replace("simulation metropolis", "simulation " + sim) + extra)
+        m0 = np.zeros((400, 3))
+        m0[:, 2] = 1.0
+        R.write_order_file(str(d / "magnetic_init.dat"), m0)
+        rows = R.run_montecarlo(str(d), seed=3)
+        lines = (d / "EM.dat").read_text().splitlines()
+        assert len(rows) == 4 and len(lines) == 5
+        Ts = [r.T for r in rows]
+        assert Ts == sorted(Ts) and Ts[0] == pytest.approx(11.769230769, rel=1e-9)
+        for tv in rows:
+            ref = min(GOLD["rows"], key=lambda r: abs(r[0] - tv.T))
+            assert abs(ref[0] - tv.T) < 1e-6
+            # a few hundred correlated samples: within 6 of the log's sample deviations
+            assert abs(tv.E - ref[1]) <= 6.0 * ref[2] + 1e-9, (sim, tv.T, tv.E, ref[1])
+
+
+_MC_DECK = """simulation metropolis
+Periodic_log .T. .T. .F.
+lattice
+1.0 0.0 0.0
+0.0 1.0 0.0
+0.0 0.0 1.0
+Nsize 20 20 1
+atomtypes 1
+Fe 3.0 0.0 1.0 F
+atoms 1
+Fe 0.0 0.0 0.0
+magnetic_J
+1 1 1 0.5d-3
+magnetic_anisotropy
+1 0.0 0.0 1.0 5.0d-7
+Tini 11.769230769230769
+Tfin 16.384615384615383
+n_Tsteps 4
+n_relaxation 100
+T_relax 1
+T_auto 2
+Total_MC_Steps 600
+cone 1.0
+ising .T.
+"""

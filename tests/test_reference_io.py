@@ -120,3 +120,47 @@ def test_em_dat_rows():
     assert vals[14:19] == [10.0, 9.5, 0.0, 0.0, 1.0]
     # without calc_topo the topology columns hold the reference's placeholder values
     assert vals[11] == pytest.approx(2 * 1.2345789e98, rel=1e-9)
+
+
+MC_DECK = """simulation metropolis
+Periodic_log .T. .T. .F.
+lattice
+1.0 0.0 0.0
+0.0 1.0 0.0
+0.0 0.0 1.0
+Nsize 20 20 1
+atomtypes 1
+Fe 3.0 0.0 1.0 F
+atoms 1
+Fe 0.0 0.0 0.0
+magnetic_J
+1 1 1 0.5d-3
+magnetic_anisotropy
+1 0.0 0.0 1.0 5.0d-7
+Tini 10.0
+Tfin 30.0
+n_Tsteps 3
+n_relaxation 50
+T_relax 2
+T_auto 3
+Total_MC_Steps 400
+cone 0.8
+ising .T.
+"""
+
+
+def test_monte_carlo_keywords():
+    from matjes_b200 import reference_io as R
+
+    ri = R.parse_input(MC_DECK)
+    mc = ri.monte_carlo
+    assert ri.simulation == "metropolis" and mc.sampling == "ising"
+    assert (mc.n_Tsteps, mc.N_relaxation, mc.T_relax, mc.T_auto, mc.Total_MC_Steps) == (3, 50, 2, 3, 400)
+    assert mc.cone == 0.8 and mc.n_sizerelax == 1
+    assert (ri.dynamics.Tini, ri.dynamics.Tfin) == (10.0, 30.0)
+    # rw_MC: one method exactly; get_bool needs the value after the keyword
+    assert R.parse_input(MC_DECK.replace("ising .T.", "ising .F.")).monte_carlo is None
+    with pytest.raises(ValueError, match="more than one"):
+        R.parse_input(MC_DECK + "sphere_samp .T.\n")
+    with pytest.raises(ValueError, match="expected 1 values"):
+        R.parse_input(MC_DECK.replace("ising .T.", "ising"))
