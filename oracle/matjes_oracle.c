@@ -16,6 +16,7 @@
 #include <string.h>
 
 #ifdef _OPENMP
+#include <float.h>
 #include <omp.h>
 #endif
 
@@ -1212,3 +1213,173 @@ int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double*
 }
 
 void orc_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }
+
+/* ------------------------------------------------------------------ */
+/* GNEB minimum-energy path (GNEB/gneb_utils.f90:19-240 find_path)      */
+
+static double gn_ang(const double* a, const double* b) {
+    double c[3];
+    cross3(a, b, c);
+    return atan2(nrm3(c), a[0] * b[0] + a[1] * b[1] + a[2] * b[2]);
+}
+
+/* the_path (GNEB/path.f90:10-29): cumulative geodesic length of the images */
+static void gn_path(const double* img, int nim, int64_t N, double* pl) {
+    pl[0] = 0.0;
+    for (int i = 1; i < nim; i++) {
+        double t = 0.0;
+        for (int64_t s = 0; s < N; s++) {
+            double l = gn_ang(img + ((int64_t)(i - 1) * N + s) * 3, img + ((int64_t)i * N + s) * 3);
+            t += l * l;
+        }
+        pl[i] = pl[i - 1] + sqrt(t);
+    }
+}
+
+/* tau minus its component along each spin, normalised over the image */
+static void gn_project_normalise(const double* m, double* tau, int64_t N) {
+    double t2 = 0.0;
+    for (int64_t s = 0; s < N; s++) {
+        double* t = tau + 3 * s;
+        const double* ms = m + 3 * s;
+        double d = t[0] * ms[0] + t[1] * ms[1] + t[2] * ms[2];
+        for (int k = 0; k < 3; k++) { t[k] -= d * ms[k]; t2 += t[k] * t[k]; }
+    }
+    double inv = 1.0 / sqrt(t2);
+    for (int64_t r = 0; r < 3 * N; r++) tau[r] *= inv;
+}
+
+/* lattice_single (tangent.f90:169-180) and lattice_special (:89-124) */
+static void gn_tang_single(const double* img, int nim, int64_t N, int im, double* tau) {
+    int u1 = im + 1 < nim ? im + 1 : im, u2 = im > 0 ? im - 1 : im;
+    for (int64_t r = 0; r < 3 * N; r++) tau[r] = img[(int64_t)u1 * 3 * N + r] - img[(int64_t)u2 * 3 * N + r];
+    gn_project_normalise(img + (int64_t)im * 3 * N, tau, N);
+}
+static void gn_tang_special(const double* img, int64_t N, int im, const double* u, double* tau) {
+    double u1 = u[im - 1], u2 = u[im], u3 = u[im + 1];
+    const double *a = img + (int64_t)(im - 1) * 3 * N, *b = img + (int64_t)im * 3 * N, *c = img + (int64_t)(im + 1) * 3 * N;
+    if (u3 > u2 && u2 > u1) {
+        for (int64_t r = 0; r < 3 * N; r++) tau[r] = c[r] - b[r];
+    } else if (u1 > u2 && u2 > u3) {
+        for (int64_t r = 0; r < 3 * N; r++) tau[r] = b[r] - a[r];
+    } else {
+        double dmax = fabs(u3 - u2), dmin = fabs(u1 - u2);
+        if (dmax < dmin) { double t = dmax; dmax = dmin; dmin = t; }
+        double wp = u3 > u1 ? dmax : dmin, wm = u3 > u1 ? dmin : dmax;
+        for (int64_t r = 0; r < 3 * N; r++) tau[r] = wp * (c[r] - b[r]) + wm * (b[r] - a[r]);
+    }
+    gn_project_normalise(b, tau, N);
+}
+
+/* rotate_vector_arr (utilities/rotation.f90): v cos + sin (v x ax) + (1 - cos)(ax.v) ax */
+static void gn_rotate(const double* v, const double* ax, double ang, double* out) {
+    double t = ax[0] * v[0] + ax[1] * v[1] + ax[2] * v[2], s = sin(ang), c = cos(ang);
+    out[0] = v[0] * c + s * (ax[2] * v[1] - ax[1] * v[2]) + (1.0 - c) * t * ax[0];
+    out[1] = v[1] * c + s * (ax[0] * v[2] - ax[2] * v[0]) + (1.0 - c) * t * ax[1];
+    out[2] = v[2] * c + s * (ax[1] * v[0] - ax[0] * v[1]) + (1.0 - c) * t * ax[2];
+}
+
+/* the field projected on each spin's tangent plane, and the energy, of every image */
+static void gn_fields(const orc_model* M, const double* img, int i0, int i1, int64_t N, double* F, double* E) {
+    for (int i = i0; i < i1; i++) {
+        const double* m = img + (int64_t)i * 3 * N;
+        double* f = F + (int64_t)i * 3 * N;
+        orc_field(M, m, f, NULL);
+        E[i] = orc_energy(M, m);
+        for (int64_t s = 0; s < N; s++) {
+            double d = f[3 * s] * m[3 * s] + f[3 * s + 1] * m[3 * s + 1] + f[3 * s + 2] * m[3 * s + 2];
+            for (int k = 0; k < 3; k++) f[3 * s + k] -= d * m[3 * s + k];
+        }
+    }
+}
+
+/* GNEB forces of the interior images: the perpendicular part of the force plus the
+ * spring force along the energy-weighted tangent; fpp the force along the simple
+ * tangent (the energy derivative along the path) */
+static void gn_gneb_forces(const double* img, int nim, int64_t N, const double* E, const double* pl, double spring,
+                           double* F, double* fpp, double* tau, double* tau_i) {
+    for (int im = 1; im < nim - 1; im++) {
+        double* f = F + (int64_t)im * 3 * N;
+        gn_tang_special(img, N, im, E, tau);
+        gn_tang_single(img, nim, N, im, tau_i);
+        double fp = 0.0, fi = 0.0;
+        for (int64_t r = 0; r < 3 * N; r++) { fi += f[r] * tau_i[r]; fp += f[r] * tau[r]; }
+        fpp[im] = fi;
+        double sp = spring * (pl[im + 1] + pl[im - 1] - 2.0 * pl[im]);
+        for (int64_t r = 0; r < 3 * N; r++) f[r] = f[r] - tau[r] * fp + sp * tau[r];
+    }
+}
+
+int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, double dt, double mass, double ftol,
+                       int64_t itrmax, int en_zero, double* rx, double* ene, double* dene, int64_t* iters,
+                       double* fchk_out) {
+    if (M->nmag != 1 || nim < 3) return -3;
+    const int64_t N = M->nsite, n3 = 3 * N, tot = (int64_t)nim * n3;
+    double *F1 = calloc((size_t)tot, sizeof(double)), *F2 = calloc((size_t)tot, sizeof(double));
+    double *vel = calloc((size_t)tot, sizeof(double)), *ax = calloc((size_t)tot, sizeof(double));
+    double *ang = calloc((size_t)nim * N, sizeof(double)), *tau = malloc(sizeof(double) * n3);
+    double *tau_i = malloc(sizeof(double) * n3), *E = calloc((size_t)nim, sizeof(double));
+    double *fpp = calloc((size_t)nim, sizeof(double)), *pl = calloc((size_t)nim, sizeof(double));
+    if (!F1 || !F2 || !vel || !ax || !ang || !tau || !tau_i || !E || !fpp || !pl) return -1;
+    gn_path(img, nim, N, pl);
+    gn_fields(M, img, 0, nim, N, F1, E);
+    double eref = en_zero == 'I' ? E[0] : (en_zero == 'F' ? E[nim - 1] : 0.0);
+    gn_gneb_forces(img, nim, N, E, pl, spring, F1, fpp, tau, tau_i);
+    double fchk = 0.0;
+    for (int64_t r = 0; r < tot; r++) fchk = fmax(fchk, fabs(F1[r]));
+    int64_t itr = 0, done = 0;
+    for (itr = 1; itr <= itrmax; itr++) {
+        /* move the interior images: r = m + v dt + F/(2 mass) dt^2, normalised;
+         * the rotation axis m x F1 and the angle of each spin's move kept */
+        for (int im = 1; im < nim - 1; im++)
+            for (int64_t s = 0; s < N; s++) {
+                int64_t o = ((int64_t)im * N + s) * 3;
+                double* m = img + o;
+                double fn[3] = {F1[o], F1[o + 1], F1[o + 2]}, a[3], r[3];
+                double nf = nrm3(fn);
+                if (nf > 1e-30) for (int k = 0; k < 3; k++) fn[k] /= nf;
+                cross3(m, fn, a);
+                double na = nrm3(a);
+                if (na > DBL_EPSILON) for (int k = 0; k < 3; k++) a[k] /= na;
+                for (int k = 0; k < 3; k++) { ax[o + k] = a[k]; r[k] = m[k] + vel[o + k] * dt + 0.5 * F1[o + k] / mass * dt * dt; }
+                double nr = nrm3(r);
+                if (nr > 1e-30) for (int k = 0; k < 3; k++) r[k] /= nr;
+                ang[(int64_t)im * N + s] = gn_ang(r, m);
+                for (int k = 0; k < 3; k++) m[k] = r[k];
+            }
+        gn_fields(M, img, 1, nim - 1, N, F2, E);
+        gn_path(img, nim, N, pl);
+        gn_gneb_forces(img, nim, N, E, pl, spring, F2, fpp, tau, tau_i);
+        /* parallel transport of the velocity and the old force, velocity Verlet */
+        for (int im = 1; im < nim - 1; im++)
+            for (int64_t s = 0; s < N; s++) {
+                int64_t o = ((int64_t)im * N + s) * 3;
+                double vr[3], fr[3], a = ang[(int64_t)im * N + s];
+                gn_rotate(vel + o, ax + o, a, vr);
+                gn_rotate(F1 + o, ax + o, a, fr);
+                for (int k = 0; k < 3; k++) vel[o + k] = vr[k] + 0.5 * (fr[k] + F2[o + k]) / mass * dt;
+            }
+        /* velocity projection on the force (VPO) */
+        double fv = 0.0, fd = 0.0;
+        for (int64_t r = 0; r < tot; r++) { fv += vel[r] * F2[r]; fd += F2[r] * F2[r]; }
+        fv /= nim;
+        fd /= nim;
+        for (int64_t r = 0; r < tot; r++) vel[r] = fv < 0.0 ? 0.0 : F2[r] * fv / fd;
+        fchk = 0.0;
+        for (int64_t r = 0; r < tot; r++) { F1[r] = F2[r]; fchk = fmax(fchk, fabs(F2[r])); }
+        done = itr;
+        if (fchk < ftol) break;
+    }
+    /* the energy derivative along the path at the end images, from their forces */
+    gn_tang_single(img, nim, N, 0, tau_i);
+    fpp[0] = 0.0;
+    for (int64_t r = 0; r < n3; r++) fpp[0] += F1[r] * tau_i[r];
+    gn_tang_single(img, nim, N, nim - 1, tau_i);
+    fpp[nim - 1] = 0.0;
+    for (int64_t r = 0; r < n3; r++) fpp[nim - 1] += F1[(int64_t)(nim - 1) * n3 + r] * tau_i[r];
+    for (int i = 0; i < nim; i++) { rx[i] = pl[i]; ene[i] = E[i] - eref; dene[i] = -fpp[i]; }
+    if (iters) *iters = done;
+    if (fchk_out) *fchk_out = fchk;
+    free(F1); free(F2); free(vel); free(ax); free(ang); free(tau); free(tau_i); free(E); free(fpp); free(pl);
+    return 0;
+}

@@ -27,6 +27,8 @@
  *   - noise sigma = sqrt(alpha kT hbar / dt) ..... dynamics/spindynamics.f90:268-272
  *   - constants .................................. fixed-parameters/constant.f90:11-32
  *   - Metropolis move, acceptance ................ Metropolis-MC/MCstep.f90:37-89
+ *   - GNEB path relaxation (VPO) ................. GNEB/gneb_utils.f90:19-240, GNEB/path.f90:10-29,
+ *                                                  GNEB/tangent.f90:89-180, utilities/rotation.f90
  *   - random site, proposals, cone update ........ Metropolis-MC/choosespin.f90:13-21,
  *                                                  Metropolis-MC/track_value.f90:84-160,
  *                                                  Metropolis-MC/relaxationtype.f90:15-70,
@@ -124,6 +126,21 @@ int orc_minimize_vpo(const orc_model* M, double* m, double dt, double mass, doub
                      int64_t* iters, double* max_torque);
 int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int64_t niter, const int colors[3],
                          int64_t* iters, double* max_torque);
+/* GNEB minimum-energy path of nim images img (nim x N x 3, AoS per image; the
+ * end images stay fixed), single-atom models: find_path (GNEB/gneb_utils.f90:
+ * 19-240) without the climbing image.  Each iteration moves the interior images
+ * by velocity Verlet on the unit sphere (m + v dt + F dt^2 / 2 mass,
+ * normalised), parallel-transports velocity and old force by the rotation of
+ * each spin's move (utilities/rotation.f90 rotate), recomputes the projected
+ * fields, energies, path length (path.f90 the_path) and GNEB forces (force
+ * perpendicular to the energy-weighted tangent, tangent.f90:89-124, plus the
+ * spring force k (l_{i+1} + l_{i-1} - 2 l_i) along it), and projects the
+ * velocity on the force (VPO); it stops when max |F| < ftol.  rx, ene (minus
+ * the initial (en_zero 'I'), final ('F') or no ('N') image energy) and dene =
+ * -F.tau_single per image as en_path.out holds them. */
+int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, double dt, double mass, double ftol,
+                       int64_t itrmax, int en_zero, double* rx, double* ene, double* dene, int64_t* iters,
+                       double* fchk_out);
 /* OpenMP threads of the parallel loops (n <= 0: all processors). */
 void orc_set_threads(int n);
 /* Metropolis Monte Carlo.  proposal: 0 sphereft cone, 1 Ising flip,

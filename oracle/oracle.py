@@ -290,6 +290,24 @@ def mc_random(model, m, st: MC, nsweeps):
     return E, Mg, acc.value
 
 
+def gneb_find_path(model, images, spring=0.5, dt=0.01, mass=1.0, ftol=1e-8, itrmax=10 ** 7, en_zero="I"):
+    """GNEB find_path on images (nim, N, 3), relaxed in place; returns (rx, ene,
+    dene, iterations, max |F|) as en_path.out holds them."""
+    lib.orc_gneb_find_path.restype = C.c_int
+    lib.orc_gneb_find_path.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+    assert images.dtype == np.float64 and images.flags.c_contiguous and images.ndim == 3
+    nim = images.shape[0]
+    rx, ene, dene = np.zeros(nim), np.zeros(nim), np.zeros(nim)
+    it, fc = C.c_int64(), C.c_double()
+    rc = lib.orc_gneb_find_path(model.h, _p(images), nim, spring, dt, mass, ftol, int(itrmax), ord(en_zero), _p(rx),
+                                _p(ene), _p(dene), C.byref(it), C.byref(fc))
+    if rc != 0:
+        raise RuntimeError(f"oracle GNEB failed ({rc})")
+    return rx, ene, dene, it.value, fc.value
+
+
 def set_threads(n: int) -> None:
     """OpenMP threads of the oracle's parallel loops (n <= 0: all processors)."""
     lib.orc_set_threads.argtypes = [C.c_int]
