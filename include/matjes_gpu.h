@@ -397,6 +397,25 @@ mj_status mj_batch_field(mj_batch* b, double* B_dev_soa, double* E_dev, int32_t 
  * difference; each tangent is projected on the tangent space of its image and
  * normalised over the image. */
 mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, double* tau_dev_soa, void* stream);
+/* GNEB minimum-energy path of replicas taken as the images of a path (all of
+ * one size, 3 or more; replica 0 and the last are the fixed end points): the
+ * find_path relaxation of GNEB/gneb_utils.f90:19-240 on the batch's current
+ * state, which it leaves holding the relaxed path.  Per iteration the interior
+ * images move by velocity Verlet, r = m + v dt + F dt^2 / (2 mass) normalised;
+ * F is the projected field minus its component along the energy-weighted
+ * tangent plus the spring force spring (l_{i+1} + l_{i-1} - 2 l_i) along it,
+ * l the geodesic path length; velocity and old force are carried along each
+ * spin's rotation, and the velocity is projected on the force (VPO).  Stops
+ * when max |F| < ftol or after itrmax iterations.  Host outputs (nrep each):
+ * rx the path length at every image, ene the energy above image 0 (en_zero
+ * 'I'), the last image ('F') or zero ('N'), dene the derivative of the energy
+ * along the path (en_path.out of GNEB/io-gneb.f90:83-111); iterations and
+ * max_force (may be NULL) the iterations taken and the final max |F|.
+ * Synchronous: starts after the work queued on the legacy default stream,
+ * returns with the relaxed path in the batch. */
+mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass, double ftol, int64_t itrmax,
+                             int32_t en_zero, double* rx, double* ene, double* dene, int64_t* iterations,
+                             double* max_force);
 /* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
  * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);

@@ -423,6 +423,317 @@ __global__ void __launch_bounds__(256) k_gneb_norm(double* __restrict__ tau, int
     }
 }
 
+// ---------------------------------------------------------------------------
+// GNEB path relaxation (GNEB/gneb_utils.f90:19-240 find_path) on the replicas
+// taken as the images of one path (all of one size n, image r at sites
+// [r n, (r + 1) n)).  Before the first move and for the outputs: the field pass
+// gives the projected forces and energies; k_gneb_seg / k_gneb_pathlen the
+// geodesic path length; k_gneb_tau / k_gneb_norm the tangents; k_gneb_dot_img
+// and k_gneb_force the GNEB force.  An iteration is five launches: the field
+// pass and image energies, k_gneb_tan (per-image |tau|, F.tau, path segments),
+// k_gneb_step (GNEB force, transport, velocity Verlet, velocity projection,
+// stop flag), k_gneb_move.  After the projection the velocity is lam F, lam one
+// number, so neither the velocity nor the tangents are stored.  Every sum is a
+// block partial summed in a fixed order: the iterations are deterministic.
+struct GnebBufs {
+    double *F1, *F2, *ax, *ang, *tau, *E, *pl, *fp, *part, *part2, *scal;
+};
+
+__device__ __forceinline__ double3 gneb_rotate(double3 v, double3 a, double sn, double cs) {
+    // utilities/rotation.f90 rotate_vector_arr: v cos + sin (v x a) + (1 - cos)(a.v) a
+    const double t = dot(a, v);
+    return make_double3(v.x * cs + sn * (a.z * v.y - a.y * v.z) + (1.0 - cs) * t * a.x,
+                        v.y * cs + sn * (a.x * v.z - a.z * v.x) + (1.0 - cs) * t * a.y,
+                        v.z * cs + sn * (a.y * v.x - a.x * v.y) + (1.0 - cs) * t * a.z);
+}
+__device__ __forceinline__ double gneb_ang(double3 a, double3 b) {
+    const double3 c = cross(a, b);
+    return atan2(sqrt(dot(c, c)), dot(a, b));
+}
+
+// one spin's move: r = m + v dt + F dt^2 / (2 mass), normalised; the rotation
+// axis m x F/|F| (rotation_axis_arr) and the angle between r and m kept
+__device__ __forceinline__ void gneb_move_site(double* m, double3 f, double3 v, double* ax, double* ang, int64_t i,
+                                               int64_t Ntot, double dt, double mass) {
+    const double3 m0 = ld3(m, i, Ntot);
+    double3 fn = f;
+    const double nf = sqrt(dot(f, f));
+    if (nf > 1e-30) fn = make_double3(f.x / nf, f.y / nf, f.z / nf);
+    double3 a = cross(m0, fn);
+    const double na = sqrt(dot(a, a));
+    if (na > 2.220446049250313e-16) a = make_double3(a.x / na, a.y / na, a.z / na);
+    st3(ax, i, Ntot, a);
+    const double h = 0.5 / mass * dt * dt;
+    double3 r = make_double3(m0.x + v.x * dt + f.x * h, m0.y + v.y * dt + f.y * h, m0.z + v.z * dt + f.z * h);
+    const double nr = sqrt(dot(r, r));
+    if (nr > 1e-30) r = make_double3(r.x / nr, r.y / nr, r.z / nr);
+    ang[i] = gneb_ang(r, m0);
+    st3(m, i, Ntot, r);
+}
+
+// partial sums of the squared spin angles between images r and r + 1 (the_path)
+__global__ void __launch_bounds__(256) k_gneb_seg(const double* __restrict__ m, int64_t n, int64_t Ntot, double* part) {
+    const int r = blockIdx.y;
+    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double v[1] = {0.0};
+    if (li < n) {
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        const double l = gneb_ang(ld3(m, i, Ntot), ld3(m, i + n, Ntot));
+        v[0] = l * l;
+    }
+    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_gneb_pathlen(const double* part, int nblk, int nrep, double* pl) {
+    __shared__ double seg;
+    if (threadIdx.x == 0) pl[0] = 0.0;
+    for (int r = 0; r + 1 < nrep; ++r) {
+        ordered_sum<1>(part + static_cast<int64_t>(r) * nblk, nblk, &seg);
+        __syncthreads();
+        if (threadIdx.x == 0) pl[r + 1] = pl[r] + sqrt(seg);
+        __syncthreads();
+    }
+}
+
+// partial sums of a.b per image
+__global__ void __launch_bounds__(256) k_gneb_dot(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
+                                                  int64_t Ntot, double* part) {
+    const int r = blockIdx.y;
+    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double v[1] = {0.0};
+    if (li < n) {
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        v[0] = dot(ld3(a, i, Ntot), ld3(b, i, Ntot));
+    }
+    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
+}
+
+// per image: the ordered sum of its partials
+__global__ void __launch_bounds__(256) k_gneb_dot_img(const double* part, int nblk, double* out) {
+    ordered_sum<1>(part + static_cast<int64_t>(blockIdx.x) * nblk, nblk, out + blockIdx.x);
+}
+
+// interior: F = F - tau (F.tau) + k (l_{r+1} + l_{r-1} - 2 l_r) tau; end images:
+// 0, or left as they are (keep_ends, the forces before the first move)
+__global__ void __launch_bounds__(256) k_gneb_force(double* F, const double* __restrict__ tau, const double* __restrict__ fp,
+                                                    const double* __restrict__ pl, int64_t n, int64_t Ntot, int nrep,
+                                                    double spring, int keep_ends) {
+    const int r = blockIdx.y;
+    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (li >= n) return;
+    const int64_t i = static_cast<int64_t>(r) * n + li;
+    if (r == 0 || r == nrep - 1) {
+        if (!keep_ends) st3(F, i, Ntot, make_double3(0.0, 0.0, 0.0));
+        return;
+    }
+    const double3 f = ld3(F, i, Ntot), t = ld3(tau, i, Ntot);
+    const double a = fp[r], k = spring * (pl[r + 1] + pl[r - 1] - 2.0 * pl[r]);
+    st3(F, i, Ntot, make_double3(f.x - t.x * a + k * t.x, f.y - t.y * a + k * t.y, f.z - t.z * a + k * t.z));
+}
+
+// one partial max |F| per block (the forces before the first move)
+__global__ void __launch_bounds__(256) k_gneb_absmax(const double* __restrict__ F, int64_t n3, double* pmax) {
+    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    double fm = k < n3 ? fabs(F[k]) : 0.0;
+    __shared__ double wmax[8];
+    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
+        pmax[blockIdx.x] = mx;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gneb_maxof(const double* __restrict__ pmax, int nb, double* out) {
+    double fm = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) fm = fmax(fm, pmax[b]);
+    __shared__ double wmax[8];
+    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
+        *out = mx;
+    }
+}
+
+// Iteration state on the device: done set by the iteration that stopped (max |F|
+// < ftol or itrmax reached; the iterations after it in a graph do no work but
+// the field pass); the iterations taken.
+struct GnebCtl {
+    int done;
+    int pad;
+    long long iters;
+};
+
+// The energy-weighted tangent of image r at site i (unnormalised, projected on
+// the spin: lattice_special, GNEB/tangent.f90:93-124); m0, mp its spin and the
+// next image's.
+__device__ __forceinline__ double3 gneb_tangent_site(const double* __restrict__ m, int64_t i, int64_t n, int64_t Ntot,
+                                                     int r, int nrep, double wp, double wm, double3& m0, double3& mp) {
+    m0 = ld3(m, i, Ntot);
+    mp = r + 1 < nrep ? ld3(m, i + n, Ntot) : m0;
+    const double3 mm = r > 0 ? ld3(m, i - n, Ntot) : m0;
+    double3 t = make_double3(wp * (mp.x - m0.x) + wm * (m0.x - mm.x), wp * (mp.y - m0.y) + wm * (m0.y - mm.y),
+                             wp * (mp.z - m0.z) + wm * (m0.z - mm.z));
+    const double d = dot(t, m0);
+    return make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
+}
+
+// Per image (r = blockIdx.x: the images of one site range run side by side, so
+// a spin read for the neighbouring images' tangents comes from L2): the
+// partials of |tau|^2, F.tau and the squared angles to the next image; the last
+// block of an image sums them in block order: inv[r] = 1/|tau|, fp[r] = F.tau
+// / |tau|, seg[r] = the geodesic distance from image r to r + 1.
+template <int SPT>
+__global__ void __launch_bounds__(256) k_gneb_tan(const double* __restrict__ m, const double* __restrict__ F,
+                                                  const double* __restrict__ E, int64_t n, int64_t Ntot, int nrep,
+                                                  double* part, unsigned int* cnt, double* img, const GnebCtl* ctl) {
+    if (ctl->done) return;
+    const int r = blockIdx.x;
+    const int nblk = gridDim.y;
+    double wp, wm;
+    gneb_weights(E, r, nrep, 0, wp, wm);
+    double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < SPT; ++k) {
+        const int64_t li = (static_cast<int64_t>(blockIdx.y) * SPT + k) * blockDim.x + threadIdx.x;
+        if (li >= n) break;
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        double3 m0, mp;
+        const double3 t = gneb_tangent_site(m, i, n, Ntot, r, nrep, wp, wm, m0, mp);
+        v[0] += dot(t, t);
+        v[1] += dot(ld3(F, i, Ntot), t);
+        if (r + 1 < nrep) {
+            const double l = gneb_ang(m0, mp);
+            v[2] += l * l;
+        }
+    }
+    double* pr = part + static_cast<int64_t>(r) * 3 * nblk;
+    block_partials<3>(v, pr, nblk, blockIdx.y);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(cnt + r, 1u) == static_cast<unsigned int>(nblk - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sums[3];
+    ordered_sum<3>(pr, nblk, sums);
+    if (threadIdx.x == 0) {
+        const double inv = sums[0] > 0.0 ? 1.0 / sqrt(sums[0]) : 0.0;
+        img[r] = sums[1] * inv;
+        img[nrep + r] = inv;
+        img[2 * nrep + r] = sqrt(sums[2]);
+        cnt[r] = 0u;
+    }
+}
+
+// Interior images: tau the tangent again (the same arithmetic as k_gneb_tan)
+// over |tau|, F = F - tau fp + k (seg_r - seg_{r-1}) tau, stored; the old
+// velocity lam Fo (the projection of the previous iteration, lam = scal[3]) and
+// the old force Fo carried along the spin's rotation R of the move, v = lam R Fo
+// + (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
+// and F.F in block order, takes max |F|, sets lam = v.F / F.F (0 when v.F < 0;
+// the velocity projection, v = lam F), counts the iteration and sets the stop
+// flag.
+template <int SPT>
+__global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ Fo,
+                                                   double* Fn, const double* __restrict__ E,
+                                                   const double* __restrict__ ax, const double* __restrict__ ang,
+                                                   const double* __restrict__ img, int64_t n, int64_t Ntot, int nrep,
+                                                   double spring, double dt, double mass, double ftol, long long itrmax,
+                                                   double* part, double* pmax, unsigned int* cnt, GnebCtl* ctl,
+                                                   double* scal) {
+    if (ctl->done) return;
+    const int r = blockIdx.x;
+    const int nb = gridDim.x * gridDim.y, bid = blockIdx.x + gridDim.x * blockIdx.y;
+    const bool inner = r > 0 && r < nrep - 1;
+    double wp = 0.0, wm = 0.0;
+    if (inner) gneb_weights(E, r, nrep, 0, wp, wm);
+    const double inv = inner ? img[nrep + r] : 0.0, a = inner ? img[r] : 0.0;
+    const double k = inner ? spring * (img[2 * nrep + r] - img[2 * nrep + r - 1]) : 0.0;
+    const double h = 0.5 / mass * dt, lam = scal[3];
+    double v2[2] = {0.0, 0.0}, fm = 0.0;
+#pragma unroll
+    for (int q = 0; q < SPT; ++q) {
+        const int64_t li = (static_cast<int64_t>(blockIdx.y) * SPT + q) * blockDim.x + threadIdx.x;
+        if (li >= n) break;
+        const int64_t i = static_cast<int64_t>(r) * n + li;
+        double3 f = make_double3(0.0, 0.0, 0.0), v = f;
+        if (inner) {
+            double3 m0, mp;
+            const double3 t0 = gneb_tangent_site(m, i, n, Ntot, r, nrep, wp, wm, m0, mp);
+            const double3 t = make_double3(t0.x * inv, t0.y * inv, t0.z * inv);
+            const double3 g = ld3(Fn, i, Ntot);
+            f = make_double3(g.x - t.x * a + k * t.x, g.y - t.y * a + k * t.y, g.z - t.z * a + k * t.z);
+            double sn, cs;
+            sincos(ang[i], &sn, &cs);
+            const double3 fr = gneb_rotate(ld3(Fo, i, Ntot), ld3(ax, i, Ntot), sn, cs);
+            v = make_double3(lam * fr.x + (fr.x + f.x) * h, lam * fr.y + (fr.y + f.y) * h,
+                             lam * fr.z + (fr.z + f.z) * h);
+        }
+        st3(Fn, i, Ntot, f);
+        v2[0] += dot(v, f);
+        v2[1] += dot(f, f);
+        fm = fmax(fm, fmax(fabs(f.x), fmax(fabs(f.y), fabs(f.z))));
+    }
+    block_partials<2>(v2, part, nb, bid);
+    __shared__ double wmax[8];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
+        pmax[bid] = mx;
+        __threadfence();
+        last = atomicAdd(cnt, 1u) == static_cast<unsigned int>(nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sums[2];
+    ordered_sum<2>(part, nb, sums);
+    fm = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) fm = fmax(fm, __ldcg(pmax + b));
+    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
+        const double fv = sums[0] / nrep, fd = sums[1] / nrep;
+        scal[0] = fv;
+        scal[1] = fd;
+        scal[2] = mx;
+        scal[3] = fv < 0.0 ? 0.0 : fv / fd;
+        const long long it = ctl->iters + 1;
+        ctl->iters = it;
+        if (mx < ftol || it >= itrmax) ctl->done = 1;
+        *cnt = 0u;
+    }
+}
+
+// Unless stopped: the move of the interior images with v = lam F (lam = scal[3])
+// and F the force of the iteration, r = m + F (lam dt + dt^2 / (2 mass)).
+__global__ void __launch_bounds__(256) k_gneb_move(double* m, const double* __restrict__ F, double* ax, double* ang,
+                                                   const double* __restrict__ scal, const GnebCtl* ctl, int64_t n,
+                                                   int64_t Ntot, double dt, double mass) {
+    if (ctl->done) return;
+    const int64_t i = n + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= Ntot - n) return;
+    const double3 f = ld3(F, i, Ntot);
+    const double lam = scal[3];
+    gneb_move_site(m, f, make_double3(lam * f.x, lam * f.y, lam * f.z), ax, ang, i, Ntot, dt, mass);
+}
+
 template <class S, int BYT, int RY>
 struct BatchLauncher {
     using G = TileGeom<S, BYT, RY>;
@@ -1142,6 +1453,215 @@ mj_status mj_batch_mc_state(mj_batch* b, double* cone, int64_t* accepted, int64_
         st = cuda_status(cudaMemcpy(accepted, b->d_mc_acc, sizeof(int64_t) * n, cudaMemcpyDeviceToHost), "MC state");
     if (st == MJ_OK && proposed)
         st = cuda_status(cudaMemcpy(proposed, b->d_mc_prop, sizeof(int64_t) * n, cudaMemcpyDeviceToHost), "MC state");
+    return st;
+}
+
+// ---- GNEB path relaxation --------------------------------------------------
+
+mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass, double ftol, int64_t itrmax,
+                             int32_t en_zero, double* rx, double* ene, double* dene, int64_t* iterations,
+                             double* max_force) {
+    if (!b || !rx || !ene || !dene || b->nrep < 3 || !(dt > 0.0) || !(mass > 0.0) || itrmax < 0 ||
+        (en_zero != 'I' && en_zero != 'F' && en_zero != 'N'))
+        return set_error(MJ_ERR_ARG, "bad GNEB arguments (3 or more images, dt > 0, mass > 0, en_zero I/F/N)");
+    for (int r = 1; r < b->nrep; ++r)
+        if (b->reps[r].Lx != b->reps[0].Lx || b->reps[r].Ly != b->reps[0].Ly)
+            return set_error(MJ_ERR_UNSUPPORTED, "a path needs images of one size");
+    cudaSetDevice(b->device);
+    const int nrep = b->nrep;
+    const int64_t Ntot = b->Ntot, n = Ntot / nrep;
+    const int nblk = static_cast<int>((n + 255) / 256);
+    const int nbv = nblk * nrep;
+    const int n3b = static_cast<int>((3 * Ntot + 255) / 256);
+    const int nsite_b = static_cast<int>((Ntot + 255) / 256);
+    mj_status st;
+    if (!b->d_gneb_part &&
+        (st = cuda_status(cudaMalloc(&b->d_gneb_part, sizeof(double) * nblk * nrep), "tangent partials")) != MJ_OK)
+        return st;
+    if (!b->cap_stream &&
+        (st = cuda_status(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "capture stream")) != MJ_OK)
+        return st;
+    // F1 / F2 the forces of alternate iterations, ax / ang the moves' rotations,
+    // tau the tangents of the forces before the first move and of the outputs
+    // (SoA, 3 Ntot each); E / pl / fp per image, img the iteration's per-image
+    // 1/|tau|, F.tau / |tau| and segment lengths, scal (v.F, F.F, max |F|, lam);
+    // part / part2 block partials; cnt the last-block counters; ctl the stop flag
+    GnebBufs g;
+    std::memset(&g, 0, sizeof(g));
+    double* img = nullptr;
+    unsigned int* cnt = nullptr;
+    GnebCtl* ctl = nullptr;
+    double** bufs[] = {&g.F1, &g.F2, &g.ax, &g.tau};
+    st = MJ_OK;
+    for (double** q : bufs)
+        if (st == MJ_OK) st = cuda_status(cudaMalloc(q, sizeof(double) * 3 * Ntot), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.ang, sizeof(double) * Ntot), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.E, sizeof(double) * (6 * nrep + 4)), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part, sizeof(double) * 3 * nbv), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part2, sizeof(double) * std::max(3 * nbv, n3b)), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * (nrep + 1)), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&ctl, sizeof(GnebCtl)), "GNEB buffers");
+    cudaGraphExec_t exec = nullptr;
+    auto release = [&]() {
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaFree(g.F1);
+        cudaFree(g.F2);
+        cudaFree(g.ax);
+        cudaFree(g.tau);
+        cudaFree(g.ang);
+        cudaFree(g.E);
+        cudaFree(g.part);
+        cudaFree(g.part2);
+        cudaFree(cnt);
+        cudaFree(ctl);
+    };
+    if (st != MJ_OK) {
+        release();
+        return st;
+    }
+    g.pl = g.E + nrep;
+    g.fp = g.E + 2 * nrep;
+    img = g.E + 3 * nrep;
+    g.scal = g.E + 6 * nrep;
+    // the path as the work queued on the legacy default stream (an upload) leaves it
+    cudaStream_t s = b->cap_stream;
+    if ((st = cuda_status(cudaStreamSynchronize(0), "GNEB start")) != MJ_OK) {
+        release();
+        return st;
+    }
+    GnebCtl c0;
+    std::memset(&c0, 0, sizeof(c0));
+    cudaMemsetAsync(g.ang, 0, sizeof(double) * Ntot, s);
+    cudaMemsetAsync(g.scal, 0, sizeof(double) * 4, s);
+    cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * (nrep + 1), s);
+    cudaMemcpyAsync(ctl, &c0, sizeof(c0), cudaMemcpyHostToDevice, s);
+    DynCoef c;
+    std::memset(&c, 0, sizeof(c));
+    const dim3 gi(nblk, nrep), gs(nblk, nrep - 1);
+    const int nmove = static_cast<int>((Ntot - 2 * n + 255) / 256);
+    // the field pass: projected fields into F, tile energies, image energies E
+    auto field = [&](double* F) -> mj_status {
+        BatchArgs A = batch_args(b, 0, 0.0);
+        A.out = F;
+        A.project = 1;
+        A.tile_e = b->d_tile_e;
+        mj_status e = batch_pass(b->shape, b->variant, BPASS_FIELD, b->sp, c, A, batch_blocks(b), s);
+        if (e != MJ_OK) return e;
+        k_batch_energy<<<nrep, 256, 0, s>>>(b->d_reps, nrep, b->d_tile_e, g.E);
+        return cuda_status(cudaGetLastError(), "k_batch_energy");
+    };
+    // field pass, path length pl, tangents of the given mode, fp = F.tau per image
+    auto forces = [&](double* F, int mode) -> mj_status {
+        mj_status e = field(F);
+        if (e != MJ_OK) return e;
+        k_gneb_seg<<<gs, 256, 0, s>>>(b->d_m, n, Ntot, g.part);
+        k_gneb_pathlen<<<1, 256, 0, s>>>(g.part, nblk, nrep, g.pl);
+        k_gneb_tau<<<gi, 256, 0, s>>>(b->d_m, n, Ntot, nrep, g.E, mode, g.tau, b->d_gneb_part);
+        k_gneb_norm<<<nrep, 256, 0, s>>>(g.tau, n, Ntot, b->d_gneb_part, nblk);
+        k_gneb_dot<<<gi, 256, 0, s>>>(F, g.tau, n, Ntot, g.part);
+        k_gneb_dot_img<<<nrep, 256, 0, s>>>(g.part, nblk, g.fp);
+        return cuda_status(cudaGetLastError(), "GNEB forces");
+    };
+    // initial forces: every image's projected field, the GNEB force of the interior
+    // ones; max |F| over them all (the convergence check before any move)
+    if ((st = forces(g.F1, 0)) != MJ_OK) {
+        release();
+        return st;
+    }
+    k_gneb_force<<<gi, 256, 0, s>>>(g.F1, g.tau, g.fp, g.pl, n, Ntot, nrep, spring, 1);
+    k_gneb_absmax<<<n3b, 256, 0, s>>>(g.F1, 3 * Ntot, g.part2);
+    k_gneb_maxof<<<1, 256, 0, s>>>(g.part2, n3b, g.scal + 2);
+    double h0[4];
+    cudaMemcpyAsync(h0, g.E, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h0 + 1, g.E + nrep - 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(h0 + 2, g.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if ((st = cuda_status(cudaStreamSynchronize(s), "GNEB initial forces")) != MJ_OK) {
+        release();
+        return st;
+    }
+    const double E_first = h0[0], E_last = h0[1];
+    double fchk = h0[2];
+    int64_t done = 0;
+    if (itrmax > 0) {
+        // the first move (lam = 0: the velocity starts at zero), then chunks of
+        // iterations replayed as one graph: field pass, image energies,
+        // k_gneb_tan, k_gneb_step, k_gneb_move.  The force buffers alternate (an
+        // even chunk starts each replay on F1).  The stop flag is read after each
+        // chunk; the iterations of a chunk after the stop do no work but the
+        // field pass.
+        const int chunk = 32;
+        // four sites per thread once that still gives two blocks per SM: the loads
+        // of four sites in flight before each block's reduction
+        const bool spt4 = Ntot >= 2LL * 1024 * b->num_sms;
+        const dim3 gt(nrep, static_cast<unsigned>(spt4 ? (n + 1023) / 1024 : nblk));
+        k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, g.F1, g.ax, g.ang, g.scal, ctl, n, Ntot, dt, mass);
+        st = cuda_status(cudaGetLastError(), "k_gneb_move");
+        if (st == MJ_OK) st = cuda_status(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        if (st == MJ_OK) {
+            mj_status inner = MJ_OK;
+            for (int k = 0; k < chunk && inner == MJ_OK; ++k) {
+                double* Fo = (k & 1) ? g.F2 : g.F1;
+                double* Fn = (k & 1) ? g.F1 : g.F2;
+                inner = field(Fn);
+                if (inner != MJ_OK) break;
+                const long long im = static_cast<long long>(itrmax);
+                if (spt4) {
+                    k_gneb_tan<4><<<gt, 256, 0, s>>>(b->d_m, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                    k_gneb_step<4><<<gt, 256, 0, s>>>(b->d_m, Fo, Fn, g.E, g.ax, g.ang, img, n, Ntot, nrep, spring, dt,
+                                                      mass, ftol, im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl,
+                                                      g.scal);
+                } else {
+                    k_gneb_tan<1><<<gt, 256, 0, s>>>(b->d_m, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                    k_gneb_step<1><<<gt, 256, 0, s>>>(b->d_m, Fo, Fn, g.E, g.ax, g.ang, img, n, Ntot, nrep, spring, dt,
+                                                      mass, ftol, im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl,
+                                                      g.scal);
+                }
+                k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, Fn, g.ax, g.ang, g.scal, ctl, n, Ntot, dt, mass);
+                inner = cuda_status(cudaGetLastError(), "GNEB iteration");
+            }
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(s, &graph);
+            if (inner != MJ_OK) st = inner;
+            else if ((st = cuda_status(e, "end capture")) == MJ_OK)
+                st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+            if (graph) cudaGraphDestroy(graph);
+        }
+        GnebCtl hc = c0;
+        while (st == MJ_OK) {
+            const long long before = hc.iters;
+            if ((st = cuda_status(cudaGraphLaunch(exec, s), "GNEB graph launch")) != MJ_OK) break;
+            cudaMemcpyAsync(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost, s);
+            if ((st = cuda_status(cudaStreamSynchronize(s), "GNEB iterations")) != MJ_OK) break;
+            if (hc.done) break;
+            if (hc.iters != before + chunk) st = set_error(MJ_ERR_CUDA, "GNEB iterations did not advance");
+        }
+        done = hc.iters;
+        if (st == MJ_OK) {
+            cudaMemcpyAsync(&fchk, g.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
+            st = cuda_status(cudaStreamSynchronize(s), "GNEB force");
+        }
+    }
+    // outputs (en_path.out): path length, energy above the reference image, and the
+    // derivative along the path -F.tau of the final images' projected fields along
+    // the simple tangent (lattice_single); the end images' forces are zero after a
+    // move, their projected fields before any
+    std::vector<double> h(3 * nrep);
+    if (st == MJ_OK) st = forces(g.F2, 1);
+    if (st == MJ_OK) {
+        cudaMemcpyAsync(h.data(), g.E, sizeof(double) * 3 * nrep, cudaMemcpyDeviceToHost, s);
+        st = cuda_status(cudaStreamSynchronize(s), "GNEB outputs");
+    }
+    if (st == MJ_OK) {
+        const double eref = en_zero == 'I' ? E_first : (en_zero == 'F' ? E_last : 0.0);
+        for (int r = 0; r < nrep; ++r) {
+            rx[r] = h[nrep + r];
+            ene[r] = (r == 0 ? E_first : (r == nrep - 1 ? E_last : h[r])) - eref;
+            dene[r] = (r == 0 || r == nrep - 1) && done > 0 ? 0.0 : -h[2 * nrep + r];
+        }
+        if (iterations) *iterations = done;
+        if (max_force) *max_force = fchk;
+    }
+    release();
     return st;
 }
 

@@ -3,8 +3,9 @@
 ``GNEBInput`` carries the reference's GNEB input (IO-input/GNEB_io.f90, same
 names and defaults).  ``geodesic_path`` builds the initial path
 (GNEB/path.f90:100-174), ``find_path`` relaxes it on the device
-(GNEB/gneb_utils.f90:19-240 find_path, velocity projection on the images of a
-ReplicaBatch: mj_batch_gneb_find_path), ``hermite_fit``, ``find_sp`` and
+(GNEB/gneb_utils.f90:19-240 find_path, velocity projection on the images held
+as the replicas of a ReplicaBatch: mj_batch_gneb_path), ``hermite_fit``,
+``find_sp`` and
 ``spline_hermite_val`` interpolate the energy along the path and locate the
 saddle point (extrapolation/spline.f90, gneb_utils.f90:242-291), ``write_en``
 writes en_path.out / enfit_path.out / ensp_path.out (GNEB/io-gneb.f90:83-111).
@@ -154,6 +155,24 @@ def find_sp(rx, c) -> Tuple[int, float]:
     if 0.0 < x2 < dl:
         return imax, float(x2)
     raise ValueError("energy maximum has not been found")
+
+
+def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: int = 0):
+    """Relax the path images (nim, N, 3) of the single-atom 2D lattice of deck
+    (its L, boundaries, couplings and field) on the device: GNEB find_path with
+    the end images fixed.  Returns (relaxed images (nim, N, 3), rx, ene, dene,
+    iterations, max |F|); rx / ene / dene as en_path.out holds them."""
+    from .batch import ReplicaBatch
+
+    img = np.ascontiguousarray(images, np.float64)
+    nim, N = img.shape[0], img.shape[1]
+    if img.ndim != 3 or img.shape[2] != 3 or nim < 3 or N != deck.ncell:
+        raise ValueError("images are (nim >= 3, deck sites, 3)")
+    batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)), [0.0] * nim,
+                         device=device)
+    batch.upload(img.reshape(nim * N, 3))
+    rx, ene, dene, iters, fchk = batch.gneb_path(inp.spring, inp.dt, inp.mass, inp.mepftol, inp.itrmax, inp.en_zero)
+    return batch.download().reshape(nim, N, 3), rx, ene, dene, iters, fchk
 
 
 def write_en(path: str, x, y, dy, x0: Optional[float] = None) -> None:
