@@ -548,6 +548,71 @@ def run_monte_carlo(dev: int, sweeps: int = 100) -> dict:
                              "sample": "256x256 square film, 60 sweeps of random-site moves (orc_mc_random)"}}
 
 
+def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
+    """GNEB path relaxation (find_path, velocity projection): a DMI film side x
+    side (J + D + K + Bz = 0.3 T, periodic) with a path of nim images from +z to
+    -z (geodesic, every interior spin moved by up to 1e-2), max |F| tolerance 0
+    so that every call runs its itrmax iterations.  The iteration rate is the
+    difference of a 600- and a 100-iteration call, each the fastest of three
+    (setup, first forces and outputs cancel; the call is synchronous and timed
+    on the host); the rate is image-site iterations per second.  Algorithmic
+    bytes per site and iteration: field pass m in, F out (48); per-image sums m,
+    F in (48); GNEB force and transport m, m_old, F, F_old in (96), F out (24);
+    move m, F in (48), m out (24): 288.
+    The CPU baseline is the oracle's find_path on one host core on the same
+    path for 20 iterations."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200.gneb import geodesic_path
+    from oracle import oracle as O
+
+    deck = mj.square_film((side, side, 1), Jv=1e-3, Dv=0.4e-3, Kv=-0.2e-3, Bz=0.3, mu_s=2.0, periodic=(1, 1, 0))
+    n = side * side
+    up = np.tile([0.0, 0.0, 1.0], (n, 1))
+    path = geodesic_path(up, -up, nim, amp_rnd=1e-2, seed=1)
+    path[0], path[-1] = up, -up
+    path = np.ascontiguousarray(path)
+    batch = mj.ReplicaBatch(deck, [(side, side)] * nim, np.tile(deck.B_ext, (nim, 1)), [0.0] * nim, device=dev)
+
+    def call(its):
+        batch.upload(path.reshape(-1, 3))
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = batch.gneb_path(0.3, 0.02, 1.0, 0.0, its, "I")
+        dt = time.perf_counter() - t0
+        assert r[3] == its
+        return dt
+
+    call(40)
+    short = min(call(100) for _ in range(3))
+    long_ = min(call(600) for _ in range(3))
+    per_it = (long_ - short) / 500
+    pk = peaks()
+    bpsite = 288.0
+    ach = bpsite * n * nim / per_it / 1e9
+    mod = O.Model(deck)
+    O.set_threads(1)
+    try:
+        t0 = time.perf_counter()
+        O.gneb_find_path(mod, path.copy(), spring=0.3, dt=0.02, mass=1.0, ftol=0.0, itrmax=20, en_zero="I")
+        ct = time.perf_counter() - t0
+    finally:
+        O.set_threads(0)
+    return {"workload": f"square{side}_path{nim}_gneb", "sites": n * nim, "images": nim,
+            "value": n * nim / per_it, "unit": "image-site iterations/s", "us_per_iteration": 1e6 * per_it,
+            "launches_per_iteration": 5,
+            "roofline": {"bound": "hbm", "alg_bytes_per_site": bpsite, "achieved": ach, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"]},
+            "cpu_baseline": {"value": n * nim * 20 / ct, "unit": "image-site iterations/s", "cores": 1,
+                             "kind": "port",
+                             "sample": f"{side}x{side} film, {nim} images, 20 iterations (orc_gneb_find_path, "
+                                       f"forces before the first move and outputs included)"}}
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -675,6 +740,7 @@ def run_gpu(args, rank, world):
     dipolar = run_dipolar(dev) if (world == 1 and not args.no_batch) else None
     monte_carlo = run_monte_carlo(dev) if (world == 1 and not args.no_batch) else None
     hbm_resident = run_hbm_resident(dev) if (world == 1 and not args.no_batch) else None
+    gneb = run_gneb(dev) if (world == 1 and not args.no_batch) else None
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -704,6 +770,7 @@ def run_gpu(args, rank, world):
         "dipolar": dipolar,
         "monte_carlo": monte_carlo,
         "hbm_resident_4096": hbm_resident,
+        "gneb": gneb,
     }
     print(json.dumps(line), flush=True)
 

@@ -406,21 +406,27 @@ __global__ void __launch_bounds__(256) k_gneb_tau(const double* __restrict__ m, 
     block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
 }
 
-// per image: the ordered sum of its partials, then tau /= sqrt(sum)
-__global__ void __launch_bounds__(256) k_gneb_norm(double* __restrict__ tau, int64_t n, int64_t Ntot,
-                                                   const double* __restrict__ part, int nblk) {
+// per image: the ordered sum of its partials; 1/sqrt(sum) left in the image's
+// first partial
+__global__ void __launch_bounds__(256) k_gneb_norm_sum(double* part, int nblk) {
     const int r = blockIdx.x;
     __shared__ double tot;
-    if (threadIdx.x == 0) tot = 0.0;
     ordered_sum<1>(part + static_cast<int64_t>(r) * nblk, nblk, &tot);
     __syncthreads();
-    const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
-    for (int64_t li = threadIdx.x; li < n; li += blockDim.x) {
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        tau[i] *= inv;
-        tau[Ntot + i] *= inv;
-        tau[2 * Ntot + i] *= inv;
-    }
+    if (threadIdx.x == 0) part[static_cast<int64_t>(r) * nblk] = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+}
+
+// tau /= |tau| of its image
+__global__ void __launch_bounds__(256) k_gneb_scale(double* __restrict__ tau, int64_t n, int64_t Ntot,
+                                                    const double* __restrict__ part, int nblk) {
+    const int r = blockIdx.y;
+    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (li >= n) return;
+    const double inv = part[static_cast<int64_t>(r) * nblk];
+    const int64_t i = static_cast<int64_t>(r) * n + li;
+    tau[i] *= inv;
+    tau[Ntot + i] *= inv;
+    tau[2 * Ntot + i] *= inv;
 }
 
 // ---------------------------------------------------------------------------
@@ -428,15 +434,16 @@ __global__ void __launch_bounds__(256) k_gneb_norm(double* __restrict__ tau, int
 // taken as the images of one path (all of one size n, image r at sites
 // [r n, (r + 1) n)).  Before the first move and for the outputs: the field pass
 // gives the projected forces and energies; k_gneb_seg / k_gneb_pathlen the
-// geodesic path length; k_gneb_tau / k_gneb_norm the tangents; k_gneb_dot_img
-// and k_gneb_force the GNEB force.  An iteration is five launches: the field
-// pass and image energies, k_gneb_tan (per-image |tau|, F.tau, path segments),
+// geodesic path length; k_gneb_tau / k_gneb_norm_sum / k_gneb_scale the
+// tangents; k_gneb_dot_img and k_gneb_force the GNEB force.  An iteration is
+// five launches: the field pass and image energies, k_gneb_tan (per-image
+// |tau|, F.tau, path segments),
 // k_gneb_step (GNEB force, transport, velocity Verlet, velocity projection,
 // stop flag), k_gneb_move.  After the projection the velocity is lam F, lam one
 // number, so neither the velocity nor the tangents are stored.  Every sum is a
 // block partial summed in a fixed order: the iterations are deterministic.
 struct GnebBufs {
-    double *F1, *F2, *ax, *ang, *tau, *E, *pl, *fp, *part, *part2, *scal;
+    double *F1, *F2, *mB, *tau, *E, *pl, *fp, *part, *part2, *scal;
 };
 
 __device__ __forceinline__ double3 gneb_rotate(double3 v, double3 a, double sn, double cs) {
@@ -449,26 +456,6 @@ __device__ __forceinline__ double3 gneb_rotate(double3 v, double3 a, double sn, 
 __device__ __forceinline__ double gneb_ang(double3 a, double3 b) {
     const double3 c = cross(a, b);
     return atan2(sqrt(dot(c, c)), dot(a, b));
-}
-
-// one spin's move: r = m + v dt + F dt^2 / (2 mass), normalised; the rotation
-// axis m x F/|F| (rotation_axis_arr) and the angle between r and m kept
-__device__ __forceinline__ void gneb_move_site(double* m, double3 f, double3 v, double* ax, double* ang, int64_t i,
-                                               int64_t Ntot, double dt, double mass) {
-    const double3 m0 = ld3(m, i, Ntot);
-    double3 fn = f;
-    const double nf = sqrt(dot(f, f));
-    if (nf > 1e-30) fn = make_double3(f.x / nf, f.y / nf, f.z / nf);
-    double3 a = cross(m0, fn);
-    const double na = sqrt(dot(a, a));
-    if (na > 2.220446049250313e-16) a = make_double3(a.x / na, a.y / na, a.z / na);
-    st3(ax, i, Ntot, a);
-    const double h = 0.5 / mass * dt * dt;
-    double3 r = make_double3(m0.x + v.x * dt + f.x * h, m0.y + v.y * dt + f.y * h, m0.z + v.z * dt + f.z * h);
-    const double nr = sqrt(dot(r, r));
-    if (nr > 1e-30) r = make_double3(r.x / nr, r.y / nr, r.z / nr);
-    ang[i] = gneb_ang(r, m0);
-    st3(m, i, Ntot, r);
 }
 
 // partial sums of the squared spin angles between images r and r + 1 (the_path)
@@ -636,16 +623,16 @@ __global__ void __launch_bounds__(256) k_gneb_tan(const double* __restrict__ m, 
 // Interior images: tau the tangent again (the same arithmetic as k_gneb_tan)
 // over |tau|, F = F - tau fp + k (seg_r - seg_{r-1}) tau, stored; the old
 // velocity lam Fo (the projection of the previous iteration, lam = scal[3]) and
-// the old force Fo carried along the spin's rotation R of the move, v = lam R Fo
-// + (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
+// the old force Fo carried along the rotation R that took the spin from mo to
+// m, v = lam R Fo + (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
 // and F.F in block order, takes max |F|, sets lam = v.F / F.F (0 when v.F < 0;
 // the velocity projection, v = lam F), counts the iteration and sets the stop
 // flag.
 template <int SPT>
-__global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ Fo,
-                                                   double* Fn, const double* __restrict__ E,
-                                                   const double* __restrict__ ax, const double* __restrict__ ang,
-                                                   const double* __restrict__ img, int64_t n, int64_t Ntot, int nrep,
+__global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ mo,
+                                                   const double* __restrict__ Fo, double* Fn,
+                                                   const double* __restrict__ E, const double* __restrict__ img,
+                                                   int64_t n, int64_t Ntot, int nrep,
                                                    double spring, double dt, double mass, double ftol, long long itrmax,
                                                    double* part, double* pmax, unsigned int* cnt, GnebCtl* ctl,
                                                    double* scal) {
@@ -671,9 +658,17 @@ __global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m,
             const double3 t = make_double3(t0.x * inv, t0.y * inv, t0.z * inv);
             const double3 g = ld3(Fn, i, Ntot);
             f = make_double3(g.x - t.x * a + k * t.x, g.y - t.y * a + k * t.y, g.z - t.z * a + k * t.z);
-            double sn, cs;
-            sincos(ang[i], &sn, &cs);
-            const double3 fr = gneb_rotate(ld3(Fo, i, Ntot), ld3(ax, i, Ntot), sn, cs);
+            // the move's rotation: axis mo x Fo/|Fo| (rotation_axis_arr), angle
+            // between mo and m (sin |m x mo|, cos m.mo)
+            const double3 m1 = ld3(mo, i, Ntot), fo = ld3(Fo, i, Ntot);
+            double3 fn = fo;
+            const double nf = sqrt(dot(fo, fo));
+            if (nf > 1e-30) fn = make_double3(fo.x / nf, fo.y / nf, fo.z / nf);
+            double3 e = cross(m1, fn);
+            const double ne = sqrt(dot(e, e));
+            if (ne > 2.220446049250313e-16) e = make_double3(e.x / ne, e.y / ne, e.z / ne);
+            const double3 c = cross(m0, m1);
+            const double3 fr = gneb_rotate(fo, e, sqrt(dot(c, c)), dot(m0, m1));
             v = make_double3(lam * fr.x + (fr.x + f.x) * h, lam * fr.y + (fr.y + f.y) * h,
                              lam * fr.z + (fr.z + f.z) * h);
         }
@@ -721,17 +716,27 @@ __global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m,
     }
 }
 
-// Unless stopped: the move of the interior images with v = lam F (lam = scal[3])
-// and F the force of the iteration, r = m + F (lam dt + dt^2 / (2 mass)).
-__global__ void __launch_bounds__(256) k_gneb_move(double* m, const double* __restrict__ F, double* ax, double* ang,
-                                                   const double* __restrict__ scal, const GnebCtl* ctl, int64_t n,
-                                                   int64_t Ntot, double dt, double mass) {
+// Unless stopped: the spins of the next iteration into mn, the interior images
+// moved with v = lam F (lam = scal[3]) and F the force of the iteration, r = m +
+// F (lam dt + dt^2 / (2 mass)) normalised; the end images copied.
+__global__ void __launch_bounds__(256) k_gneb_move(const double* __restrict__ m, double* __restrict__ mn,
+                                                   const double* __restrict__ F, const double* __restrict__ scal,
+                                                   const GnebCtl* ctl, int64_t n, int64_t Ntot, double dt,
+                                                   double mass) {
     if (ctl->done) return;
-    const int64_t i = n + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (i >= Ntot - n) return;
+    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (i >= Ntot) return;
+    const double3 m0 = ld3(m, i, Ntot);
+    if (i < n || i >= Ntot - n) {
+        st3(mn, i, Ntot, m0);
+        return;
+    }
     const double3 f = ld3(F, i, Ntot);
-    const double lam = scal[3];
-    gneb_move_site(m, f, make_double3(lam * f.x, lam * f.y, lam * f.z), ax, ang, i, Ntot, dt, mass);
+    const double c = scal[3] * dt + 0.5 / mass * dt * dt;
+    double3 r = make_double3(m0.x + f.x * c, m0.y + f.y * c, m0.z + f.z * c);
+    const double nr = sqrt(dot(r, r));
+    if (nr > 1e-30) r = make_double3(r.x / nr, r.y / nr, r.z / nr);
+    st3(mn, i, Ntot, r);
 }
 
 template <class S, int BYT, int RY>
@@ -1257,8 +1262,9 @@ mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     k_gneb_tau<<<dim3(nblk, b->nrep), 256, 0, s>>>(b->d_m, n, b->Ntot, b->nrep, E_dev, mode, tau_dev, b->d_gneb_part);
     if ((st = cuda_status(cudaGetLastError(), "k_gneb_tau")) != MJ_OK) return st;
-    k_gneb_norm<<<b->nrep, 256, 0, s>>>(tau_dev, n, b->Ntot, b->d_gneb_part, nblk);
-    return cuda_status(cudaGetLastError(), "k_gneb_norm");
+    k_gneb_norm_sum<<<b->nrep, 256, 0, s>>>(b->d_gneb_part, nblk);
+    k_gneb_scale<<<dim3(nblk, b->nrep), 256, 0, s>>>(tau_dev, n, b->Ntot, b->d_gneb_part, nblk);
+    return cuda_status(cudaGetLastError(), "k_gneb_scale");
 }
 
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm) {
@@ -1481,9 +1487,9 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     if (!b->cap_stream &&
         (st = cuda_status(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "capture stream")) != MJ_OK)
         return st;
-    // F1 / F2 the forces of alternate iterations, ax / ang the moves' rotations,
-    // tau the tangents of the forces before the first move and of the outputs
-    // (SoA, 3 Ntot each); E / pl / fp per image, img the iteration's per-image
+    // F1 / F2 the forces and b->d_m / mB the spins of alternate iterations, tau
+    // the tangents of the forces before the first move and of the outputs (SoA,
+    // 3 Ntot each); E / pl / fp per image, img the iteration's per-image
     // 1/|tau|, F.tau / |tau| and segment lengths, scal (v.F, F.F, max |F|, lam);
     // part / part2 block partials; cnt the last-block counters; ctl the stop flag
     GnebBufs g;
@@ -1491,24 +1497,30 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     double* img = nullptr;
     unsigned int* cnt = nullptr;
     GnebCtl* ctl = nullptr;
-    double** bufs[] = {&g.F1, &g.F2, &g.ax, &g.tau};
+    double** bufs[] = {&g.F1, &g.F2, &g.mB, &g.tau};
     st = MJ_OK;
     for (double** q : bufs)
         if (st == MJ_OK) st = cuda_status(cudaMalloc(q, sizeof(double) * 3 * Ntot), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.ang, sizeof(double) * Ntot), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.E, sizeof(double) * (6 * nrep + 4)), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part, sizeof(double) * 3 * nbv), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part2, sizeof(double) * std::max(3 * nbv, n3b)), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * (nrep + 1)), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&ctl, sizeof(GnebCtl)), "GNEB buffers");
+    GnebCtl* hctl = nullptr;
+    if (st == MJ_OK) st = cuda_status(cudaMallocHost(&hctl, 2 * sizeof(GnebCtl)), "GNEB buffers");
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (int q = 0; q < 2 && st == MJ_OK; ++q)
+        st = cuda_status(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming), "GNEB events");
     cudaGraphExec_t exec = nullptr;
     auto release = [&]() {
         if (exec) cudaGraphExecDestroy(exec);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        cudaFreeHost(hctl);
         cudaFree(g.F1);
         cudaFree(g.F2);
-        cudaFree(g.ax);
+        cudaFree(g.mB);
         cudaFree(g.tau);
-        cudaFree(g.ang);
         cudaFree(g.E);
         cudaFree(g.part);
         cudaFree(g.part2);
@@ -1531,17 +1543,17 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     }
     GnebCtl c0;
     std::memset(&c0, 0, sizeof(c0));
-    cudaMemsetAsync(g.ang, 0, sizeof(double) * Ntot, s);
     cudaMemsetAsync(g.scal, 0, sizeof(double) * 4, s);
     cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * (nrep + 1), s);
     cudaMemcpyAsync(ctl, &c0, sizeof(c0), cudaMemcpyHostToDevice, s);
     DynCoef c;
     std::memset(&c, 0, sizeof(c));
     const dim3 gi(nblk, nrep), gs(nblk, nrep - 1);
-    const int nmove = static_cast<int>((Ntot - 2 * n + 255) / 256);
-    // the field pass: projected fields into F, tile energies, image energies E
-    auto field = [&](double* F) -> mj_status {
+    // the field pass of the spins m: projected fields into F, tile energies,
+    // image energies E
+    auto field = [&](double* F, double* m) -> mj_status {
         BatchArgs A = batch_args(b, 0, 0.0);
+        A.ms = A.mn = m;
         A.out = F;
         A.project = 1;
         A.tile_e = b->d_tile_e;
@@ -1552,12 +1564,13 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     };
     // field pass, path length pl, tangents of the given mode, fp = F.tau per image
     auto forces = [&](double* F, int mode) -> mj_status {
-        mj_status e = field(F);
+        mj_status e = field(F, b->d_m);
         if (e != MJ_OK) return e;
         k_gneb_seg<<<gs, 256, 0, s>>>(b->d_m, n, Ntot, g.part);
         k_gneb_pathlen<<<1, 256, 0, s>>>(g.part, nblk, nrep, g.pl);
         k_gneb_tau<<<gi, 256, 0, s>>>(b->d_m, n, Ntot, nrep, g.E, mode, g.tau, b->d_gneb_part);
-        k_gneb_norm<<<nrep, 256, 0, s>>>(g.tau, n, Ntot, b->d_gneb_part, nblk);
+        k_gneb_norm_sum<<<nrep, 256, 0, s>>>(b->d_gneb_part, nblk);
+        k_gneb_scale<<<gi, 256, 0, s>>>(g.tau, n, Ntot, b->d_gneb_part, nblk);
         k_gneb_dot<<<gi, 256, 0, s>>>(F, g.tau, n, Ntot, g.part);
         k_gneb_dot_img<<<nrep, 256, 0, s>>>(g.part, nblk, g.fp);
         return cuda_status(cudaGetLastError(), "GNEB forces");
@@ -1583,18 +1596,19 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     double fchk = h0[2];
     int64_t done = 0;
     if (itrmax > 0) {
-        // the first move (lam = 0: the velocity starts at zero), then chunks of
-        // iterations replayed as one graph: field pass, image energies,
-        // k_gneb_tan, k_gneb_step, k_gneb_move.  The force buffers alternate (an
-        // even chunk starts each replay on F1).  The stop flag is read after each
-        // chunk; the iterations of a chunk after the stop do no work but the
-        // field pass.
+        // the first move (lam = 0: the velocity starts at zero) into mB, then
+        // chunks of iterations replayed as one graph: field pass, image energies,
+        // k_gneb_tan, k_gneb_step, k_gneb_move.  Forces and spins alternate
+        // between their two buffers (an even chunk starts each replay on F1 and
+        // mB).  Two chunks are in flight: the stop flag of one is read while the
+        // next runs; the iterations after the stop do no work but the field pass.
         const int chunk = 32;
         // four sites per thread once that still gives two blocks per SM: the loads
         // of four sites in flight before each block's reduction
         const bool spt4 = Ntot >= 2LL * 1024 * b->num_sms;
         const dim3 gt(nrep, static_cast<unsigned>(spt4 ? (n + 1023) / 1024 : nblk));
-        k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, g.F1, g.ax, g.ang, g.scal, ctl, n, Ntot, dt, mass);
+        const int nmove = static_cast<int>((Ntot + 255) / 256);
+        k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, g.mB, g.F1, g.scal, ctl, n, Ntot, dt, mass);
         st = cuda_status(cudaGetLastError(), "k_gneb_move");
         if (st == MJ_OK) st = cuda_status(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (st == MJ_OK) {
@@ -1602,21 +1616,21 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
             for (int k = 0; k < chunk && inner == MJ_OK; ++k) {
                 double* Fo = (k & 1) ? g.F2 : g.F1;
                 double* Fn = (k & 1) ? g.F1 : g.F2;
-                inner = field(Fn);
+                double* mc = (k & 1) ? b->d_m : g.mB;
+                double* mo = (k & 1) ? g.mB : b->d_m;
+                inner = field(Fn, mc);
                 if (inner != MJ_OK) break;
                 const long long im = static_cast<long long>(itrmax);
                 if (spt4) {
-                    k_gneb_tan<4><<<gt, 256, 0, s>>>(b->d_m, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
-                    k_gneb_step<4><<<gt, 256, 0, s>>>(b->d_m, Fo, Fn, g.E, g.ax, g.ang, img, n, Ntot, nrep, spring, dt,
-                                                      mass, ftol, im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl,
-                                                      g.scal);
+                    k_gneb_tan<4><<<gt, 256, 0, s>>>(mc, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                    k_gneb_step<4><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
+                                                      im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
                 } else {
-                    k_gneb_tan<1><<<gt, 256, 0, s>>>(b->d_m, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
-                    k_gneb_step<1><<<gt, 256, 0, s>>>(b->d_m, Fo, Fn, g.E, g.ax, g.ang, img, n, Ntot, nrep, spring, dt,
-                                                      mass, ftol, im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl,
-                                                      g.scal);
+                    k_gneb_tan<1><<<gt, 256, 0, s>>>(mc, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                    k_gneb_step<1><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
+                                                      im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
                 }
-                k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, Fn, g.ax, g.ang, g.scal, ctl, n, Ntot, dt, mass);
+                k_gneb_move<<<nmove, 256, 0, s>>>(mc, mo, Fn, g.scal, ctl, n, Ntot, dt, mass);
                 inner = cuda_status(cudaGetLastError(), "GNEB iteration");
             }
             cudaGraph_t graph = nullptr;
@@ -1626,16 +1640,32 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
                 st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
             if (graph) cudaGraphDestroy(graph);
         }
-        GnebCtl hc = c0;
-        while (st == MJ_OK) {
-            const long long before = hc.iters;
-            if ((st = cuda_status(cudaGraphLaunch(exec, s), "GNEB graph launch")) != MJ_OK) break;
-            cudaMemcpyAsync(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost, s);
-            if ((st = cuda_status(cudaStreamSynchronize(s), "GNEB iterations")) != MJ_OK) break;
+        // chunk q: replay, its flag into hctl[q & 1], event ev[q & 1]
+        auto launch = [&](int64_t q) -> mj_status {
+            mj_status e = cuda_status(cudaGraphLaunch(exec, s), "GNEB graph launch");
+            if (e != MJ_OK) return e;
+            cudaMemcpyAsync(hctl + (q & 1), ctl, sizeof(GnebCtl), cudaMemcpyDeviceToHost, s);
+            return cuda_status(cudaEventRecord(ev[q & 1], s), "GNEB event");
+        };
+        if (st == MJ_OK) st = launch(0);
+        if (st == MJ_OK) st = launch(1);
+        for (int64_t q = 0; st == MJ_OK; ++q) {
+            if ((st = cuda_status(cudaEventSynchronize(ev[q & 1]), "GNEB iterations")) != MJ_OK) break;
+            const GnebCtl hc = hctl[q & 1];
+            done = hc.iters;
             if (hc.done) break;
-            if (hc.iters != before + chunk) st = set_error(MJ_ERR_CUDA, "GNEB iterations did not advance");
+            if (hc.iters != (q + 1) * chunk) {
+                st = set_error(MJ_ERR_CUDA, "GNEB iterations did not advance");
+                break;
+            }
+            st = launch(q + 2);
         }
-        done = hc.iters;
+        // the chunk still in flight (or, after an error, all queued work) ends first
+        const mj_status fin = cuda_status(cudaStreamSynchronize(s), "GNEB iterations");
+        if (st == MJ_OK) st = fin;
+        // the relaxed path is in mB after an odd number of iterations
+        if (st == MJ_OK && (done & 1))
+            cudaMemcpyAsync(b->d_m, g.mB, sizeof(double) * 3 * Ntot, cudaMemcpyDeviceToDevice, s);
         if (st == MJ_OK) {
             cudaMemcpyAsync(&fchk, g.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
             st = cuda_status(cudaStreamSynchronize(s), "GNEB force");

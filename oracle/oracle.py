@@ -144,7 +144,8 @@ class Model:
         self.N = int(lib.orc_nsites(h))
 
     def __del__(self):
-        if getattr(self, "h", None):
+        # at interpreter exit the module globals (lib) may already be gone
+        if getattr(self, "h", None) and lib is not None:
             lib.orc_model_free(self.h)
             self.h = None
 
