@@ -397,6 +397,16 @@ mj_status mj_batch_field(mj_batch* b, double* B_dev_soa, double* E_dev, int32_t 
  * difference; each tangent is projected on the tangent space of its image and
  * normalised over the image. */
 mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, double* tau_dev_soa, void* stream);
+/* GNEB_input's path-relaxation part (IO-input/GNEB_io.f90): spring, vpo_dt,
+ * vpo_mass, mep_ftol (or mep_ftol_ci), mep_itrmax, en_zero ('I', 'F' or 'N'),
+ * climb != 0 for the climbing-image run (do_gneb_ci). */
+typedef struct mj_gneb_params {
+    double spring, dt, mass, ftol;
+    int64_t itrmax;
+    int32_t en_zero;
+    int32_t climb;
+} mj_gneb_params;
+
 /* GNEB minimum-energy path of replicas taken as the images of a path (all of
  * one size, 3 or more; replica 0 and the last are the fixed end points): the
  * find_path relaxation of GNEB/gneb_utils.f90:19-240 on the batch's current
@@ -404,18 +414,19 @@ mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, 
  * images move by velocity Verlet, r = m + v dt + F dt^2 / (2 mass) normalised;
  * F is the projected field minus its component along the energy-weighted
  * tangent plus the spring force spring (l_{i+1} + l_{i-1} - 2 l_i) along it,
- * l the geodesic path length; velocity and old force are carried along each
- * spin's rotation, and the velocity is projected on the force (VPO).  Stops
- * when max |F| < ftol or after itrmax iterations.  Host outputs (nrep each):
- * rx the path length at every image, ene the energy above image 0 (en_zero
- * 'I'), the last image ('F') or zero ('N'), dene the derivative of the energy
- * along the path (en_path.out of GNEB/io-gneb.f90:83-111); iterations and
- * max_force (may be NULL) the iterations taken and the final max |F|.
- * Synchronous: starts after the work queued on the legacy default stream,
- * returns with the relaxed path in the batch. */
-mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass, double ftol, int64_t itrmax,
-                             int32_t en_zero, double* rx, double* ene, double* dene, int64_t* iterations,
-                             double* max_force);
+ * l the geodesic path length; with climb, the first image of highest energy
+ * (chosen again each iteration) takes F - 2 tau (F.tau) instead; velocity and
+ * old force are carried along each spin's rotation, and the velocity is
+ * projected on the force (VPO).  Stops when max |F| < ftol or after itrmax
+ * iterations.  Host outputs (nrep each): rx the path length at every image,
+ * ene the energy above image 0 (en_zero 'I'), the last image ('F') or zero
+ * ('N'), dene the derivative of the energy along the path (en_path.out of
+ * GNEB/io-gneb.f90:83-111); iterations, max_force and climbing (may be NULL)
+ * the iterations taken, the final max |F| and the climbing image (0-based; -1
+ * without climb).  Synchronous: starts after the work queued on the legacy
+ * default stream, returns with the relaxed path in the batch. */
+mj_status mj_batch_gneb_path(mj_batch* b, const mj_gneb_params* p, double* rx, double* ene, double* dene,
+                             int64_t* iterations, double* max_force, int32_t* climbing);
 /* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
  * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);

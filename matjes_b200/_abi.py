@@ -98,6 +98,11 @@ class McParams(C.Structure):
                 ("round0", C.c_uint32), ("track_totals", C.c_int32)]
 
 
+class GnebParams(C.Structure):
+    _fields_ = [("spring", C.c_double), ("dt", C.c_double), ("mass", C.c_double), ("ftol", C.c_double),
+                ("itrmax", C.c_int64), ("en_zero", C.c_int32), ("climb", C.c_int32)]
+
+
 MJ_MC_CONE = 0
 MJ_MC_ISING = 1
 MJ_MC_UNDERRELAX = 2
@@ -181,8 +186,7 @@ SIGNATURES = {
     "mj_batch_temperatures": (C.c_int32, [P, P, P]),
     "mj_batch_field": (C.c_int32, [P, P, P, C.c_int32, P]),
     "mj_batch_gneb_tangent": (C.c_int32, [P, P, C.c_int32, P, P]),
-    "mj_batch_gneb_path": (C.c_int32, [P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int32, P, P,
-                                       P, P, P]),
+    "mj_batch_gneb_path": (C.c_int32, [P, P, P, P, P, P, P, P]),
     "mj_batch_set_config": (C.c_int32, [P, C.c_int32, C.c_int32]),
     "mj_batch_autotune": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
                                       C.POINTER(C.c_int32), P]),

@@ -129,17 +129,20 @@ class ReplicaBatch:
         return tau
 
     def gneb_path(self, spring: float = 0.5, dt: float = 1.0e-2, mass: float = 1.0, ftol: float = 1.0e-3,
-                  itrmax: int = 2 ** 62, en_zero: str = "N"):
+                  itrmax: int = 2 ** 62, en_zero: str = "N", climb: bool = False):
         """GNEB relaxation of the path the replicas hold (GNEB/gneb_utils.f90
-        find_path); the batch is left holding the relaxed path.  Returns (rx,
-        ene, dene, iterations, max |F|)."""
+        find_path; climb: the climbing-image run); the batch is left holding the
+        relaxed path.  Returns (rx, ene, dene, iterations, max |F|, climbing
+        image or -1)."""
         if en_zero not in ("I", "F", "N"):
             raise ValueError("en_zero is 'I', 'F' or 'N'")
+        p = _abi.GnebParams(float(spring), float(dt), float(mass), float(ftol), int(itrmax), ord(en_zero),
+                            int(bool(climb)))
         rx, ene, dene = np.zeros(self.nrep), np.zeros(self.nrep), np.zeros(self.nrep)
-        it, fc = C.c_int64(), C.c_double()
-        check(lib.mj_batch_gneb_path(self.handle, float(spring), float(dt), float(mass), float(ftol), int(itrmax),
-                                     ord(en_zero), ptr(rx), ptr(ene), ptr(dene), C.byref(it), C.byref(fc)))
-        return rx, ene, dene, int(it.value), float(fc.value)
+        it, fc, ci = C.c_int64(), C.c_double(), C.c_int32()
+        check(lib.mj_batch_gneb_path(self.handle, C.byref(p), ptr(rx), ptr(ene), ptr(dene), C.byref(it),
+                                     C.byref(fc), C.byref(ci)))
+        return rx, ene, dene, int(it.value), float(fc.value), int(ci.value)
 
     def energies(self) -> np.ndarray:
         out = np.empty(self.nrep)

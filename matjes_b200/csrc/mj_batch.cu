@@ -52,9 +52,18 @@ struct BatchArgs {
     uint32_t step;
     double dt;          // SIB timestep (fs); sigma = sqrt(alpha kT hbar / dt) per replica
     int project;        // field pass: remove the component along m (B - (B.m) m)
+    double* tile_g;     // GNEB pass: per-tile path sums (6 x ntile)
+    int64_t gneb_n;     // GNEB pass: sites of an image (every replica one image)
+    int gneb_nimg;      // GNEB pass: images
 };
 
-enum { BPASS_ENERGY = 0, BPASS_FIELD = 1, BPASS_SIB1 = 4, BPASS_SIB2 = 5 };
+// BPASS_GNEB: the projected field pass with, per tile, the sums a GNEB iteration
+// needs of every image r whatever the tangent's energy weights: with P the
+// projection on the spin's tangent plane, A = P(m_{r+1} - m), B = P(m - m_{r-1})
+// (zero at the path's ends), |A|^2, A.B, |B|^2, F.A, F.B and the squared angle
+// to image r + 1; the energy-weighted tangent wp A + wm B then has |tau|^2 =
+// wp^2 |A|^2 + 2 wp wm A.B + wm^2 |B|^2 and F.tau = wp F.A + wm F.B.
+enum { BPASS_ENERGY = 0, BPASS_FIELD = 1, BPASS_GNEB = 2, BPASS_SIB1 = 4, BPASS_SIB2 = 5 };
 
 template <class S, int BYT, int RY>
 __device__ __forceinline__ void load_tile_b(const StencilParams& P, const BatchRep& R, const double* ms, int64_t Ntot,
@@ -91,7 +100,8 @@ __device__ __forceinline__ void load_tile_b(const StencilParams& P, const BatchR
 
 template <class S, int BYT, int RY, int PASS>
 __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const DynCoef& C, const BatchArgs& A,
-                                                 const BatchRep& R, const double* sm, int x0, int y0) {
+                                                 const BatchRep& R, int rep, const double* sm, int x0, int y0,
+                                                 double (&gs)[6]) {
     using G = TileGeom<S, BYT, RY>;
     const int64_t Nt = A.Ntot;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -138,14 +148,34 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
             const double3 zero = make_double3(0.0, 0.0, 0.0);
             if constexpr (PASS == BPASS_ENERGY) {
                 e += total_energy_part(f, m0, zero);
-            } else if constexpr (PASS == BPASS_FIELD) {
+            } else if constexpr (PASS == BPASS_FIELD || PASS == BPASS_GNEB) {
                 e += total_energy_part(f, m0, zero);
                 double3 Bv = f.B;
-                if (A.project) {
+                if (PASS == BPASS_GNEB || A.project) {
                     const double d = dot(Bv, m0);
                     Bv = make_double3(Bv.x - d * m0.x, Bv.y - d * m0.y, Bv.z - d * m0.z);
                 }
                 st3(A.out, i, Nt, Bv);
+                if constexpr (PASS == BPASS_GNEB) {
+                    const bool up = rep + 1 < A.gneb_nimg, down = rep > 0;
+                    const double3 mp = up ? ld3(A.ms, i + A.gneb_n, Nt) : m0;
+                    const double3 mm = down ? ld3(A.ms, i - A.gneb_n, Nt) : m0;
+                    double3 u = make_double3(mp.x - m0.x, mp.y - m0.y, mp.z - m0.z);
+                    double3 w = make_double3(m0.x - mm.x, m0.y - mm.y, m0.z - mm.z);
+                    const double du = dot(u, m0), dw = dot(w, m0);
+                    u = make_double3(u.x - du * m0.x, u.y - du * m0.y, u.z - du * m0.z);
+                    w = make_double3(w.x - dw * m0.x, w.y - dw * m0.y, w.z - dw * m0.z);
+                    gs[0] += dot(u, u);
+                    gs[1] += dot(u, w);
+                    gs[2] += dot(w, w);
+                    gs[3] += dot(Bv, u);
+                    gs[4] += dot(Bv, w);
+                    if (up) {
+                        const double3 c = cross(m0, mp);
+                        const double l = atan2(sqrt(dot(c, c)), dot(m0, mp));
+                        gs[5] += l * l;
+                    }
+                }
             } else if constexpr (PASS == BPASS_SIB1) {
                 e += total_energy_part(f, m0, zero);
                 double3 H = f.B;
@@ -172,7 +202,9 @@ __global__ void __launch_bounds__(32 * BYT) k_batch(const __grid_constant__ Sten
                                                      const BatchArgs A) {
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_b[];
-    __shared__ double wsum[8];
+    // per tile: the energy, and for the GNEB pass its six path sums
+    constexpr int NV = PASS == BPASS_GNEB ? 7 : 1;
+    __shared__ double wsum[NV][8];
     BatchArgs Ar = A;
     if (C.step_base) Ar.step = A.step + *C.step_base;
     const int tid = threadIdx.x + 32 * threadIdx.y;
@@ -181,16 +213,28 @@ __global__ void __launch_bounds__(32 * BYT) k_batch(const __grid_constant__ Sten
         const BatchRep R = A.reps[tl.x];
         load_tile_b<S, BYT, RY>(P, R, A.ms, A.Ntot, tl.y, tl.z, smem_b);
         __syncthreads();
-        double e = compute_tile_b<S, BYT, RY, PASS>(P, C, Ar, R, smem_b, tl.y, tl.z);
+        double v[NV];
+        double gs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        v[0] = compute_tile_b<S, BYT, RY, PASS>(P, C, Ar, R, tl.x, smem_b, tl.y, tl.z, gs);
+#pragma unroll
+        for (int q = 1; q < NV; ++q) v[q] = gs[q - 1];
         if (A.tile_e) {
-            for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
-            if ((tid & 31) == 0) wsum[tid >> 5] = e;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                double e = v[q];
+                for (int o = 16; o > 0; o >>= 1) e += __shfl_down_sync(0xffffffffu, e, o);
+                if ((tid & 31) == 0) wsum[q][tid >> 5] = e;
+            }
         }
         __syncthreads();  // tile buffer and wsum are reused by the next tile
         if (A.tile_e && tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < BYT; ++w) s += wsum[w];
-            A.tile_e[t] = s;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                double s = 0.0;
+                for (int w = 0; w < BYT; ++w) s += wsum[q][w];
+                if (q == 0) A.tile_e[t] = s;
+                else A.tile_g[static_cast<int64_t>(q - 1) * A.ntile + t] = s;
+            }
         }
     }
 }
@@ -436,12 +480,12 @@ __global__ void __launch_bounds__(256) k_gneb_scale(double* __restrict__ tau, in
 // gives the projected forces and energies; k_gneb_seg / k_gneb_pathlen the
 // geodesic path length; k_gneb_tau / k_gneb_norm_sum / k_gneb_scale the
 // tangents; k_gneb_dot_img and k_gneb_force the GNEB force.  An iteration is
-// five launches: the field pass and image energies, k_gneb_tan (per-image
-// |tau|, F.tau, path segments),
-// k_gneb_step (GNEB force, transport, velocity Verlet, velocity projection,
-// stop flag), k_gneb_move.  After the projection the velocity is lam F, lam one
-// number, so neither the velocity nor the tangents are stored.  Every sum is a
-// block partial summed in a fixed order: the iterations are deterministic.
+// four launches: the GNEB field pass (projected fields, energies and the path
+// sums of every tile), k_gneb_img (per-image sums), k_gneb_step (GNEB force,
+// transport, velocity Verlet, velocity projection, stop flag), k_gneb_move.
+// After the projection the velocity is lam F, lam one number, so neither the
+// velocity nor the tangents are stored.  Every sum is a block or tile partial
+// summed in a fixed order: the iterations are deterministic.
 struct GnebBufs {
     double *F1, *F2, *mB, *tau, *E, *pl, *fp, *part, *part2, *scal;
 };
@@ -500,11 +544,22 @@ __global__ void __launch_bounds__(256) k_gneb_dot_img(const double* part, int nb
     ordered_sum<1>(part + static_cast<int64_t>(blockIdx.x) * nblk, nblk, out + blockIdx.x);
 }
 
-// interior: F = F - tau (F.tau) + k (l_{r+1} + l_{r-1} - 2 l_r) tau; end images:
-// 0, or left as they are (keep_ends, the forces before the first move)
+// maxloc of the image energies: the first image of highest energy (the climbing
+// image, gneb_utils.f90:84,159)
+__device__ __forceinline__ int gneb_maxloc(const double* E, int nrep) {
+    int c = 0;
+    for (int q = 1; q < nrep; ++q)
+        if (E[q] > E[c]) c = q;
+    return c;
+}
+
+// interior: F = F - tau (F.tau) + k (l_{r+1} + l_{r-1} - 2 l_r) tau, at the
+// climbing image (climb != 0) F - 2 tau (F.tau); end images: 0, or left as they
+// are (keep_ends, the forces before the first move)
 __global__ void __launch_bounds__(256) k_gneb_force(double* F, const double* __restrict__ tau, const double* __restrict__ fp,
-                                                    const double* __restrict__ pl, int64_t n, int64_t Ntot, int nrep,
-                                                    double spring, int keep_ends) {
+                                                    const double* __restrict__ pl, const double* __restrict__ E,
+                                                    int64_t n, int64_t Ntot, int nrep, double spring, int keep_ends,
+                                                    int climb) {
     const int r = blockIdx.y;
     const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     if (li >= n) return;
@@ -514,6 +569,11 @@ __global__ void __launch_bounds__(256) k_gneb_force(double* F, const double* __r
         return;
     }
     const double3 f = ld3(F, i, Ntot), t = ld3(tau, i, Ntot);
+    if (climb && gneb_maxloc(E, nrep) == r) {
+        const double a2 = 2.0 * fp[r];
+        st3(F, i, Ntot, make_double3(f.x - t.x * a2, f.y - t.y * a2, f.z - t.z * a2));
+        return;
+    }
     const double a = fp[r], k = spring * (pl[r + 1] + pl[r - 1] - 2.0 * pl[r]);
     st3(F, i, Ntot, make_double3(f.x - t.x * a + k * t.x, f.y - t.y * a + k * t.y, f.z - t.z * a + k * t.z));
 }
@@ -570,80 +630,75 @@ __device__ __forceinline__ double3 gneb_tangent_site(const double* __restrict__ 
     return make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
 }
 
-// Per image (r = blockIdx.x: the images of one site range run side by side, so
-// a spin read for the neighbouring images' tangents comes from L2): the
-// partials of |tau|^2, F.tau and the squared angles to the next image; the last
-// block of an image sums them in block order: inv[r] = 1/|tau|, fp[r] = F.tau
-// / |tau|, seg[r] = the geodesic distance from image r to r + 1.
-template <int SPT>
-__global__ void __launch_bounds__(256) k_gneb_tan(const double* __restrict__ m, const double* __restrict__ F,
-                                                  const double* __restrict__ E, int64_t n, int64_t Ntot, int nrep,
-                                                  double* part, unsigned int* cnt, double* img, const GnebCtl* ctl) {
+// Per image r (one block each): the energy and the six path sums of the GNEB
+// field pass, each summed over the image's tiles in tile order as
+// k_batch_energy sums the energies (thread t the tiles t, t + 256, ...; then
+// those partials in thread order, the all-zero ones beyond the image's tile
+// count left out), into E[r] and img[q nrep + r]; the seven sums side by side.
+__global__ void __launch_bounds__(256) k_gneb_img(const BatchRep* reps, int nrep, const double* __restrict__ tile_e,
+                                                  const double* __restrict__ tile_g, int ntile, double* E,
+                                                  double* img, const GnebCtl* ctl) {
     if (ctl->done) return;
     const int r = blockIdx.x;
-    const int nblk = gridDim.y;
-    double wp, wm;
-    gneb_weights(E, r, nrep, 0, wp, wm);
-    double v[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < SPT; ++k) {
-        const int64_t li = (static_cast<int64_t>(blockIdx.y) * SPT + k) * blockDim.x + threadIdx.x;
-        if (li >= n) break;
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        double3 m0, mp;
-        const double3 t = gneb_tangent_site(m, i, n, Ntot, r, nrep, wp, wm, m0, mp);
-        v[0] += dot(t, t);
-        v[1] += dot(ld3(F, i, Ntot), t);
-        if (r + 1 < nrep) {
-            const double l = gneb_ang(m0, mp);
-            v[2] += l * l;
-        }
-    }
-    double* pr = part + static_cast<int64_t>(r) * 3 * nblk;
-    block_partials<3>(v, pr, nblk, blockIdx.y);
-    __shared__ bool last;
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(cnt + r, 1u) == static_cast<unsigned int>(nblk - 1);
+    __shared__ double part[7][256];
+    const BatchRep R = reps[r];
+    for (int q = 0; q < 7; ++q) {
+        const double* src = q == 0 ? tile_e : tile_g + static_cast<int64_t>(q - 1) * ntile;
+        double s = 0.0;
+        for (int t = threadIdx.x; t < R.ntiles; t += blockDim.x) s += src[R.tile0 + t];
+        part[q][threadIdx.x] = s;
     }
     __syncthreads();
-    if (!last) return;
-    __threadfence();
-    __shared__ double sums[3];
-    ordered_sum<3>(pr, nblk, sums);
-    if (threadIdx.x == 0) {
-        const double inv = sums[0] > 0.0 ? 1.0 / sqrt(sums[0]) : 0.0;
-        img[r] = sums[1] * inv;
-        img[nrep + r] = inv;
-        img[2 * nrep + r] = sqrt(sums[2]);
-        cnt[r] = 0u;
+    if (threadIdx.x < 7) {
+        const int q = threadIdx.x;
+        const int nk = min(R.ntiles, static_cast<int>(blockDim.x));
+        double tot = 0.0;
+        for (int k = 0; k < nk; ++k) tot += part[q][k];
+        if (q == 0) E[r] = tot;
+        else img[(q - 1) * nrep + r] = tot;
     }
 }
 
-// Interior images: tau the tangent again (the same arithmetic as k_gneb_tan)
-// over |tau|, F = F - tau fp + k (seg_r - seg_{r-1}) tau, stored; the old
-// velocity lam Fo (the projection of the previous iteration, lam = scal[3]) and
-// the old force Fo carried along the rotation R that took the spin from mo to
-// m, v = lam R Fo + (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
+// Interior images: tau = wp A + wm B (the energy-weighted tangent at the site,
+// the weights of the image energies) over |tau| from the image's path sums, F =
+// F - tau (F.tau) + k (seg_r - seg_{r-1}) tau, stored; the old velocity lam Fo
+// (the projection of the previous iteration, lam = scal[3]) and the old force Fo
+// carried along the rotation R that took the spin from mo to m, v = lam R Fo +
+// (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
 // and F.F in block order, takes max |F|, sets lam = v.F / F.F (0 when v.F < 0;
 // the velocity projection, v = lam F), counts the iteration and sets the stop
-// flag.
+// flag.  r = blockIdx.x: the images of one site range run side by side, so the
+// neighbouring images' spins come from L2.
 template <int SPT>
 __global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ mo,
                                                    const double* __restrict__ Fo, double* Fn,
                                                    const double* __restrict__ E, const double* __restrict__ img,
                                                    int64_t n, int64_t Ntot, int nrep,
                                                    double spring, double dt, double mass, double ftol, long long itrmax,
-                                                   double* part, double* pmax, unsigned int* cnt, GnebCtl* ctl,
-                                                   double* scal) {
+                                                   int climb, double* part, double* pmax, unsigned int* cnt,
+                                                   GnebCtl* ctl, double* scal) {
     if (ctl->done) return;
     const int r = blockIdx.x;
     const int nb = gridDim.x * gridDim.y, bid = blockIdx.x + gridDim.x * blockIdx.y;
     const bool inner = r > 0 && r < nrep - 1;
-    double wp = 0.0, wm = 0.0;
-    if (inner) gneb_weights(E, r, nrep, 0, wp, wm);
-    const double inv = inner ? img[nrep + r] : 0.0, a = inner ? img[r] : 0.0;
-    const double k = inner ? spring * (img[2 * nrep + r] - img[2 * nrep + r - 1]) : 0.0;
+    double wp = 0.0, wm = 0.0, inv = 0.0, a = 0.0, k = 0.0;
+    if (inner) {
+        gneb_weights(E, r, nrep, 0, wp, wm);
+        const double t2 = wp * wp * img[r] + 2.0 * wp * wm * img[nrep + r] + wm * wm * img[2 * nrep + r];
+        inv = t2 > 0.0 ? 1.0 / sqrt(t2) : 0.0;
+        a = (wp * img[3 * nrep + r] + wm * img[4 * nrep + r]) * inv;
+        k = spring * (sqrt(img[5 * nrep + r]) - sqrt(img[5 * nrep + r - 1]));
+        if (climb) {
+            __shared__ int ci_s;
+            if (threadIdx.x == 0) ci_s = gneb_maxloc(E, nrep);
+            __syncthreads();
+            if (ci_s == r) {
+                // the climbing image: F - 2 tau (F.tau), no spring
+                a *= 2.0;
+                k = 0.0;
+            }
+        }
+    }
     const double h = 0.5 / mass * dt, lam = scal[3];
     double v2[2] = {0.0, 0.0}, fm = 0.0;
 #pragma unroll
@@ -754,6 +809,7 @@ struct BatchLauncher {
             case BPASS_SIB1: return launch<BPASS_SIB1>(P, C, A, nblocks, s);
             case BPASS_SIB2: return launch<BPASS_SIB2>(P, C, A, nblocks, s);
             case BPASS_FIELD: return launch<BPASS_FIELD>(P, C, A, nblocks, s);
+            case BPASS_GNEB: return launch<BPASS_GNEB>(P, C, A, nblocks, s);
             default: return launch<BPASS_ENERGY>(P, C, A, nblocks, s);
         }
     }
@@ -941,6 +997,9 @@ BatchArgs batch_args(mj_batch* b, uint32_t step, double dt) {
     A.step = step;
     A.dt = dt;
     A.project = 0;
+    A.tile_g = nullptr;
+    A.gneb_n = 0;
+    A.gneb_nimg = 0;
     return A;
 }
 
@@ -1464,15 +1523,18 @@ mj_status mj_batch_mc_state(mj_batch* b, double* cone, int64_t* accepted, int64_
 
 // ---- GNEB path relaxation --------------------------------------------------
 
-mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass, double ftol, int64_t itrmax,
-                             int32_t en_zero, double* rx, double* ene, double* dene, int64_t* iterations,
-                             double* max_force) {
-    if (!b || !rx || !ene || !dene || b->nrep < 3 || !(dt > 0.0) || !(mass > 0.0) || itrmax < 0 ||
-        (en_zero != 'I' && en_zero != 'F' && en_zero != 'N'))
+mj_status mj_batch_gneb_path(mj_batch* b, const mj_gneb_params* p, double* rx, double* ene, double* dene,
+                             int64_t* iterations, double* max_force, int32_t* climbing) {
+    if (!b || !p || !rx || !ene || !dene || b->nrep < 3 || !(p->dt > 0.0) || !(p->mass > 0.0) || p->itrmax < 0 ||
+        (p->en_zero != 'I' && p->en_zero != 'F' && p->en_zero != 'N'))
         return set_error(MJ_ERR_ARG, "bad GNEB arguments (3 or more images, dt > 0, mass > 0, en_zero I/F/N)");
     for (int r = 1; r < b->nrep; ++r)
         if (b->reps[r].Lx != b->reps[0].Lx || b->reps[r].Ly != b->reps[0].Ly)
             return set_error(MJ_ERR_UNSUPPORTED, "a path needs images of one size");
+    const double spring = p->spring, dt = p->dt, mass = p->mass, ftol = p->ftol;
+    const int64_t itrmax = p->itrmax;
+    const int32_t en_zero = p->en_zero;
+    const int climb = p->climb ? 1 : 0;
     cudaSetDevice(b->device);
     const int nrep = b->nrep;
     const int64_t Ntot = b->Ntot, n = Ntot / nrep;
@@ -1489,8 +1551,8 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
         return st;
     // F1 / F2 the forces and b->d_m / mB the spins of alternate iterations, tau
     // the tangents of the forces before the first move and of the outputs (SoA,
-    // 3 Ntot each); E / pl / fp per image, img the iteration's per-image
-    // 1/|tau|, F.tau / |tau| and segment lengths, scal (v.F, F.F, max |F|, lam);
+    // 3 Ntot each); E / pl / fp per image, img the iteration's six path sums per
+    // image, tile_g their tile partials, scal (v.F, F.F, max |F|, lam);
     // part / part2 block partials; cnt the last-block counters; ctl the stop flag
     GnebBufs g;
     std::memset(&g, 0, sizeof(g));
@@ -1501,7 +1563,9 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     st = MJ_OK;
     for (double** q : bufs)
         if (st == MJ_OK) st = cuda_status(cudaMalloc(q, sizeof(double) * 3 * Ntot), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.E, sizeof(double) * (6 * nrep + 4)), "GNEB buffers");
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.E, sizeof(double) * (9 * nrep + 4)), "GNEB buffers");
+    double* tile_g = nullptr;
+    if (st == MJ_OK) st = cuda_status(cudaMalloc(&tile_g, sizeof(double) * 6 * b->ntile), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part, sizeof(double) * 3 * nbv), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part2, sizeof(double) * std::max(3 * nbv, n3b)), "GNEB buffers");
     if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * (nrep + 1)), "GNEB buffers");
@@ -1522,6 +1586,7 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
         cudaFree(g.mB);
         cudaFree(g.tau);
         cudaFree(g.E);
+        cudaFree(tile_g);
         cudaFree(g.part);
         cudaFree(g.part2);
         cudaFree(cnt);
@@ -1534,7 +1599,7 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     g.pl = g.E + nrep;
     g.fp = g.E + 2 * nrep;
     img = g.E + 3 * nrep;
-    g.scal = g.E + 6 * nrep;
+    g.scal = g.E + 9 * nrep;
     // the path as the work queued on the legacy default stream (an upload) leaves it
     cudaStream_t s = b->cap_stream;
     if ((st = cuda_status(cudaStreamSynchronize(0), "GNEB start")) != MJ_OK) {
@@ -1581,7 +1646,7 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
         release();
         return st;
     }
-    k_gneb_force<<<gi, 256, 0, s>>>(g.F1, g.tau, g.fp, g.pl, n, Ntot, nrep, spring, 1);
+    k_gneb_force<<<gi, 256, 0, s>>>(g.F1, g.tau, g.fp, g.pl, g.E, n, Ntot, nrep, spring, 1, climb);
     k_gneb_absmax<<<n3b, 256, 0, s>>>(g.F1, 3 * Ntot, g.part2);
     k_gneb_maxof<<<1, 256, 0, s>>>(g.part2, n3b, g.scal + 2);
     double h0[4];
@@ -1597,8 +1662,8 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
     int64_t done = 0;
     if (itrmax > 0) {
         // the first move (lam = 0: the velocity starts at zero) into mB, then
-        // chunks of iterations replayed as one graph: field pass, image energies,
-        // k_gneb_tan, k_gneb_step, k_gneb_move.  Forces and spins alternate
+        // chunks of iterations replayed as one graph: GNEB field pass,
+        // k_gneb_img, k_gneb_step, k_gneb_move.  Forces and spins alternate
         // between their two buffers (an even chunk starts each replay on F1 and
         // mB).  Two chunks are in flight: the stop flag of one is read while the
         // next runs; the iterations after the stop do no work but the field pass.
@@ -1618,18 +1683,23 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
                 double* Fn = (k & 1) ? g.F1 : g.F2;
                 double* mc = (k & 1) ? b->d_m : g.mB;
                 double* mo = (k & 1) ? g.mB : b->d_m;
-                inner = field(Fn, mc);
+                BatchArgs A = batch_args(b, 0, 0.0);
+                A.ms = A.mn = mc;
+                A.out = Fn;
+                A.tile_e = b->d_tile_e;
+                A.tile_g = tile_g;
+                A.gneb_n = n;
+                A.gneb_nimg = nrep;
+                inner = batch_pass(b->shape, b->variant, BPASS_GNEB, b->sp, c, A, batch_blocks(b), s);
                 if (inner != MJ_OK) break;
+                k_gneb_img<<<nrep, 256, 0, s>>>(b->d_reps, nrep, b->d_tile_e, tile_g, b->ntile, g.E, img, ctl);
                 const long long im = static_cast<long long>(itrmax);
-                if (spt4) {
-                    k_gneb_tan<4><<<gt, 256, 0, s>>>(mc, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                if (spt4)
                     k_gneb_step<4><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
-                                                      im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
-                } else {
-                    k_gneb_tan<1><<<gt, 256, 0, s>>>(mc, Fn, g.E, n, Ntot, nrep, g.part, cnt, img, ctl);
+                                                      im, climb, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
+                else
                     k_gneb_step<1><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
-                                                      im, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
-                }
+                                                      im, climb, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
                 k_gneb_move<<<nmove, 256, 0, s>>>(mc, mo, Fn, g.scal, ctl, n, Ntot, dt, mass);
                 inner = cuda_status(cudaGetLastError(), "GNEB iteration");
             }
@@ -1690,6 +1760,14 @@ mj_status mj_batch_gneb_path(mj_batch* b, double spring, double dt, double mass,
         }
         if (iterations) *iterations = done;
         if (max_force) *max_force = fchk;
+        // the climbing image of the last iteration (the image energies it saw)
+        if (climbing) {
+            auto en = [&](int r) { return r == 0 ? E_first : (r == nrep - 1 ? E_last : h[r]); };
+            int c = 0;
+            for (int r = 1; r < nrep; ++r)
+                if (en(r) > en(c)) c = r;
+            *climbing = climb ? c : -1;
+        }
     }
     release();
     return st;

@@ -4,38 +4,64 @@
 names and defaults).  ``geodesic_path`` builds the initial path
 (GNEB/path.f90:100-174), ``find_path`` relaxes it on the device
 (GNEB/gneb_utils.f90:19-240 find_path, velocity projection on the images held
-as the replicas of a ReplicaBatch: mj_batch_gneb_path), ``hermite_fit``,
-``find_sp`` and
-``spline_hermite_val`` interpolate the energy along the path and locate the
-saddle point (extrapolation/spline.f90, gneb_utils.f90:242-291), ``write_en``
-writes en_path.out / enfit_path.out / ensp_path.out (GNEB/io-gneb.f90:83-111).
+as the replicas of a ReplicaBatch: mj_batch_gneb_path; with the climbing image
+for do_gneb_ci), ``hermite_fit``, ``find_sp`` and ``spline_hermite_val``
+interpolate the energy along the path and locate the saddle point
+(extrapolation/spline.f90, gneb_utils.f90:242-291), ``saddle_configuration``
+interpolates the spins there (find_SP_conf, gneb_utils.f90:305-380),
+``write_en`` writes en_path.in / en_path.out / enfit_path.out / ensp_path.out
+(GNEB/io-gneb.f90:91-120), ``write_image`` the image-GNEB_<k>.dat files
+(io-gneb.f90 write_path), and ``gneb_run`` is GNEB_run (GNEB/gneb.f90:33-120):
+path initialisation, the relaxations, the outputs.
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
+import os
 from dataclasses import dataclass
 from typing import Optional, Tuple
 
 import numpy as np
 
-from . import _abi
-from ._abi import check, lib, ptr
-
 
 @dataclass
 class GNEBInput:
-    """IO-input/GNEB_io.f90 GNEB_input (the path-relaxation part)."""
-    nim: int = 10
-    spring: float = 0.5
-    dt: float = 1.0e-2          # vpo_dt
-    mass: float = 1.0           # vpo_mass
-    itrmax: int = 2 ** 62       # mep_itrmax
-    mepftol: float = 1.0e-3     # mep_ftol
-    amp_rnd_path: float = 0.0
-    en_zero: str = "N"          # 'I' initial image, 'F' final image, 'N' none
-    do_norm_rx: str = "N"
-    sample_num: int = 500
+    """IO-input/GNEB_io.f90 GNEB_input (keyword names in the comments)."""
+    nim: int = 10                       # nim
+    spring: float = 0.5                 # spring
+    dt: float = 1.0e-2                  # vpo_dt
+    mass: float = 1.0                   # vpo_mass
+    itrmax: int = 2 ** 63 - 1           # mep_itrmax
+    mepftol: float = 1.0e-3             # mep_ftol
+    mepftol_ci: float = 1.0e-5          # mep_ftol_ci
+    every: int = 10                     # meptraj_step
+    amp_rnd: float = 0.0                # amp_rnd
+    amp_rnd_path: float = 0.0           # amp_rnd_path
+    en_zero: str = "N"                  # en_zero: 'I' initial image, 'F' final image, 'N' none
+    do_norm_rx: str = "N"               # do_norm_rx
+    sample_num: int = 500               # sample_num
+    do_gneb: bool = False               # do_gneb_simple
+    do_gneb_ci: bool = False            # do_gneb_ci
+    momfile_i: str = "momfile_i"        # momfile_i
+    momfile_f: str = "momfile_f"        # momfile_f
+    restartfile_path: str = "nofile"    # restartfile_path
+    initpath: int = -1                  # initpath
+    read_path: bool = False             # gnebinit_read_path
+    read_outer: bool = True             # gnebinit_read_outer
+    min_type: int = 1                   # gnebinit_min_type: 0 none, 1 minimize_infdamp, 2 minimize
+
+
+@dataclass
+class GNEBResult:
+    """A relaxed path: images (nim, N, 3); rx, ene, dene as en_path.out holds
+    them; iterations and final max |F|; the climbing image (0-based, -1 none)."""
+    images: np.ndarray
+    rx: np.ndarray
+    ene: np.ndarray
+    dene: np.ndarray
+    iterations: int
+    max_force: float
+    ci: int = -1
 
 
 def _calc_ang(a: np.ndarray, b: np.ndarray) -> np.ndarray:
@@ -157,11 +183,11 @@ def find_sp(rx, c) -> Tuple[int, float]:
     raise ValueError("energy maximum has not been found")
 
 
-def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: int = 0):
+def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: int = 0,
+              climb: bool = False) -> GNEBResult:
     """Relax the path images (nim, N, 3) of the single-atom 2D lattice of deck
     (its L, boundaries, couplings and field) on the device: GNEB find_path with
-    the end images fixed.  Returns (relaxed images (nim, N, 3), rx, ene, dene,
-    iterations, max |F|); rx / ene / dene as en_path.out holds them."""
+    the end images fixed, tolerance mep_ftol (mep_ftol_ci with climb)."""
     from .batch import ReplicaBatch
 
     img = np.ascontiguousarray(images, np.float64)
@@ -171,15 +197,78 @@ def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: in
     batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)), [0.0] * nim,
                          device=device)
     batch.upload(img.reshape(nim * N, 3))
-    rx, ene, dene, iters, fchk = batch.gneb_path(inp.spring, inp.dt, inp.mass, inp.mepftol, inp.itrmax, inp.en_zero)
-    return batch.download().reshape(nim, N, 3), rx, ene, dene, iters, fchk
+    return _relax(batch, nim, N, inp, climb)
 
 
-def write_en(path: str, x, y, dy, x0: Optional[float] = None) -> None:
-    """write_en (GNEB/io-gneb.f90:83-111): rows x/x0, y, dy in 3(E20.12E3, 3X)."""
+def _relax(batch, nim: int, N: int, inp: GNEBInput, climb: bool, itrmax: Optional[int] = None) -> GNEBResult:
+    ftol = inp.mepftol_ci if climb else inp.mepftol
+    rx, ene, dene, iters, fchk, ci = batch.gneb_path(inp.spring, inp.dt, inp.mass, ftol,
+                                                     inp.itrmax if itrmax is None else itrmax, inp.en_zero, climb)
+    return GNEBResult(batch.download().reshape(nim, N, 3), rx, ene, dene, iters, fchk, ci)
+
+
+def saddle_configuration(m1: np.ndarray, m2: np.ndarray, l1: float, l2: float, lsp: float,
+                         seed: int = 0) -> np.ndarray:
+    """find_SP_conf (GNEB/gneb_utils.f90:305-380): every spin on the geodesic
+    from its image-imax direction m1 to its image-imax+1 direction m2, a
+    fraction (lsp - l1) / (l2 - l1) of the way: linear and renormalised for
+    parallel spins; about m1 x m2 by that fraction of their angle otherwise; for
+    antiparallel spins by that fraction of pi about an axis drawn at random
+    (numpy's generator from seed, not the reference's) and kept for the
+    following sites.  Returns (N, 3)."""
+    rng = np.random.default_rng(seed)
+    m1 = np.asarray(m1, float)
+    m2 = np.asarray(m2, float)
+    eps = np.finfo(float).eps
+    frac = (lsp - l1) / (l2 - l1)
+    out = np.empty_like(m1)
+    ax = np.zeros(3)
+    for s in range(m1.shape[0]):
+        ni, nf = m1[s], m2[s]
+        angle = float(_calc_ang(ni, nf))
+        if angle < eps:
+            p = ni + (nf - ni) * frac
+            out[s] = p / np.linalg.norm(p)
+            continue
+        if abs(angle - math.pi) < eps:
+            ax = ax - (ax @ ni) * ni
+            while np.linalg.norm(ax) < eps:
+                ax = np.sign(2.0 * rng.uniform(size=3) - 1.0) * (rng.uniform(size=3) + 1.0)
+                ax = ax - (ax @ ni) * ni
+            ax = ax / np.linalg.norm(ax)
+            theta = math.pi * frac
+        else:
+            c = np.cross(ni, nf)
+            ax = c / np.linalg.norm(c)
+            theta = angle * frac
+        p = ni * math.cos(theta) + math.sin(theta) * np.cross(ax, ni)
+        out[s] = p / np.linalg.norm(p)
+    return out
+
+
+def write_image(path: str, m: np.ndarray) -> None:
+    """One spin per line, 3(F14.8) then two blanks (IO-utils/io-utils.f90
+    dump_config of a 2D array, as image-GNEB_<k>.dat holds the images)."""
+    m = np.asarray(m, float).reshape(-1, 3)
+    with open(path, "w") as f:
+        for row in m:
+            f.write("".join(f"{v:14.8f}" for v in row) + "  \n")
+
+
+def write_path(directory: str, images: np.ndarray) -> None:
+    """write_path (GNEB/io-gneb.f90:46-57): image-GNEB_<k>.dat, k = 1 .. nim."""
+    for k, m in enumerate(images, start=1):
+        write_image(os.path.join(directory, f"image-GNEB_{k}.dat"), m)
+
+
+def write_en(path: str, x, y, dy, x0: Optional[float] = None, do_norm_rx: str = "Y") -> None:
+    """write_en (GNEB/io-gneb.f90:91-120): rows x / x0 (do_norm_rx 'Y', x0
+    given) or x ('N'), y, dy in 3(E20.12E3, 3X)."""
     from .reference_io import fortran_e
 
-    norm = 1.0 if x0 is None else float(x0)
+    if do_norm_rx not in ("Y", "N"):
+        raise ValueError("Invalid value for do_norm_rx!")
+    norm = float(x0) if (do_norm_rx == "Y" and x0 is not None) else 1.0
     with open(path, "w") as f:
         for a, b, d in zip(x, y, dy):
             f.write("".join(fortran_e(v, 20, 12, 3) + "   " for v in (a / norm, b, d)) + "\n")
@@ -193,3 +282,97 @@ def saddle_point(rx, ene, dene, sample_num: int = 500):
     rx0 = float(np.asarray(rx)[imax] + drx0)
     e0, de0 = spline_hermite_val(rx, c, rx0)
     return (xx, yy, dyy), (rx0, e0, de0)
+
+
+def gneb_run(deck, inp: GNEBInput, m_first: Optional[np.ndarray] = None, m_last: Optional[np.ndarray] = None,
+             path: Optional[np.ndarray] = None, minimize_input=None, directory: Optional[str] = None,
+             device: int = 0, seed: int = 0) -> dict:
+    """GNEB_run (GNEB/gneb.f90:33-120) of a single-atom 2D lattice.  Path
+    initialisation (GNEB/initialize_path.f90): the given path (read_path), its
+    end images replaced by m_first / m_last (read_outer), those minimised
+    (min_type 1 minimize_infdamp, 2 minimize, with minimize_input: mass,
+    timestep, steps, conv_torque; 0 none), then, unless read_path, the geodesic
+    path between them perturbed by amp_rnd_path.  Then find_path (do_gneb,
+    mep_ftol) and the climbing-image find_path (do_gneb_ci, mep_ftol_ci), each
+    writing en_path.in (the path it starts from); en_path.out, the images, the
+    Hermite fit (enfit_path.out), the saddle point (ensp_path.out) and its spins
+    (image-GNEB-saddlepoint.dat; the climbing image with do_gneb_ci, else
+    saddle_configuration).  Files go to directory when given (the povray files
+    of the reference are not written).  Returns the path, rx, ene, dene, the
+    saddle point (rx0, E0, dE0) and its spins, and the results of the runs."""
+    import torch
+
+    from . import Hamiltonian
+    from .batch import ReplicaBatch
+    from .hamiltonian import minimize
+
+    nim, N = inp.nim, deck.ncell
+    if nim < 3:
+        raise ValueError("GNEB needs nim >= 3")
+    images = np.zeros((nim, N, 3))
+    if inp.read_path:
+        if path is None:
+            raise ValueError("read_path needs the path")
+        images[:] = np.asarray(path, float).reshape(nim, N, 3)
+    if inp.read_outer:
+        if m_first is None or m_last is None:
+            raise ValueError("read_outer needs the initial and final states")
+        images[0] = m_first
+        images[-1] = m_last
+
+    def out(name):
+        return None if directory is None else os.path.join(directory, name)
+
+    if directory is not None:
+        write_image(out("SpinSTM_GNEB_ini.dat"), images[0])
+        write_image(out("SpinSTM_GNEB_fin.dat"), images[-1])
+    if inp.min_type in (1, 2):
+        ham = Hamiltonian(deck, device=device)
+        mi = minimize_input
+        kw = {} if mi is None else dict(timestep=mi.timestep, mass=mi.mass, conv_torque=mi.conv_torque,
+                                        max_iter=int(min(mi.steps, 2 ** 62)))
+        for k in (0, nim - 1):
+            m = torch.tensor(images[k].T.copy(), device=f"cuda:{device}")
+            minimize(ham, m, "infdamp" if inp.min_type == 1 else "vpo", **kw)
+            images[k] = m.cpu().numpy().T
+    elif inp.min_type != 0:
+        raise ValueError("UNEXPECTED io_gneb%min_type")
+    if not inp.read_path:
+        images = geodesic_path(images[0], images[-1], nim, inp.amp_rnd_path, seed)
+    if directory is not None:
+        write_path(directory, images)
+    batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)), [0.0] * nim,
+                         device=device)
+    batch.upload(np.ascontiguousarray(images).reshape(nim * N, 3))
+    rx, ene, dene = np.zeros(nim), np.zeros(nim), np.zeros(nim)
+    runs = []
+    for climb, on in ((False, inp.do_gneb), (True, inp.do_gneb_ci)):
+        if not on:
+            continue
+        start = _relax(batch, nim, N, inp, climb, itrmax=0)
+        if directory is not None:
+            write_en(out("en_path.in"), start.rx, start.ene, start.dene, start.rx[-1], inp.do_norm_rx)
+        r = _relax(batch, nim, N, inp, climb)
+        runs.append(r)
+        images, rx, ene, dene = r.images, r.rx, r.ene, r.dene
+    if directory is not None:
+        write_en(out("en_path.out"), rx, ene, dene, rx[-1], inp.do_norm_rx)
+        write_path(directory, images)
+    c, xx, yy, dyy = hermite_fit(rx, ene, dene, inp.sample_num)
+    if directory is not None:
+        write_en(out("enfit_path.out"), xx, yy, dyy, rx[-1], inp.do_norm_rx)
+    if inp.do_gneb_ci and runs:
+        ci = runs[-1].ci
+        rx0 = float(rx[ci])
+        spinsp = images[ci].copy()
+    else:
+        imax, drx0 = find_sp(rx, c)
+        rx0 = float(rx[imax] + drx0)
+        spinsp = images[-1].copy() if imax == nim - 1 else saddle_configuration(
+            images[imax], images[imax + 1], rx[imax], rx[imax + 1], rx0, seed)
+    e0, de0 = spline_hermite_val(rx, c, rx0)
+    if directory is not None:
+        write_en(out("ensp_path.out"), [rx0], [e0], [de0], rx[-1], inp.do_norm_rx)
+        write_image(out("image-GNEB-saddlepoint.dat"), spinsp)
+    return {"images": images, "rx": rx, "ene": ene, "dene": dene, "saddle": (rx0, e0, de0), "saddle_spins": spinsp,
+            "runs": runs}

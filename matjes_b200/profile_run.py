@@ -15,7 +15,13 @@ steps the 256-replica batch workload;
 
     python -m matjes_b200.profile_run --mc --lattice square --L 2048 --steps 3
 
-runs Metropolis sweeps (cone proposals, 10 K) instead of time steps.
+runs Metropolis sweeps (cone proposals, 10 K) instead of time steps;
+
+    python -m matjes_b200.profile_run --gneb --L 256 --nim 16 --steps 64
+
+relaxes a GNEB path of --nim images of an L x L DMI film (J + D + K + Bz =
+0.3 T, periodic; geodesic from +z to -z, interior spins moved by up to 1e-2)
+for --steps iterations (force tolerance 0).
 """
 from __future__ import annotations
 
@@ -38,7 +44,11 @@ def main(argv=None):
     ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
     ap.add_argument("--batch", action="store_true", help="step the 256-replica batch workload")
     ap.add_argument("--mc", action="store_true", help="Metropolis sweeps (cone proposals) instead of time steps")
+    ap.add_argument("--gneb", action="store_true", help="GNEB path relaxation iterations instead of time steps")
+    ap.add_argument("--nim", type=int, default=16, help="GNEB images")
     a = ap.parse_args(argv)
+    if a.gneb:
+        return gneb(a)
     if a.adjoint:
         return adjoint(a)
     if a.batch:
@@ -103,6 +113,21 @@ def adjoint(a):
     g0, gt, gb = traj.backward(mT - m0)
     torch.cuda.synchronize()
     print("ok", gt.tolist(), float(g0.abs().sum()), float(gb.abs().sum()))
+
+
+def gneb(a):
+    import matjes_b200 as mj
+    from matjes_b200.gneb import geodesic_path
+
+    deck = mj.square_film((a.L, a.L, 1), Jv=1e-3, Dv=0.4e-3, Kv=-0.2e-3, Bz=0.3, mu_s=2.0, periodic=(1, 1, 0))
+    n = a.L * a.L
+    up = np.tile([0.0, 0.0, 1.0], (n, 1))
+    path = geodesic_path(up, -up, a.nim, amp_rnd=1e-2, seed=1)
+    path[0], path[-1] = up, -up
+    bt = mj.ReplicaBatch(deck, [(a.L, a.L)] * a.nim, np.tile(deck.B_ext, (a.nim, 1)), [0.0] * a.nim)
+    bt.upload(path.reshape(-1, 3))
+    rx, ene, dene, its, fchk, _ = bt.gneb_path(0.3, 0.02, 1.0, 0.0, a.steps, "I")
+    print("ok", its, fchk, ene.tolist())
 
 
 def batch(a):

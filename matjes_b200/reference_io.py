@@ -208,6 +208,8 @@ class ReferenceInput:
     # the Monte Carlo input (IO-input/MC_io.f90 rw_MC), None when the deck sets
     # no sampling method
     monte_carlo: Optional[object] = None
+    # the GNEB input (IO-input/GNEB_io.f90 rw_gneb)
+    gneb: Optional[object] = None
 
 
 MC_SAMPLING_KEYS = (("ising", "ising"), ("underrelaxation", "underrelax"), ("overrelaxation", "overrelax"),
@@ -229,6 +231,43 @@ def parse_monte_carlo(inp: "InputDeck"):
                    N_relaxation=inp.values("n_relaxation", 1, int, 1000), T_relax=inp.values("T_relax", 1, int, 1),
                    T_auto=inp.values("T_auto", 1, int, 1), Total_MC_Steps=inp.values("Total_MC_Steps", 1, int, 1000),
                    cone=inp.values("cone", 1, default=math.pi), sampling=methods[0])
+
+
+def parse_gneb(inp: "InputDeck"):
+    """rw_gneb (IO-input/GNEB_io.f90:43-112): the GNEB keywords with their
+    defaults; initpath sets read_path / read_outer / min_type (-1: unchanged;
+    1: geodesic path, no minimisation; 2: path read, minimize; 3: path read,
+    minimize_infdamp; other values: geodesic path, minimize_infdamp), the
+    gnebinit_* keywords override them."""
+    from .gneb import GNEBInput
+
+    d = GNEBInput()
+    g = GNEBInput(
+        momfile_i=inp.values("momfile_i", 1, str, d.momfile_i), momfile_f=inp.values("momfile_f", 1, str, d.momfile_f),
+        restartfile_path=inp.values("restartfile_path", 1, str, d.restartfile_path),
+        spring=inp.values("spring", 1, default=d.spring), initpath=inp.values("initpath", 1, int, d.initpath),
+        amp_rnd=inp.values("amp_rnd", 1, default=d.amp_rnd),
+        amp_rnd_path=inp.values("amp_rnd_path", 1, default=d.amp_rnd_path),
+        itrmax=inp.values("mep_itrmax", 1, int, d.itrmax), every=inp.values("meptraj_step", 1, int, d.every),
+        mepftol=inp.values("mep_ftol", 1, default=d.mepftol),
+        mepftol_ci=inp.values("mep_ftol_ci", 1, default=d.mepftol_ci),
+        do_gneb=bool(inp.values("do_gneb_simple", 1, fortran_bool, d.do_gneb)),
+        do_gneb_ci=bool(inp.values("do_gneb_ci", 1, fortran_bool, d.do_gneb_ci)),
+        do_norm_rx=inp.values("do_norm_rx", 1, str, d.do_norm_rx), en_zero=inp.values("en_zero", 1, str, d.en_zero),
+        dt=inp.values("vpo_dt", 1, default=d.dt), mass=inp.values("vpo_mass", 1, default=d.mass),
+        sample_num=inp.values("sample_num", 1, int, d.sample_num), nim=inp.values("nim", 1, int, d.nim))
+    if g.initpath == 1:
+        g.read_path, g.read_outer, g.min_type = False, True, 0
+    elif g.initpath == 2:
+        g.read_path, g.read_outer, g.min_type = True, True, 2
+    elif g.initpath == 3:
+        g.read_path, g.read_outer, g.min_type = True, True, 1
+    elif g.initpath != -1:
+        g.read_path, g.read_outer, g.min_type = False, True, 1
+    g.read_path = bool(inp.values("gnebinit_read_path", 1, fortran_bool, g.read_path))
+    g.read_outer = bool(inp.values("gnebinit_read_outer", 1, fortran_bool, g.read_outer))
+    g.min_type = inp.values("gnebinit_min_type", 1, int, g.min_type)
+    return g
 
 
 def _rotation_zxz(angles_pi: Sequence[float]) -> np.ndarray:
@@ -333,7 +372,7 @@ def parse_input(path_or_text: str) -> ReferenceInput:
                        conv_torque=inp.values("convergence_criteria", 1, default=1e-6))
     sim = inp.values("simulation", 1, str, "")
     return ReferenceInput(deck=deck, dynamics=dyn, minimize=mn, atom_names=names, simulation=sim,
-                          monte_carlo=parse_monte_carlo(inp))
+                          monte_carlo=parse_monte_carlo(inp), gneb=parse_gneb(inp))
 
 
 # ----------------------------------------------------------------------
@@ -491,3 +530,31 @@ def run_montecarlo(directory: str, seed: int = 1, write: bool = True):
     if write:
         thermo_print(os.path.join(directory, "EM.dat"), rows)
     return rows
+
+
+def run_gneb(directory: str, seed: int = 0, write: bool = True) -> dict:
+    """The GNEB of an input directory on the GPU (`simulation GNEB`, GNEB_run of
+    GNEB/gneb.f90): reads `input` (the lattice, Hamiltonian, GNEB and
+    minimisation keywords), the initial and final states momfile_i / momfile_f
+    (read_outer) and the path <restartfile_path>_<k>.dat, k = 1 .. nim
+    (read_path), each as an order-parameter file of the lattice; then
+    gneb.gneb_run, writing en_path.in, en_path.out, enfit_path.out,
+    ensp_path.out, image-GNEB_<k>.dat, image-GNEB-saddlepoint.dat and
+    SpinSTM_GNEB_ini.dat / SpinSTM_GNEB_fin.dat into the directory."""
+    from .gneb import gneb_run
+
+    ri = parse_input(os.path.join(directory, "input"))
+    if ri.simulation != "GNEB":
+        raise ValueError(f"simulation {ri.simulation!r} is not GNEB")
+    g = ri.gneb
+    deck = ri.deck
+    N = deck.nsites
+
+    def read(name):
+        return read_order_file(os.path.join(directory, name), N)
+
+    m_i = read(g.momfile_i) if g.read_outer else None
+    m_f = read(g.momfile_f) if g.read_outer else None
+    path = np.stack([read(f"{g.restartfile_path}_{k}.dat") for k in range(1, g.nim + 1)]) if g.read_path else None
+    return gneb_run(deck, g, m_i, m_f, path, minimize_input=ri.minimize, directory=directory if write else None,
+                    seed=seed)

@@ -1294,10 +1294,12 @@ static void gn_fields(const orc_model* M, const double* img, int i0, int i1, int
 }
 
 /* GNEB forces of the interior images: the perpendicular part of the force plus the
- * spring force along the energy-weighted tangent; fpp the force along the simple
- * tangent (the energy derivative along the path) */
+ * spring force along the energy-weighted tangent; at the climbing image ci (-1:
+ * none) the force with its component along the tangent reversed and no spring
+ * (gneb_utils.f90:105-111); fpp the force along the simple tangent (the energy
+ * derivative along the path) */
 static void gn_gneb_forces(const double* img, int nim, int64_t N, const double* E, const double* pl, double spring,
-                           double* F, double* fpp, double* tau, double* tau_i) {
+                           int ci, double* F, double* fpp, double* tau, double* tau_i) {
     for (int im = 1; im < nim - 1; im++) {
         double* f = F + (int64_t)im * 3 * N;
         gn_tang_special(img, N, im, E, tau);
@@ -1305,14 +1307,26 @@ static void gn_gneb_forces(const double* img, int nim, int64_t N, const double* 
         double fp = 0.0, fi = 0.0;
         for (int64_t r = 0; r < 3 * N; r++) { fi += f[r] * tau_i[r]; fp += f[r] * tau[r]; }
         fpp[im] = fi;
+        if (im == ci) {
+            for (int64_t r = 0; r < 3 * N; r++) f[r] = f[r] - 2.0 * tau[r] * fp;
+            continue;
+        }
         double sp = spring * (pl[im + 1] + pl[im - 1] - 2.0 * pl[im]);
         for (int64_t r = 0; r < 3 * N; r++) f[r] = f[r] - tau[r] * fp + sp * tau[r];
     }
 }
 
+/* maxloc: the first image of highest energy */
+static int gn_maxloc(const double* E, int nim) {
+    int c = 0;
+    for (int i = 1; i < nim; i++)
+        if (E[i] > E[c]) c = i;
+    return c;
+}
+
 int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, double dt, double mass, double ftol,
-                       int64_t itrmax, int en_zero, double* rx, double* ene, double* dene, int64_t* iters,
-                       double* fchk_out) {
+                       int64_t itrmax, int en_zero, int climb, double* rx, double* ene, double* dene, int64_t* iters,
+                       double* fchk_out, int* ci_out) {
     if (M->nmag != 1 || nim < 3) return -3;
     const int64_t N = M->nsite, n3 = 3 * N, tot = (int64_t)nim * n3;
     double *F1 = calloc((size_t)tot, sizeof(double)), *F2 = calloc((size_t)tot, sizeof(double));
@@ -1324,7 +1338,8 @@ int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, 
     gn_path(img, nim, N, pl);
     gn_fields(M, img, 0, nim, N, F1, E);
     double eref = en_zero == 'I' ? E[0] : (en_zero == 'F' ? E[nim - 1] : 0.0);
-    gn_gneb_forces(img, nim, N, E, pl, spring, F1, fpp, tau, tau_i);
+    int ci = climb ? gn_maxloc(E, nim) : -1;
+    gn_gneb_forces(img, nim, N, E, pl, spring, ci, F1, fpp, tau, tau_i);
     double fchk = 0.0;
     for (int64_t r = 0; r < tot; r++) fchk = fmax(fchk, fabs(F1[r]));
     int64_t itr = 0, done = 0;
@@ -1349,7 +1364,8 @@ int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, 
             }
         gn_fields(M, img, 1, nim - 1, N, F2, E);
         gn_path(img, nim, N, pl);
-        gn_gneb_forces(img, nim, N, E, pl, spring, F2, fpp, tau, tau_i);
+        if (climb) ci = gn_maxloc(E, nim);
+        gn_gneb_forces(img, nim, N, E, pl, spring, ci, F2, fpp, tau, tau_i);
         /* parallel transport of the velocity and the old force, velocity Verlet */
         for (int im = 1; im < nim - 1; im++)
             for (int64_t s = 0; s < N; s++) {
@@ -1380,6 +1396,7 @@ int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, 
     for (int i = 0; i < nim; i++) { rx[i] = pl[i]; ene[i] = E[i] - eref; dene[i] = -fpp[i]; }
     if (iters) *iters = done;
     if (fchk_out) *fchk_out = fchk;
+    if (ci_out) *ci_out = ci;
     free(F1); free(F2); free(vel); free(ax); free(ang); free(tau); free(tau_i); free(E); free(fpp); free(pl);
     return 0;
 }

@@ -128,7 +128,12 @@ int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int6
                          int64_t* iters, double* max_torque);
 /* GNEB minimum-energy path of nim images img (nim x N x 3, AoS per image; the
  * end images stay fixed), single-atom models: find_path (GNEB/gneb_utils.f90:
- * 19-240) without the climbing image.  Each iteration moves the interior images
+ * 19-240), with the climbing image when climb != 0 (the first image of highest
+ * energy, chosen again each iteration; its force F - 2 tau (F.tau), no spring;
+ * ci_out, may be NULL, the last one, 0-based, or -1).  The reference's
+ * truncation of velocity and force components below 1e-50 of their maximum
+ * (vector_utils/precision.f90) is left out: it cannot change a double result
+ * here.  Each iteration moves the interior images
  * by velocity Verlet on the unit sphere (m + v dt + F dt^2 / 2 mass,
  * normalised), parallel-transports velocity and old force by the rotation of
  * each spin's move (utilities/rotation.f90 rotate), recomputes the projected
@@ -139,8 +144,8 @@ int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int6
  * the initial (en_zero 'I'), final ('F') or no ('N') image energy) and dene =
  * -F.tau_single per image as en_path.out holds them. */
 int orc_gneb_find_path(const orc_model* M, double* img, int nim, double spring, double dt, double mass, double ftol,
-                       int64_t itrmax, int en_zero, double* rx, double* ene, double* dene, int64_t* iters,
-                       double* fchk_out);
+                       int64_t itrmax, int en_zero, int climb, double* rx, double* ene, double* dene, int64_t* iters,
+                       double* fchk_out, int* ci_out);
 /* OpenMP threads of the parallel loops (n <= 0: all processors). */
 void orc_set_threads(int n);
 /* Metropolis Monte Carlo.  proposal: 0 sphereft cone, 1 Ising flip,

@@ -291,21 +291,25 @@ def mc_random(model, m, st: MC, nsweeps):
     return E, Mg, acc.value
 
 
-def gneb_find_path(model, images, spring=0.5, dt=0.01, mass=1.0, ftol=1e-8, itrmax=10 ** 7, en_zero="I"):
+def gneb_find_path(model, images, spring=0.5, dt=0.01, mass=1.0, ftol=1e-8, itrmax=10 ** 7, en_zero="I",
+                   climb=False, return_ci=False):
     """GNEB find_path on images (nim, N, 3), relaxed in place; returns (rx, ene,
-    dene, iterations, max |F|) as en_path.out holds them."""
+    dene, iterations, max |F|) as en_path.out holds them, and the climbing
+    image (0-based, -1 without) when return_ci."""
     lib.orc_gneb_find_path.restype = C.c_int
     lib.orc_gneb_find_path.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
-                                       C.c_double, C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
-                                       C.POINTER(C.c_int64), C.POINTER(C.c_double)]
+                                       C.c_double, C.c_int64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     assert images.dtype == np.float64 and images.flags.c_contiguous and images.ndim == 3
     nim = images.shape[0]
     rx, ene, dene = np.zeros(nim), np.zeros(nim), np.zeros(nim)
-    it, fc = C.c_int64(), C.c_double()
-    rc = lib.orc_gneb_find_path(model.h, _p(images), nim, spring, dt, mass, ftol, int(itrmax), ord(en_zero), _p(rx),
-                                _p(ene), _p(dene), C.byref(it), C.byref(fc))
+    it, fc, ci = C.c_int64(), C.c_double(), C.c_int()
+    rc = lib.orc_gneb_find_path(model.h, _p(images), nim, spring, dt, mass, ftol, int(itrmax), ord(en_zero),
+                                int(bool(climb)), _p(rx), _p(ene), _p(dene), C.byref(it), C.byref(fc), C.byref(ci))
     if rc != 0:
         raise RuntimeError(f"oracle GNEB failed ({rc})")
+    if return_ci:
+        return rx, ene, dene, it.value, fc.value, ci.value
     return rx, ene, dene, it.value, fc.value
 
 

@@ -88,3 +88,100 @@ def test_oracle_path_reproduces_the_reference_gneb_test():
     assert e0 == pytest.approx(GOLD["ensp"][1], abs=5e-9)
     for k in range(len(path)):
         assert mz_matches(path[k, :, 2], np.array(GOLD["images"][k])[:, 2], 1e-4), k
+
+
+def test_oracle_climbing_image_reaches_the_saddle():
+    """do_gneb_ci after the plain relaxation (GNEB_run's order): the climbing
+    image is the image of highest energy, the energy's derivative along the
+    path vanishes there (|dE/dx| < 1e-7 eV against 2e-3 eV of barrier), and its
+    energy is the saddle point of the reference's fit to 5e-7 eV (the Hermite
+    fit of 12 images overshoots the barrier by 2e-7 eV)."""
+    g = GOLD["deck"]
+    mod = O.Model(chain_deck())
+    path = chain_path()
+    O.set_threads(1)
+    try:
+        O.gneb_find_path(mod, path, spring=g["spring"], dt=g["vpo_dt"], mass=g["vpo_mass"], ftol=g["mep_ftol"],
+                         en_zero="I")
+        rx, ene, dene, iters, fchk, ci = O.gneb_find_path(mod, path, spring=g["spring"], dt=g["vpo_dt"],
+                                                          mass=g["vpo_mass"], ftol=g["mep_ftol"], en_zero="I",
+                                                          climb=True, return_ci=True)
+    finally:
+        O.set_threads(0)
+    assert fchk < g["mep_ftol"] and 0 < ci < len(ene) - 1
+    assert ci == int(np.argmax(ene))
+    assert abs(dene[ci]) < 1e-7
+    assert abs(ene[ci] - GOLD["ensp"][1]) < 5e-7
+
+
+GNEB_DECK = """simulation GNEB
+Periodic_log .F. .F. .F.
+lattice
+1.0 0.0 0.0
+0.0 1.0 0.0
+0.0 0.0 1.0
+Nsize 10 1 1
+atomtypes 1
+Fe 1.0 0.0 1.0 F
+atoms 1
+Fe 0.0 0.0 0.0
+magnetic_J
+1 1 1 1.0d-3
+magnetic_anisotropy
+1 0.0 0.0 -0.3d-3
+#spring 12.5
+nim 12
+do_gneb_simple .T.
+mep_ftol 1.0d-8
+vpo_dt 0.01
+en_zero I
+initpath 2
+restartfile_path image-GNEB-start
+momfile_i momfile_i
+momfile_f momfile_f
+"""
+
+
+def test_gneb_keywords():
+    """rw_gneb: keyword values and defaults, and initpath's settings with the
+    gnebinit_* overrides; the deck builds the chain of the reference's test."""
+    from matjes_b200 import reference_io as R
+    from matjes_b200.deck import random_sphere
+
+    ri = R.parse_input(GNEB_DECK)
+    gi = ri.gneb
+    assert ri.simulation == "GNEB" and gi.nim == 12 and gi.do_gneb and not gi.do_gneb_ci
+    assert (gi.mepftol, gi.dt, gi.mass, gi.spring, gi.en_zero) == (1e-8, 0.01, 1.0, 0.5, "I")
+    assert (gi.read_path, gi.read_outer, gi.min_type) == (True, True, 2)
+    assert gi.restartfile_path == "image-GNEB-start" and gi.every == 10 and gi.itrmax == 2 ** 63 - 1
+    for ip, want in ((1, (False, True, 0)), (3, (True, True, 1)), (7, (False, True, 1)), (-1, (False, True, 1))):
+        g2 = R.parse_input(GNEB_DECK.replace("initpath 2", f"initpath {ip}")).gneb
+        assert (g2.read_path, g2.read_outer, g2.min_type) == want, ip
+    g3 = R.parse_input(GNEB_DECK + "gnebinit_min_type 0\ngnebinit_read_path .F.\ndo_gneb_ci .T.\n").gneb
+    assert (g3.read_path, g3.min_type, g3.do_gneb_ci) == (False, 0, True)
+    m = random_sphere(10, 3)
+    assert np.array_equal(O.Model(ri.deck).field(m)[0], O.Model(chain_deck()).field(m)[0])
+
+
+def test_gneb_files_and_saddle_configuration(tmp_path):
+    """image files (3 F14.8 and two blanks per spin), en_path files (x / x0 with
+    do_norm_rx 'Y'), and the spins at the saddle point on the geodesic between
+    two images (find_SP_conf)."""
+    from matjes_b200.gneb import saddle_configuration, write_en, write_image
+
+    write_image(str(tmp_path / "i.dat"), np.array([[0.6, -0.8, 0.0], [0.0, 0.0, -1.0]]))
+    assert (tmp_path / "i.dat").read_text() == ("    0.60000000   -0.80000000    0.00000000  \n"
+                                                "    0.00000000    0.00000000   -1.00000000  \n")
+    write_en(str(tmp_path / "e.out"), [1.0, 4.0], [0.5, -0.25], [0.0, 1e-3], 4.0, "Y")
+    rows = [[float(v) for v in ln.split()] for ln in (tmp_path / "e.out").read_text().splitlines()]
+    assert rows == [[0.25, 0.5, 0.0], [1.0, -0.25, 1e-3]]
+    with pytest.raises(ValueError):
+        write_en(str(tmp_path / "x.out"), [1.0], [0.0], [0.0], 1.0, "Q")
+    a = np.array([[0.0, 0.0, 1.0], [1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    b = np.array([[1.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.0, -1.0]])
+    sp = saddle_configuration(a, b, 2.0, 4.0, 3.0)
+    # a quarter turn: halfway is 45 degrees in the x-z plane
+    np.testing.assert_allclose(sp[0], [math.sqrt(0.5), 0.0, math.sqrt(0.5)], atol=1e-15)
+    np.testing.assert_allclose(sp[1], [1.0, 0.0, 0.0], atol=1e-15)
+    # antiparallel: a half turn's half about an axis perpendicular to the spin
+    assert abs(sp[2, 2]) < 1e-15 and abs(np.linalg.norm(sp[2]) - 1.0) < 1e-15

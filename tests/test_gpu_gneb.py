@@ -47,7 +47,8 @@ def test_device_path_reproduces_the_reference_gneb_test():
     deck, path = _chain()
     inp = GNEBInput(nim=g["nim"], spring=g["spring"], dt=g["vpo_dt"], mass=g["vpo_mass"], mepftol=g["mep_ftol"],
                     en_zero="I")
-    out, rx, ene, dene, iters, fchk = find_path(deck, path, inp)
+    res = find_path(deck, path, inp)
+    out, rx, ene, dene, iters, fchk = res.images, res.rx, res.ene, res.dene, res.iterations, res.max_force
     assert fchk < g["mep_ftol"] and 10000 < iters < 200000
     ref = np.array(GOLD["en_path_out"])
     np.testing.assert_allclose(rx, ref[:, 0], rtol=0, atol=3e-5)
@@ -87,7 +88,8 @@ def test_device_iterations_follow_the_oracle(en_zero):
 
     deck, path = _film_path()
     inp = GNEBInput(spring=0.3, dt=0.02, mass=1.0, mepftol=0.0, itrmax=200, en_zero=en_zero)
-    out, rx, ene, dene, iters, fchk = find_path(deck, path, inp)
+    res = find_path(deck, path, inp)
+    out, rx, ene, dene, iters, fchk = res.images, res.rx, res.ene, res.dene, res.iterations, res.max_force
     op = path.copy()
     orx, oene, odene, oit, ofc = O.gneb_find_path(O.Model(deck), op, spring=0.3, dt=0.02, mass=1.0, ftol=0.0,
                                                   itrmax=200, en_zero=en_zero)
@@ -107,7 +109,8 @@ def test_large_path_iterations_follow_the_oracle():
 
     deck, path = _film_path(nim=12, L=(160, 160), seed=3)
     inp = GNEBInput(spring=0.3, dt=0.02, mass=1.0, mepftol=0.0, itrmax=20, en_zero="I")
-    out, rx, ene, dene, iters, fchk = find_path(deck, path, inp)
+    res = find_path(deck, path, inp)
+    out, rx, ene, dene, iters, fchk = res.images, res.rx, res.ene, res.dene, res.iterations, res.max_force
     op = path.copy()
     orx, oene, odene, oit, ofc = O.gneb_find_path(O.Model(deck), op, spring=0.3, dt=0.02, mass=1.0, ftol=0.0,
                                                   itrmax=20, en_zero="I")
@@ -125,7 +128,8 @@ def test_no_iteration_reports_the_initial_path():
     from matjes_b200.gneb import GNEBInput, find_path
 
     deck, path = _film_path(nim=4, seed=9, fixed_ends=False)
-    out, rx, ene, dene, iters, fchk = find_path(deck, path, GNEBInput(itrmax=0, en_zero="N"))
+    res = find_path(deck, path, GNEBInput(itrmax=0, en_zero="N"))
+    out, rx, ene, dene, iters, fchk = res.images, res.rx, res.ene, res.dene, res.iterations, res.max_force
     op = path.copy()
     orx, oene, odene, oit, ofc = O.gneb_find_path(O.Model(deck), op, itrmax=0, en_zero="N")
     assert iters == oit == 0
@@ -139,7 +143,9 @@ def test_no_iteration_reports_the_initial_path():
 
 def test_path_arguments_are_checked():
     import matjes_b200 as mj
-    from matjes_b200._abi import MJ_ERR_ARG, MJ_ERR_UNSUPPORTED, lib
+    import ctypes as C
+
+    from matjes_b200._abi import MJ_ERR_ARG, MJ_ERR_UNSUPPORTED, GnebParams, lib
 
     deck, path = _film_path(nim=3)
     n = path.shape[1]
@@ -153,10 +159,77 @@ def test_path_arguments_are_checked():
         three.gneb_path(en_zero="X")
     rx, ene, dene = np.zeros(3), np.zeros(3), np.zeros(3)
     p = lambda a: a.ctypes.data  # noqa: E731
-    assert lib.mj_batch_gneb_path(three.handle, 0.5, 0.01, 1.0, 1e-3, 10, ord("X"), p(rx), p(ene), p(dene), None,
+    gp = lambda dt, ez: C.byref(GnebParams(0.5, dt, 1.0, 1e-3, 10, ord(ez), 0))  # noqa: E731
+    assert lib.mj_batch_gneb_path(three.handle, gp(0.01, "X"), p(rx), p(ene), p(dene), None, None,
                                   None) == MJ_ERR_ARG
-    assert lib.mj_batch_gneb_path(three.handle, 0.5, -0.01, 1.0, 1e-3, 10, ord("I"), p(rx), p(ene), p(dene), None,
+    assert lib.mj_batch_gneb_path(three.handle, gp(-0.01, "I"), p(rx), p(ene), p(dene), None, None,
                                   None) == MJ_ERR_ARG
+    assert lib.mj_batch_gneb_path(three.handle, None, p(rx), p(ene), p(dene), None, None, None) == MJ_ERR_ARG
     mixed = mj.ReplicaBatch(deck, [deck.L[:2], (4, 6), deck.L[:2]], np.zeros((3, 3)), [0.0] * 3)
-    assert lib.mj_batch_gneb_path(mixed.handle, 0.5, 0.01, 1.0, 1e-3, 10, ord("I"), p(rx), p(ene), p(dene), None,
+    assert lib.mj_batch_gneb_path(mixed.handle, gp(0.01, "I"), p(rx), p(ene), p(dene), None, None,
                                   None) == MJ_ERR_UNSUPPORTED
+
+
+def test_device_climbing_image_follows_the_oracle():
+    """The climbing-image relaxation (do_gneb_ci): 200 iterations of a 2D film
+    path against the oracle's (1e-10), the same climbing image."""
+    from matjes_b200.gneb import GNEBInput, find_path
+
+    deck, path = _film_path()
+    inp = GNEBInput(spring=0.3, dt=0.02, mass=1.0, mepftol_ci=0.0, itrmax=200, en_zero="I")
+    res = find_path(deck, path, inp, climb=True)
+    op = path.copy()
+    orx, oene, odene, oit, ofc, oci = O.gneb_find_path(O.Model(deck), op, spring=0.3, dt=0.02, mass=1.0, ftol=0.0,
+                                                       itrmax=200, en_zero="I", climb=True, return_ci=True)
+    assert res.iterations == oit == 200 and res.ci == oci and 0 < oci < len(path) - 1
+    assert np.abs(res.images - op).max() < 1e-10
+    np.testing.assert_allclose(res.rx, orx, rtol=1e-10, atol=1e-12)
+    assert np.abs(res.ene - oene).max() <= 1e-10 * np.abs(oene).max()
+    assert np.abs(res.dene - odene).max() <= 1e-10 * np.abs(odene).max()
+    # without climbing the same path goes elsewhere
+    plain = find_path(deck, path, inp)
+    assert plain.ci == -1 and np.abs(plain.images - res.images).max() > 1e-6
+
+
+def test_reference_deck_directory_runs_the_gneb(tmp_path):
+    """run_gneb on an input directory holding the reference's chain test in
+    the current input format (the path read from image-GNEB-start_<k>.dat, the
+    end states from momfile_i / momfile_f, minimised by `minimize`): en_path.out,
+    ensp_path.out and the images against the reference's own outputs; then with
+    do_gneb_ci the climbing image against the oracle's."""
+    from matjes_b200 import reference_io as R
+    from test_gneb_oracle import GNEB_DECK, mz_matches
+
+    g = GOLD["deck"]
+    _, path = _chain()
+    for k, img in enumerate(path, start=1):
+        R.write_order_file(str(tmp_path / f"image-GNEB-start_{k}.dat"), img)
+    R.write_order_file(str(tmp_path / "momfile_i"), path[0])
+    R.write_order_file(str(tmp_path / "momfile_f"), path[-1])
+    (tmp_path / "input").write_text(GNEB_DECK)
+    out = R.run_gneb(str(tmp_path))
+    rows = np.array([[float(v) for v in ln.split()] for ln in (tmp_path / "en_path.out").read_text().splitlines()])
+    ref = np.array(GOLD["en_path_out"])
+    np.testing.assert_allclose(rows[:, 0], ref[:, 0], rtol=0, atol=3e-5)
+    np.testing.assert_allclose(rows[:, 1], ref[:, 1], rtol=0, atol=5e-9)
+    np.testing.assert_allclose(rows[1:-1, 2], ref[1:-1, 2], rtol=0, atol=5e-9)
+    sp = [float(v) for v in (tmp_path / "ensp_path.out").read_text().split()]
+    assert sp[0] == pytest.approx(GOLD["ensp"][0], abs=3e-5) and sp[1] == pytest.approx(GOLD["ensp"][1], abs=5e-9)
+    assert len((tmp_path / "enfit_path.out").read_text().splitlines()) == 500
+    assert len((tmp_path / "en_path.in").read_text().splitlines()) == 12
+    for k in range(1, 13):
+        img = np.loadtxt(str(tmp_path / f"image-GNEB_{k}.dat"))
+        assert img.shape == (10, 3)
+        assert mz_matches(img[:, 2], np.array(GOLD["images"][k - 1])[:, 2], 1e-4), k
+    saddle = np.loadtxt(str(tmp_path / "image-GNEB-saddlepoint.dat"))
+    assert saddle.shape == (10, 3) and np.abs(np.linalg.norm(saddle, axis=1) - 1.0).max() < 1e-7
+    # the climbing image after the plain relaxation, against the oracle's
+    (tmp_path / "input").write_text(GNEB_DECK + "do_gneb_ci .T.\nmep_ftol_ci 1.0d-8\n")
+    ci_out = R.run_gneb(str(tmp_path))
+    run = ci_out["runs"][-1]
+    op = out["images"].copy()
+    orx, oene, odene, oit, ofc, oci = O.gneb_find_path(O.Model(R.parse_input(GNEB_DECK).deck), op.copy(),
+                                                       spring=g["spring"], dt=g["vpo_dt"], mass=g["vpo_mass"],
+                                                       ftol=1e-8, en_zero="I", climb=True, return_ci=True)
+    assert run.ci == oci and ci_out["saddle"][0] == pytest.approx(run.rx[run.ci], abs=0)
+    assert abs(run.ene[run.ci] - oene[oci]) < 1e-9 and abs(run.dene[run.ci]) < 1e-7
