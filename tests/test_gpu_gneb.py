@@ -102,6 +102,34 @@ def test_device_iterations_follow_the_oracle(en_zero):
     assert fchk == pytest.approx(ofc, rel=1e-9)
 
 
+def test_triangular_three_shell_path_follows_the_oracle():
+    """The GNEB field pass on the triangular three-shell stencil (J1..J3 + D1 + K
+    + Bz = 1 T, 24 x 20, 7 images): 120 iterations, plain and climbing, against
+    the oracle's (1e-10; the oracle carries a 1e-13 change of this path's start
+    unamplified through 150 iterations)."""
+    from matjes_b200.deck import triangular
+    from matjes_b200.gneb import GNEBInput, find_path, geodesic_path
+
+    deck = triangular((24, 20))
+    n = 24 * 20
+    up = np.tile([0.0, 0.0, 1.0], (n, 1))
+    path = geodesic_path(up, -up, 7, amp_rnd=1e-2, seed=4)
+    path[0], path[-1] = up, -up
+    path = np.ascontiguousarray(path)
+    for climb in (False, True):
+        inp = GNEBInput(spring=0.3, dt=0.02, mass=1.0, mepftol=0.0, mepftol_ci=0.0, itrmax=120, en_zero="F")
+        res = find_path(deck, path, inp, climb=climb)
+        op = path.copy()
+        orx, oene, odene, oit, ofc, oci = O.gneb_find_path(O.Model(deck), op, spring=0.3, dt=0.02, mass=1.0,
+                                                           ftol=0.0, itrmax=120, en_zero="F", climb=climb,
+                                                           return_ci=True)
+        assert res.iterations == oit == 120 and res.ci == oci
+        assert np.abs(res.images - op).max() < 1e-10
+        np.testing.assert_allclose(res.rx, orx, rtol=1e-10)
+        assert np.abs(res.ene - oene).max() <= 1e-10 * np.abs(oene).max()
+        assert np.abs(res.dene - odene).max() <= 1e-10 * np.abs(odene).max()
+
+
 def test_large_path_iterations_follow_the_oracle():
     """A path of 12 images of 160 x 160 (307,200 sites: the kernels then take four
     sites per thread): 20 iterations against the oracle's (1e-10)."""
