@@ -595,6 +595,29 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
     pk = peaks()
     bpsite = 240.0
     ach = bpsite * n * nim / per_it / 1e9
+    del batch
+    # the same path held on the deck's plan (mj_gneb_path: one field launch of
+    # the plan per image, then the path sums): 312 algorithmic bytes per image
+    # site and iteration (the field pass 48, the sums m and F in, F out 72, the
+    # step 120, the move 72)
+    from matjes_b200.gneb import PlanPath
+
+    holder = PlanPath(mj.Hamiltonian(deck, device=dev), path)
+
+    def call_plan(its):
+        holder.m.copy_(torch.tensor(path.transpose(0, 2, 1).copy(), device=holder.m.device))
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = holder.gneb_path(0.3, 0.02, 1.0, 0.0, its, "I")
+        dt = time.perf_counter() - t0
+        assert r[3] == its
+        return dt
+
+    call_plan(40)
+    per_it_plan = (min(call_plan(600) for _ in range(3)) - min(call_plan(100) for _ in range(3))) / 500
+    del holder
+    plan_bpsite = 312.0
+    plan_ach = plan_bpsite * n * nim / per_it_plan / 1e9
     mod = O.Model(deck)
     O.set_threads(1)
     try:
@@ -608,6 +631,12 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
             "launches_per_iteration": 4,
             "roofline": {"bound": "hbm", "alg_bytes_per_site": bpsite, "achieved": ach, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"]},
+            "on_plan": {"path": "mj_gneb_path: the images held on the deck's plan, one tiled field launch per image",
+                        "value": n * nim / per_it_plan, "us_per_iteration": 1e6 * per_it_plan,
+                        "launches_per_iteration": nim + 3,
+                        "roofline": {"bound": "hbm", "alg_bytes_per_site": plan_bpsite, "achieved": plan_ach,
+                                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": plan_ach / pk["hbm_gbs"],
+                                     "peak_source": pk["source"]}},
             "cpu_baseline": {"value": n * nim * 20 / ct, "unit": "image-site iterations/s", "cores": 1,
                              "kind": "port",
                              "sample": f"{side}x{side} film, {nim} images, 20 iterations (orc_gneb_find_path, "

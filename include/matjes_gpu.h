@@ -427,6 +427,21 @@ typedef struct mj_gneb_params {
  * default stream, returns with the relaxed path in the batch. */
 mj_status mj_batch_gneb_path(mj_batch* b, const mj_gneb_params* p, double* rx, double* ene, double* dene,
                              int64_t* iterations, double* max_force, int32_t* climbing);
+/* The same relaxation (GNEB/gneb_utils.f90:19-240 find_path) on a path of
+ * nimg images (3 or more) of any plan: the images' fields and energies are the
+ * plan's own get_eff_field and H%energy (GNEB/gneb_utils.f90:77-81,154-157),
+ * so every lattice and term a plan holds, the FFT dipolar term, 3D films and
+ * ELL couplings included, reaches the GNEB.  One magnetic atom per cell, as
+ * the reference requires (GNEB/gneb_utils.f90:69): MJ_ERR_UNSUPPORTED else.  m_dev (device,
+ * nimg * 3 N doubles; image r the SoA block x[N] | y[N] | z[N] at 3 N r)
+ * holds the path and receives the relaxed one.  Outputs as mj_batch_gneb_path.
+ * Starts after the work queued on `stream` (the iterations run as CUDA graphs
+ * on a stream of the plan's own) and returns with the path relaxed; at most
+ * 65535 * 256 spins per image.  Replaces the GNEB driver's image loop over get_eff_field/energy
+ * (GNEB/gneb_utils.f90:72-200) for a Hamiltonian held by a plan. */
+mj_status mj_gneb_path(mj_plan* plan, double* m_dev_images, int32_t nimg, const mj_gneb_params* p, double* rx,
+                       double* ene, double* dene, int64_t* iterations, double* max_force, int32_t* climbing,
+                       void* stream);
 /* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
  * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);

@@ -187,6 +187,7 @@ SIGNATURES = {
     "mj_batch_field": (C.c_int32, [P, P, P, C.c_int32, P]),
     "mj_batch_gneb_tangent": (C.c_int32, [P, P, C.c_int32, P, P]),
     "mj_batch_gneb_path": (C.c_int32, [P, P, P, P, P, P, P, P]),
+    "mj_gneb_path": (C.c_int32, [P, P, C.c_int32, P, P, P, P, P, P, P, P]),
     "mj_batch_set_config": (C.c_int32, [P, C.c_int32, C.c_int32]),
     "mj_batch_autotune": (C.c_int32, [P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
                                       C.POINTER(C.c_int32), P]),

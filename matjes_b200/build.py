@@ -16,9 +16,9 @@ OUT = os.path.join(HERE, "libmatjes_b200.so")
 OBJDIR = os.path.join(os.path.dirname(HERE), "_build", "obj")
 SOURCES = ["mj_kernels.cu", "mj_tiled.cu", "mj_tiled_square_nn.cu", "mj_tiled_square2.cu", "mj_tiled_tri_nn.cu",
            "mj_tiled_tri3.cu", "mj_dipolar.cu", "mj_batch.cu", "mj_adjoint.cu", "mj_minimize.cu", "mj_mc.cu",
-           "mj_lattice.cpp", "mj_abi.cpp"]
+           "mj_gneb.cu", "mj_lattice.cpp", "mj_abi.cpp"]
 HEADERS = ["mj_internal.hpp", "mj_device.cuh", "mj_shapes.hpp", "mj_tiled_impl.cuh", "mj_stencil.cuh",
-           os.path.join("..", "..", "include", "matjes_gpu.h")]
+           "mj_gneb.cuh", "mj_mc.cuh", os.path.join("..", "..", "include", "matjes_gpu.h")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

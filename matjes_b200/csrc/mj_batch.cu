@@ -22,6 +22,7 @@
 #include <numeric>
 #include <vector>
 
+#include "mj_gneb.cuh"
 #include "mj_mc.cuh"
 #include "mj_tiled_impl.cuh"
 
@@ -380,255 +381,11 @@ __global__ void __launch_bounds__(256) k_batch_magnet(const BatchRep* reps, cons
     if (slot && threadIdx.x == 0) slot[r] = R.slot;
 }
 
-// GNEB path tangents (GNEB/tangent.f90): for image r with neighbours r-1, r+1
-// tau = wp (m_{r+1} - m_r) + wm (m_r - m_{r-1}), projected on the tangent space
-// of m_r (vec_project, vector_utils/vector.f90:61-72) and normalised over the
-// image.  mode 0 (lattice_special, :93-124, doi:10.1016/j.cpc.2015.07.001):
-// the energy-weighted tangent of interior images; mode 1 (lattice_single,
-// :163-180): m_{r+1} - m_{r-1}.  End images take the one-sided difference.
-__device__ __forceinline__ void gneb_weights(const double* E, int r, int nrep, int mode, double& wp, double& wm) {
-    if (r == 0) {
-        wp = 1.0;
-        wm = 0.0;
-        return;
-    }
-    if (r == nrep - 1) {
-        wp = 0.0;
-        wm = 1.0;
-        return;
-    }
-    if (mode == 1) {
-        wp = wm = 1.0;
-        return;
-    }
-    const double u1 = E[r - 1], u2 = E[r], u3 = E[r + 1];
-    if (u3 > u2 && u2 > u1) {
-        wp = 1.0;
-        wm = 0.0;
-    } else if (u1 > u2 && u2 > u3) {
-        wp = 0.0;
-        wm = 1.0;
-    } else {
-        double dmax = fabs(u3 - u2), dmin = fabs(u1 - u2);
-        if (dmax < dmin) {
-            const double t = dmax;
-            dmax = dmin;
-            dmin = t;
-        }
-        if (u3 > u1) {
-            wp = dmax;
-            wm = dmin;
-        } else {
-            wp = dmin;
-            wm = dmax;
-        }
-    }
-}
-
-// unnormalised projected tangents; partial |tau|^2 per (image, block)
-__global__ void __launch_bounds__(256) k_gneb_tau(const double* __restrict__ m, int64_t n, int64_t Ntot, int nrep,
-                                                  const double* __restrict__ E, int mode, double* __restrict__ tau,
-                                                  double* __restrict__ part) {
-    const int r = blockIdx.y;
-    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double wp, wm;
-    gneb_weights(E, r, nrep, mode, wp, wm);
-    double q = 0.0;
-    if (li < n) {
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        const double3 m0 = ld3(m, i, Ntot);
-        const double3 mp = r + 1 < nrep ? ld3(m, i + n, Ntot) : m0;
-        const double3 mm = r > 0 ? ld3(m, i - n, Ntot) : m0;
-        double3 t = make_double3(wp * (mp.x - m0.x) + wm * (m0.x - mm.x), wp * (mp.y - m0.y) + wm * (m0.y - mm.y),
-                                 wp * (mp.z - m0.z) + wm * (m0.z - mm.z));
-        const double d = dot(t, m0);
-        t = make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
-        st3(tau, i, Ntot, t);
-        q = dot(t, t);
-    }
-    double v[1] = {q};
-    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
-}
-
-// per image: the ordered sum of its partials; 1/sqrt(sum) left in the image's
-// first partial
-__global__ void __launch_bounds__(256) k_gneb_norm_sum(double* part, int nblk) {
-    const int r = blockIdx.x;
-    __shared__ double tot;
-    ordered_sum<1>(part + static_cast<int64_t>(r) * nblk, nblk, &tot);
-    __syncthreads();
-    if (threadIdx.x == 0) part[static_cast<int64_t>(r) * nblk] = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
-}
-
-// tau /= |tau| of its image
-__global__ void __launch_bounds__(256) k_gneb_scale(double* __restrict__ tau, int64_t n, int64_t Ntot,
-                                                    const double* __restrict__ part, int nblk) {
-    const int r = blockIdx.y;
-    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (li >= n) return;
-    const double inv = part[static_cast<int64_t>(r) * nblk];
-    const int64_t i = static_cast<int64_t>(r) * n + li;
-    tau[i] *= inv;
-    tau[Ntot + i] *= inv;
-    tau[2 * Ntot + i] *= inv;
-}
-
 // ---------------------------------------------------------------------------
-// GNEB path relaxation (GNEB/gneb_utils.f90:19-240 find_path) on the replicas
-// taken as the images of one path (all of one size n, image r at sites
-// [r n, (r + 1) n)).  Before the first move and for the outputs: the field pass
-// gives the projected forces and energies; k_gneb_seg / k_gneb_pathlen the
-// geodesic path length; k_gneb_tau / k_gneb_norm_sum / k_gneb_scale the
-// tangents; k_gneb_dot_img and k_gneb_force the GNEB force.  An iteration is
-// four launches: the GNEB field pass (projected fields, energies and the path
-// sums of every tile), k_gneb_img (per-image sums), k_gneb_step (GNEB force,
-// transport, velocity Verlet, velocity projection, stop flag), k_gneb_move.
-// After the projection the velocity is lam F, lam one number, so neither the
-// velocity nor the tangents are stored.  Every sum is a block or tile partial
-// summed in a fixed order: the iterations are deterministic.
-struct GnebBufs {
-    double *F1, *F2, *mB, *tau, *E, *pl, *fp, *part, *part2, *scal;
-};
-
-__device__ __forceinline__ double3 gneb_rotate(double3 v, double3 a, double sn, double cs) {
-    // utilities/rotation.f90 rotate_vector_arr: v cos + sin (v x a) + (1 - cos)(a.v) a
-    const double t = dot(a, v);
-    return make_double3(v.x * cs + sn * (a.z * v.y - a.y * v.z) + (1.0 - cs) * t * a.x,
-                        v.y * cs + sn * (a.x * v.z - a.z * v.x) + (1.0 - cs) * t * a.y,
-                        v.z * cs + sn * (a.y * v.x - a.x * v.y) + (1.0 - cs) * t * a.z);
-}
-__device__ __forceinline__ double gneb_ang(double3 a, double3 b) {
-    const double3 c = cross(a, b);
-    return atan2(sqrt(dot(c, c)), dot(a, b));
-}
-
-// partial sums of the squared spin angles between images r and r + 1 (the_path)
-__global__ void __launch_bounds__(256) k_gneb_seg(const double* __restrict__ m, int64_t n, int64_t Ntot, double* part) {
-    const int r = blockIdx.y;
-    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double v[1] = {0.0};
-    if (li < n) {
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        const double l = gneb_ang(ld3(m, i, Ntot), ld3(m, i + n, Ntot));
-        v[0] = l * l;
-    }
-    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
-}
-
-__global__ void __launch_bounds__(256) k_gneb_pathlen(const double* part, int nblk, int nrep, double* pl) {
-    __shared__ double seg;
-    if (threadIdx.x == 0) pl[0] = 0.0;
-    for (int r = 0; r + 1 < nrep; ++r) {
-        ordered_sum<1>(part + static_cast<int64_t>(r) * nblk, nblk, &seg);
-        __syncthreads();
-        if (threadIdx.x == 0) pl[r + 1] = pl[r] + sqrt(seg);
-        __syncthreads();
-    }
-}
-
-// partial sums of a.b per image
-__global__ void __launch_bounds__(256) k_gneb_dot(const double* __restrict__ a, const double* __restrict__ b, int64_t n,
-                                                  int64_t Ntot, double* part) {
-    const int r = blockIdx.y;
-    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double v[1] = {0.0};
-    if (li < n) {
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        v[0] = dot(ld3(a, i, Ntot), ld3(b, i, Ntot));
-    }
-    block_partials<1>(v, part + static_cast<int64_t>(r) * gridDim.x, gridDim.x, blockIdx.x);
-}
-
-// per image: the ordered sum of its partials
-__global__ void __launch_bounds__(256) k_gneb_dot_img(const double* part, int nblk, double* out) {
-    ordered_sum<1>(part + static_cast<int64_t>(blockIdx.x) * nblk, nblk, out + blockIdx.x);
-}
-
-// maxloc of the image energies: the first image of highest energy (the climbing
-// image, gneb_utils.f90:84,159)
-__device__ __forceinline__ int gneb_maxloc(const double* E, int nrep) {
-    int c = 0;
-    for (int q = 1; q < nrep; ++q)
-        if (E[q] > E[c]) c = q;
-    return c;
-}
-
-// interior: F = F - tau (F.tau) + k (l_{r+1} + l_{r-1} - 2 l_r) tau, at the
-// climbing image (climb != 0) F - 2 tau (F.tau); end images: 0, or left as they
-// are (keep_ends, the forces before the first move)
-__global__ void __launch_bounds__(256) k_gneb_force(double* F, const double* __restrict__ tau, const double* __restrict__ fp,
-                                                    const double* __restrict__ pl, const double* __restrict__ E,
-                                                    int64_t n, int64_t Ntot, int nrep, double spring, int keep_ends,
-                                                    int climb) {
-    const int r = blockIdx.y;
-    const int64_t li = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (li >= n) return;
-    const int64_t i = static_cast<int64_t>(r) * n + li;
-    if (r == 0 || r == nrep - 1) {
-        if (!keep_ends) st3(F, i, Ntot, make_double3(0.0, 0.0, 0.0));
-        return;
-    }
-    const double3 f = ld3(F, i, Ntot), t = ld3(tau, i, Ntot);
-    if (climb && gneb_maxloc(E, nrep) == r) {
-        const double a2 = 2.0 * fp[r];
-        st3(F, i, Ntot, make_double3(f.x - t.x * a2, f.y - t.y * a2, f.z - t.z * a2));
-        return;
-    }
-    const double a = fp[r], k = spring * (pl[r + 1] + pl[r - 1] - 2.0 * pl[r]);
-    st3(F, i, Ntot, make_double3(f.x - t.x * a + k * t.x, f.y - t.y * a + k * t.y, f.z - t.z * a + k * t.z));
-}
-
-// one partial max |F| per block (the forces before the first move)
-__global__ void __launch_bounds__(256) k_gneb_absmax(const double* __restrict__ F, int64_t n3, double* pmax) {
-    const int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double fm = k < n3 ? fabs(F[k]) : 0.0;
-    __shared__ double wmax[8];
-    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mx = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
-        pmax[blockIdx.x] = mx;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_gneb_maxof(const double* __restrict__ pmax, int nb, double* out) {
-    double fm = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) fm = fmax(fm, pmax[b]);
-    __shared__ double wmax[8];
-    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mx = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
-        *out = mx;
-    }
-}
-
-// Iteration state on the device: done set by the iteration that stopped (max |F|
-// < ftol or itrmax reached; the iterations after it in a graph do no work but
-// the field pass); the iterations taken.
-struct GnebCtl {
-    int done;
-    int pad;
-    long long iters;
-};
-
-// The energy-weighted tangent of image r at site i (unnormalised, projected on
-// the spin: lattice_special, GNEB/tangent.f90:93-124); m0, mp its spin and the
-// next image's.
-__device__ __forceinline__ double3 gneb_tangent_site(const double* __restrict__ m, int64_t i, int64_t n, int64_t Ntot,
-                                                     int r, int nrep, double wp, double wm, double3& m0, double3& mp) {
-    m0 = ld3(m, i, Ntot);
-    mp = r + 1 < nrep ? ld3(m, i + n, Ntot) : m0;
-    const double3 mm = r > 0 ? ld3(m, i - n, Ntot) : m0;
-    double3 t = make_double3(wp * (mp.x - m0.x) + wm * (m0.x - mm.x), wp * (mp.y - m0.y) + wm * (m0.y - mm.y),
-                             wp * (mp.z - m0.z) + wm * (m0.z - mm.z));
-    const double d = dot(t, m0);
-    return make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
-}
+// GNEB on the replicas taken as the images of one path (all of one size n, image
+// r at sites [r n, (r + 1) n) of every component block): the kernels and the
+// relaxation driver are in mj_gneb.cuh; the batch adds the fused GNEB field
+// pass (BPASS_GNEB, the path sums per tile) and k_gneb_img.
 
 // Per image r (one block each): the energy and the six path sums of the GNEB
 // field pass, each summed over the image's tiles in tile order as
@@ -657,141 +414,6 @@ __global__ void __launch_bounds__(256) k_gneb_img(const BatchRep* reps, int nrep
         if (q == 0) E[r] = tot;
         else img[(q - 1) * nrep + r] = tot;
     }
-}
-
-// Interior images: tau = wp A + wm B (the energy-weighted tangent at the site,
-// the weights of the image energies) over |tau| from the image's path sums, F =
-// F - tau (F.tau) + k (seg_r - seg_{r-1}) tau, stored; the old velocity lam Fo
-// (the projection of the previous iteration, lam = scal[3]) and the old force Fo
-// carried along the rotation R that took the spin from mo to m, v = lam R Fo +
-// (R Fo + F) dt / (2 mass).  End images: F = v = 0.  The last block sums v.F
-// and F.F in block order, takes max |F|, sets lam = v.F / F.F (0 when v.F < 0;
-// the velocity projection, v = lam F), counts the iteration and sets the stop
-// flag.  r = blockIdx.x: the images of one site range run side by side, so the
-// neighbouring images' spins come from L2.
-template <int SPT>
-__global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ mo,
-                                                   const double* __restrict__ Fo, double* Fn,
-                                                   const double* __restrict__ E, const double* __restrict__ img,
-                                                   int64_t n, int64_t Ntot, int nrep,
-                                                   double spring, double dt, double mass, double ftol, long long itrmax,
-                                                   int climb, double* part, double* pmax, unsigned int* cnt,
-                                                   GnebCtl* ctl, double* scal) {
-    if (ctl->done) return;
-    const int r = blockIdx.x;
-    const int nb = gridDim.x * gridDim.y, bid = blockIdx.x + gridDim.x * blockIdx.y;
-    const bool inner = r > 0 && r < nrep - 1;
-    double wp = 0.0, wm = 0.0, inv = 0.0, a = 0.0, k = 0.0;
-    if (inner) {
-        gneb_weights(E, r, nrep, 0, wp, wm);
-        const double t2 = wp * wp * img[r] + 2.0 * wp * wm * img[nrep + r] + wm * wm * img[2 * nrep + r];
-        inv = t2 > 0.0 ? 1.0 / sqrt(t2) : 0.0;
-        a = (wp * img[3 * nrep + r] + wm * img[4 * nrep + r]) * inv;
-        k = spring * (sqrt(img[5 * nrep + r]) - sqrt(img[5 * nrep + r - 1]));
-        if (climb) {
-            __shared__ int ci_s;
-            if (threadIdx.x == 0) ci_s = gneb_maxloc(E, nrep);
-            __syncthreads();
-            if (ci_s == r) {
-                // the climbing image: F - 2 tau (F.tau), no spring
-                a *= 2.0;
-                k = 0.0;
-            }
-        }
-    }
-    const double h = 0.5 / mass * dt, lam = scal[3];
-    double v2[2] = {0.0, 0.0}, fm = 0.0;
-#pragma unroll
-    for (int q = 0; q < SPT; ++q) {
-        const int64_t li = (static_cast<int64_t>(blockIdx.y) * SPT + q) * blockDim.x + threadIdx.x;
-        if (li >= n) break;
-        const int64_t i = static_cast<int64_t>(r) * n + li;
-        double3 f = make_double3(0.0, 0.0, 0.0), v = f;
-        if (inner) {
-            double3 m0, mp;
-            const double3 t0 = gneb_tangent_site(m, i, n, Ntot, r, nrep, wp, wm, m0, mp);
-            const double3 t = make_double3(t0.x * inv, t0.y * inv, t0.z * inv);
-            const double3 g = ld3(Fn, i, Ntot);
-            f = make_double3(g.x - t.x * a + k * t.x, g.y - t.y * a + k * t.y, g.z - t.z * a + k * t.z);
-            // the move's rotation: axis mo x Fo/|Fo| (rotation_axis_arr), angle
-            // between mo and m (sin |m x mo|, cos m.mo)
-            const double3 m1 = ld3(mo, i, Ntot), fo = ld3(Fo, i, Ntot);
-            double3 fn = fo;
-            const double nf = sqrt(dot(fo, fo));
-            if (nf > 1e-30) fn = make_double3(fo.x / nf, fo.y / nf, fo.z / nf);
-            double3 e = cross(m1, fn);
-            const double ne = sqrt(dot(e, e));
-            if (ne > 2.220446049250313e-16) e = make_double3(e.x / ne, e.y / ne, e.z / ne);
-            const double3 c = cross(m0, m1);
-            const double3 fr = gneb_rotate(fo, e, sqrt(dot(c, c)), dot(m0, m1));
-            v = make_double3(lam * fr.x + (fr.x + f.x) * h, lam * fr.y + (fr.y + f.y) * h,
-                             lam * fr.z + (fr.z + f.z) * h);
-        }
-        st3(Fn, i, Ntot, f);
-        v2[0] += dot(v, f);
-        v2[1] += dot(f, f);
-        fm = fmax(fm, fmax(fabs(f.x), fmax(fabs(f.y), fabs(f.z))));
-    }
-    block_partials<2>(v2, part, nb, bid);
-    __shared__ double wmax[8];
-    __shared__ bool last;
-    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mx = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
-        pmax[bid] = mx;
-        __threadfence();
-        last = atomicAdd(cnt, 1u) == static_cast<unsigned int>(nb - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    __shared__ double sums[2];
-    ordered_sum<2>(part, nb, sums);
-    fm = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) fm = fmax(fm, __ldcg(pmax + b));
-    for (int o = 16; o > 0; o >>= 1) fm = fmax(fm, __shfl_down_sync(0xffffffffu, fm, o));
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = fm;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mx = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x) / 32; ++w) mx = fmax(mx, wmax[w]);
-        const double fv = sums[0] / nrep, fd = sums[1] / nrep;
-        scal[0] = fv;
-        scal[1] = fd;
-        scal[2] = mx;
-        scal[3] = fv < 0.0 ? 0.0 : fv / fd;
-        const long long it = ctl->iters + 1;
-        ctl->iters = it;
-        if (mx < ftol || it >= itrmax) ctl->done = 1;
-        *cnt = 0u;
-    }
-}
-
-// Unless stopped: the spins of the next iteration into mn, the interior images
-// moved with v = lam F (lam = scal[3]) and F the force of the iteration, r = m +
-// F (lam dt + dt^2 / (2 mass)) normalised; the end images copied.
-__global__ void __launch_bounds__(256) k_gneb_move(const double* __restrict__ m, double* __restrict__ mn,
-                                                   const double* __restrict__ F, const double* __restrict__ scal,
-                                                   const GnebCtl* ctl, int64_t n, int64_t Ntot, double dt,
-                                                   double mass) {
-    if (ctl->done) return;
-    const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    if (i >= Ntot) return;
-    const double3 m0 = ld3(m, i, Ntot);
-    if (i < n || i >= Ntot - n) {
-        st3(mn, i, Ntot, m0);
-        return;
-    }
-    const double3 f = ld3(F, i, Ntot);
-    const double c = scal[3] * dt + 0.5 / mass * dt * dt;
-    double3 r = make_double3(m0.x + f.x * c, m0.y + f.y * c, m0.z + f.z * c);
-    const double nr = sqrt(dot(r, r));
-    if (nr > 1e-30) r = make_double3(r.x / nr, r.y / nr, r.z / nr);
-    st3(mn, i, Ntot, r);
 }
 
 template <class S, int BYT, int RY>
@@ -1039,6 +661,41 @@ mj_status batch_sequence(mj_batch* b, const DynCoef& c0, double dt, uint32_t ste
     if (E_out) return batch_energy(b, c, E_out, s);
     return MJ_OK;
 }
+
+// The field of the images for gneb_relax: the batch's field pass with the
+// projection (BPASS_FIELD) and k_batch_energy; per iteration the GNEB field pass
+// (projected fields and the path sums per tile) and k_gneb_img.
+struct BatchFields {
+    mj_batch* b;
+    cudaStream_t s;
+    double* tile_g;  // 6 path sums per tile
+    DynCoef c;       // unused by the field passes (no dynamics)
+
+    mj_status field(double* F, double* m, double* E) {
+        BatchArgs A = batch_args(b, 0, 0.0);
+        A.ms = A.mn = m;
+        A.out = F;
+        A.project = 1;
+        A.tile_e = b->d_tile_e;
+        mj_status e = batch_pass(b->shape, b->variant, BPASS_FIELD, b->sp, c, A, batch_blocks(b), s);
+        if (e != MJ_OK) return e;
+        k_batch_energy<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, E);
+        return cuda_status(cudaGetLastError(), "k_batch_energy");
+    }
+    mj_status iterate(double* F, double* m, double* E, double* img, const GnebCtl* ctl) {
+        BatchArgs A = batch_args(b, 0, 0.0);
+        A.ms = A.mn = m;
+        A.out = F;
+        A.tile_e = b->d_tile_e;
+        A.tile_g = tile_g;
+        A.gneb_n = b->Ntot / b->nrep;
+        A.gneb_nimg = b->nrep;
+        mj_status e = batch_pass(b->shape, b->variant, BPASS_GNEB, b->sp, c, A, batch_blocks(b), s);
+        if (e != MJ_OK) return e;
+        k_gneb_img<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, tile_g, b->ntile, E, img, ctl);
+        return cuda_status(cudaGetLastError(), "k_gneb_img");
+    }
+};
 
 }  // namespace
 }  // namespace mj
@@ -1319,10 +976,11 @@ mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, 
         (st = cuda_status(cudaMalloc(&b->d_gneb_part, sizeof(double) * nblk * b->nrep), "tangent partials")) != MJ_OK)
         return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_gneb_tau<<<dim3(nblk, b->nrep), 256, 0, s>>>(b->d_m, n, b->Ntot, b->nrep, E_dev, mode, tau_dev, b->d_gneb_part);
+    const GnebIdx X{n, n, b->Ntot};
+    k_gneb_tau<<<dim3(nblk, b->nrep), 256, 0, s>>>(b->d_m, X, b->nrep, E_dev, mode, tau_dev, b->d_gneb_part);
     if ((st = cuda_status(cudaGetLastError(), "k_gneb_tau")) != MJ_OK) return st;
     k_gneb_norm_sum<<<b->nrep, 256, 0, s>>>(b->d_gneb_part, nblk);
-    k_gneb_scale<<<dim3(nblk, b->nrep), 256, 0, s>>>(tau_dev, n, b->Ntot, b->d_gneb_part, nblk);
+    k_gneb_scale<<<dim3(nblk, b->nrep), 256, 0, s>>>(tau_dev, X, b->d_gneb_part, nblk);
     return cuda_status(cudaGetLastError(), "k_gneb_scale");
 }
 
@@ -1525,251 +1183,27 @@ mj_status mj_batch_mc_state(mj_batch* b, double* cone, int64_t* accepted, int64_
 
 mj_status mj_batch_gneb_path(mj_batch* b, const mj_gneb_params* p, double* rx, double* ene, double* dene,
                              int64_t* iterations, double* max_force, int32_t* climbing) {
-    if (!b || !p || !rx || !ene || !dene || b->nrep < 3 || !(p->dt > 0.0) || !(p->mass > 0.0) || p->itrmax < 0 ||
-        (p->en_zero != 'I' && p->en_zero != 'F' && p->en_zero != 'N'))
-        return set_error(MJ_ERR_ARG, "bad GNEB arguments (3 or more images, dt > 0, mass > 0, en_zero I/F/N)");
+    if (!b) return set_error(MJ_ERR_ARG, "bad GNEB arguments (no batch)");
+    mj_status st = gneb_check(p, b->nrep, rx, ene, dene);
+    if (st != MJ_OK) return st;
     for (int r = 1; r < b->nrep; ++r)
         if (b->reps[r].Lx != b->reps[0].Lx || b->reps[r].Ly != b->reps[0].Ly)
             return set_error(MJ_ERR_UNSUPPORTED, "a path needs images of one size");
-    const double spring = p->spring, dt = p->dt, mass = p->mass, ftol = p->ftol;
-    const int64_t itrmax = p->itrmax;
-    const int32_t en_zero = p->en_zero;
-    const int climb = p->climb ? 1 : 0;
     cudaSetDevice(b->device);
     const int nrep = b->nrep;
     const int64_t Ntot = b->Ntot, n = Ntot / nrep;
-    const int nblk = static_cast<int>((n + 255) / 256);
-    const int nbv = nblk * nrep;
-    const int n3b = static_cast<int>((3 * Ntot + 255) / 256);
-    const int nsite_b = static_cast<int>((Ntot + 255) / 256);
-    mj_status st;
-    if (!b->d_gneb_part &&
-        (st = cuda_status(cudaMalloc(&b->d_gneb_part, sizeof(double) * nblk * nrep), "tangent partials")) != MJ_OK)
-        return st;
     if (!b->cap_stream &&
         (st = cuda_status(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "capture stream")) != MJ_OK)
         return st;
-    // F1 / F2 the forces and b->d_m / mB the spins of alternate iterations, tau
-    // the tangents of the forces before the first move and of the outputs (SoA,
-    // 3 Ntot each); E / pl / fp per image, img the iteration's six path sums per
-    // image, tile_g their tile partials, scal (v.F, F.F, max |F|, lam);
-    // part / part2 block partials; cnt the last-block counters; ctl the stop flag
-    GnebBufs g;
-    std::memset(&g, 0, sizeof(g));
-    double* img = nullptr;
-    unsigned int* cnt = nullptr;
-    GnebCtl* ctl = nullptr;
-    double** bufs[] = {&g.F1, &g.F2, &g.mB, &g.tau};
-    st = MJ_OK;
-    for (double** q : bufs)
-        if (st == MJ_OK) st = cuda_status(cudaMalloc(q, sizeof(double) * 3 * Ntot), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.E, sizeof(double) * (9 * nrep + 4)), "GNEB buffers");
-    double* tile_g = nullptr;
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&tile_g, sizeof(double) * 6 * b->ntile), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part, sizeof(double) * 3 * nbv), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&g.part2, sizeof(double) * std::max(3 * nbv, n3b)), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * (nrep + 1)), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&ctl, sizeof(GnebCtl)), "GNEB buffers");
-    GnebCtl* hctl = nullptr;
-    if (st == MJ_OK) st = cuda_status(cudaMallocHost(&hctl, 2 * sizeof(GnebCtl)), "GNEB buffers");
-    cudaEvent_t ev[2] = {nullptr, nullptr};
-    for (int q = 0; q < 2 && st == MJ_OK; ++q)
-        st = cuda_status(cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming), "GNEB events");
-    cudaGraphExec_t exec = nullptr;
-    auto release = [&]() {
-        if (exec) cudaGraphExecDestroy(exec);
-        for (cudaEvent_t e : ev)
-            if (e) cudaEventDestroy(e);
-        cudaFreeHost(hctl);
-        cudaFree(g.F1);
-        cudaFree(g.F2);
-        cudaFree(g.mB);
-        cudaFree(g.tau);
-        cudaFree(g.E);
-        cudaFree(tile_g);
-        cudaFree(g.part);
-        cudaFree(g.part2);
-        cudaFree(cnt);
-        cudaFree(ctl);
-    };
-    if (st != MJ_OK) {
-        release();
-        return st;
-    }
-    g.pl = g.E + nrep;
-    g.fp = g.E + 2 * nrep;
-    img = g.E + 3 * nrep;
-    g.scal = g.E + 9 * nrep;
+    BatchFields fl{b, b->cap_stream, nullptr, DynCoef{}};
+    std::memset(&fl.c, 0, sizeof(fl.c));
+    if ((st = cuda_status(cudaMalloc(&fl.tile_g, sizeof(double) * 6 * b->ntile), "GNEB buffers")) != MJ_OK) return st;
     // the path as the work queued on the legacy default stream (an upload) leaves it
-    cudaStream_t s = b->cap_stream;
-    if ((st = cuda_status(cudaStreamSynchronize(0), "GNEB start")) != MJ_OK) {
-        release();
-        return st;
-    }
-    GnebCtl c0;
-    std::memset(&c0, 0, sizeof(c0));
-    cudaMemsetAsync(g.scal, 0, sizeof(double) * 4, s);
-    cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * (nrep + 1), s);
-    cudaMemcpyAsync(ctl, &c0, sizeof(c0), cudaMemcpyHostToDevice, s);
-    DynCoef c;
-    std::memset(&c, 0, sizeof(c));
-    const dim3 gi(nblk, nrep), gs(nblk, nrep - 1);
-    // the field pass of the spins m: projected fields into F, tile energies,
-    // image energies E
-    auto field = [&](double* F, double* m) -> mj_status {
-        BatchArgs A = batch_args(b, 0, 0.0);
-        A.ms = A.mn = m;
-        A.out = F;
-        A.project = 1;
-        A.tile_e = b->d_tile_e;
-        mj_status e = batch_pass(b->shape, b->variant, BPASS_FIELD, b->sp, c, A, batch_blocks(b), s);
-        if (e != MJ_OK) return e;
-        k_batch_energy<<<nrep, 256, 0, s>>>(b->d_reps, nrep, b->d_tile_e, g.E);
-        return cuda_status(cudaGetLastError(), "k_batch_energy");
-    };
-    // field pass, path length pl, tangents of the given mode, fp = F.tau per image
-    auto forces = [&](double* F, int mode) -> mj_status {
-        mj_status e = field(F, b->d_m);
-        if (e != MJ_OK) return e;
-        k_gneb_seg<<<gs, 256, 0, s>>>(b->d_m, n, Ntot, g.part);
-        k_gneb_pathlen<<<1, 256, 0, s>>>(g.part, nblk, nrep, g.pl);
-        k_gneb_tau<<<gi, 256, 0, s>>>(b->d_m, n, Ntot, nrep, g.E, mode, g.tau, b->d_gneb_part);
-        k_gneb_norm_sum<<<nrep, 256, 0, s>>>(b->d_gneb_part, nblk);
-        k_gneb_scale<<<gi, 256, 0, s>>>(g.tau, n, Ntot, b->d_gneb_part, nblk);
-        k_gneb_dot<<<gi, 256, 0, s>>>(F, g.tau, n, Ntot, g.part);
-        k_gneb_dot_img<<<nrep, 256, 0, s>>>(g.part, nblk, g.fp);
-        return cuda_status(cudaGetLastError(), "GNEB forces");
-    };
-    // initial forces: every image's projected field, the GNEB force of the interior
-    // ones; max |F| over them all (the convergence check before any move)
-    if ((st = forces(g.F1, 0)) != MJ_OK) {
-        release();
-        return st;
-    }
-    k_gneb_force<<<gi, 256, 0, s>>>(g.F1, g.tau, g.fp, g.pl, g.E, n, Ntot, nrep, spring, 1, climb);
-    k_gneb_absmax<<<n3b, 256, 0, s>>>(g.F1, 3 * Ntot, g.part2);
-    k_gneb_maxof<<<1, 256, 0, s>>>(g.part2, n3b, g.scal + 2);
-    double h0[4];
-    cudaMemcpyAsync(h0, g.E, sizeof(double), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(h0 + 1, g.E + nrep - 1, sizeof(double), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(h0 + 2, g.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
-    if ((st = cuda_status(cudaStreamSynchronize(s), "GNEB initial forces")) != MJ_OK) {
-        release();
-        return st;
-    }
-    const double E_first = h0[0], E_last = h0[1];
-    double fchk = h0[2];
-    int64_t done = 0;
-    if (itrmax > 0) {
-        // the first move (lam = 0: the velocity starts at zero) into mB, then
-        // chunks of iterations replayed as one graph: GNEB field pass,
-        // k_gneb_img, k_gneb_step, k_gneb_move.  Forces and spins alternate
-        // between their two buffers (an even chunk starts each replay on F1 and
-        // mB).  Two chunks are in flight: the stop flag of one is read while the
-        // next runs; the iterations after the stop do no work but the field pass.
-        const int chunk = 32;
-        // four sites per thread once that still gives two blocks per SM: the loads
-        // of four sites in flight before each block's reduction
-        const bool spt4 = Ntot >= 2LL * 1024 * b->num_sms;
-        const dim3 gt(nrep, static_cast<unsigned>(spt4 ? (n + 1023) / 1024 : nblk));
-        const int nmove = static_cast<int>((Ntot + 255) / 256);
-        k_gneb_move<<<nmove, 256, 0, s>>>(b->d_m, g.mB, g.F1, g.scal, ctl, n, Ntot, dt, mass);
-        st = cuda_status(cudaGetLastError(), "k_gneb_move");
-        if (st == MJ_OK) st = cuda_status(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-        if (st == MJ_OK) {
-            mj_status inner = MJ_OK;
-            for (int k = 0; k < chunk && inner == MJ_OK; ++k) {
-                double* Fo = (k & 1) ? g.F2 : g.F1;
-                double* Fn = (k & 1) ? g.F1 : g.F2;
-                double* mc = (k & 1) ? b->d_m : g.mB;
-                double* mo = (k & 1) ? g.mB : b->d_m;
-                BatchArgs A = batch_args(b, 0, 0.0);
-                A.ms = A.mn = mc;
-                A.out = Fn;
-                A.tile_e = b->d_tile_e;
-                A.tile_g = tile_g;
-                A.gneb_n = n;
-                A.gneb_nimg = nrep;
-                inner = batch_pass(b->shape, b->variant, BPASS_GNEB, b->sp, c, A, batch_blocks(b), s);
-                if (inner != MJ_OK) break;
-                k_gneb_img<<<nrep, 256, 0, s>>>(b->d_reps, nrep, b->d_tile_e, tile_g, b->ntile, g.E, img, ctl);
-                const long long im = static_cast<long long>(itrmax);
-                if (spt4)
-                    k_gneb_step<4><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
-                                                      im, climb, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
-                else
-                    k_gneb_step<1><<<gt, 256, 0, s>>>(mc, mo, Fo, Fn, g.E, img, n, Ntot, nrep, spring, dt, mass, ftol,
-                                                      im, climb, g.part2, g.part2 + 2 * nbv, cnt + nrep, ctl, g.scal);
-                k_gneb_move<<<nmove, 256, 0, s>>>(mc, mo, Fn, g.scal, ctl, n, Ntot, dt, mass);
-                inner = cuda_status(cudaGetLastError(), "GNEB iteration");
-            }
-            cudaGraph_t graph = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(s, &graph);
-            if (inner != MJ_OK) st = inner;
-            else if ((st = cuda_status(e, "end capture")) == MJ_OK)
-                st = cuda_status(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
-            if (graph) cudaGraphDestroy(graph);
-        }
-        // chunk q: replay, its flag into hctl[q & 1], event ev[q & 1]
-        auto launch = [&](int64_t q) -> mj_status {
-            mj_status e = cuda_status(cudaGraphLaunch(exec, s), "GNEB graph launch");
-            if (e != MJ_OK) return e;
-            cudaMemcpyAsync(hctl + (q & 1), ctl, sizeof(GnebCtl), cudaMemcpyDeviceToHost, s);
-            return cuda_status(cudaEventRecord(ev[q & 1], s), "GNEB event");
-        };
-        if (st == MJ_OK) st = launch(0);
-        if (st == MJ_OK) st = launch(1);
-        for (int64_t q = 0; st == MJ_OK; ++q) {
-            if ((st = cuda_status(cudaEventSynchronize(ev[q & 1]), "GNEB iterations")) != MJ_OK) break;
-            const GnebCtl hc = hctl[q & 1];
-            done = hc.iters;
-            if (hc.done) break;
-            if (hc.iters != (q + 1) * chunk) {
-                st = set_error(MJ_ERR_CUDA, "GNEB iterations did not advance");
-                break;
-            }
-            st = launch(q + 2);
-        }
-        // the chunk still in flight (or, after an error, all queued work) ends first
-        const mj_status fin = cuda_status(cudaStreamSynchronize(s), "GNEB iterations");
-        if (st == MJ_OK) st = fin;
-        // the relaxed path is in mB after an odd number of iterations
-        if (st == MJ_OK && (done & 1))
-            cudaMemcpyAsync(b->d_m, g.mB, sizeof(double) * 3 * Ntot, cudaMemcpyDeviceToDevice, s);
-        if (st == MJ_OK) {
-            cudaMemcpyAsync(&fchk, g.scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
-            st = cuda_status(cudaStreamSynchronize(s), "GNEB force");
-        }
-    }
-    // outputs (en_path.out): path length, energy above the reference image, and the
-    // derivative along the path -F.tau of the final images' projected fields along
-    // the simple tangent (lattice_single); the end images' forces are zero after a
-    // move, their projected fields before any
-    std::vector<double> h(3 * nrep);
-    if (st == MJ_OK) st = forces(g.F2, 1);
-    if (st == MJ_OK) {
-        cudaMemcpyAsync(h.data(), g.E, sizeof(double) * 3 * nrep, cudaMemcpyDeviceToHost, s);
-        st = cuda_status(cudaStreamSynchronize(s), "GNEB outputs");
-    }
-    if (st == MJ_OK) {
-        const double eref = en_zero == 'I' ? E_first : (en_zero == 'F' ? E_last : 0.0);
-        for (int r = 0; r < nrep; ++r) {
-            rx[r] = h[nrep + r];
-            ene[r] = (r == 0 ? E_first : (r == nrep - 1 ? E_last : h[r])) - eref;
-            dene[r] = (r == 0 || r == nrep - 1) && done > 0 ? 0.0 : -h[2 * nrep + r];
-        }
-        if (iterations) *iterations = done;
-        if (max_force) *max_force = fchk;
-        // the climbing image of the last iteration (the image energies it saw)
-        if (climbing) {
-            auto en = [&](int r) { return r == 0 ? E_first : (r == nrep - 1 ? E_last : h[r]); };
-            int c = 0;
-            for (int r = 1; r < nrep; ++r)
-                if (en(r) > en(c)) c = r;
-            *climbing = climb ? c : -1;
-        }
-    }
-    release();
+    st = cuda_status(cudaStreamSynchronize(0), "GNEB start");
+    if (st == MJ_OK)
+        st = gneb_relax(fl, b->d_m, nrep, GnebIdx{n, n, Ntot}, b->num_sms, b->cap_stream, p, 32, rx, ene, dene,
+                        iterations, max_force, climbing);
+    cudaFree(fl.tile_g);
     return st;
 }
 

@@ -3,8 +3,9 @@
 ``GNEBInput`` carries the reference's GNEB input (IO-input/GNEB_io.f90, same
 names and defaults).  ``geodesic_path`` builds the initial path
 (GNEB/path.f90:100-174), ``find_path`` relaxes it on the device
-(GNEB/gneb_utils.f90:19-240 find_path, velocity projection on the images held
-as the replicas of a ReplicaBatch: mj_batch_gneb_path; with the climbing image
+(GNEB/gneb_utils.f90:19-240 find_path, velocity projection; the images held
+as the replicas of a ReplicaBatch, mj_batch_gneb_path, or, for lattices and
+terms a batch does not hold, on a plan, mj_gneb_path; with the climbing image
 for do_gneb_ci), ``hermite_fit``, ``find_sp`` and ``spline_hermite_val``
 interpolate the energy along the path and locate the saddle point
 (extrapolation/spline.f90, gneb_utils.f90:242-291), ``saddle_configuration``
@@ -183,21 +184,92 @@ def find_sp(rx, c) -> Tuple[int, float]:
     raise ValueError("energy maximum has not been found")
 
 
-def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: int = 0,
-              climb: bool = False) -> GNEBResult:
-    """Relax the path images (nim, N, 3) of the single-atom 2D lattice of deck
-    (its L, boundaries, couplings and field) on the device: GNEB find_path with
-    the end images fixed, tolerance mep_ftol (mep_ftol_ci with climb)."""
+class PlanPath:
+    """A path of nim images held on the device for one plan (a Hamiltonian):
+    image r the SoA block (3, N) of a (nim, 3, N) tensor.  The images' fields
+    and energies are the plan's own, so any lattice of one magnetic atom per
+    cell and any term a plan holds (the FFT dipolar term, 3D films, ELL
+    couplings) reaches the GNEB: mj_gneb_path.  The same calls as a ReplicaBatch holding a path."""
+
+    def __init__(self, ham, images: np.ndarray):
+        import torch
+
+        img = np.ascontiguousarray(images, np.float64)
+        if img.ndim != 3 or img.shape[2] != 3 or img.shape[0] < 3 or img.shape[1] != ham.N:
+            raise ValueError("images are (nim >= 3, plan sites, 3)")
+        self.ham = ham
+        self.nrep = img.shape[0]
+        self.m = torch.tensor(img.transpose(0, 2, 1).copy(), device=f"cuda:{ham.device}")
+
+    def gneb_path(self, spring: float = 0.5, dt: float = 1.0e-2, mass: float = 1.0, ftol: float = 1.0e-3,
+                  itrmax: int = 2 ** 62, en_zero: str = "N", climb: bool = False):
+        """As ReplicaBatch.gneb_path: (rx, ene, dene, iterations, max |F|,
+        climbing image or -1); the path is left relaxed."""
+        import ctypes as C
+
+        import torch
+
+        from . import _abi
+        from ._abi import check, lib, ptr
+
+        if en_zero not in ("I", "F", "N"):
+            raise ValueError("en_zero is 'I', 'F' or 'N'")
+        p = _abi.GnebParams(float(spring), float(dt), float(mass), float(ftol), int(itrmax), ord(en_zero),
+                            int(bool(climb)))
+        rx, ene, dene = np.zeros(self.nrep), np.zeros(self.nrep), np.zeros(self.nrep)
+        it, fc, ci = C.c_int64(), C.c_double(), C.c_int32()
+        stream = torch.cuda.current_stream(self.m.device).cuda_stream
+        check(lib.mj_gneb_path(self.ham.plan, ptr(self.m), self.nrep, C.byref(p), ptr(rx), ptr(ene), ptr(dene),
+                               C.byref(it), C.byref(fc), C.byref(ci), stream))
+        return rx, ene, dene, int(it.value), float(fc.value), int(ci.value)
+
+    def download(self) -> np.ndarray:
+        """The images as (nim * N, 3)."""
+        return self.m.cpu().numpy().transpose(0, 2, 1).reshape(-1, 3)
+
+
+def path_holder(deck, images: np.ndarray, device: int = 0, ham=None):
+    """The device holder of a path of deck: the replicas of a ReplicaBatch (the
+    fused GNEB field pass) for a single-atom 2D square or triangular lattice
+    without the dipolar term, else a PlanPath on the deck's plan (ham, when
+    given, is that plan)."""
+    from . import Hamiltonian
+    from ._abi import MJ_ERR_UNSUPPORTED, MatjesError
     from .batch import ReplicaBatch
 
     img = np.ascontiguousarray(images, np.float64)
     nim, N = img.shape[0], img.shape[1]
-    if img.ndim != 3 or img.shape[2] != 3 or nim < 3 or N != deck.ncell:
+    if deck.nmag == 1 and not deck.dip and deck.L[2] == 1:
+        try:
+            batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)),
+                                 [0.0] * nim, device=device)
+        except MatjesError as e:
+            if e.status != MJ_ERR_UNSUPPORTED:
+                raise
+        else:
+            batch.upload(img.reshape(nim * N, 3))
+            return batch
+    return PlanPath(ham if ham is not None else Hamiltonian(deck, device=device), img)
+
+
+def find_path(deck, images: np.ndarray, inp: GNEBInput = GNEBInput(), device: int = 0,
+              climb: bool = False) -> GNEBResult:
+    """Relax the path images (nim, N, 3) of deck (its lattice, boundaries,
+    couplings, field and dipolar term) on the device: GNEB find_path with the
+    end images fixed, tolerance mep_ftol (mep_ftol_ci with climb); the images
+    held as replicas or on the deck's plan (path_holder)."""
+    img = np.ascontiguousarray(images, np.float64)
+    nim, N = img.shape[0], img.shape[1]
+    if img.ndim != 3 or img.shape[2] != 3 or nim < 3 or N != deck.nsites:
         raise ValueError("images are (nim >= 3, deck sites, 3)")
-    batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)), [0.0] * nim,
-                         device=device)
-    batch.upload(img.reshape(nim * N, 3))
-    return _relax(batch, nim, N, inp, climb)
+    return _relax(path_holder(deck, img, device), nim, N, inp, climb)
+
+
+def find_path_plan(ham, images: np.ndarray, inp: GNEBInput = GNEBInput(), climb: bool = False) -> GNEBResult:
+    """find_path on the plan of a Hamiltonian (a deck's, or an ELL plan from
+    COO couplings): images (nim, ham.N, 3)."""
+    img = np.ascontiguousarray(images, np.float64)
+    return _relax(PlanPath(ham, img), img.shape[0], img.shape[1], inp, climb)
 
 
 def _relax(batch, nim: int, N: int, inp: GNEBInput, climb: bool, itrmax: Optional[int] = None) -> GNEBResult:
@@ -287,7 +359,7 @@ def saddle_point(rx, ene, dene, sample_num: int = 500):
 def gneb_run(deck, inp: GNEBInput, m_first: Optional[np.ndarray] = None, m_last: Optional[np.ndarray] = None,
              path: Optional[np.ndarray] = None, minimize_input=None, directory: Optional[str] = None,
              device: int = 0, seed: int = 0) -> dict:
-    """GNEB_run (GNEB/gneb.f90:33-120) of a single-atom 2D lattice.  Path
+    """GNEB_run (GNEB/gneb.f90:33-120) of any deck a plan holds.  Path
     initialisation (GNEB/initialize_path.f90): the given path (read_path), its
     end images replaced by m_first / m_last (read_outer), those minimised
     (min_type 1 minimize_infdamp, 2 minimize, with minimize_input: mass,
@@ -303,10 +375,9 @@ def gneb_run(deck, inp: GNEBInput, m_first: Optional[np.ndarray] = None, m_last:
     import torch
 
     from . import Hamiltonian
-    from .batch import ReplicaBatch
     from .hamiltonian import minimize
 
-    nim, N = inp.nim, deck.ncell
+    nim, N = inp.nim, deck.nsites
     if nim < 3:
         raise ValueError("GNEB needs nim >= 3")
     images = np.zeros((nim, N, 3))
@@ -341,9 +412,7 @@ def gneb_run(deck, inp: GNEBInput, m_first: Optional[np.ndarray] = None, m_last:
         images = geodesic_path(images[0], images[-1], nim, inp.amp_rnd_path, seed)
     if directory is not None:
         write_path(directory, images)
-    batch = ReplicaBatch(deck, [deck.L[:2]] * nim, np.tile(np.asarray(deck.B_ext, float), (nim, 1)), [0.0] * nim,
-                         device=device)
-    batch.upload(np.ascontiguousarray(images).reshape(nim * N, 3))
+    batch = path_holder(deck, images, device, ham if inp.min_type in (1, 2) else None)
     rx, ene, dene = np.zeros(nim), np.zeros(nim), np.zeros(nim)
     runs = []
     for climb, on in ((False, inp.do_gneb), (True, inp.do_gneb_ci)):
