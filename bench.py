@@ -560,8 +560,9 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
     neighbouring images' spins it also reads come from L2); GNEB force and
     transport m, m_old, F, F_old in (96), F out (24); move m, F in (48), m out
     (24): 240.
-    The CPU baseline is the oracle's find_path on one host core on the same
-    path for 20 iterations."""
+    The same path is then held on the deck's plan (mj_gneb_path, key
+    `on_plan`), timed the same way.  The CPU baseline is the oracle's find_path
+    on one host core on the same path for 20 iterations."""
     import time
 
     import numpy as np
