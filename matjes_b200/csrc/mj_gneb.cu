@@ -7,9 +7,11 @@
 // :154-157).  The path is nimg images of the plan's N spins in one device
 // array, image r the SoA block x[N] | y[N] | z[N] at 3 N r.
 //
-// Per image one field launch (launch_field: field and total energy); then
-// k_gneb_project (before the first move and for the outputs) or k_gneb_sums
-// (each iteration: projection and the six path sums per image).  The rest of
+// Per image one field launch (launch_field), the images side by side on forked
+// streams unless the dipolar term's FFT grid is shared; then k_gneb_sums
+// (projection, the six path sums and, for side-by-side images, the energy of
+// every image) or, for the dipolar term's one-by-one launches that reduce
+// their energies themselves, k_gneb_project outside the iterations.  The rest of
 // the relaxation is mj_gneb.cuh's, shared with the replica batch.
 #include <algorithm>
 #include <cstring>
@@ -20,25 +22,84 @@
 namespace mj {
 namespace {
 
+// The field of the images for gneb_relax.  Without the dipolar term the images'
+// field launches share no scratch (no total energy asked, per-site energies
+// into their own slices): they run side by side on kSide forked streams, and
+// k_gneb_sums sums each image's site energies with its path sums.  With the
+// dipolar term (one padded FFT grid per plan) they run one after another, each
+// reducing its own total energy.
 struct PlanFields {
+    static constexpr int kSide = 8;
     mj_plan* p;
     int nrep;
     GnebIdx X;
     cudaStream_t s;
-    double* part;       // path-sum partials: 6 per (image, block)
-    unsigned int* cnt;  // last-block counters, one per image
+    bool concurrent;
+    double* part = nullptr;       // partials: 7 per (image, block)
+    unsigned int* cnt = nullptr;  // last-block counters, one per image
+    double* esite = nullptr;      // per-site energies, image r at [r N, (r + 1) N) (concurrent form)
+    double* img0 = nullptr;       // path sums of the calls outside the iterations (unused)
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kSide] = {};
 
-    mj_status images(double* F, const double* m, double* E) {
-        for (int r = 0; r < nrep; ++r) {
-            const int64_t o = static_cast<int64_t>(r) * X.is;
-            mj_status e = launch_field(p, m + o, F + o, nullptr, E + r, s);
-            if (e != MJ_OK) return e;
+    mj_status setup(int64_t nblk) {
+        mj_status st = cuda_status(cudaMalloc(&part, sizeof(double) * 7 * nblk * nrep), "GNEB buffers");
+        if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * nrep), "GNEB buffers");
+        if (st == MJ_OK) st = cuda_status(cudaMalloc(&img0, sizeof(double) * 6 * nrep), "GNEB buffers");
+        if (st == MJ_OK) st = cuda_status(cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * nrep, s), "GNEB buffers");
+        if (st != MJ_OK || !concurrent) return st;
+        st = cuda_status(cudaMalloc(&esite, sizeof(double) * X.n * nrep), "GNEB buffers");
+        if (st == MJ_OK) st = cuda_status(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "GNEB events");
+        for (int k = 0; k < kSide && st == MJ_OK; ++k) {
+            st = cuda_status(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking), "GNEB streams");
+            if (st == MJ_OK) st = cuda_status(cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming), "GNEB events");
         }
-        return MJ_OK;
+        return st;
+    }
+    void release() {
+        for (int k = 0; k < kSide; ++k) {
+            if (side[k]) cudaStreamDestroy(side[k]);
+            if (join[k]) cudaEventDestroy(join[k]);
+        }
+        if (fork) cudaEventDestroy(fork);
+        for (double* b : {part, esite, img0}) cudaFree(b);
+        cudaFree(cnt);
+    }
+    mj_status images(double* F, const double* m, double* E) {
+        if (!concurrent) {
+            for (int r = 0; r < nrep; ++r) {
+                const int64_t o = static_cast<int64_t>(r) * X.is;
+                mj_status e = launch_field(p, m + o, F + o, nullptr, E + r, s);
+                if (e != MJ_OK) return e;
+            }
+            return MJ_OK;
+        }
+        const int nside = std::min(kSide, nrep);
+        mj_status e = cuda_status(cudaEventRecord(fork, s), "GNEB fork");
+        for (int k = 0; k < nside && e == MJ_OK; ++k) e = cuda_status(cudaStreamWaitEvent(side[k], fork, 0), "GNEB fork");
+        for (int r = 0; r < nrep && e == MJ_OK; ++r) {
+            const int64_t o = static_cast<int64_t>(r) * X.is;
+            e = launch_field(p, m + o, F + o, esite + r * X.n, nullptr, side[r % nside]);
+        }
+        // the forked streams join the main one even after a failed launch
+        for (int k = 0; k < nside; ++k) {
+            const mj_status j = cuda_status(cudaEventRecord(join[k], side[k]), "GNEB join");
+            const mj_status w = j == MJ_OK ? cuda_status(cudaStreamWaitEvent(s, join[k], 0), "GNEB join") : j;
+            if (e == MJ_OK) e = w;
+        }
+        return e;
+    }
+    mj_status sums(double* F, double* m, double* E, double* img, const GnebCtl* ctl) {
+        const int nblk = static_cast<int>((X.n + 255) / 256);
+        k_gneb_sums<<<dim3(nrep, nblk), 256, 0, s>>>(m, F, X, nrep, concurrent ? esite : nullptr, E, part, cnt, img,
+                                                     ctl);
+        return cuda_status(cudaGetLastError(), "k_gneb_sums");
     }
     mj_status field(double* F, double* m, double* E) {
         mj_status e = images(F, m, E);
         if (e != MJ_OK) return e;
+        if (concurrent) return sums(F, m, E, img0, nullptr);
         const int nblk = static_cast<int>((X.n + 255) / 256);
         k_gneb_project<<<dim3(nblk, nrep), 256, 0, s>>>(F, m, X);
         return cuda_status(cudaGetLastError(), "k_gneb_project");
@@ -46,9 +107,7 @@ struct PlanFields {
     mj_status iterate(double* F, double* m, double* E, double* img, const GnebCtl* ctl) {
         mj_status e = images(F, m, E);
         if (e != MJ_OK) return e;
-        const int nblk = static_cast<int>((X.n + 255) / 256);
-        k_gneb_sums<<<dim3(nrep, nblk), 256, 0, s>>>(m, F, X, nrep, part, cnt, img, ctl);
-        return cuda_status(cudaGetLastError(), "k_gneb_sums");
+        return sums(F, m, E, img, ctl);
     }
 };
 
@@ -83,10 +142,8 @@ mj_status mj_gneb_path(mj_plan* plan, double* m, int32_t nimg, const mj_gneb_par
     st = cuda_status(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "GNEB start");
     if (st == MJ_OK) st = cuda_status(cudaEventRecord(ready, static_cast<cudaStream_t>(stream)), "GNEB start");
     if (st == MJ_OK) st = cuda_status(cudaStreamWaitEvent(s, ready, 0), "GNEB start");
-    PlanFields fl{plan, nimg, GnebIdx{n, 3 * n, n}, s, nullptr, nullptr};
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&fl.part, sizeof(double) * 6 * nblk * nimg), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMalloc(&fl.cnt, sizeof(unsigned int) * nimg), "GNEB buffers");
-    if (st == MJ_OK) st = cuda_status(cudaMemsetAsync(fl.cnt, 0, sizeof(unsigned int) * nimg, s), "GNEB buffers");
+    PlanFields fl{plan, nimg, GnebIdx{n, 3 * n, n}, s, !plan->dip_on};
+    if (st == MJ_OK) st = fl.setup(nblk);
     // no per-kernel event records inside the captured iterations
     const bool prof = plan->prof_on;
     plan->prof_on = false;
@@ -95,8 +152,7 @@ mj_status mj_gneb_path(mj_plan* plan, double* m, int32_t nimg, const mj_gneb_par
     plan->prof_on = prof;
     const mj_status fin = cuda_status(cudaStreamSynchronize(s), "GNEB end");
     if (st == MJ_OK) st = fin;
-    cudaFree(fl.part);
-    cudaFree(fl.cnt);
+    fl.release();
     if (ready) cudaEventDestroy(ready);
     return st;
 }

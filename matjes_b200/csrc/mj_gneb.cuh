@@ -300,14 +300,17 @@ __device__ __forceinline__ void gneb_path_terms(double3 m0, double3 mp, double3 
 
 // Per image (r = blockIdx.x): F projected in place and the six path sums; the
 // last block of an image sums the partials in block order into img[q nrep + r].
-// For fields that come without them (a plan's field kernels).
+// With esite (per-site energies, image r at esite[r n, (r + 1) n)) also their
+// sum into E[r].  For fields that come without them (a plan's field kernels);
+// ctl may be null (always runs).
 __global__ void __launch_bounds__(256) k_gneb_sums(const double* __restrict__ m, double* F, GnebIdx X, int nrep,
-                                                   double* part, unsigned int* cnt, double* img, const GnebCtl* ctl) {
+                                                   const double* __restrict__ esite, double* E, double* part,
+                                                   unsigned int* cnt, double* img, const GnebCtl* ctl) {
     if (ctl && ctl->done) return;
     const int r = blockIdx.x;
     const int nblk = gridDim.y;
     const int64_t li = blockIdx.y * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    double g[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double g[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (li < X.n) {
         const int64_t i = r * X.is + li;
         const double3 m0 = ld3(m, i, X.cs);
@@ -318,10 +321,13 @@ __global__ void __launch_bounds__(256) k_gneb_sums(const double* __restrict__ m,
         const double d = dot(f, m0);
         f = make_double3(f.x - d * m0.x, f.y - d * m0.y, f.z - d * m0.z);
         st3(F, i, X.cs, f);
-        gneb_path_terms(m0, mp, mm, up, f, g);
+        double g6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        gneb_path_terms(m0, mp, mm, up, f, g6);
+        for (int q = 0; q < 6; ++q) g[q] = g6[q];
+        if (esite) g[6] = esite[r * X.n + li];
     }
-    double* pr = part + static_cast<int64_t>(r) * 6 * nblk;
-    block_partials<6>(g, pr, nblk, blockIdx.y);
+    double* pr = part + static_cast<int64_t>(r) * 7 * nblk;
+    block_partials<7>(g, pr, nblk, blockIdx.y);
     __shared__ bool last;
     if (threadIdx.x == 0) {
         __threadfence();
@@ -330,10 +336,11 @@ __global__ void __launch_bounds__(256) k_gneb_sums(const double* __restrict__ m,
     __syncthreads();
     if (!last) return;
     __threadfence();
-    __shared__ double sums[6];
-    ordered_sum<6>(pr, nblk, sums);
+    __shared__ double sums[7];
+    ordered_sum<7>(pr, nblk, sums);
     if (threadIdx.x == 0) {
         for (int q = 0; q < 6; ++q) img[q * nrep + r] = sums[q];
+        if (esite) E[r] = sums[6];
         cnt[r] = 0u;
     }
 }

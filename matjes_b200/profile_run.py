@@ -21,7 +21,8 @@ runs Metropolis sweeps (cone proposals, 10 K) instead of time steps;
 
 relaxes a GNEB path of --nim images of an L x L DMI film (J + D + K + Bz =
 0.3 T, periodic; geodesic from +z to -z, interior spins moved by up to 1e-2)
-for --steps iterations (force tolerance 0).
+for --steps iterations (force tolerance 0); with --plan the images are held on
+the deck's plan (mj_gneb_path) instead of as the replicas of a batch.
 """
 from __future__ import annotations
 
@@ -46,6 +47,7 @@ def main(argv=None):
     ap.add_argument("--mc", action="store_true", help="Metropolis sweeps (cone proposals) instead of time steps")
     ap.add_argument("--gneb", action="store_true", help="GNEB path relaxation iterations instead of time steps")
     ap.add_argument("--nim", type=int, default=16, help="GNEB images")
+    ap.add_argument("--plan", action="store_true", help="GNEB images held on the deck's plan (mj_gneb_path)")
     a = ap.parse_args(argv)
     if a.gneb:
         return gneb(a)
@@ -124,8 +126,13 @@ def gneb(a):
     up = np.tile([0.0, 0.0, 1.0], (n, 1))
     path = geodesic_path(up, -up, a.nim, amp_rnd=1e-2, seed=1)
     path[0], path[-1] = up, -up
-    bt = mj.ReplicaBatch(deck, [(a.L, a.L)] * a.nim, np.tile(deck.B_ext, (a.nim, 1)), [0.0] * a.nim)
-    bt.upload(path.reshape(-1, 3))
+    if a.plan:
+        from matjes_b200.gneb import PlanPath
+
+        bt = PlanPath(mj.Hamiltonian(deck), path)
+    else:
+        bt = mj.ReplicaBatch(deck, [(a.L, a.L)] * a.nim, np.tile(deck.B_ext, (a.nim, 1)), [0.0] * a.nim)
+        bt.upload(path.reshape(-1, 3))
     rx, ene, dene, its, fchk, _ = bt.gneb_path(0.3, 0.02, 1.0, 0.0, a.steps, "I")
     print("ok", its, fchk, ene.tolist())
 
