@@ -164,45 +164,76 @@ def job_rate(sites: int, steps: int, world: int, seconds: float) -> float:
 
 
 # ----------------------------------------------------------------------
-def cpu_oracle_rate(wname, seconds=10.0, side=512):
-    """The oracle (C restatement, OpenMP over all host threads) on a bounded
-    sample of the same workload: the same couplings and dynamics on a
-    side x side lattice."""
-    from matjes_b200.deck import workload
-    from oracle import oracle as O
+def cpu_oracle_rate(wname, seconds=15.0):
+    """The oracle (C restatement, -O3 -march=native, OpenMP over all host
+    threads) on a bounded sample of the same workload: the full lattice, the
+    same couplings and dynamics, as many steps as fit in about `seconds`, with
+    the energy of each step's incoming state fused as in the GPU arm; then the
+    same on one core."""
+    workload = deck_module().workload
+    O = oracle_native()
 
-    w = workload(wname, scale=1024 // side)
+    w = workload(wname)
     dyn = dict(w["dyn"])
     dyn.pop("steps")
     M = O.Model(w["deck"])
     m = w["m0"].copy()
+    N = w["deck"].nsites
     t = time.perf_counter()
-    M.run(m, 2, **dyn)
+    M.run(m, 2, energies=True, energy_before=True, **dyn)
     per = (time.perf_counter() - t) / 2
-    nst = int(max(3, min(400, seconds / max(per, 1e-6))))
+    nst = int(max(3, min(2000, seconds / max(per, 1e-6))))
     t = time.perf_counter()
-    M.run(m, nst, step0=2, **dyn)
+    M.run(m, nst, step0=2, energies=True, energy_before=True, **dyn)
     el = time.perf_counter() - t
     # the same on one core (a few seconds)
     O.set_threads(1)
-    n1 = max(2, nst // max(1, os.cpu_count() or 1) // 2)
+    n1 = max(1, int(min(nst, 0.3 * seconds / max(per * (os.cpu_count() or 1), 1e-6))))
     t = time.perf_counter()
-    M.run(m, n1, step0=2 + nst, **dyn)
+    M.run(m, n1, step0=2 + nst, energies=True, energy_before=True, **dyn)
     el1 = time.perf_counter() - t
     O.set_threads(0)
-    return {"value": w["deck"].nsites * nst / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"oracle SIB+Philox on {side}x{side} triangular (same couplings), {nst} steps, {el:.1f} s",
-            "single_core": {"value": w["deck"].nsites * n1 / el1, "unit": UNIT, "cores": 1,
+    L = w["deck"].L
+    return {"value": N * nst / el, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle SIB+Philox, full {L[0]}x{L[1]} lattice, {nst} steps, {el:.1f} s, "
+                      f"energy of the incoming state fused",
+            "build": "oracle/liboracle_native.so (-O3 -march=native -fopenmp -ffp-contract=off, built on this host)",
+            "single_core": {"value": N * n1 / el1, "unit": UNIT, "cores": 1,
                             "sample": f"the same, {n1} steps, {el1:.1f} s"}}
+
+
+def deck_module():
+    """matjes_b200/deck.py loaded by its path, outside the package: the package's
+    import loads the CUDA library, which the CPU legs have no use for."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("matjes_deck_cpu", os.path.join(ROOT, "matjes_b200", "deck.py"))
+    if spec.name in sys.modules:
+        return sys.modules[spec.name]
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses look their module up while the file runs
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_native():
+    """The oracle built -O3 -march=native on this machine (the CPU legs' timed
+    build; the tests' checker is the portable -O2 build of the same source)."""
+    os.environ["ORACLE_NATIVE"] = "1"
+    from oracle import oracle as O
+
+    return O
 
 
 def run_reference(args, rank, world):
     """--impl reference: the oracle port (the reference cannot be compiled here:
-    no Fortran compiler) on the full workload, all host threads."""
+    no Fortran compiler) on the full workload, all host threads, with the
+    energy of the state each step starts from summed in its first field pass,
+    the convention of the GPU arm."""
     if rank != 0:
         return
-    from matjes_b200.deck import workload
-    from oracle import oracle as O
+    workload = deck_module().workload
+    O = oracle_native()
 
     w = workload(args.workload)
     dyn = dict(w["dyn"])
@@ -211,7 +242,7 @@ def run_reference(args, rank, world):
     m = w["m0"].copy()
     M.run(m, args.warmup, **dyn)
     t = time.perf_counter()
-    E = M.run(m, args.steps, step0=args.warmup, energies=True, **dyn)
+    E = M.run(m, args.steps, step0=args.warmup, energies=True, energy_before=True, **dyn)
     el = time.perf_counter() - t
     N = w["deck"].nsites
     value = N * args.steps / el
@@ -219,11 +250,13 @@ def run_reference(args, rank, world):
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": workload_config(args.workload, w["deck"], w["dyn"], {"energy_per_step": "after each step"}),
+        "config": workload_config(args.workload, w["deck"], w["dyn"],
+                                  {"energy_per_step": "energy of the incoming state, fused into the first field pass"}),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                          "sample": f"full {w['deck'].L[0]}x{w['deck'].L[1]} lattice, {args.steps} SIB steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "final_energy_eV": float(E[-1]),
+        "oracle_build": "oracle/liboracle_native.so: -O3 -march=native -fopenmp -ffp-contract=off, built on this host",
     }
     print(json.dumps(line), flush=True)
 
@@ -806,7 +839,165 @@ def run_gpu(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------
+# --profile-run: a few launches of a synthetic workload for a profiler (ncu)
+# to capture; nothing is timed or printed as a bench line.
+PROFILE_RUN_DOC = """Run a few LLG steps of a synthetic workload, for profilers (ncu) to capture.
+
+    python bench.py --profile-run --lattice triangular --L 4096 --T 10 \
+        --integrator sib --variant 2 --steps 3
+
+--variant: -1 generic kernel, 0..3 tiled tile shapes, "auto" = the autotuner's pick.
+
+    python bench.py --profile-run --adjoint --L 256 --steps 20 --every 10
+
+runs one forward + backward sweep of the reverse-mode SIB trajectory instead;
+
+    python bench.py --profile-run --batch --steps 3
+
+steps the 256-replica batch workload;
+
+    python bench.py --profile-run --mc --lattice square --L 2048 --steps 3
+
+runs Metropolis sweeps (cone proposals, 10 K) instead of time steps;
+
+    python bench.py --profile-run --gneb --L 256 --nim 16 --steps 64
+
+relaxes a GNEB path of --nim images of an L x L DMI film (J + D + K + Bz =
+0.3 T, periodic; geodesic from +z to -z, interior spins moved by up to 1e-2)
+for --steps iterations (force tolerance 0); with --plan the images are held on
+the deck's plan (mj_gneb_path) instead of as the replicas of a batch.
+"""
+
+
+def _prof_main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lattice", default="triangular", choices=["triangular", "square", "film"])
+    ap.add_argument("--L", type=int, default=4096)
+    ap.add_argument("--Lz", type=int, default=16)
+    ap.add_argument("--T", type=float, default=10.0)
+    ap.add_argument("--integrator", default="sib")
+    ap.add_argument("--variant", default="auto")
+    ap.add_argument("--tma", type=int, default=1, help="halo staging of the tiled kernels: 1 TMA, 0 plain loads")
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--adjoint", action="store_true", help="one forward + backward sweep of the SIB adjoint")
+    ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
+    ap.add_argument("--batch", action="store_true", help="step the 256-replica batch workload")
+    ap.add_argument("--mc", action="store_true", help="Metropolis sweeps (cone proposals) instead of time steps")
+    ap.add_argument("--gneb", action="store_true", help="GNEB path relaxation iterations instead of time steps")
+    ap.add_argument("--nim", type=int, default=16, help="GNEB images")
+    ap.add_argument("--plan", action="store_true", help="GNEB images held on the deck's plan (mj_gneb_path)")
+    a = ap.parse_args(argv)
+    if a.gneb:
+        return _prof_gneb(a)
+    if a.adjoint:
+        return _prof_adjoint(a)
+    if a.batch:
+        return _prof_batch(a)
+
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    if a.lattice == "triangular":
+        deck = mj.triangular((a.L, a.L))
+        m0 = mj.reversed_disks(deck, 20, 8.0, 1)
+    elif a.lattice == "square":
+        deck = mj.square_film((a.L, a.L, 1))
+        m0 = mj.random_sphere(deck.nsites, 0)
+    else:
+        deck = mj.square_film((a.L, a.L, a.Lz), Jv=1e-3, Dv=0.15e-3, Kv=-0.02e-3, Bz=0.2, a=0.25, med_z=-0.3, dip=True)
+        m0 = mj.random_sphere(deck.nsites, 4)
+    ham = mj.Hamiltonian(deck)
+    m = torch.tensor(m0.T.copy(), device="cuda")
+    if a.mc:
+        from matjes_b200.montecarlo import MetropolisMC
+
+        ch = MetropolisMC(ham, "sphere", cone=0.5, seed=3, adapt_cone=False)
+        E, _, acc = ch.sweeps(m, a.steps, a.T)
+        torch.cuda.synchronize()
+        print("ok", ch.colors, acc, E.tolist())
+        return
+    sd = mj.SpinDynamics(ham, integrator=a.integrator, timestep=0.1, alpha=0.1, temperature=a.T, noise="philox", seed=1)
+    sd.p.energy_mode = _abi.MJ_ENERGY_BEFORE
+    if a.variant == "auto":
+        best = _abi.C.c_int32()
+        _abi.check(_abi.lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(sd.p), 3, _abi.C.byref(best), None,
+                                             None))
+    elif ham.noffsets:
+        _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, int(a.variant)))
+        _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, int(a.tma)))
+    E = torch.zeros(a.steps + 1, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for k in range(a.steps):
+        sd.p.step0 = k
+        _abi.check(_abi.lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(sd.p), 1, E[k:].data_ptr(), stream))
+    torch.cuda.synchronize()
+    print("ok", E[: a.steps].tolist())
+
+
+def _prof_adjoint(a):
+    import torch
+
+    import matjes_b200 as mj
+
+    deck = mj.square_film((a.L, a.L, 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5)
+    ham = mj.Hamiltonian(deck)
+    traj = mj.SIBTrajectory(ham, a.steps, checkpoint_every=a.every, timestep=0.1, alpha=0.2)
+    rng = np.random.default_rng(3)
+    b = torch.tensor(np.stack([np.zeros(deck.nsites), np.zeros(deck.nsites),
+                               0.5 + 0.05 * rng.standard_normal(deck.nsites)]), device="cuda")
+    traj.set_bfield(b)
+    m0 = torch.tensor(mj.random_sphere(deck.nsites, 3).T.copy(), device="cuda")
+    mT = traj.forward(m0)
+    g0, gt, gb = traj.backward(mT - m0)
+    torch.cuda.synchronize()
+    print("ok", gt.tolist(), float(g0.abs().sum()), float(gb.abs().sum()))
+
+
+def _prof_gneb(a):
+    import matjes_b200 as mj
+    from matjes_b200.gneb import geodesic_path
+
+    deck = mj.square_film((a.L, a.L, 1), Jv=1e-3, Dv=0.4e-3, Kv=-0.2e-3, Bz=0.3, mu_s=2.0, periodic=(1, 1, 0))
+    n = a.L * a.L
+    up = np.tile([0.0, 0.0, 1.0], (n, 1))
+    path = geodesic_path(up, -up, a.nim, amp_rnd=1e-2, seed=1)
+    path[0], path[-1] = up, -up
+    if a.plan:
+        from matjes_b200.gneb import PlanPath
+
+        bt = PlanPath(mj.Hamiltonian(deck), path)
+    else:
+        bt = mj.ReplicaBatch(deck, [(a.L, a.L)] * a.nim, np.tile(deck.B_ext, (a.nim, 1)), [0.0] * a.nim)
+        bt.upload(path.reshape(-1, 3))
+    rx, ene, dene, its, fchk, _ = bt.gneb_path(0.3, 0.02, 1.0, 0.0, a.steps, "I")
+    print("ok", its, fchk, ene.tolist())
+
+
+def _prof_batch(a):
+    import torch
+
+    import matjes_b200 as mj
+
+    w = mj.workload("square_replicas256")
+    bt = mj.ReplicaBatch(w["cell"], w["sizes"], w["B_ext"], w["temperature"])
+    bt.upload(w["m0"])
+    d = w["dyn"]
+    p = bt.params(timestep=d["timestep"], alpha=d["alpha"], noise="philox", seed=d["seed"])
+    bt.step(p, a.steps)
+    torch.cuda.synchronize()
+    print("ok", bt.energies()[:4].tolist())
+
+
 def main():
+    # every oracle import of this process (the CPU legs) loads the build made on this host
+    os.environ["ORACLE_NATIVE"] = "1"
+    if "--profile-run" in sys.argv[1:]:
+        argv = [a for a in sys.argv[1:] if a != "--profile-run"]
+        _prof_main(argv)
+        return
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)

@@ -193,9 +193,13 @@ mj_status mj_energy(mj_plan* plan, const mj_state* st, double* E_host);
  * driver that must not allocate inside its time loop.  Its scratch (one
  * partial sum per thread block and a ticket counter) is a fixed static device
  * array of MJ_NOALLOC_MAX_BLOCKS doubles (512 KiB) that every GPU loading the
- * library holds until the process exits; lattices needing more blocks than
- * that (more than 2^24 sites) are rejected with MJ_ERR_ARG, and plans with the
- * FFT dipolar term with MJ_ERR_UNSUPPORTED.  The first call on a device looks
+ * library holds until the process exits.  The limit is on thread blocks, one
+ * per 32 x 8 tile of a layer for stencil plans (ceil(Lx/32) * ceil(Ly/8) * Lz
+ * <= 65536) and one per 256 sites for ELL plans (ceil(N/256) <= 65536); a
+ * lattice over it is rejected with MJ_ERR_ARG.  2^24 sites is an upper bound,
+ * not a guarantee: 4095 x 4097 (2^24 - 1 sites) already needs 128 x 513 =
+ * 65664 blocks.  Plans with the FFT dipolar term are rejected with
+ * MJ_ERR_UNSUPPORTED.  The first call on a device looks
  * up the array's device address: make that first call before any stream
  * capture.  All calls share the one array and each leaves its partial sums in
  * it: calls that overlap on the GPU (different streams or host threads) race,

@@ -689,7 +689,8 @@ extern "C" mj_status mj_energy_noalloc(const mj_plan* plan, const double* m, dou
     if (nblocks > MJ_NOALLOC_MAX_BLOCKS)
         return set_error(MJ_ERR_ARG, "lattice needs " + std::to_string(nblocks) +
                                          " thread blocks; the no-allocation scratch holds MJ_NOALLOC_MAX_BLOCKS = " +
-                                         std::to_string(MJ_NOALLOC_MAX_BLOCKS) + " (at most 2^24 sites)");
+                                         std::to_string(MJ_NOALLOC_MAX_BLOCKS) +
+                                         " (one per 32 x 8 tile of a layer, or per 256 sites of an ELL plan)");
     double* scratch = nullptr;
     if ((st = noalloc_scratch(&scratch)) != MJ_OK) return st;
     unsigned int* counter = reinterpret_cast<unsigned int*>(scratch + MJ_NOALLOC_MAX_BLOCKS);

@@ -28,8 +28,6 @@ from typing import List, Sequence, Tuple
 
 import numpy as np
 
-from . import _abi
-
 Vec3 = Tuple[float, float, float]
 
 
@@ -75,6 +73,10 @@ class Deck:
     # ------------------------------------------------------------------
     def c_structs(self):
         """(LatticeDesc, HamiltonianDesc, keep-alive arrays) for the C ABI."""
+        # imported here, not at module level: the deck itself needs no CUDA
+        # library (a CPU-only consumer can load this file on its own)
+        from . import _abi
+
         lat = _abi.LatticeDesc()
         for d in range(3):
             lat.L[d] = int(self.L[d])

@@ -916,7 +916,8 @@ int orc_run(const orc_model* M, const orc_dyn* d, double* m, int nsteps, double*
         if (thermal) draw_noise(M, d, step, sigma, b);
         if (d->integrator == ORC_EULER || d->integrator == ORC_HEUN_MATJES) {
             if (thermal) orc_llg_torque(b, d->alpha, m, DT, N); /* langevin_bath at m_n */
-            orc_field(M, m, B, NULL);
+            if (E_step && d->energy_before) field_impl(M, m, B, NULL, NULL, NULL, NULL, &E_step[s]);
+            else orc_field(M, m, B, NULL);
             orc_llg_torque(B, d->alpha, m, D1, N);
             if (d->integrator == ORC_EULER) {
                 euler_update(m, D1, thermal ? DT : NULL, dt, mt, N);
@@ -932,13 +933,14 @@ int orc_run(const orc_model* M, const orc_dyn* d, double* m, int nsteps, double*
             }
         } else {
             double hc = -0.5 * (d->timestep / ORC_HBAR) / (1.0 + d->alpha * d->alpha);
-            orc_field(M, m, B, NULL);
+            if (E_step && d->energy_before) field_impl(M, m, B, NULL, NULL, NULL, NULL, &E_step[s]);
+            else orc_field(M, m, B, NULL);
             sib_stage(m, m, B, thermal ? b : NULL, hc, d->alpha, mt, 1, N);  /* mt = midpoint */
             orc_field(M, mt, B, NULL);
             sib_stage(m, mt, B, thermal ? b : NULL, hc, d->alpha, D2, 0, N);
             memcpy(m, D2, sizeof(double) * n3);
         }
-        if (E_step) E_step[s] = orc_energy(M, m);
+        if (E_step && !d->energy_before) E_step[s] = orc_energy(M, m);
     }
     free(B); free(D1); free(D2); free(DT); free(b); free(mt); free(Dint);
     return 0;

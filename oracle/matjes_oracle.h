@@ -197,9 +197,12 @@ typedef struct {
     uint32_t step0;      /* global step index of the first step */
     const double* inject;/* N(0,1) buffer, layout [nbuf][3][N] */
     int inject_nbuf;
+    int energy_before;   /* E_step[k]: 0 = energy after step k (an extra field pass,
+                            spindynamics.f90:323); 1 = energy of the state step k
+                            starts from, summed in the first stage's field pass */
 } orc_dyn;
 
-/* Advance nsteps; m updated in place; E_step[k] = energy after step k (may be NULL). */
+/* Advance nsteps; m updated in place; E_step[k] as orc_dyn.energy_before says (may be NULL). */
 int orc_run(const orc_model* m, const orc_dyn* d, double* mvec, int nsteps, double* E_step);
 
 /* Rotation sense helpers for tests */

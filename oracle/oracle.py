@@ -17,7 +17,10 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB = os.path.join(HERE, "liboracle.so")
+# ORACLE_NATIVE=1 (set by bench.py's CPU-baseline and reference legs before the
+# import) loads the -O3 -march=native build made on this machine instead
+NATIVE = os.environ.get("ORACLE_NATIVE") == "1"
+LIB = os.path.join(HERE, "liboracle_native.so" if NATIVE else "liboracle.so")
 MAXAT = 16
 MAXTERM = 32
 KB = 0.000086173324
@@ -26,7 +29,9 @@ HBAR = 0.658211928
 
 
 def build() -> str:
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    # the native build is always remade: a copy made on another machine may
+    # use instructions this one lacks
+    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if NATIVE else []) + [os.path.basename(LIB)], check=True)
     return LIB
 
 
@@ -57,7 +62,8 @@ class _Input(C.Structure):
 class _Dyn(C.Structure):
     _fields_ = [("integrator", C.c_int), ("timestep", C.c_double), ("alpha", C.c_double),
                 ("temperature", C.c_double), ("noise", C.c_int), ("seed", C.c_uint64), ("stream", C.c_uint32),
-                ("step0", C.c_uint32), ("inject", C.c_void_p), ("inject_nbuf", C.c_int)]
+                ("step0", C.c_uint32), ("inject", C.c_void_p), ("inject_nbuf", C.c_int),
+                ("energy_before", C.c_int)]
 
 
 INTEGRATORS = {"euler": 1, "heun": 2, "heun_matjes": 2, "sib": 3}
@@ -65,8 +71,8 @@ NOISES = {"off": 0, "philox": 1, "inject": 2}
 
 
 def _lib():
-    if not os.path.exists(LIB):
-        build()
+    if NATIVE or not os.path.exists(LIB):
+        build()  # the native build is made for (and on) the machine that runs it
     lib = C.CDLL(LIB)
     P, DP = C.c_void_p, C.POINTER(C.c_double)
     lib.orc_input_defaults.argtypes = [C.POINTER(_Input)]
@@ -189,14 +195,18 @@ class Model:
         return r, c, v
 
     def run(self, m, nsteps, integrator="sib", timestep=0.1, alpha=0.1, temperature=0.0, noise="off", seed=0,
-            stream=0, step0=0, inject=None, energies=False, **_ignored):
-        """Advance m (N,3) in place; inject is a host array [nbuf][3][N]."""
+            stream=0, step0=0, inject=None, energies=False, energy_before=False, **_ignored):
+        """Advance m (N,3) in place; inject is a host array [nbuf][3][N].  With
+        `energies`, returns the energy after each step (an extra field pass per
+        step), or with `energy_before` the energy of the state each step starts
+        from, summed in the step's first field pass."""
         assert m.dtype == np.float64 and m.flags.c_contiguous
         d = _Dyn()
         d.integrator = INTEGRATORS[integrator]
         d.timestep, d.alpha, d.temperature = timestep, alpha, temperature
         d.noise = NOISES[noise]
         d.seed, d.stream, d.step0 = seed, stream, step0
+        d.energy_before = int(bool(energy_before))
         keep = None
         if inject is not None:
             keep = np.ascontiguousarray(inject, np.float64)

@@ -1,7 +1,7 @@
 """Extract the reference's isolated-spin-precession golden logs into a fixture.
 
 Reads tests/serial/isolated_spin_precession/{Euler/REF,Heun/EM.dat} of the
-Matjes source tree (argument 1, default /root/reference) and writes
+Matjes source tree (the one argument) and writes
 isolated_spin_precession.json beside this script: per step the columns
 time (fs), E_av (eV), |M|, Mx, My, Mz of the 4x4 ferromagnet in B = 10 T z,
 m0 = x, dt = 1 fs, alpha = 0, mu_s = 1, J_1 = 1e-6 eV (the decks beside the logs).
@@ -10,7 +10,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]
 base = os.path.join(ref, "tests", "serial", "isolated_spin_precession")
 out = {}
 for name, fn in (("euler", "Euler/REF"), ("heun", "Heun/EM.dat")):

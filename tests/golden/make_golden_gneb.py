@@ -1,7 +1,7 @@
 """Extract the reference's GNEB test into a fixture.
 
-Reads tests/serial/gneb/heisenberg_chain/ of the Matjes source tree (argument 1,
-default /root/reference) and writes gneb_chain10.json beside this script: the
+Reads tests/serial/gneb/heisenberg_chain/ of the Matjes source tree (the one argument)
+and writes gneb_chain10.json beside this script: the
 initial and converged path energies (en_path-REF.in / en_path-REF.out: reaction
 coordinate, energy above the first image, energy derivative along the path), the
 saddle point of the Hermite fit (ensp_path-REF.out) and the spins of the 12
@@ -16,7 +16,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]
 base = os.path.join(ref, "tests", "serial", "gneb", "heisenberg_chain")
 
 

@@ -1,7 +1,7 @@
 """Extract the reference's parallel-tempering Monte Carlo golden log into a fixture.
 
-Reads tests/serial/PTMC/EM.dat of the Matjes source tree (argument 1, default
-/root/reference) and writes ptmc_ising_square20.json beside this script: per
+Reads tests/serial/PTMC/EM.dat of the Matjes source tree (the one argument)
+and writes ptmc_ising_square20.json beside this script: per
 temperature the columns T (K), E_av (eV per site), E_err (per-site sample
 standard deviation of the measured energies), C, M (norm of the averaged
 summed spins per site), Mx, My, Mz; plus the text tokens of three rows for the
@@ -16,7 +16,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]
 path = os.path.join(ref, "tests", "serial", "PTMC", "EM.dat")
 rows, tokens = [], []
 with open(path) as f:
