@@ -63,7 +63,7 @@ def workload_config(name, deck, dyn, extra=None) -> dict:
         "temperature_K": dyn["temperature"],
         "noise": dyn.get("noise", "off"),
         "sites": int(deck.nsites),
-        "l2": "flushed between timed steps (256 MiB write), fields 2 x 25 MB",
+        "l2": "flushed before every timed step: 256 MiB written, then 256 MiB of another buffer read",
     }
     if extra:
         cfg.update(extra)
@@ -677,6 +677,115 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
                                        f"forces before the first move and outputs included)"}}
 
 
+class L2Flush:
+    """Before every timed step: a 256 MiB write, then a read of another 256 MiB
+    buffer, so that the step starts from an L2 (126 MB) that holds none of its
+    fields and no dirty lines of the flush (which the step would otherwise
+    write back on the flush's behalf)."""
+
+    def __init__(self, device):
+        import torch
+
+        self.w = torch.empty(FLUSH_BYTES // 8, dtype=torch.float64, device=device)
+        self.r = torch.zeros(FLUSH_BYTES // 8, dtype=torch.float64, device=device)
+
+    def __call__(self):
+        self.w.zero_()
+        self.r.sum()
+
+
+def timed_steps(lib, _abi, plan, m, p, first_step, K, flush, E, stream):
+    """K single steps of `p` on device spins m, L2 flushed before each; CUDA
+    events around each step on the launching stream.  Returns the summed ms."""
+    import torch
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    torch.cuda.synchronize()
+    for k in range(K):
+        flush()
+        p.step0 = first_step + k
+        ev[k][0].record()
+        _abi.check(lib.mj_step_dev(plan, m.data_ptr(), _abi.C.byref(p), 1, E[k:].data_ptr() if E is not None else None,
+                                   stream))
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def kernel_table(prof, bytes_site, N):
+    """Per-kernel launches, average time and achieved algorithmic GB/s."""
+    out = {}
+    for name, (tot, cnt) in prof.items():
+        avg = tot / max(cnt, 1)
+        b = bytes_site.get(name, 0.0) * N
+        out[name] = {"launches": cnt, "avg_us": round(1e3 * avg, 3), "alg_bytes_per_site": bytes_site.get(name),
+                     "achieved_gbs": round(b / (avg / 1e3) / 1e9, 1) if b else None}
+    return out
+
+
+def run_integrator_key(dev, wname, integrator, K, W, noise=None, inject_steps=0):
+    """The headline workload's lattice, couplings and temperature with another
+    integrator or noise source, timed as the headline (L2 flushed before every
+    step, CUDA events per step), with the per-kernel split.  Algorithmic bytes
+    per site: SIB 48 + 72 (+24 written and read back for the draw at T > 0);
+    Matjes Heun 72 + 72 (pass 1 reads m, writes the predictor and D(m_n); pass 2
+    reads the predictor and D(m_n), writes m) + 48 for the thermal torque DT
+    (written by pass 1, read by pass 2); injected noise: the SIB passes read the
+    step's N(0,1) slot (24 B per pass) instead of drawing."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+    from matjes_b200.deck import workload
+
+    w = workload(wname)
+    deck, dyn = w["deck"], dict(w["dyn"])
+    dyn.pop("steps")
+    dyn["integrator"] = integrator
+    N = deck.nsites
+    ham = mj.Hamiltonian(deck, device=dev)
+    buf = None
+    if noise == "inject":
+        dyn["noise"] = "inject"
+        g = torch.Generator(device=f"cuda:{dev}").manual_seed(1)
+        buf = torch.randn((inject_steps, 3, N), dtype=torch.float64, device=f"cuda:{dev}", generator=g)
+    sd = mj.SpinDynamics(ham, inject=buf, **dyn)
+    p = sd.p
+    p.energy_mode = _abi.MJ_ENERGY_BEFORE
+    m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
+    lib = _abi.lib
+    best, best_tma = _abi.C.c_int32(), _abi.C.c_int32()
+    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 3, _abi.C.byref(best),
+                                    _abi.C.byref(best_tma), None))
+    flush = L2Flush(m.device)
+    E = torch.zeros(K + W + 8, dtype=torch.float64, device=m.device)
+    stream = torch.cuda.current_stream().cuda_stream
+    timed_steps(lib, _abi, ham.plan, m, p, 0, W, flush, E, stream)
+    ms = timed_steps(lib, _abi, ham.plan, m, p, W, K, flush, E, stream)
+    _abi.check(lib.mj_profile_enable(ham.plan, 1))
+    timed_steps(lib, _abi, ham.plan, m, p, W + K, K, flush, E, stream)
+    prof = _abi.profile_read(ham.plan)
+    _abi.check(lib.mj_profile_enable(ham.plan, 0))
+    _abi.check(lib.mj_plan_check_status(ham.plan))
+    pk = peaks()
+    thermal = dyn.get("temperature", 0.0) > 0
+    if integrator == "sib":
+        extra = 24.0 if thermal else 0.0
+        bytes_site = {"k_sib1": 48.0 + extra, "k_sib2": 72.0 + extra}
+    else:
+        bytes_site = {"k_heun1": 72.0 + (24.0 if thermal else 0.0), "k_heun2": 72.0 + (24.0 if thermal else 0.0)}
+    step_b = sum(bytes_site.values())
+    sec = ms / K / 1e3
+    return {"workload": wname, "integrator": integrator, "noise": dyn.get("noise", "off"),
+            "kernel_variant": int(best.value), "tma_halo": bool(best_tma.value),
+            "value": N / sec, "unit": UNIT, "ms_per_step": ms / K,
+            "step_roofline": {"alg_bytes_per_site": step_b, "achieved_gbs": step_b * N / sec / 1e9,
+                              "frac": step_b * N / sec / 1e9 / pk["hbm_gbs"]},
+            "kernels": kernel_table(prof, bytes_site, N),
+            **({"inject_buffer": f"{inject_steps} steps x 3 x {N} doubles ({buf.numel() * 8 / 1e9:.2f} GB)"}
+               if buf is not None else {})}
+
+
 def run_gpu(args, rank, world):
     import torch
 
@@ -700,16 +809,10 @@ def run_gpu(args, rank, world):
     p.energy_mode = _abi.MJ_ENERGY_BEFORE
     m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
     K, W = args.steps, args.warmup
-    E = torch.zeros(W + 2 * K + 8, dtype=torch.float64, device=m.device)
-    flush = torch.empty(FLUSH_BYTES // 8, dtype=torch.float64, device=m.device)
+    E = torch.zeros(W + 2 * K + 16, dtype=torch.float64, device=m.device)
+    flush = L2Flush(m.device)
     stream = torch.cuda.current_stream().cuda_stream
     lib = _abi.lib
-
-    def step(k, slot=None):
-        """SIB step number k; its incoming energy lands in E[slot] (E[k] by default)."""
-        p.step0 = k
-        e = E[k if slot is None else slot:]
-        _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, e.data_ptr(), stream))
 
     # kernel variant (tile shape, TMA halo staging) timed under the conditions of
     # the timed loop below (L2 flushed before every step, per-step events); the
@@ -724,47 +827,28 @@ def run_gpu(args, rank, world):
     for ci, (v, t) in enumerate(configs if args.variant is None else []):
         _abi.check(lib.mj_plan_set_variant(ham.plan, v))
         _abi.check(lib.mj_plan_set_tma(ham.plan, t))
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(8)]
-        for k in range(10):
-            flush.zero_()
-            if k >= 2:
-                evs[k - 2][0].record()
-            step(1000 + k, slot=0)
-            if k >= 2:
-                evs[k - 2][1].record()
-        torch.cuda.synchronize()
-        tune[ci] = sorted(a.elapsed_time(b) for a, b in evs)[len(evs) // 2]
+        timed_steps(lib, _abi, ham.plan, m, p, 1000, 2, flush, E, stream)
+        evs = [timed_steps(lib, _abi, ham.plan, m, p, 1002 + k, 1, flush, E, stream) for k in range(8)]
+        tune[ci] = sorted(evs)[len(evs) // 2]
     bv, bt = configs[int(np.argmin(tune))]
     _abi.check(lib.mj_plan_set_variant(ham.plan, bv))
     _abi.check(lib.mj_plan_set_tma(ham.plan, bt))
 
-    for k in range(W):
-        flush.zero_()
-        step(k)
-    torch.cuda.synchronize()
+    timed_steps(lib, _abi, ham.plan, m, p, 0, W, flush, E, stream)
     if dist:
         td.barrier()
     clocks = Clocks(dev)
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    torch.cuda.synchronize()
-    for k in range(K):
-        flush.zero_()
-        ev[k][0].record()
-        step(W + k)
-        ev[k][1].record()
-    torch.cuda.synchronize()
+    ms = timed_steps(lib, _abi, ham.plan, m, p, W, K, flush, E, stream)
     if dist:
         td.barrier()
     ck = clocks.stop()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
     # per-kernel live timing on a second pass of the same K steps
     _abi.check(lib.mj_profile_enable(ham.plan, 1))
-    for k in range(K):
-        flush.zero_()
-        step(W + K + k)
+    timed_steps(lib, _abi, ham.plan, m, p, W + K, K, flush, E, stream)
     prof = _abi.profile_read(ham.plan)
     _abi.check(lib.mj_profile_enable(ham.plan, 0))
+    _abi.check(lib.mj_plan_check_status(ham.plan))
     ms_max = max_over_ranks(ms, m.device, dist)
     value = job_rate(N, K, world, ms_max / 1e3)
 
@@ -788,40 +872,46 @@ def run_gpu(args, rank, world):
     if rank != 0:
         return
     pk = peaks()
+    thermal = dyn.get("temperature", 0.0) > 0 and dyn.get("noise") == "philox"
+    # algorithmic bytes per site of the two SIB passes (the stored draw counted
+    # separately: written by pass 1, read by pass 2 at T > 0)
     bytes_site = {"k_sib1": 48.0, "k_sib2": 72.0}
-    kernels = {}
-    for name, (tot, cnt) in prof.items():
-        avg = tot / max(cnt, 1)
-        b = bytes_site.get(name, 0.0) * N
-        kernels[name] = {"launches": cnt, "avg_us": 1e3 * avg, "alg_bytes": b,
-                         "achieved_gbs": (b / (avg / 1e3) / 1e9) if b else None}
+    kernels = kernel_table(prof, bytes_site, N)
     dom = max((k for k in kernels if k in bytes_site), key=lambda k: kernels[k]["avg_us"])
     ach = kernels[dom]["achieved_gbs"]
     tr = ncu_traffic(dom)
     cpu = cpu_oracle_rate(args.workload) if (world == 1 and not args.no_cpu_baseline) else None
-    batch = run_batch(dev) if (world == 1 and not args.no_batch) else None
-    adjoint = run_adjoint(dev) if (world == 1 and not args.no_batch) else None
-    dipolar = run_dipolar(dev) if (world == 1 and not args.no_batch) else None
-    monte_carlo = run_monte_carlo(dev) if (world == 1 and not args.no_batch) else None
-    hbm_resident = run_hbm_resident(dev) if (world == 1 and not args.no_batch) else None
-    gneb = run_gneb(dev) if (world == 1 and not args.no_batch) else None
+    extras = {}
+    if world == 1 and not args.no_batch:
+        extras["heun"] = run_integrator_key(dev, args.workload, "heun", K, W)
+        extras["inject"] = run_integrator_key(dev, args.workload, "sib", K, W, noise="inject", inject_steps=200)
+        extras["batch"] = run_batch(dev)
+        extras["adjoint"] = run_adjoint(dev)
+        extras["dipolar"] = run_dipolar(dev)
+        extras["monte_carlo"] = run_monte_carlo(dev)
+        extras["hbm_resident_4096"] = run_hbm_resident(dev)
+        extras["gneb"] = run_gneb(dev)
+    # bulky tables go to stderr, not into the bench line
+    verbose = {"variant_sweep_ms_per_step": {("generic" if v < 0 else f"tile{v}" + ("_tma" if t else "")):
+                                             round(float(x), 5) for (v, t), x in zip(configs, tune)}}
+    for k, v in extras.items():
+        if isinstance(v, dict) and "autotune_ms_per_step" in v:
+            verbose[f"{k}_autotune_ms_per_step"] = v.pop("autotune_ms_per_step")
+    sys.stderr.write(json.dumps({"bench_tables": verbose}) + "\n")
+    step_frac = 120.0 * N / (ms_max / K / 1e3) / 1e9 / pk["hbm_gbs"]
     line = {
         "metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(args.workload, deck, w["dyn"],
                                                        {"parallelism": f"replicas x{world}" if world > 1 else "single",
-                                                        "energy_per_step": "fused into pass 1",
-                                                        "kernel_variant": int(bv),
-                                                        "tma_halo": bool(bt),
-                                                        "variant_sweep_ms_per_step": {
-                                                            ("generic" if v < 0 else f"tile{v}" + ("_tma" if t else "")):
-                                                                round(float(x), 5) for (v, t), x in zip(configs, tune)}}),
+                                                        "energy_per_step": "energy of the incoming state, fused "
+                                                                           "into the first field pass",
+                                                        "kernel_variant": int(bv), "tma_halo": bool(bt)}),
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
                      "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},
-        "step_roofline": {"alg_bytes_per_site": 120.0,
-                          "achieved_gbs": 120.0 * N / (ms_max / K / 1e3) / 1e9,
-                          "frac": 120.0 * N / (ms_max / K / 1e3) / 1e9 / pk["hbm_gbs"]},
+        "step_roofline": {"alg_bytes_per_site": 120.0, "achieved_gbs": 120.0 * N / (ms_max / K / 1e3) / 1e9,
+                          "frac": step_frac, "draw_bytes_per_site": 48.0 if thermal else 0.0},
         "kernels": kernels,
         "clocks": ck,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 24 * N + 8,
@@ -829,15 +919,26 @@ def run_gpu(args, rank, world):
                         "transposes and passes overlapped in 12 stripes of tile rows"},
         "gpu_launches": 2 * K,
         "cpu_baseline": cpu,
-        "batch": batch,
-        "adjoint": adjoint,
-        "dipolar": dipolar,
-        "monte_carlo": monte_carlo,
-        "hbm_resident_4096": hbm_resident,
-        "gneb": gneb,
+        **extras,
     }
+    # the figures to compare at a glance, last in the line
+    summ = {"step_roofline_frac": round(step_frac, 4), "kernel_roofline_frac": round(ach / pk["hbm_gbs"], 4)}
+    if extras:
+        b, a, d, h, inj = extras["batch"], extras["adjoint"], extras["dipolar"], extras["heun"], extras["inject"]
+        summ.update({
+            "heun_spin_updates_per_s": h["value"], "heun_step_roofline_frac": round(h["step_roofline"]["frac"], 4),
+            "inject_spin_updates_per_s": inj["value"],
+            "batch_spin_updates_per_s": b["value"],
+            "batch_speedup_vs_sequential_plain": round(b["speedup_vs_sequential_plain"], 3),
+            "batch_speedup_vs_sequential_graphs": round(b["speedup_vs_sequential_graphs"], 3),
+            "adjoint_cost_ratio": round(a["cost_ratio"], 3),
+            "adjoint_cost_ratio_vs_graph_forward": round(a["cost_ratio_vs_graph_forward"], 3),
+            "dipolar_spin_updates_per_s": d["value"],
+            "hbm_resident_4096_step_roofline_frac": round(extras["hbm_resident_4096"]["step_roofline"]["frac"], 4)})
+    if cpu:
+        summ["cpu_baseline_spin_updates_per_s"] = cpu["value"]
+    line["summary"] = summ
     print(json.dumps(line), flush=True)
-
 
 # ----------------------------------------------------------------------
 # --profile-run: a few launches of a synthetic workload for a profiler (ncu)

@@ -134,9 +134,12 @@ mj_status mj_plan_noffsets(const mj_plan* plan, int32_t* n);
 mj_status mj_plan_set_variant(mj_plan* plan, int32_t variant);
 /* Current variant (-1 generic) and the matched compile-time shape id (0 none). */
 mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape);
-/* Halo staging of the tiled kernels: enable = 1 (default) uses TMA bulk-tensor
- * copies in persistent, double-buffered blocks (tiles whose halo wraps a
- * periodic edge fall back to plain loads); 0 = plain loads, one tile per block. */
+/* Halo staging of the tiled kernels (one tile per block either way): enable = 1
+ * (default) stages tile + halo with one TMA bulk-tensor copy while the block
+ * computes its thermal draw, then rewrites the halo cells across a periodic
+ * edge with plain loads (the copy fills cells outside the lattice with zeros,
+ * the open boundary); 0 = plain loads with the periodic wrap per element.
+ * Lattices with an odd Lx or a spin array not 16-byte aligned use plain loads. */
 mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable);
 /* Autotuner: times `steps` steps of `p` for every kernel configuration of the
  * plan on a scratch copy of the device spins m_dev_soa (left untouched), keeps
@@ -147,8 +150,22 @@ mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable);
 mj_status mj_plan_autotune(mj_plan* plan, const double* m_dev_soa, const mj_dyn_params* p, int32_t steps,
                            int32_t* best, int32_t* best_tma, double* ms_per_step);
 /* Device status word of the plan's kernels (synchronises, then clears it):
- * MJ_ERR_TIMEOUT when a bounded device wait gave up since the last check. */
+ * MJ_ERR_TIMEOUT when a bounded device wait gave up since the last check (the
+ * results of that launch are invalid), else MJ_ERR_NAN when a time step wrote a
+ * non-finite spin component (the state is invalid from that step on).  The
+ * asynchronous step calls (mj_step, mj_step_dev, mj_graph_run) leave the report
+ * to this call; mj_step_host and mj_gneb_path return it themselves.  The
+ * reference has no such report: its only check is the energy-increase warning of
+ * dynamics/spindynamics.f90:376-381. */
 mj_status mj_plan_check_status(mj_plan* plan);
+/* Self-test of the failure path of the bounded device waits (no counterpart in
+ * the reference): one block arms an mbarrier for 16 bytes that no copy delivers
+ * (nothing is issued, so nothing is in flight), polls it `polls` times (1 ..
+ * 65536) through the same bounded wait as the tiled kernels' TMA staging, gives
+ * up and records the timeout in the plan's status word as they do; the next
+ * mj_plan_check_status returns MJ_ERR_TIMEOUT and clears it.  Asynchronous on
+ * `stream`. */
+mj_status mj_plan_selftest_timeout(mj_plan* plan, uint32_t polls, void* stream);
 /* Per-site applied field map (Tesla, host AoS 3*Ncell; NULL = uniform H_ext):
  * the Bfield_init.dat input read by initialization/orders_initialize.f90:28. */
 mj_status mj_plan_set_bfield(mj_plan* plan, const double* b_cell_host);
@@ -219,7 +236,9 @@ mj_status mj_step(mj_plan* plan, mj_state* st, const mj_dyn_params* p, int32_t n
 /* Same on caller-owned device SoA spins. */
 mj_status mj_step_dev(mj_plan* plan, double* m_dev_soa, const mj_dyn_params* p, int32_t nsteps,
                       double* E_dev, void* stream);
-/* Host-array convenience: upload m, run nsteps, download m and E (host, may be NULL). */
+/* Host-array convenience: upload m, run nsteps, download m and E (host, may be NULL).
+ * Synchronous; returns MJ_ERR_NAN when a step wrote a non-finite spin component
+ * (MJ_ERR_TIMEOUT when a bounded wait gave up), as mj_plan_check_status. */
 mj_status mj_step_host(mj_plan* plan, double* m_host_aos, const mj_dyn_params* p, int32_t nsteps,
                        double* E_host);
 /* The step loop captured once as a CUDA graph of `nsteps` steps and replayed
@@ -442,7 +461,9 @@ mj_status mj_batch_gneb_path(mj_batch* b, const mj_gneb_params* p, double* rx, d
  * Starts after the work queued on `stream` (the iterations run as CUDA graphs
  * on a stream of the plan's own) and returns with the path relaxed; at most
  * 65535 * 256 spins per image.  Replaces the GNEB driver's image loop over get_eff_field/energy
- * (GNEB/gneb_utils.f90:72-200) for a Hamiltonian held by a plan. */
+ * (GNEB/gneb_utils.f90:72-200) for a Hamiltonian held by a plan.  Returns
+ * MJ_ERR_TIMEOUT when an image's field launch gave up a bounded wait during the
+ * relaxation: the path and the outputs are then invalid. */
 mj_status mj_gneb_path(mj_plan* plan, double* m_dev_images, int32_t nimg, const mj_gneb_params* p, double* rx,
                        double* ene, double* dene, int64_t* iterations, double* max_force, int32_t* climbing,
                        void* stream);

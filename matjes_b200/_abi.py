@@ -140,6 +140,7 @@ SIGNATURES = {
                                      C.POINTER(C.c_int32), P]),
     "mj_plan_set_tma": (C.c_int32, [P, C.c_int32]),
     "mj_plan_check_status": (C.c_int32, [P]),
+    "mj_plan_selftest_timeout": (C.c_int32, [P, C.c_uint32, P]),
     "mj_plan_set_bfield": (C.c_int32, [P, P]),
     "mj_plan_set_bfield_device": (C.c_int32, [P, P, P]),
     "mj_state_create": (C.c_int32, [P, C.POINTER(P)]),

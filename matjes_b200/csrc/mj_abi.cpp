@@ -26,6 +26,17 @@ mj_status cuda_status(cudaError_t e, const char* where) {
 
 void match_shape(StencilParams& sp);
 
+mj_status status_from_word(mj_plan* p, int word) {
+    if (word == 0) return MJ_OK;
+    // clear the word; re-arm the ticket counter of the energy reduction, which a
+    // launch that failed may have left part-way
+    cudaMemset(p->d_status, 0, sizeof(int));
+    cudaMemset(p->d_counter, 0, 4 * sizeof(unsigned int));
+    if (word & kStatusTimeout)
+        return set_error(MJ_ERR_TIMEOUT, "a bounded device wait (TMA mbarrier) gave up; results of that launch are invalid");
+    return set_error(MJ_ERR_NAN, "a time step wrote a non-finite spin component; the state is invalid from that step on");
+}
+
 int prof_begin(mj_plan* p, const char* name, cudaStream_t s) {
     if (!p->prof_on) return -1;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -267,10 +278,11 @@ mj_status alloc_scratch(mj_plan* p) {
     if ((st = dalloc(&p->d_status, 4, "status")) != MJ_OK) return st;
     if ((st = cuda_status(cudaMemset(p->d_status, 0, 4 * sizeof(int)), "status init")) != MJ_OK) return st;
     cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device);
-    double tab[768];
-    build_noise_tables(tab);
-    if ((st = dalloc(&p->d_noise_tab, 768, "noise tables")) != MJ_OK) return st;
-    return cuda_status(cudaMemcpy(p->d_noise_tab, tab, sizeof(tab), cudaMemcpyHostToDevice), "noise tables");
+    std::vector<double> tab(kNoiseTabDoubles);
+    build_noise_tables(tab.data());
+    if ((st = dalloc(&p->d_noise_tab, kNoiseTabDoubles, "noise tables")) != MJ_OK) return st;
+    return cuda_status(cudaMemcpy(p->d_noise_tab, tab.data(), sizeof(double) * kNoiseTabDoubles, cudaMemcpyHostToDevice),
+                       "noise tables");
 }
 
 void free_plan(mj_plan* p) {
@@ -295,6 +307,7 @@ void free_plan(mj_plan* p) {
     cudaFree(p->d_counter);
     cudaFree(p->d_scalar);
     cudaFree(p->d_status);
+    if (p->h_status) cudaFreeHost(p->h_status);
     cudaFree(p->d_noise_tab);
     cudaFree(p->d_stage);
     cudaFree(p->d_tmp_m);
@@ -313,6 +326,11 @@ mj_status ensure_host_scratch(mj_plan* p) {
     if (!p->d_tmp_m && (st = dalloc(&p->d_tmp_m, 3 * N, "tmp m")) != MJ_OK) return st;
     if (!p->d_tmp_b && (st = dalloc(&p->d_tmp_b, 3 * N, "tmp b")) != MJ_OK) return st;
     if (!p->d_tmp_e && (st = dalloc(&p->d_tmp_e, N + 8, "tmp e")) != MJ_OK) return st;
+    if (!p->h_status) {
+        if ((st = cuda_status(cudaHostAlloc(&p->h_status, sizeof(int), cudaHostAllocDefault), "status mirror")) != MJ_OK)
+            return st;
+        *p->h_status = 0;
+    }
     return MJ_OK;
 }
 
@@ -576,16 +594,21 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
         done[lvl][kk] = 1;
         --remaining;
     }
+    // every stripe's last task (its passes, energy partials included) has
+    // finished before sc[0] reads the status word and sums the energy
+    for (int k = 0; k < K; ++k)
+        if (k % kPipeCompute != 0) cudaStreamWaitEvent(sc[0], ev_task[(nlev - 1) * K + k], 0);
+    if ((st = cuda_status(cudaMemcpyAsync(p->h_status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, sc[0]),
+                          "status mirror")) != MJ_OK)
+        return st;
     if (E_host) {
-        // the energy pass of every stripe has finished before its stripe's last task
-        for (int k = 0; k < K; ++k)
-            if (k % kPipeCompute != 0) cudaStreamWaitEvent(sc[0], ev_task[(nlev - 1) * K + k], 0);
         const int nthr = 32 * kTiledVariantBYT[p->tile_variant];
         if ((st = launch_ordered_sum(p->d_partials, static_cast<int>(tiled_energy_blocks(p)), nthr, p->d_scalar, sc[0])) != MJ_OK)
             return st;
     }
     for (cudaStream_t ps : p->pipe_stream)
         if ((st = cuda_status(cudaStreamSynchronize(ps), "striped step")) != MJ_OK) return st;
+    if ((st = status_from_word(p, *p->h_status)) != MJ_OK) return st;
     if (E_host) return cuda_status(cudaMemcpy(E_host, p->d_scalar, sizeof(double), cudaMemcpyDeviceToHost), "energy");
     return MJ_OK;
 }
@@ -909,11 +932,7 @@ mj_status mj_plan_check_status(mj_plan* plan) {
     if (st != MJ_OK) return st;
     if ((st = cuda_status(cudaMemcpy(&word, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status read")) != MJ_OK)
         return st;
-    if (word == 0) return MJ_OK;
-    // a timed-out block skipped the energy reduction: re-arm its ticket counter too
-    cudaMemset(plan->d_status, 0, sizeof(int));
-    cudaMemset(plan->d_counter, 0, 4 * sizeof(unsigned int));
-    return set_error(MJ_ERR_TIMEOUT, "a bounded device wait (TMA mbarrier) gave up; results of that launch are invalid");
+    return status_from_word(plan, word);
 }
 
 mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* shape) {
@@ -1072,7 +1091,9 @@ mj_status mj_step_host(mj_plan* plan, double* m, const mj_dyn_params* prm, int32
         (st = run_steps(plan, plan->d_tmp_m, prm, nsteps, dE, 0)) == MJ_OK &&
         (st = soa_to_aos(plan->d_tmp_m, plan->d_stage, N, 0)) == MJ_OK &&
         (st = cuda_status(cudaMemcpy(m, plan->d_stage, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost), "download")) == MJ_OK &&
-        dE) {
+        (st = cuda_status(cudaMemcpy(plan->h_status, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status")) ==
+            MJ_OK &&
+        (st = status_from_word(plan, *plan->h_status)) == MJ_OK && dE) {
         st = cuda_status(cudaMemcpy(E_host, dE, sizeof(double) * nsteps, cudaMemcpyDeviceToHost), "energies");
     }
     cudaFree(dE);

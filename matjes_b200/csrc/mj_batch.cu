@@ -780,7 +780,7 @@ mj_status mj_batch_create(const mj_lattice_desc* cell, const mj_hamiltonian_desc
     if ((st = dal(&b->d_m, f3, "batch m")) != MJ_OK || (st = dal(&b->d_mid, f3, "batch mid")) != MJ_OK ||
         (st = dal(&b->d_aux, f3, "batch aux")) != MJ_OK || (st = dal(&b->d_E, sizeof(double) * nrep, "batch E")) != MJ_OK ||
         (st = dal(&b->d_slot_kT, sizeof(double) * nrep, "batch ladder")) != MJ_OK ||
-        (st = dal(&b->d_noise_tab, sizeof(double) * 768, "batch tables")) != MJ_OK ||
+        (st = dal(&b->d_noise_tab, sizeof(double) * kNoiseTabDoubles, "batch tables")) != MJ_OK ||
         (st = dal(&b->d_reps, sizeof(BatchRep) * nrep, "batch table")) != MJ_OK ||
         (st = dal(&b->d_image, sizeof(int) * nrep, "batch image")) != MJ_OK ||
         (st = dal(&b->d_accept, sizeof(int) * nrep, "batch accept")) != MJ_OK ||
@@ -788,9 +788,11 @@ mj_status mj_batch_create(const mj_lattice_desc* cell, const mj_hamiltonian_desc
         batch_free(b);
         return st;
     }
-    double tab[768];
-    build_noise_tables(tab);
-    cudaMemcpy(b->d_noise_tab, tab, sizeof(tab), cudaMemcpyHostToDevice);
+    {
+        std::vector<double> tab(kNoiseTabDoubles);
+        build_noise_tables(tab.data());
+        cudaMemcpy(b->d_noise_tab, tab.data(), sizeof(double) * kNoiseTabDoubles, cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(b->d_slot_kT, b->slot_kT.data(), sizeof(double) * nrep, cudaMemcpyHostToDevice);
     cudaMemcpy(b->d_image, image.data(), sizeof(int) * nrep, cudaMemcpyHostToDevice);
     cudaMemset(b->d_accept, 0, sizeof(int) * nrep);

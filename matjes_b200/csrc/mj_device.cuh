@@ -11,8 +11,10 @@ namespace mj {
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
 // as 1, 2, 3", SC'11) and Box-Muller normals.  Counter = (site, step, stream,
-// call), key = the 64-bit seed.  Two calls give two Box-Muller pairs of 53-bit
-// uniforms: (r1 cos t1, r1 sin t1, r2 cos t2).
+// 0), key = the 64-bit seed: one block per site and step, whose four 32-bit
+// words give the three normals (r1 cos t1, r1 sin t1, r2 cos t2) with
+// r = sqrt(-2 ln u), u = (w0 + 1/2) 2^-32 and (w2 + 1/2) 2^-32, and
+// t = 2 pi (w + 1/2) 2^-32 for w1 and w3.
 __device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
     const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
 #pragma unroll
@@ -32,15 +34,6 @@ __device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1
     }
 }
 
-__device__ __forceinline__ double u53_open(uint32_t a, uint32_t b) {
-    const uint64_t k = (static_cast<uint64_t>(a >> 5) << 26) | static_cast<uint64_t>(b >> 6);
-    return static_cast<double>(k + 1) * (1.0 / 9007199254740992.0);
-}
-__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
-    const uint64_t k = (static_cast<uint64_t>(a >> 5) << 26) | static_cast<uint64_t>(b >> 6);
-    return static_cast<double>(k) * (1.0 / 9007199254740992.0);
-}
-
 // Philox4x32-10 with the ten round keys precomputed (keys[2r], keys[2r+1]).
 __device__ __forceinline__ void philox10k(uint32_t c[4], const uint32_t* keys) {
     const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
@@ -57,66 +50,66 @@ __device__ __forceinline__ void philox10k(uint32_t c[4], const uint32_t* keys) {
     }
 }
 
-// Table-driven FP64 log and sin/cos of 2 pi u (our own evaluation, the same
-// arithmetic as the oracle's): tab[0..511] = (sin, cos)(2 pi i/256) pairs,
-// tab[512..767] = (1/F, ln F) pairs for F = (j + 96)/128 (j = 0..96 used).
-//   ln u = e ln2 + ln F + ln(1 + r), mantissa m in [0.75, 1.5), F the nearest
-//   multiple of 1/128, r = (m - F)/F, |r| <= 1/192, series to r^7;
-//   2 pi u = 2 pi i/256 + x, |x| < pi/128, Taylor sin to x^7 and cos to x^8.
-constexpr double kLn2 = 0.6931471805599453;        // ln 2
-constexpr double kPiOver128 = 0.02454369260617026;  // pi / 128
+// Table-driven FP64 log and sin/cos (our own evaluation, the same arithmetic
+// as the oracle's; every step is one rounded operation or an explicit fma):
+// tab[2i], tab[2i+1]         (sin, cos)(2 pi (i + 1/2)/1024),  i = 0..1023
+// tab[2048+2j], tab[2049+2j] (1/F_j, ln F_j), F_j = 1 + (j + 1/2)/1024, j = 0..1023
+//   ln u = e ln2 + ln F + ln(1 + r), u = 2^e m, m in [1, 2), j = the top ten
+//   mantissa bits, r = m/F - 1 (|r| < 1/2049), ln(1 + r) to r^4 (error below
+//   6e-18); ln u within 3 ulp plus 3e-16 absolute (above u = 1/2 it cancels
+//   against -ln 2);
+//   sin/cos(a_i + x), |x| <= pi/1024, sin x to x^5 and cos x - 1 to x^4 (errors
+//   below 1.2e-18); absolute error below 3e-16.
+constexpr double kLn2 = 0.6931471805599453;                 // ln 2
+constexpr double kTwoPiOver2p32 = 1.4629180792671596e-09;   // 2 pi / 2^32
+constexpr double kPiOver2p32 = 7.314590396335798e-10;       // pi / 2^32
+
+// 53-bit uniform in [0, 1) from two words (the parallel-tempering acceptance draw)
+__device__ __forceinline__ double u53(uint32_t a, uint32_t b) {
+    const uint64_t k = (static_cast<uint64_t>(a >> 5) << 26) | static_cast<uint64_t>(b >> 6);
+    return static_cast<double>(k) * (1.0 / 9007199254740992.0);
+}
+
+// u = (w + 1/2) 2^-32 in (0, 1), exact in double
+__device__ __forceinline__ double u32_half(uint32_t w) { return fma(static_cast<double>(w), 0x1p-32, 0x1p-33); }
 
 __device__ __forceinline__ double tab_log(double u, const double* __restrict__ tab) {
-    const long long b = __double_as_longlong(u);
-    int e = static_cast<int>((b >> 52) & 0x7ff) - 1023;
-    double m = __longlong_as_double((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
-    if (m >= 1.5) {  // centre the mantissa in [0.75, 1.5): no cancellation against e ln2 near u = 1
-        m *= 0.5;
-        e += 1;
-    }
-    const int j = static_cast<int>(m * 128.0 + 0.5);  // nearest F = j/128, j = 96..192
-    const double F = static_cast<double>(j) * (1.0 / 128.0);
-    const double2 t = __ldg(reinterpret_cast<const double2*>(tab + 512) + (j - 96));
-    const double r = (m - F) * t.x;
-    double p = fma(r, 1.0 / 7.0, -1.0 / 6.0);
-    p = fma(p, r, 1.0 / 5.0);
-    p = fma(p, r, -0.25);
-    p = fma(p, r, 1.0 / 3.0);
-    p = fma(p, r, -0.5);
+    const int hi = __double2hiint(u);
+    const int e = ((hi >> 20) & 0x7ff) - 1023;
+    const int j = (hi >> 10) & 0x3ff;
+    const double m = __hiloint2double((hi & 0x000fffff) | 0x3ff00000, __double2loint(u));
+    const double2 t = __ldg(reinterpret_cast<const double2*>(tab + 2048) + j);
+    const double r = fma(m, t.x, -1.0);
+    const double p = fma(fma(r, -0.25, 1.0 / 3.0), r, -0.5);
     const double l1p = fma(r * r, p, r);
     return fma(static_cast<double>(e), kLn2, t.y + l1p);
 }
 
-__device__ __forceinline__ void tab_sincos2pi(double u, const double* __restrict__ tab, double* s, double* c) {
-    const double t = u * 256.0;
-    const int i = static_cast<int>(t);
-    const double x = (t - static_cast<double>(i)) * kPiOver128;
+// sin and cos of 2 pi (w + 1/2) 2^-32: table point a_i = 2 pi (i + 1/2)/1024 with
+// i = w >> 22, remainder x = 2 pi ((w mod 2^22) - 2^21 + 1/2) 2^-32
+__device__ __forceinline__ void sincos2pi_word(uint32_t w, const double* __restrict__ tab, double* s, double* c) {
+    const int i = static_cast<int>(w >> 22);
+    const int d = static_cast<int>(w & 0x3fffffu) - 2097152;
+    const double x = fma(static_cast<double>(d), kTwoPiOver2p32, kPiOver2p32);
     const double x2 = x * x;
-    double ps = fma(x2, -1.0 / 5040.0, 1.0 / 120.0);
-    ps = fma(ps, x2, -1.0 / 6.0);
-    const double sx = fma(x * x2, ps, x);
-    double pc = fma(x2, 1.0 / 40320.0, -1.0 / 720.0);
-    pc = fma(pc, x2, 1.0 / 24.0);
-    pc = fma(pc, x2, -0.5);
-    const double cm = x2 * pc;
-    const double2 sc = __ldg(reinterpret_cast<const double2*>(tab) + i);
-    *s = sc.x + fma(sc.x, cm, sc.y * sx);
-    *c = sc.y + fma(sc.y, cm, -(sc.x * sx));
+    const double sx = fma(x * x2, fma(x2, 1.0 / 120.0, -1.0 / 6.0), x);
+    const double cm = x2 * fma(x2, 1.0 / 24.0, -0.5);
+    const double2 t = __ldg(reinterpret_cast<const double2*>(tab) + i);
+    *s = t.x + fma(t.x, cm, t.y * sx);
+    *c = t.y + fma(t.y, cm, -(t.x * sx));
 }
 
-// N(0,1) triple of one site and step: two Box-Muller pairs from two Philox
-// blocks, counter = (site, step, stream, call), 53-bit uniforms.
+// N(0,1) triple of one site and step from one Philox block, counter = (site,
+// step, stream, 0)
 __device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, const double* __restrict__ tab,
                                                       uint32_t step, uint32_t stream, uint32_t site) {
     uint32_t c[4] = {site, step, stream, 0u};
     philox10k(c, keys);
-    uint32_t d[4] = {site, step, stream, 1u};
-    philox10k(d, keys);
-    const double r1 = sqrt(-2.0 * tab_log(u53_open(c[0], c[1]), tab));
-    const double r2 = sqrt(-2.0 * tab_log(u53_open(d[0], d[1]), tab));
+    const double r1 = sqrt(-2.0 * tab_log(u32_half(c[0]), tab));
+    const double r2 = sqrt(-2.0 * tab_log(u32_half(c[2]), tab));
     double s1, c1, s2, c2;
-    tab_sincos2pi(u53(c[2], c[3]), tab, &s1, &c1);
-    tab_sincos2pi(u53(d[2], d[3]), tab, &s2, &c2);
+    sincos2pi_word(c[1], tab, &s1, &c1);
+    sincos2pi_word(c[3], tab, &s2, &c2);
     return make_double3(r1 * c1, r1 * s1, r2 * c2);
 }
 
@@ -146,6 +139,12 @@ __device__ __forceinline__ double3 thermal_field(const DynCoef& C, uint32_t step
 }
 
 // ---------------------------------------------------------------------------
+// A step's new spin: a non-finite component sets kStatusNonFinite in the plan's
+// status word (mj_plan_check_status then reports MJ_ERR_NAN).
+__device__ __forceinline__ void flag_nonfinite(int* status, double3 v) {
+    if (!isfinite(v.x + v.y + v.z) && status) atomicOr(status, kStatusNonFinite);
+}
+
 __device__ __forceinline__ double3 cross(double3 a, double3 b) {
     return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
@@ -165,15 +164,34 @@ __device__ __forceinline__ double3 ld_dip(const DipView& v, int x, int y, int z)
     return make_double3(__ldg(v.h + q), __ldg(v.h + v.cs + q), __ldg(v.h + 2 * v.cs + q));
 }
 
+// 1/|v| and |v| from n2 = |v|^2 for the vectors of the step, unit spins or the
+// midpoint of two (n2 = 1 - O(|h|^2)): with d = n2 - 1, |d| < 2^-20, the series
+// 1 + d (-1/2 + 3/8 d) and 1 + d (1/2 - d/8) (truncation below 3e-19 and 4e-20,
+// below a rounding), else rsqrt / sqrt.  inv_norm returns 1 for n2 <= 1e-16
+// (the 1e-8 guard of vector.f90:76-85).
+__device__ __forceinline__ double inv_norm(double n2) {
+    const double d = n2 - 1.0;
+    if (fabs(d) < 0x1p-20) return fma(d, fma(d, 0.375, -0.5), 1.0);
+    return n2 > 1e-16 ? rsqrt(n2) : 1.0;
+}
+__device__ __forceinline__ double norm_of(double n2) {
+    const double d = n2 - 1.0;
+    if (fabs(d) < 0x1p-20) return fma(d, fma(d, -0.125, 0.5), 1.0);
+    return sqrt(n2);
+}
+
+// 2/(1 + q), q = |h|^2 of a SIB stage: 2 (1 - q + q^2 - q^3) for q < 2^-14
+// (truncation below 1.4e-17 relative), else the division
+__device__ __forceinline__ double cayley_scale(double q) {
+    if (q < 0x1p-14) return fma(q, fma(q, fma(q, -2.0, 2.0), -2.0), 2.0);
+    return 2.0 / (1.0 + q);
+}
+
 // Matjes LLG right-hand side (solvers/propagator.f90:13-58):
 // D = -[m^ x B + alpha m^ x (m^ x B)] / (1 + alpha^2), m^ = m/|m| when |m| > 1e-8.
 __device__ __forceinline__ double3 llg_rhs(double3 B, double3 m, double alpha, double inv_den) {
-    const double n2 = dot(m, m);
-    double3 mn = m;
-    if (n2 > 1e-16) {
-        const double inv = rsqrt(n2);
-        mn = make_double3(m.x * inv, m.y * inv, m.z * inv);
-    }
+    const double inv = inv_norm(dot(m, m));
+    const double3 mn = make_double3(m.x * inv, m.y * inv, m.z * inv);
     const double3 t = cross(mn, B);
     const double3 l = make_double3(B.x + alpha * t.x, B.y + alpha * t.y, B.z + alpha * t.z);
     const double3 o = cross(mn, l);
@@ -182,9 +200,9 @@ __device__ __forceinline__ double3 llg_rhs(double3 B, double3 m, double alpha, d
 
 // Projection onto the old norm (solvers/solver.f90:113-116), |t| > 1e-8 guard.
 __device__ __forceinline__ double3 project(double3 t, double3 m) {
-    const double nt = sqrt(dot(t, t));
-    if (!(nt > 1e-8)) return m;
-    const double s = sqrt(dot(m, m)) / nt;
+    const double nt2 = dot(t, t);
+    if (!(nt2 > 1e-16)) return m;
+    const double s = norm_of(dot(m, m)) * inv_norm(nt2);
     return make_double3(t.x * s, t.y * s, t.z * s);
 }
 
@@ -193,17 +211,13 @@ __device__ __forceinline__ double3 project(double3 t, double3 m) {
 // Closed form (the Cayley transform of the rotation): y = m + 2/(1+|h|^2) (u + u x h),
 // u = m x h  (|y| = |m|).
 __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, double alpha, double hc) {
-    const double np2 = dot(p, p);
-    double3 pn = p;
-    if (np2 > 1e-16) {
-        const double inv = rsqrt(np2);
-        pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
-    }
+    const double inv = inv_norm(dot(p, p));
+    const double3 pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
     const double3 pxh = cross(pn, H);
     const double3 h = make_double3(hc * (H.x + alpha * pxh.x), hc * (H.y + alpha * pxh.y), hc * (H.z + alpha * pxh.z));
     const double3 u = cross(m, h);
     const double3 w = cross(u, h);
-    const double c = 2.0 / (1.0 + dot(h, h));
+    const double c = cayley_scale(dot(h, h));
     return make_double3(fma(c, u.x + w.x, m.x), fma(c, u.y + w.y, m.y), fma(c, u.z + w.z, m.z));
 }
 

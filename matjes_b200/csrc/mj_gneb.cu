@@ -152,6 +152,12 @@ mj_status mj_gneb_path(mj_plan* plan, double* m, int32_t nimg, const mj_gneb_par
     plan->prof_on = prof;
     const mj_status fin = cuda_status(cudaStreamSynchronize(s), "GNEB end");
     if (st == MJ_OK) st = fin;
+    // an image field launch whose bounded wait gave up left that image's forces
+    // unfinished: the whole path is invalid
+    int word = 0;
+    if (st == MJ_OK)
+        st = cuda_status(cudaMemcpy(&word, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost), "GNEB status");
+    if (st == MJ_OK) st = status_from_word(plan, word);
     fl.release();
     if (ready) cudaEventDestroy(ready);
     return st;

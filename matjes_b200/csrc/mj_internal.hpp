@@ -87,12 +87,13 @@ struct DynCoef {
     // graph replay: the thermal step index is *step_base + step (null = step)
     const uint32_t* step_base;
     uint32_t keys[20];          // Philox round keys of `seed`
-    const double* noise_tab;    // device tables of the Box-Muller evaluation (768 doubles)
+    const double* noise_tab;    // device tables of the Box-Muller evaluation (kNoiseTabDoubles)
 };
 
-// Box-Muller tables (host-built, identical to the oracle's): 256 (sin, cos) pairs
-// of 2 pi i/256 followed by 128 (1/F, ln F) pairs of F = 1 + j/128.
-void build_noise_tables(double* tab768);
+// Box-Muller tables (host-built, identical to the oracle's): 1024 (sin, cos) pairs
+// of 2 pi (i + 1/2)/1024 followed by 1024 (1/F, ln F) pairs of F = 1 + (j + 1/2)/1024.
+constexpr int kNoiseTabDoubles = 4096;
+void build_noise_tables(double* tab);
 
 }  // namespace mj
 
@@ -105,10 +106,10 @@ struct mj_plan {
     mj::StencilParams sp{};
     int tile_variant = 0;            // tiled-kernel shape (threads in y x sites per thread), see mj_tiled.cu
     int tiled_shape = 0;             // matched compile-time shape (sp.shape is 0 while the generic path is forced)
-    bool use_tma = true;             // tiled kernels stage halos with TMA (persistent, double-buffered)
-    int tma_blocks[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // persistent grid per tile variant (occupancy x SMs)
+    bool use_tma = true;             // tiled kernels stage tile + halo with one TMA copy per block
     int num_sms = 148;
-    int* d_status = nullptr;         // device status word: bit 0 = bounded wait timed out
+    int* d_status = nullptr;         // device status word: kStatusTimeout | kStatusNonFinite
+    int* h_status = nullptr;         // pinned host copy of it (host-array step calls)
     int defer_nblocks = 0;           // energy partials written by the last pass launched with emode 1
     // ELL form (multi-atom cells, COO input): width entries per site
     int ell_width = 0;
@@ -130,7 +131,7 @@ struct mj_plan {
     double* d_partials = nullptr;    // per-block energy partials
     unsigned int* d_counter = nullptr;
     double* d_scalar = nullptr;      // 8 doubles of device scratch
-    double* d_noise_tab = nullptr;   // Box-Muller tables (768 doubles)
+    double* d_noise_tab = nullptr;   // Box-Muller tables (kNoiseTabDoubles)
     int64_t partial_cap = 0;
     // host-array convenience calls (allocated on first use)
     double* d_stage = nullptr;       // 3N AoS staging
@@ -174,6 +175,14 @@ struct mj_state {
 };
 
 namespace mj {
+// Bits of a plan's device status word (read and cleared by mj_plan_check_status):
+// a bounded device wait gave up; a step wrote a non-finite spin component.
+constexpr int kStatusTimeout = 1;
+constexpr int kStatusNonFinite = 2;
+// The error a status word reports (MJ_OK for 0); a non-zero word is cleared on
+// the device and the energy ticket counter re-armed (mj_abi.cpp).
+mj_status status_from_word(mj_plan* p, int word);
+
 // error reporting (mj_abi.cpp)
 mj_status set_error(mj_status st, const std::string& msg);
 mj_status cuda_status(cudaError_t e, const char* where);
@@ -206,8 +215,6 @@ int64_t energy_blocks(const mj_plan* p);
 constexpr int kTiledVariants = 6;
 constexpr int kTiledVariantTY[kTiledVariants] = {16, 32, 16, 16, 16, 8};  // tile height per variant
 constexpr int kTiledVariantBYT[kTiledVariants] = {4, 8, 8, 4, 8, 4};     // warps per block per variant
-static_assert(kTiledVariants <= static_cast<int>(sizeof(mj_plan::tma_blocks) / sizeof(int)),
-              "mj_plan::tma_blocks holds one persistent grid size per tiled variant");
 // emode: energy reduction of the launch (0: into E_out at once; 1: per-block
 // partials only, counted in p->defer_nblocks; 2: block 0 sums the previous
 // pass's partials into E_out).  nty >= 0 limits the launch to the tile rows

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) k_field(const __grid_constant__ F fp, con
 template <class F>
 __global__ void __launch_bounds__(256) k_euler(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
                                                const double* __restrict__ m, double* __restrict__ mout,
-                                               const DipView Hd, Reduce R) {
+                                               const DipView Hd, Reduce R, int* status) {
     int64_t i;
     int x, y, z;
     const bool act = fp.site(i, x, y, z);
@@ -199,7 +199,9 @@ __global__ void __launch_bounds__(256) k_euler(const __grid_constant__ F fp, con
             const double3 DT = llg_rhs(thermal_field(C, step, i, N), m0, C.alpha, C.inv_den);
             t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
         }
-        st3(mout, i, N, project(t, m0));
+        const double3 mo = project(t, m0);
+        flag_nonfinite(status, mo);
+        st3(mout, i, N, mo);
     }
     if (R.out) {
         double v[1] = {e};
@@ -241,7 +243,7 @@ template <class F>
 __global__ void __launch_bounds__(256) k_heun2(const __grid_constant__ F fp, const DynCoef C,
                                                const double* __restrict__ mid, const double* __restrict__ D1,
                                                const double* __restrict__ DTi, double* __restrict__ mout,
-                                               const DipView Hd) {
+                                               const DipView Hd, int* status) {
     int64_t i;
     int x, y, z;
     if (!fp.site(i, x, y, z)) return;
@@ -258,7 +260,9 @@ __global__ void __launch_bounds__(256) k_heun2(const __grid_constant__ F fp, con
         const double3 DT = ld3(DTi, i, N);
         t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
     }
-    st3(mout, i, N, project(t, mt));
+    const double3 mo = project(t, mt);
+    flag_nonfinite(status, mo);
+    st3(mout, i, N, mo);
 }
 
 // SIB pass 1: Cayley predictor from m_n with A(m_n); writes the midpoint (m_n + m~)/2.
@@ -293,7 +297,8 @@ __global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, cons
 // SIB pass 2: corrector from m_n with A(midpoint); in place (only the own site of m is read).
 template <class F>
 __global__ void __launch_bounds__(256) k_sib2(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
-                                              const double* __restrict__ mid, double* m, const DipView Hd) {
+                                              const double* __restrict__ mid, double* m, const DipView Hd,
+                                              int* status) {
     int64_t i;
     int x, y, z;
     if (!fp.site(i, x, y, z)) return;
@@ -307,7 +312,9 @@ __global__ void __launch_bounds__(256) k_sib2(const __grid_constant__ F fp, cons
         H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
     }
     const double3 m0 = make_double3(m[i], m[N + i], m[2 * N + i]);
-    st3(m, i, N, sib_solve(m0, mb, H, C.alpha, C.sib_hc));
+    const double3 mo = sib_solve(m0, mb, H, C.alpha, C.sib_hc);
+    flag_nonfinite(status, mo);
+    st3(m, i, N, mo);
 }
 
 // Reference temperature estimator (dynamics/measure_temp.f90:21-43): sum |m x B|^2, sum m.B.
@@ -460,7 +467,7 @@ mj_status step_impl(mj_plan* p, const Launch<F>& L, double* m, double* m_out, co
         case MJ_EULER: {
             DipView Hd = dip_field(p, m, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_euler", k_euler<F>, L.fp, c, step, m, m_out, Hd, make_reduce(p, E_prev));
+            MJ_LAUNCH("k_euler", k_euler<F>, L.fp, c, step, m, m_out, Hd, make_reduce(p, E_prev), p->d_status);
             return MJ_OK;
         }
         case MJ_HEUN_MATJES: {
@@ -469,7 +476,7 @@ mj_status step_impl(mj_plan* p, const Launch<F>& L, double* m, double* m_out, co
             MJ_LAUNCH("k_heun1", k_heun1<F>, L.fp, c, step, m, p->d_mid, p->d_aux, p->d_aux2, Hd, make_reduce(p, E_prev));
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_heun2", k_heun2<F>, L.fp, c, p->d_mid, p->d_aux, p->d_aux2, m, Hd);
+            MJ_LAUNCH("k_heun2", k_heun2<F>, L.fp, c, p->d_mid, p->d_aux, p->d_aux2, m, Hd, p->d_status);
             return MJ_OK;
         }
         case MJ_SIB: {
@@ -478,7 +485,7 @@ mj_status step_impl(mj_plan* p, const Launch<F>& L, double* m, double* m_out, co
             MJ_LAUNCH("k_sib1", k_sib1<F>, L.fp, c, step, m, p->d_mid, Hd, make_reduce(p, E_prev));
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_sib2", k_sib2<F>, L.fp, c, step, p->d_mid, m, Hd);
+            MJ_LAUNCH("k_sib2", k_sib2<F>, L.fp, c, step, p->d_mid, m, Hd, p->d_status);
             return MJ_OK;
         }
         default:
@@ -598,11 +605,12 @@ mj_status launch_philox(uint64_t seed, uint32_t step, uint32_t stream_id, int64_
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return set_error(MJ_ERR_ARG, "device index out of range");
     if (!tabs[dev]) {
-        double h[768];
-        build_noise_tables(h);
-        mj_status st = cuda_status(cudaMalloc(&tabs[dev], sizeof(h)), "philox tables");
+        std::vector<double> h(kNoiseTabDoubles);
+        build_noise_tables(h.data());
+        const size_t bytes = sizeof(double) * kNoiseTabDoubles;
+        mj_status st = cuda_status(cudaMalloc(&tabs[dev], bytes), "philox tables");
         if (st != MJ_OK) return st;
-        if ((st = cuda_status(cudaMemcpy(tabs[dev], h, sizeof(h), cudaMemcpyHostToDevice), "philox tables")) != MJ_OK)
+        if ((st = cuda_status(cudaMemcpy(tabs[dev], h.data(), bytes, cudaMemcpyHostToDevice), "philox tables")) != MJ_OK)
             return st;
     }
     k_philox<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(seed, step, stream_id, n, out, tabs[dev]);

@@ -317,15 +317,15 @@ bool build_blocks(const Geometry& g, const mj_hamiltonian_desc& h, std::vector<B
 void build_noise_tables(double* tab) {
     // evaluated in extended precision, then rounded once to double
     const long double two_pi = 6.283185307179586476925286766559005768L;
-    for (int i = 0; i < 256; ++i) {
-        const long double a = two_pi * static_cast<long double>(i) / 256.0L;
+    for (int i = 0; i < 1024; ++i) {
+        const long double a = two_pi * (static_cast<long double>(i) + 0.5L) / 1024.0L;
         tab[2 * i] = static_cast<double>(sinl(a));
         tab[2 * i + 1] = static_cast<double>(cosl(a));
     }
-    for (int j = 0; j < 128; ++j) {
-        const long double F = static_cast<long double>(j + 96) / 128.0L;  // used for j + 96 = 96..192
-        tab[512 + 2 * j] = static_cast<double>(1.0L / F);
-        tab[512 + 2 * j + 1] = static_cast<double>(logl(F));
+    for (int j = 0; j < 1024; ++j) {
+        const long double F = 1.0L + (static_cast<long double>(j) + 0.5L) / 1024.0L;
+        tab[2048 + 2 * j] = static_cast<double>(1.0L / F);
+        tab[2048 + 2 * j + 1] = static_cast<double>(logl(F));
     }
 }
 

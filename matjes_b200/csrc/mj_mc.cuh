@@ -29,8 +29,9 @@ constexpr uint32_t kMcTag = 0x4D43u;  // "MC"
 __device__ __forceinline__ double u32_open(uint32_t w) { return (static_cast<double>(w) + 0.5) * (1.0 / 4294967296.0); }
 
 // sphereft: a direction in the cone of half-angle `cone` about s; sin and cos of
-// phi = 2 pi u2 from the tables of the thermal draw (tab_sincos2pi, <= 8e-16)
-__device__ __forceinline__ double3 cone_proposal(double3 s, double cos_cone, double u1, double u2,
+// phi = 2 pi (w2 + 1/2) 2^-32 from the tables of the thermal draw
+// (sincos2pi_word, absolute error below 3e-16)
+__device__ __forceinline__ double3 cone_proposal(double3 s, double cos_cone, double u1, uint32_t w2,
                                                  const double* __restrict__ tab) {
     const double ct = u1 + cos_cone * (1.0 - u1);
     const double st = sqrt(1.0 - ct * ct);
@@ -44,7 +45,7 @@ __device__ __forceinline__ double3 cone_proposal(double3 s, double cos_cone, dou
         spi = s.y * inv;
     }
     double sph, cph;
-    tab_sincos2pi(u2, tab, &sph, &cph);
+    sincos2pi_word(w2, tab, &sph, &cph);
     const double t = st * sph * cti + ct * sti;
     const double3 n = make_double3(-st * cph * spi + t * cpi, st * cph * cpi + t * spi, -st * sph * sti + ct * cti);
     const double inv_n = 1.0 / sqrt(dot(n, n));
@@ -132,7 +133,7 @@ __device__ __forceinline__ double onsite_energy(const StencilParams& P, double3 
 __device__ __forceinline__ double3 propose(int proposal, double3 s, double3 B, double cos_cone, const uint32_t c[4],
                                            const double* __restrict__ tab) {
     if (proposal == MJ_MC_ISING) return make_double3(-s.x, -s.y, -s.z);
-    if (proposal == MJ_MC_CONE) return cone_proposal(s, cos_cone, u32_open(c[0]), u32_open(c[1]), tab);
+    if (proposal == MJ_MC_CONE) return cone_proposal(s, cos_cone, u32_open(c[0]), c[1], tab);
     const double sb = dot(s, B);
     double3 n;
     if (proposal == MJ_MC_UNDERRELAX) n = make_double3(s.x * (1.0 - sb) + B.x, s.y * (1.0 - sb) + B.y, s.z * (1.0 - sb) + B.z);

@@ -1,8 +1,32 @@
-// Dispatch of the tiled kernels to the translation unit of the plan's shape.
+// Dispatch of the tiled kernels to the translation unit of the plan's shape,
+// and the self-test of their bounded-wait failure path.
 #include "mj_internal.hpp"
 #include "mj_shapes.hpp"
+#include "mj_tiled_impl.cuh"
 
 namespace mj {
+namespace {
+
+// One block arms an mbarrier for 16 bytes that no copy delivers (no TMA is
+// issued, so nothing is in flight), gives up after `polls` polls through the
+// same bounded wait as k_tiled, and records the timeout as k_tiled does.
+__global__ void k_selftest_timeout(uint32_t polls, int* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_expect_tx(&bar, 16u);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, polls);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(status, kStatusTimeout);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
+}
+
+}  // namespace
 
 int64_t tiled_energy_blocks(const mj_plan* p) {
     const int v = (p->tile_variant >= 0 && p->tile_variant < kTiledVariants) ? p->tile_variant : 0;
@@ -33,3 +57,13 @@ mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms,
 }
 
 }  // namespace mj
+
+using namespace mj;
+
+extern "C" mj_status mj_plan_selftest_timeout(mj_plan* plan, uint32_t polls, void* stream) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    if (polls < 1 || polls > (1u << 16)) return set_error(MJ_ERR_ARG, "polls must be in [1, 65536]");
+    cudaSetDevice(plan->device);
+    k_selftest_timeout<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(polls, plan->d_status);
+    return cuda_status(cudaGetLastError(), "k_selftest_timeout");
+}

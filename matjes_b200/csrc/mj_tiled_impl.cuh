@@ -8,17 +8,21 @@
 // thread's RY sites that sees it.  Offsets and tensor slots are compile-time
 // constants; the coupling values come from the launch parameters.
 //
-// Two kernels share that compute:
-//   k_tiled : one tile per block, halo staged with plain loads (periodic wrap
-//             resolved per element);
-//   k_tma   : persistent blocks walking a strided tile list with two shared
-//             buffers; the halo box of the next tile is fetched by one
-//             cp.async.bulk.tensor (TMA, 4D: x, y, z, component) completing on
-//             an mbarrier while the current tile computes.  Tiles whose halo
-//             wraps around a periodic edge take the plain-load path; on open
-//             axes the TMA zero fill of out-of-range cells is the open boundary.
-// The halo along x is rounded up to an even width so that every TMA box starts
-// on a 16-byte boundary.
+// k_tiled stages the tile + halo either with plain loads (periodic wrap resolved
+// per element) or with one cp.async.bulk.tensor (TMA, 4D box: x, y, z,
+// component) completing on an mbarrier, while the threads compute the inputs
+// of their epilogue (the thermal draw); on open axes the TMA zero fill of
+// out-of-range cells is the open boundary, and the halo cells of a tile that
+// wrap around a periodic edge are then rewritten with plain loads.  The halo
+// along x is rounded up to an even width so that every TMA box starts on a
+// 16-byte boundary.  No cluster multicast anywhere.
+//
+// Sparsity (template SP): with SP_AXIAL every anisotropic offset tensor has
+// W[0][1] = W[1][0] = 0 (exchange plus a DMI vector in the lattice plane), the
+// on-site tensor is zero but for W0[2][2] (uniaxial anisotropy along z) and a
+// uniform applied field points along z; the kernels then skip the products with
+// those zeros (7 instead of 9 per anisotropic neighbour, 1 instead of 9 on
+// site).  SP_FULL is the general form.  The host picks the form per launch.
 #pragma once
 
 #include <cuda.h>
@@ -38,6 +42,7 @@ namespace mj {
 namespace {
 
 enum { PASS_FIELD = 0, PASS_EULER = 1, PASS_HEUN1 = 2, PASS_HEUN2 = 3, PASS_SIB1 = 4, PASS_SIB2 = 5 };
+enum { SP_FULL = 0, SP_AXIAL = 1 };
 
 // Energy reduction of a launch.  mode 0: grid_reduce into `out` (if set);
 // mode 1: write one partial per block, no ticket (the next pass sums them);
@@ -61,9 +66,10 @@ struct TiledArgs {
     TReduce R;
     uint32_t step;
     int* status;        // device status word (bounded-wait timeouts)
-    int ty0;            // first tile row of a launch over a range of tile rows (k_tiled)
+    int ty0;            // first tile row of a launch over a range of tile rows
     int nty_all;        // tile rows of the whole lattice (0: the launch covers all of them)
     int ty_count;       // tile rows of this launch (host side: its grid height)
+    int tma;            // 1: tile + halo staged by TMA through the kernel's tensor map
 };
 
 template <class S, int BYT, int RY>
@@ -81,7 +87,7 @@ struct TileGeom {
 
 // ---------------------------------------------------------------------------
 // stencil accumulation, fully unrolled over compile-time offsets
-template <class S, int RY, int DX, int YY, int... Kk>
+template <class S, int RY, int DX, int YY, int SP, int... Kk>
 __device__ __forceinline__ void row_accumulate(const StencilParams& P, double vx, double vy, double vz, double* bx,
                                                double* by, double* bz, std::integer_sequence<int, Kk...>) {
     (
@@ -96,6 +102,10 @@ __device__ __forceinline__ void row_accumulate(const StencilParams& P, double vx
                         bx[r] = fma(w, vx, bx[r]);
                         by[r] = fma(w, vy, by[r]);
                         bz[r] = fma(w, vz, bz[r]);
+                    } else if constexpr (SP == SP_AXIAL) {  // W[1] = W[3] = 0
+                        bx[r] = fma(W[0], vx, fma(W[2], vz, bx[r]));
+                        by[r] = fma(W[4], vy, fma(W[5], vz, by[r]));
+                        bz[r] = fma(W[6], vx, fma(W[7], vy, fma(W[8], vz, bz[r])));
                     } else {
                         bx[r] = fma(W[0], vx, fma(W[1], vy, fma(W[2], vz, bx[r])));
                         by[r] = fma(W[3], vx, fma(W[4], vy, fma(W[5], vz, by[r])));
@@ -107,7 +117,7 @@ __device__ __forceinline__ void row_accumulate(const StencilParams& P, double vx
         ...);
 }
 
-template <class S, int BYT, int RY, int DX, int... Y>
+template <class S, int BYT, int RY, int DX, int SP, int... Y>
 __device__ __forceinline__ void column_rows(const StencilParams& P, const double* sm, int base, double* bx, double* by,
                                             double* bz, std::integer_sequence<int, Y...>) {
     using G = TileGeom<S, BYT, RY>;
@@ -116,13 +126,13 @@ __device__ __forceinline__ void column_rows(const StencilParams& P, const double
         [&] {
             constexpr int yy = ylo + Y;
             const int s = base + (yy + G::R) * G::PX + DX + G::RX;
-            row_accumulate<S, RY, DX, yy>(P, sm[s], sm[G::NS + s], sm[2 * G::NS + s], bx, by, bz,
-                                          std::make_integer_sequence<int, S::K>{});
+            row_accumulate<S, RY, DX, yy, SP>(P, sm[s], sm[G::NS + s], sm[2 * G::NS + s], bx, by, bz,
+                                              std::make_integer_sequence<int, S::K>{});
         }(),
         ...);
 }
 
-template <class S, int BYT, int RY, int... C>
+template <class S, int BYT, int RY, int SP = SP_FULL, int... C>
 __device__ __forceinline__ void all_columns(const StencilParams& P, const double* sm, int base, double* bx, double* by,
                                             double* bz, std::integer_sequence<int, C...>) {
     (
@@ -130,8 +140,8 @@ __device__ __forceinline__ void all_columns(const StencilParams& P, const double
             constexpr int dx = C - S::R;
             constexpr int ylo = shape_col_ymin<S>(dx), yhi = shape_col_ymax<S>(dx);
             if constexpr (ylo <= yhi) {
-                column_rows<S, BYT, RY, dx>(P, sm, base, bx, by, bz,
-                                            std::make_integer_sequence<int, RY + yhi - ylo>{});
+                column_rows<S, BYT, RY, dx, SP>(P, sm, base, bx, by, bz,
+                                                std::make_integer_sequence<int, RY + yhi - ylo>{});
             }
         }(),
         ...);
@@ -164,14 +174,33 @@ __device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, in
     return p;
 }
 
-template <int PASS>
+// Contribution of one site to H%energy: -m.Bmm/2 - m.Bzee (+ m.Hd with the dipolar
+// term, counted once; fft_ham_base.f90:258-267), B = Bmm + Bzee the real-space field.
+template <bool HD>
+__device__ __forceinline__ double energy_part(double3 B, double3 Bzee, double3 m, double3 hd) {
+    const double e = -0.5 * (dot(m, B) + dot(m, Bzee));
+    if constexpr (HD) return e + dot(m, hd);
+    return e;
+}
+
+// The pass's update of one site.  B = the real-space field (MM + Zeeman), Bzee
+// its Zeeman part, hd the dipolar H (HD); returns the site's energy part where
+// the pass computes one.
+template <int PASS, bool HD>
 __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N, double3 m0,
-                                           const FieldOut& f, double3 hd, const Pre& pre) {
-    const double3 B = make_double3(f.B.x - 2.0 * hd.x, f.B.y - 2.0 * hd.y, f.B.z - 2.0 * hd.z);
+                                           double3 Brs, double3 Bzee, double3 hd, const Pre& pre) {
+    double3 B = Brs;
+    if constexpr (HD) B = make_double3(Brs.x - 2.0 * hd.x, Brs.y - 2.0 * hd.y, Brs.z - 2.0 * hd.z);
     if constexpr (PASS == PASS_FIELD) {
         if (A.out) st3(A.out, i, N, B);
-        if (A.aux) A.aux[i] = site_energy(f, m0, hd);
-        return total_energy_part(f, m0, hd);
+        // per-site energy (energy_distrib, left-assigned; hamiltonian_collection.f90:332-363):
+        // the dipolar term doubled as in fft_ham_base.f90:247-256
+        if (A.aux) {
+            double es = -0.5 * (dot(m0, Brs) + dot(m0, Bzee));
+            if constexpr (HD) es += 2.0 * dot(m0, hd);
+            A.aux[i] = es;
+        }
+        return energy_part<HD>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_EULER) {
         const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double c = C.h_over_hbar;
@@ -180,8 +209,10 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
             const double3 DT = llg_rhs(pre.b, m0, C.alpha, C.inv_den);
             t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
         }
-        st3(A.out, i, N, project(t, m0));
-        return total_energy_part(f, m0, hd);
+        const double3 mo = project(t, m0);
+        flag_nonfinite(A.status, mo);
+        st3(A.out, i, N, mo);
+        return energy_part<HD>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_HEUN1) {
         const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double c = C.h_over_hbar;
@@ -189,7 +220,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         st3(A.out, i, N, project(t, m0));
         st3(A.aux, i, N, D);
         if (C.thermal) st3(A.aux2, i, N, llg_rhs(pre.b, m0, C.alpha, C.inv_den));
-        return total_energy_part(f, m0, hd);
+        return energy_part<HD>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_HEUN2) {
         const double3 D2 = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double3 d1 = pre.a;
@@ -200,7 +231,9 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
             const double3 DT = pre.b;
             t = make_double3(t.x + DT.x * c, t.y + DT.y * c, t.z + DT.z * c);
         }
-        st3(A.out, i, N, project(t, m0));
+        const double3 mo = project(t, m0);
+        flag_nonfinite(A.status, mo);
+        st3(A.out, i, N, mo);
         return 0.0;
     } else if constexpr (PASS == PASS_SIB1) {
         double3 H = B;
@@ -211,11 +244,13 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         }
         const double3 y = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
         st3(A.out, i, N, make_double3(0.5 * (m0.x + y.x), 0.5 * (m0.y + y.y), 0.5 * (m0.z + y.z)));
-        return total_energy_part(f, m0, hd);
+        return energy_part<HD>(Brs, Bzee, m0, hd);
     } else {  // PASS_SIB2: m0 is the midpoint, the corrector starts from m_n
         double3 H = B;
         if (C.thermal) H = make_double3(H.x + pre.b.x, H.y + pre.b.y, H.z + pre.b.z);
-        st3(A.out, i, N, sib_solve(pre.a, m0, H, C.alpha, C.sib_hc));
+        const double3 mo = sib_solve(pre.a, m0, H, C.alpha, C.sib_hc);
+        flag_nonfinite(A.status, mo);
+        st3(A.out, i, N, mo);
         return 0.0;
     }
 }
@@ -252,6 +287,34 @@ __device__ __forceinline__ void load_tile(const StencilParams& P, const double* 
         sm[idx] = vx;
         sm[G::NS + idx] = vy;
         sm[2 * G::NS + idx] = vz;
+    }
+}
+
+// After a TMA box landed with zeros outside the lattice: rewrite the halo cells
+// that lie across a periodic edge with the wrapped spins (cells across an open
+// edge keep the zeros).
+template <class S, int BYT, int RY>
+__device__ __forceinline__ void patch_periodic_halo(const StencilParams& P, const double* ms, int x0, int y0, int z,
+                                                    double* sm) {
+    using G = TileGeom<S, BYT, RY>;
+    const int Lx = P.L[0], Ly = P.L[1];
+    const int64_t layer = static_cast<int64_t>(Lx) * Ly;
+    const int64_t N = layer * P.L[2];
+    const double* mx = ms + layer * z;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    for (int idx = tid; idx < G::NS; idx += 32 * BYT) {
+        const int ly = idx / G::PX;
+        const int lx = idx - ly * G::PX;
+        int gx = x0 + lx - G::RX, gy = y0 + ly - G::R;
+        const bool outx = gx < 0 || gx >= Lx, outy = gy < 0 || gy >= Ly;
+        if (!(outx || outy)) continue;                      // inside: the TMA copy holds it
+        if ((outx && !P.periodic[0]) || (outy && !P.periodic[1])) continue;  // open edge: zero
+        if (outx) gx = ((gx % Lx) + Lx) % Lx;
+        if (outy) gy = ((gy % Ly) + Ly) % Ly;
+        const int64_t j = gx + static_cast<int64_t>(Lx) * gy;
+        sm[idx] = __ldg(mx + j);
+        sm[G::NS + idx] = __ldg(mx + N + j);
+        sm[2 * G::NS + idx] = __ldg(mx + 2 * N + j);
     }
 }
 
@@ -337,29 +400,19 @@ __device__ __forceinline__ void prefetch_sites(const StencilParams& P, const Dyn
     }
 }
 
-// stencil + epilogue of one staged tile; returns the energy of its sites
-// (pre_in: the epilogue inputs when the caller prefetched them, else null)
-template <class S, int BYT, int RY, int PASS>
-__device__ __forceinline__ double compute_tile(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
-                                               const double* sm, int x0, int y0, int z, const Pre* pre_in = nullptr) {
+// The epilogues of the thread's RY sites from the accumulated pair fields;
+// ZMAP: per-cell applied field, HD: dipolar term.
+template <class S, int BYT, int RY, int PASS, int SP, bool ZMAP, bool HD>
+__device__ __forceinline__ double sites_epilogue(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
+                                                 const double* sm, int x0, int y0, int z, const Pre* pre,
+                                                 const double* bx, const double* by, const double* bz) {
     using G = TileGeom<S, BYT, RY>;
     const int Lx = P.L[0], Ly = P.L[1];
     const int64_t layer = static_cast<int64_t>(Lx) * Ly;
     const int64_t N = layer * P.L[2];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x = x0 + tx;
-    Pre pre[RY];
-    if (pre_in) {
-#pragma unroll
-        for (int r = 0; r < RY; ++r) pre[r] = pre_in[r];
-    } else {
-        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
-    }
-    double bx[RY], by[RY], bz[RY];
-#pragma unroll
-    for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
     const int base = (ty * RY) * G::PX + tx;
-    all_columns<S, BYT, RY>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
     double e = 0.0;
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
@@ -371,58 +424,51 @@ __device__ __forceinline__ double compute_tile(const StencilParams& P, const Dyn
             double b0 = bx[r], b1 = by[r], b2 = bz[r];
             if (P.has_onsite) {
                 const double* W = P.W0;
-                b0 = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, b0)));
-                b1 = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, b1)));
-                b2 = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, b2)));
+                if constexpr (SP == SP_AXIAL) {
+                    b2 = fma(W[8], m0.z, b2);
+                } else {
+                    b0 = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, b0)));
+                    b1 = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, b1)));
+                    b2 = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, b2)));
+                }
             }
-            FieldOut f;
-            f.Bzee = make_double3(0.0, 0.0, 0.0);
+            double3 Bzee = make_double3(0.0, 0.0, 0.0);
             if (P.zee_on) {
-                double3 b;
-                if (A.bmap) b = make_double3(__ldg(A.bmap + i), __ldg(A.bmap + N + i), __ldg(A.bmap + 2 * N + i));
-                else b = make_double3(P.bext[0], P.bext[1], P.bext[2]);
-                f.Bzee = make_double3(P.zc * b.x, P.zc * b.y, P.zc * b.z);
+                if constexpr (ZMAP) {
+                    Bzee = make_double3(P.zc * __ldg(A.bmap + i), P.zc * __ldg(A.bmap + N + i),
+                                        P.zc * __ldg(A.bmap + 2 * N + i));
+                } else if constexpr (SP == SP_AXIAL) {
+                    Bzee.z = P.zc * P.bext[2];
+                } else {
+                    Bzee = make_double3(P.zc * P.bext[0], P.zc * P.bext[1], P.zc * P.bext[2]);
+                }
             }
-            f.B = make_double3(b0 + f.Bzee.x, b1 + f.Bzee.y, b2 + f.Bzee.z);
-            const double3 hd = A.Hd.h ? ld_dip(A.Hd, x, y, z) : make_double3(0.0, 0.0, 0.0);
-            e += epilogue<PASS>(C, A, i, N, m0, f, hd, pre[r]);
+            const double3 Brs = make_double3(b0 + Bzee.x, b1 + Bzee.y, b2 + Bzee.z);
+            double3 hd = make_double3(0.0, 0.0, 0.0);
+            if constexpr (HD) hd = ld_dip(A.Hd, x, y, z);
+            e += epilogue<PASS, HD>(C, A, i, N, m0, Brs, Bzee, hd, pre[r]);
         }
     }
     return e;
 }
 
-template <class S, int BYT, int RY, int PASS, int MINB>
-__global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant__ StencilParams P, const DynCoef C,
-                                                     const TiledArgs A) {
+// stencil + epilogue of one staged tile; returns the energy of its sites
+template <class S, int BYT, int RY, int PASS, int SP>
+__device__ __forceinline__ double compute_tile(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
+                                               const double* sm, int x0, int y0, int z, const Pre* pre) {
     using G = TileGeom<S, BYT, RY>;
-    extern __shared__ __align__(128) double smem_t[];
-    // a launch may cover the tile rows [ty0, ty0 + gridDim.y) of nty_all; block ids
-    // (energy partials) are those of the launch over the whole lattice
-    const int by = static_cast<int>(blockIdx.y) + A.ty0;
-    const int nty = A.nty_all ? A.nty_all : static_cast<int>(gridDim.y);
-    const int x0 = blockIdx.x * G::TX, y0 = by * G::TY, z = blockIdx.z;
-    const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
-    if (A.R.mode == 2 && bid == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
-    Pre pre[RY];
-    if constexpr (Staged<S, BYT, RY>::NPT <= kMaxStagedPerThread) {
-        // halo loads in flight while the epilogue inputs (the thermal draw) are computed
-        Staged<S, BYT, RY> st;
-        load_tile_issue<S, BYT, RY>(P, A.ms, x0, y0, z, st);
-        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
-        load_tile_commit<S, BYT, RY>(st, smem_t);
-    } else {
-        load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
-        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+    double bx[RY], by[RY], bz[RY];
+#pragma unroll
+    for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
+    const int base = (threadIdx.y * RY) * G::PX + threadIdx.x;
+    all_columns<S, BYT, RY, SP>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
+    // the branches are uniform over the launch
+    if (A.bmap) {
+        if (A.Hd.h) return sites_epilogue<S, BYT, RY, PASS, SP, true, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
+        return sites_epilogue<S, BYT, RY, PASS, SP, true, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
     }
-    __syncthreads();
-    const double e = compute_tile<S, BYT, RY, PASS>(P, C, A, smem_t, x0, y0, z, pre);
-    if (A.R.mode == 1) {
-        double v[1] = {e};
-        block_partials<1>(v, A.R.partials, A.R.nblocks, bid);
-    } else if (A.R.mode == 0 && A.R.out) {
-        double v[1] = {e};
-        grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
-    }
+    if (A.Hd.h) return sites_epilogue<S, BYT, RY, PASS, SP, false, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
+    return sites_epilogue<S, BYT, RY, PASS, SP, false, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
 }
 
 // ---------------------------------------------------------------------------
@@ -464,101 +510,70 @@ __device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* ba
         : "memory");
 }
 
-struct TileList {
-    int ntx, nty, nz;
-    __device__ __forceinline__ int count() const { return ntx * nty * nz; }
-};
+// Poll limit of the wait for a tile's TMA copy (about 0.3 s with the 64 ns
+// sleeps); far above any copy's latency.
+constexpr uint32_t kTmaWaitPolls = 1u << 22;
 
-template <class G>
-__device__ __forceinline__ bool tma_ok(const StencilParams& P, int x0, int y0) {
-    // a halo crossing a periodic edge needs wrap-around: plain loads
-    if (P.periodic[0] && (x0 - G::RX < 0 || x0 + G::TX + G::RX > P.L[0])) return false;
-    if (P.periodic[1] && (y0 - G::R < 0 || y0 + G::TY + G::R > P.L[1])) return false;
-    return true;
-}
-
-template <class S, int BYT, int RY, int PASS, int MINB>
-__global__ void __launch_bounds__(32 * BYT, MINB) k_tma(const __grid_constant__ CUtensorMap tmap,
-                                                   const __grid_constant__ StencilParams P, const DynCoef C,
-                                                   const TiledArgs A, const TileList T) {
+template <class S, int BYT, int RY, int PASS, int MINB, int SP>
+__global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant__ CUtensorMap tmap,
+                                                     const __grid_constant__ StencilParams P, const DynCoef C,
+                                                     const TiledArgs A) {
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_t[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar;
+    // a launch may cover the tile rows [ty0, ty0 + gridDim.y) of nty_all; block ids
+    // (energy partials) are those of the launch over the whole lattice
+    const int by = static_cast<int>(blockIdx.y) + A.ty0;
+    const int nty = A.nty_all ? A.nty_all : static_cast<int>(gridDim.y);
+    const int x0 = blockIdx.x * G::TX, y0 = by * G::TY, z = blockIdx.z;
+    const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
     const int tid = threadIdx.x + 32 * threadIdx.y;
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (A.R.mode == 2 && blockIdx.x == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
-    const int ntile = T.count();
-    auto origin = [&](int t, int& x0, int& y0, int& z) {
-        const int ix = t % T.ntx;
-        const int r = t / T.ntx;
-        x0 = ix * G::TX;
-        y0 = (r % T.nty) * G::TY;
-        z = r / T.nty;
-    };
-    auto issue = [&](int t, int b) {
-        int x0, y0, z;
-        origin(t, x0, y0, z);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[b], static_cast<uint32_t>(G::buf_bytes));
-        tma_load_4d(&tmap, &bar[b], smem_t + static_cast<size_t>(b) * G::buf_stride_d, x0 - G::RX, y0 - G::R, z, 0);
-    };
-    uint32_t phase[2] = {0u, 0u};
-    double e = 0.0;
-    bool failed = false;
-    int t = blockIdx.x;
-    bool cur_tma = false;
-    if (t < ntile) {
-        int x0, y0, z;
-        origin(t, x0, y0, z);
-        cur_tma = tma_ok<G>(P, x0, y0);
-        if (tid == 0 && cur_tma) issue(t, 0);
-    }
-    for (int it = 0; t < ntile; ++it, t += gridDim.x) {
-        const int b = it & 1;
-        const int tn = t + gridDim.x;
-        bool next_tma = false;
-        if (tn < ntile) {
-            int x1, y1, z1;
-            origin(tn, x1, y1, z1);
-            next_tma = tma_ok<G>(P, x1, y1);
-            if (tid == 0 && next_tma) issue(tn, b ^ 1);  // that buffer was released at the end of it-1
+    if (A.R.mode == 2 && bid == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
+    Pre pre[RY];
+    bool ok = true;
+    if (A.tma) {
+        // one copy of the whole box; the epilogue inputs (the thermal draw) are
+        // computed while it is in flight
+        if (tid == 0) {
+            mbar_init(&bar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bar, static_cast<uint32_t>(G::buf_bytes));
+            tma_load_4d(&tmap, &bar, smem_t, x0 - G::RX, y0 - G::R, z, 0);
         }
-        int x0, y0, z;
-        origin(t, x0, y0, z);
-        double* sm = smem_t + static_cast<size_t>(b) * G::buf_stride_d;
-        if (cur_tma) {
-            const bool ok = mbar_wait_bounded(&bar[b], phase[b], 1u << 22);
-            if (__syncthreads_or(!ok)) {  // the whole block agrees before leaving the loop
-                failed = true;
-                if (tid == 0 && A.status) atomicOr(A.status, 1);
-                break;
-            }
-            phase[b] ^= 1u;
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+        __syncthreads();  // the barrier's initialisation is visible to every waiting thread
+        ok = mbar_wait_bounded(&bar, 0u, kTmaWaitPolls);
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            if (tid == 0 && A.status) atomicOr(A.status, kStatusTimeout);
+            // let the copy land before the block leaves (bounded), then only the
+            // energy reduction below runs, so every block still takes part in it
+            mbar_wait_bounded(&bar, 0u, 1u << 16);
         } else {
-            load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, sm);
-            __syncthreads();
+            const bool wraps = (P.periodic[0] && (x0 - G::RX < 0 || x0 + G::TX + G::RX > P.L[0])) ||
+                               (P.periodic[1] && (y0 - G::R < 0 || y0 + G::TY + G::R > P.L[1]));
+            if (wraps) {
+                patch_periodic_halo<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
+                __syncthreads();
+            }
         }
-        e += compute_tile<S, BYT, RY, PASS>(P, C, A, sm, x0, y0, z);
+    } else if constexpr (Staged<S, BYT, RY>::NPT <= kMaxStagedPerThread) {
+        // halo loads in flight while the epilogue inputs (the thermal draw) are computed
+        Staged<S, BYT, RY> st;
+        load_tile_issue<S, BYT, RY>(P, A.ms, x0, y0, z, st);
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+        load_tile_commit<S, BYT, RY>(st, smem_t);
         __syncthreads();
-        cur_tma = next_tma;
+    } else {
+        load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
+        prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+        __syncthreads();
     }
-    if (failed) {
-        // let copies still in flight land before the block exits (bounded)
-        for (int b = 0; b < 2; ++b) mbar_wait_bounded(&bar[b], phase[b], 1u << 16);
-        if (A.R.mode == 1) {  // keep the partials complete; the status word reports the failure
-            double v[1] = {e};
-            block_partials<1>(v, A.R.partials, A.R.nblocks, blockIdx.x);
-        }
-        return;
-    }
+    const double e = ok ? compute_tile<S, BYT, RY, PASS, SP>(P, C, A, smem_t, x0, y0, z, pre) : 0.0;
     if (A.R.mode == 1) {
         double v[1] = {e};
-        block_partials<1>(v, A.R.partials, A.R.nblocks, blockIdx.x);
+        block_partials<1>(v, A.R.partials, A.R.nblocks, bid);
     } else if (A.R.mode == 0 && A.R.out) {
         double v[1] = {e};
         grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
@@ -574,61 +589,36 @@ struct TiledLauncher {
     static dim3 grid(const StencilParams& P) {
         return dim3((P.L[0] + G::TX - 1) / G::TX, (P.L[1] + G::TY - 1) / G::TY, P.L[2]);
     }
-    template <int PASS>
-    static mj_status launch(const StencilParams& P, const DynCoef& C, const TiledArgs& A, cudaStream_t s) {
-        auto kern = k_tiled<S, BYT, RY, PASS, MINB>;
+    template <int PASS, int SP>
+    static mj_status launch(const CUtensorMap& map, const StencilParams& P, const DynCoef& C, const TiledArgs& A,
+                            cudaStream_t s) {
+        auto kern = k_tiled<S, BYT, RY, PASS, MINB, SP>;
         dim3 g = grid(P);
         if (A.nty_all) g.y = static_cast<unsigned>(A.ty_count);  // a range of tile rows
-        kern<<<g, dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
+        kern<<<g, dim3(32, BYT), G::buf_bytes, s>>>(map, P, C, A);
         return cuda_status(cudaGetLastError(), "k_tiled");
-    }
-    template <int PASS>
-    static mj_status launch_tma(const CUtensorMap& map, const StencilParams& P, const DynCoef& C, TiledArgs A,
-                                int nblocks, cudaStream_t s) {
-        auto kern = k_tma<S, BYT, RY, PASS, MINB>;
-        const size_t smem = 2 * G::buf_stride;
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            attr = true;
-        }
-        const dim3 g = grid(P);
-        TileList T{static_cast<int>(g.x), static_cast<int>(g.y), static_cast<int>(g.z)};
-        if (A.R.mode != 2) A.R.nblocks = nblocks;  // mode 2 reads the previous pass's partial count
-        kern<<<nblocks, dim3(32, BYT), smem, s>>>(map, P, C, A, T);
-        return cuda_status(cudaGetLastError(), "k_tma");
-    }
-    static int persistent_blocks(int sms) {
-        int per = 0;
-        auto kern = k_tma<S, BYT, RY, PASS_SIB1, MINB>;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(2 * G::buf_stride));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * BYT, 2 * G::buf_stride);
-        return sms * (per > 0 ? per : 1);
     }
 };
 
-template <class S, int BYT, int RY, int MINB>
-mj_status tiled_pass(int pass, const StencilParams& P, const DynCoef& C, const TiledArgs& A, const CUtensorMap* map,
-                     int nblocks, cudaStream_t s) {
+template <class S, int BYT, int RY, int MINB, int SP>
+mj_status tiled_pass_sp(int pass, const CUtensorMap& map, const StencilParams& P, const DynCoef& C, const TiledArgs& A,
+                        cudaStream_t s) {
     using L = TiledLauncher<S, BYT, RY, MINB>;
-    if (map) {
-        switch (pass) {
-            case PASS_FIELD: return L::template launch_tma<PASS_FIELD>(*map, P, C, A, nblocks, s);
-            case PASS_EULER: return L::template launch_tma<PASS_EULER>(*map, P, C, A, nblocks, s);
-            case PASS_HEUN1: return L::template launch_tma<PASS_HEUN1>(*map, P, C, A, nblocks, s);
-            case PASS_HEUN2: return L::template launch_tma<PASS_HEUN2>(*map, P, C, A, nblocks, s);
-            case PASS_SIB1: return L::template launch_tma<PASS_SIB1>(*map, P, C, A, nblocks, s);
-            default: return L::template launch_tma<PASS_SIB2>(*map, P, C, A, nblocks, s);
-        }
-    }
     switch (pass) {
-        case PASS_FIELD: return L::template launch<PASS_FIELD>(P, C, A, s);
-        case PASS_EULER: return L::template launch<PASS_EULER>(P, C, A, s);
-        case PASS_HEUN1: return L::template launch<PASS_HEUN1>(P, C, A, s);
-        case PASS_HEUN2: return L::template launch<PASS_HEUN2>(P, C, A, s);
-        case PASS_SIB1: return L::template launch<PASS_SIB1>(P, C, A, s);
-        default: return L::template launch<PASS_SIB2>(P, C, A, s);
+        case PASS_FIELD: return L::template launch<PASS_FIELD, SP>(map, P, C, A, s);
+        case PASS_EULER: return L::template launch<PASS_EULER, SP>(map, P, C, A, s);
+        case PASS_HEUN1: return L::template launch<PASS_HEUN1, SP>(map, P, C, A, s);
+        case PASS_HEUN2: return L::template launch<PASS_HEUN2, SP>(map, P, C, A, s);
+        case PASS_SIB1: return L::template launch<PASS_SIB1, SP>(map, P, C, A, s);
+        default: return L::template launch<PASS_SIB2, SP>(map, P, C, A, s);
     }
+}
+
+template <class S, int BYT, int RY, int MINB>
+mj_status tiled_pass(int pass, bool axial, const CUtensorMap& map, const StencilParams& P, const DynCoef& C,
+                     const TiledArgs& A, cudaStream_t s) {
+    if (axial) return tiled_pass_sp<S, BYT, RY, MINB, SP_AXIAL>(pass, map, P, C, A, s);
+    return tiled_pass_sp<S, BYT, RY, MINB, SP_FULL>(pass, map, P, C, A, s);
 }
 
 // tile variants: (threads in y, sites per thread, min resident blocks per SM);
@@ -643,6 +633,18 @@ auto with_variant(int variant, F&& f) {
         case 5: return f(TiledLauncher<S, 4, 2, 8>{});
         default: return f(TiledLauncher<S, 4, 4, 1>{});
     }
+}
+
+// The sparsity form of a launch (SP_AXIAL when every zero it assumes holds).
+template <class S>
+bool stencil_axial(const StencilParams& sp, bool has_bmap) {
+    for (int k = 0; k < S::K; ++k)
+        if (S::ISO[k] == 0 && (sp.W[k][1] != 0.0 || sp.W[k][3] != 0.0)) return false;
+    if (sp.has_onsite)
+        for (int q = 0; q < 8; ++q)
+            if (sp.W0[q] != 0.0) return false;
+    if (sp.zee_on && !has_bmap && (sp.bext[0] != 0.0 || sp.bext[1] != 0.0)) return false;
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -705,30 +707,23 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
     if (emode == 2) A.R.nblocks = p->defer_nblocks;  // the partials of the previous pass
     A.step = step;
     A.status = p->d_status;
+    const bool axial = stencil_axial<S>(p->sp, p->d_bmap != nullptr);
     return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
         using Launcher = decltype(L);
         using G = typename Launcher::G;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
         if (nty >= 0) {  // tile rows [ty0, ty0 + nty) only, plain staging
             A.ty0 = ty0;
             A.nty_all = static_cast<int>(Launcher::grid(p->sp).y);
             A.ty_count = nty;
             if (nty == 0) return MJ_OK;
-            if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
-            return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, nullptr, 0, s);
-        }
-        if (p->use_tma) {
-            CUtensorMap map;
-            if (make_map(&map, ms, p->sp, G::PX, G::PY)) {
-                if (p->tma_blocks[p->tile_variant] <= 0)
-                    p->tma_blocks[p->tile_variant] = Launcher::persistent_blocks(p->num_sms);
-                const int nb = static_cast<int>(std::min<int64_t>(p->tma_blocks[p->tile_variant], tiled_energy_blocks(p)));
-                if (emode == 1) p->defer_nblocks = nb;
-                return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, &map,
-                                                                                           nb, s);
-            }
+        } else if (p->use_tma && make_map(&map, ms, p->sp, G::PX, G::PY)) {
+            A.tma = 1;
         }
         if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
-        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, p->sp, C, A, nullptr, 0, s);
+        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, axial, map,
+                                                                                                   p->sp, C, A, s);
     });
 }
 

@@ -705,79 +705,63 @@ static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
         c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
     }
 }
-/* 53-bit uniforms: open (0,1] for the logarithm, [0,1) for the angle */
-static double u53_open(uint32_t a, uint32_t b) {
-    uint64_t k = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
-    return (double)(k + 1) * (1.0 / 9007199254740992.0);
-}
-static double u53(uint32_t a, uint32_t b) {
-    uint64_t k = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);
-    return (double)k * (1.0 / 9007199254740992.0);
-}
-/* Box-Muller with table-driven FP64 log and sin/cos of 2 pi u (the same
- * evaluation as the product's, explicit fma, no contraction):
- *   tab[0..511]   (sin, cos)(2 pi i/256), i = 0..255
- *   tab[512..767] (1/F, ln F), F = (j + 96)/128, j = 0..127 (96..192 used)
- *   ln u = e ln2 + ln F + ln(1 + r), m in [0.75, 1.5), F the nearest j/128,
- *   r = (m - F)/F, |r| <= 1/192, series to r^7
- *   sin/cos(2 pi i/256 + x), |x| < pi/128, Taylor to x^7 / x^8. */
-static double g_tab[768];
+/* Box-Muller with table-driven FP64 log and sin/cos (the same evaluation as the
+ * product's: every step one rounded operation or an explicit fma, no contraction):
+ *   tab[2i], tab[2i+1]         (sin, cos)(2 pi (i + 1/2)/1024), i = 0..1023
+ *   tab[2048+2j], tab[2049+2j] (1/F_j, ln F_j), F_j = 1 + (j + 1/2)/1024
+ *   ln u = e ln2 + ln F + ln(1 + r), u = 2^e m, m in [1, 2), j = the top ten
+ *   mantissa bits, r = m/F - 1, ln(1 + r) to r^4;
+ *   sin/cos(a_i + x) for 2 pi (w + 1/2) 2^-32, i = w >> 22, |x| <= pi/1024,
+ *   sin x to x^5, cos x - 1 to x^4.
+ * One Philox block per site and step, counter (site, step, stream, 0):
+ *   (r1 cos t1, r1 sin t1, r2 cos t2), r = sqrt(-2 ln u), u = (w0 + 1/2) 2^-32,
+ *   (w2 + 1/2) 2^-32, t = 2 pi (w + 1/2) 2^-32 for w1, w3. */
+static double g_tab[4096];
 static int g_tab_ready = 0;
 #define LN2_D 0.6931471805599453
-#define PI_OVER_128 0.02454369260617026
+#define TWO_PI_OVER_2P32 1.4629180792671596e-09
+#define PI_OVER_2P32 7.314590396335798e-10
 
 static void noise_tables(void) {
     if (g_tab_ready) return;
     const long double two_pi = 6.283185307179586476925286766559005768L;
-    for (int i = 0; i < 256; i++) {
-        long double a = two_pi * (long double)i / 256.0L;
+    for (int i = 0; i < 1024; i++) {
+        long double a = two_pi * ((long double)i + 0.5L) / 1024.0L;
         g_tab[2 * i] = (double)sinl(a);
         g_tab[2 * i + 1] = (double)cosl(a);
     }
-    for (int j = 0; j < 128; j++) {
-        long double F = (long double)(j + 96) / 128.0L; /* used for j + 96 = 96..192 */
-        g_tab[512 + 2 * j] = (double)(1.0L / F);
-        g_tab[512 + 2 * j + 1] = (double)logl(F);
+    for (int j = 0; j < 1024; j++) {
+        long double F = 1.0L + ((long double)j + 0.5L) / 1024.0L;
+        g_tab[2048 + 2 * j] = (double)(1.0L / F);
+        g_tab[2048 + 2 * j + 1] = (double)logl(F);
     }
     g_tab_ready = 1;
 }
+
+/* u = (w + 1/2) 2^-32, exact */
+static double u32_half(uint32_t w) { return fma((double)w, 0x1p-32, 0x1p-33); }
 
 static double tab_log(double u) {
     uint64_t b;
     memcpy(&b, &u, 8);
     int e = (int)((b >> 52) & 0x7ff) - 1023;
+    int j = (int)((b >> 42) & 0x3ff);
     uint64_t mb = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
     double m;
     memcpy(&m, &mb, 8);
-    if (m >= 1.5) { /* centre the mantissa in [0.75, 1.5): no cancellation against e ln2 near u = 1 */
-        m *= 0.5;
-        e += 1;
-    }
-    int j = (int)(m * 128.0 + 0.5); /* nearest F_j = j/128, j = 96..192 */
-    double F = (double)j * (1.0 / 128.0);
-    j -= 96;
-    double r = (m - F) * g_tab[512 + 2 * j];
-    double p = fma(r, 1.0 / 7.0, -1.0 / 6.0);
-    p = fma(p, r, 1.0 / 5.0);
-    p = fma(p, r, -0.25);
-    p = fma(p, r, 1.0 / 3.0);
-    p = fma(p, r, -0.5);
+    double r = fma(m, g_tab[2048 + 2 * j], -1.0);
+    double p = fma(fma(r, -0.25, 1.0 / 3.0), r, -0.5);
     double l1p = fma(r * r, p, r);
-    return fma((double)e, LN2_D, g_tab[512 + 2 * j + 1] + l1p);
+    return fma((double)e, LN2_D, g_tab[2048 + 2 * j + 1] + l1p);
 }
 
-static void tab_sincos2pi(double u, double* s, double* c) {
-    double t = u * 256.0;
-    int i = (int)t;
-    double x = (t - (double)i) * PI_OVER_128;
+static void sincos2pi_word(uint32_t w, double* s, double* c) {
+    int i = (int)(w >> 22);
+    int d = (int)(w & 0x3fffffu) - 2097152;
+    double x = fma((double)d, TWO_PI_OVER_2P32, PI_OVER_2P32);
     double x2 = x * x;
-    double ps = fma(x2, -1.0 / 5040.0, 1.0 / 120.0);
-    ps = fma(ps, x2, -1.0 / 6.0);
-    double sx = fma(x * x2, ps, x);
-    double pc = fma(x2, 1.0 / 40320.0, -1.0 / 720.0);
-    pc = fma(pc, x2, 1.0 / 24.0);
-    pc = fma(pc, x2, -0.5);
-    double cm = x2 * pc;
+    double sx = fma(x * x2, fma(x2, 1.0 / 120.0, -1.0 / 6.0), x);
+    double cm = x2 * fma(x2, 1.0 / 24.0, -0.5);
     double S = g_tab[2 * i], Cc = g_tab[2 * i + 1];
     *s = S + fma(S, cm, Cc * sx);
     *c = Cc + fma(Cc, cm, -(S * sx));
@@ -787,23 +771,22 @@ static void philox_site(uint64_t seed, uint32_t step, uint32_t stream, uint32_t 
     uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
     uint32_t c[4] = {site, step, stream, 0u};
     philox4x32_10(c, k0, k1);
-    uint32_t d[4] = {site, step, stream, 1u};
-    philox4x32_10(d, k0, k1);
-    double r1 = sqrt(-2.0 * tab_log(u53_open(c[0], c[1])));
-    double r2 = sqrt(-2.0 * tab_log(u53_open(d[0], d[1])));
+    double r1 = sqrt(-2.0 * tab_log(u32_half(c[0])));
+    double r2 = sqrt(-2.0 * tab_log(u32_half(c[2])));
     double s1, c1, s2, c2;
-    tab_sincos2pi(u53(c[2], c[3]), &s1, &c1);
-    tab_sincos2pi(u53(d[2], d[3]), &s2, &c2);
+    sincos2pi_word(c[1], &s1, &c1);
+    sincos2pi_word(c[3], &s2, &c2);
     (void)s2;
     out[0] = r1 * c1;
     out[1] = r1 * s1;
     out[2] = r2 * c2;
 }
-void orc_tab_eval(const double* u, int64_t n, double* lg, double* s, double* c) {
+
+void orc_tab_eval(const uint32_t* w, int64_t n, double* lg, double* s, double* c) {
     noise_tables();
     for (int64_t i = 0; i < n; i++) {
-        lg[i] = u[i] > 0.0 ? tab_log(u[i]) : 0.0;
-        tab_sincos2pi(u[i] < 1.0 ? u[i] : 0.0, s + i, c + i);
+        lg[i] = tab_log(u32_half(w[i]));
+        sincos2pi_word(w[i], s + i, c + i);
     }
 }
 
@@ -1063,14 +1046,15 @@ int orc_minimize_infdamp(const orc_model* M, double* m, double conv_torque, int6
 static double mc_u32(uint32_t w) { return ((double)w + 0.5) * (1.0 / 4294967296.0); }
 
 /* sphereft (paratemp-MC/sampling.f90:9-62): cos(theta) uniform in [cos(cone), 1],
- * phi = 2 pi u2, the new direction rotated from the z frame onto the old spin;
- * sin and cos of phi from the tables of the thermal draw (tab_sincos2pi) */
-static void mc_sphereft(const double* s, double cos_cone, double u1, double u2, double* out) {
+ * phi = 2 pi (w2 + 1/2) 2^-32, the new direction rotated from the z frame onto
+ * the old spin; sin and cos of phi from the tables of the thermal draw
+ * (sincos2pi_word) */
+static void mc_sphereft(const double* s, double cos_cone, double u1, uint32_t w2, double* out) {
     double ct = u1 + cos_cone * (1.0 - u1);
     double st = sqrt(1.0 - ct * ct);
     double sph, cph;
     noise_tables();
-    tab_sincos2pi(u2, &sph, &cph);
+    sincos2pi_word(w2, &sph, &cph);
     double cti = s[2], rxy2 = s[0] * s[0] + s[1] * s[1], sti = sqrt(rxy2);
     double cpi = 1.0, spi = 0.0;
     if (!(rxy2 < 0.00001)) { cpi = s[0] / sqrt(rxy2); spi = s[1] / sqrt(rxy2); }
@@ -1082,10 +1066,10 @@ static void mc_sphereft(const double* s, double cos_cone, double u1, double u2, 
 
 /* the proposals of Metropolis-MC/track_value.f90 (sample_sphere, sample_ising,
  * sample_underrelax, sample_overrelax -> relaxationtype.f90); B = -dE/dm of the site */
-static void mc_propose(int proposal, const double* s, const double* B, double cos_cone, double u1, double u2,
+static void mc_propose(int proposal, const double* s, const double* B, double cos_cone, double u1, uint32_t w2,
                        double* out) {
     if (proposal == 1) { for (int k = 0; k < 3; k++) out[k] = -s[k]; return; }
-    if (proposal == 0) { mc_sphereft(s, cos_cone, u1, u2, out); return; }
+    if (proposal == 0) { mc_sphereft(s, cos_cone, u1, w2, out); return; }
     double sb = s[0] * B[0] + s[1] * B[1] + s[2] * B[2], n[3];
     if (proposal == 2) for (int k = 0; k < 3; k++) n[k] = s[k] * (1.0 - sb) + B[k];
     else for (int k = 0; k < 3; k++) n[k] = B[k] - s[k] * (1.0 + sb);
@@ -1153,7 +1137,7 @@ int orc_mc_sweeps(const orc_model* M, double* m, orc_mc* p, int nsweeps, const i
                 orc_philox4x32(c, key, w);
                 double B[3], sn[3];
                 site_field(M, m, i, B);
-                mc_propose(p->proposal, m + 3 * i, B, cos_cone, mc_u32(w[0]), mc_u32(w[1]), sn);
+                mc_propose(p->proposal, m + 3 * i, B, cos_cone, mc_u32(w[0]), w[1], sn);
                 double dE = mc_delta_energy(M, m, i, sn, B);
                 if (mc_accept(kT, dE, mc_u32(w[2]))) {
                     for (int q = 0; q < 3; q++) m[3 * i + q] = sn[q];
@@ -1196,7 +1180,7 @@ int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double*
                                          1e-4);
             double B[3], sn[3];
             site_field(M, m, i, B);
-            mc_propose(p->proposal, m + 3 * i, B, cos(p->cone), mc_u32(w[1]), mc_u32(w[2]), sn);
+            mc_propose(p->proposal, m + 3 * i, B, cos(p->cone), mc_u32(w[1]), w[2], sn);
             double dE = mc_delta_energy(M, m, i, sn, B);
             p->proposed_total++;
             if (mc_accept(kT, dE, mc_u32(w[3]))) {

@@ -178,8 +178,9 @@ void orc_field_terms(const orc_model* m, const double* mvec, double* B_mm, doubl
 /* Explicit O(N^2) dipolar field (get_dipolar, mag_dip_fft F). */
 void orc_dipolar_explicit_field(const orc_model* m, const double* mvec, double* B);
 
-/* The table-driven log(u) and sin/cos(2 pi u) of the Box-Muller draw (u in (0,1)). */
-void orc_tab_eval(const double* u, int64_t n, double* lg, double* s, double* c);
+/* The table-driven log(u) and sin/cos(2 pi u) of the Box-Muller draw for
+ * u = (w + 1/2) 2^-32 of 32-bit words w. */
+void orc_tab_eval(const uint32_t* w, int64_t n, double* lg, double* s, double* c);
 /* Raw Philox4x32-10 block (for the Random123 known-answer vectors). */
 void orc_philox4x32(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* Philox4x32-10 N(0,1) triples, identical counter layout to the product. */

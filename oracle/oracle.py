@@ -343,11 +343,12 @@ def philox4x32(ctr, key):
     return [int(x) for x in out]
 
 
-def tab_eval(u):
-    """(log u, sin 2 pi u, cos 2 pi u) through the Box-Muller tables."""
-    u = np.ascontiguousarray(u, np.float64)
-    lg, s, c = np.empty_like(u), np.empty_like(u), np.empty_like(u)
-    lib.orc_tab_eval(u.ctypes.data, u.size, lg.ctypes.data, s.ctypes.data, c.ctypes.data)
+def tab_eval(w):
+    """(log u, sin 2 pi u, cos 2 pi u) of u = (w + 1/2) 2^-32 for 32-bit words w,
+    through the Box-Muller tables."""
+    w = np.ascontiguousarray(w, np.uint32)
+    lg, s, c = (np.empty(w.size) for _ in range(3))
+    lib.orc_tab_eval(w.ctypes.data, w.size, lg.ctypes.data, s.ctypes.data, c.ctypes.data)
     return lg, s, c
 
 

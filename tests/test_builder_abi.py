@@ -30,6 +30,29 @@ def test_every_header_symbol_is_exported_and_bound():
     assert set(_abi.SIGNATURES) <= set(syms)
 
 
+def test_fortran_binding_names_header_symbols():
+    """fortran/matjes_gpu.f90 (the bind(c) module of the Fortran driver; no
+    Fortran compiler exists here to build it) binds only names that the header
+    declares and the library exports, each with as many dummy arguments as the
+    C prototype has parameters."""
+    import re
+
+    src = open(os.path.join(ROOT, "fortran", "matjes_gpu.f90")).read()
+    hdr = open(os.path.join(ROOT, "include", "matjes_gpu.h")).read()
+    syms = header_symbols()
+    lib = C.CDLL(_abi.LIB_PATH)
+    binds = re.findall(r"function\s+(\w+)\(([^)]*)\)\s*(?:&\s*\n\s*)?bind\(c,\s*name=\"(\w+)\"\)", src)
+    assert len(binds) >= 30
+    for fname, args, cname in binds:
+        if cname == "strlen":
+            continue
+        assert fname == cname and cname in syms and hasattr(lib, cname), cname
+        proto = re.search(r"\b%s\(([^;()]*)\);" % cname, hdr).group(1)
+        nparams = 0 if proto.strip() == "void" else proto.count(",") + 1
+        nargs = len([a for a in args.split(",") if a.strip()])
+        assert nargs == nparams, (cname, nargs, nparams)
+
+
 def test_version_and_error_strings():
     assert b"sm_100a" in _abi.lib.mj_version()
     assert isinstance(_abi.lib.mj_last_error(), bytes)
