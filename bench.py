@@ -409,29 +409,47 @@ def run_adjoint(dev: int, reps: int = 3) -> dict:
             "adjoint_path": "forward and backward sweeps replayed as CUDA graphs"}
 
 
+def dipolar_alg_bytes(N: int, nrep) -> float:
+    """Compulsory bytes of one FFT dipolar evaluation (FP64, 3 components): pad
+    (read 24 N, write 24 Np), D2Z (read 24 Np, write 48 Nc), pointwise (read the
+    symmetric complex K_F 96 Nc and M_F 48 Nc, write 48 Nc), Z2D (read 48 Nc,
+    write 24 Np), unpack (read H 24 N, read and write B 48 N); Np = prod(N_rep),
+    Nc = Np / N_rep,x * (N_rep,x / 2 + 1).  About 140 MB on the 128 x 128 x 32
+    grid of the 128 x 128 x 16 film."""
+    Np = int(np.prod(nrep))
+    Nc = Np // nrep[0] * (nrep[0] // 2 + 1)
+    return 24.0 * N + 24.0 * Np + 24.0 * Np + 48.0 * Nc + 96.0 * Nc + 48.0 * Nc + 48.0 * Nc + 48.0 * Nc + \
+        24.0 * Np + 24.0 * N + 48.0 * N
+
+
 def run_dipolar(dev: int, steps: int = 50) -> dict:
     """The dipolar film (128 x 128 x 16 simple cubic, a = 0.25 nm, periodic in-plane,
-    open along z, J + D + K + Zeeman + FFT dipolar on the 128 x 128 x 32 grid, SIB
-    alpha = 0.1, T = 5 K Philox): one system, and 8 systems with their own initial
-    states (seeds 4..11) advanced concurrently on 8 CUDA streams."""
+    open along z, J + D + K + Zeeman + FFT dipolar, SIB alpha = 0.1, T = 5 K
+    Philox) on the reference's grid (128 x 128 x 32) and on the fully zero-padded
+    one (256 x 256 x 32, the grid BASELINE's configuration names): one system
+    each, and on the reference's grid 8 systems with their own initial states
+    (seeds 4..11) advanced concurrently on 8 CUDA streams.  Each grid's dipolar
+    evaluation (pad, transforms, pointwise product; the unpack is fused into the
+    passes) gets its roofline against dipolar_alg_bytes."""
     import torch
 
     import matjes_b200 as mj
     from matjes_b200 import _abi
     from matjes_b200.deck import workload
 
-    w = workload("film128x16_dipolar")
-    deck, d = w["deck"], dict(w["dyn"])
-    d.pop("steps")
-    N = deck.nsites
+    lib = _abi.lib
+    pk = peaks()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    systems = []
-    for k in range(8):
+
+    def make(dip, k):
+        w = workload("film128x16_dipolar")
+        deck, d = w["deck"], dict(w["dyn"])
+        d.pop("steps")
+        deck.dip = dip
         ham = mj.Hamiltonian(deck, device=dev)
         sd = mj.SpinDynamics(ham, stream_id=k, **d)
-        m = torch.tensor(mj.random_sphere(N, 4 + k).T.copy(), device=f"cuda:{dev}")
-        systems.append((ham, sd, m, torch.cuda.Stream(device=dev)))
-    lib = _abi.lib
+        m = torch.tensor(mj.random_sphere(deck.nsites, 4 + k).T.copy(), device=f"cuda:{dev}")
+        return ham, sd, m, torch.cuda.Stream(device=dev)
 
     def run(sys_list, nsteps, concurrent):
         for ham, sd, m, st in sys_list:
@@ -452,19 +470,34 @@ def run_dipolar(dev: int, steps: int = 50) -> dict:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    one = timed(systems[:1], False)
-    ham0 = systems[0][0]
-    _abi.check(lib.mj_profile_enable(ham0.plan, 1))
-    run(systems[:1], 5, False)
-    prof = _abi.profile_read(ham0.plan)
-    _abi.check(lib.mj_profile_enable(ham0.plan, 0))
-    eight = timed(systems, True)
-    tot = sum(t for t, _ in prof.values())
-    return {"workload": "film128x16_dipolar", "sites": N, "steps": steps, "fft_grid": [128, 128, 32],
-            "value": N * steps / (one / 1e3), "unit": UNIT, "ms_per_step": one / steps,
-            "batch8": {"value": 8 * N * steps / (eight / 1e3), "ms_per_step": eight / steps,
-                       "path": "8 plans, mj_step_dev on 8 CUDA streams"},
-            "kernel_share": {k: round(t / tot, 4) for k, (t, _) in prof.items()}}
+    out = {"workload": "film128x16_dipolar", "steps": steps}
+    for dip, key in ((1, "reference_grid"), (2, "padded_grid")):
+        one = make(dip, 0)
+        ham = one[0]
+        N = ham.N
+        t = timed([one], False)
+        _abi.check(lib.mj_profile_enable(ham.plan, 1))
+        run([one], 5, False)
+        prof = _abi.profile_read(ham.plan)
+        _abi.check(lib.mj_profile_enable(ham.plan, 0))
+        tot = sum(v for v, _ in prof.values())
+        nrep = (128, 128, 32) if dip == 1 else (256, 256, 32)
+        d_ms, d_n = prof.get("dipolar_fft", (0.0, 1))
+        per_eval = d_ms / max(d_n, 1)
+        b = dipolar_alg_bytes(N, nrep)
+        out[key] = {"fft_grid": list(nrep), "sites": N, "value": N * steps / (t / 1e3), "unit": UNIT,
+                    "ms_per_step": t / steps, "kernel_share": {k: round(v / tot, 4) for k, (v, _) in prof.items()},
+                    "dipolar_eval": {"us": 1e3 * per_eval, "alg_bytes": b, "achieved_gbs": b / (per_eval / 1e3) / 1e9,
+                                     "frac": b / (per_eval / 1e3) / 1e9 / pk["hbm_gbs"], "peak_source": pk["source"]}}
+        if dip == 1:
+            systems = [one] + [make(1, k) for k in range(1, 8)]
+            eight = timed(systems, True)
+            out[key]["batch8"] = {"value": 8 * N * steps / (eight / 1e3), "ms_per_step": eight / steps,
+                                  "path": "8 plans, mj_step_dev on 8 CUDA streams"}
+            del systems
+        del one
+    out["value"] = out["reference_grid"]["value"]
+    return out
 
 
 def run_hbm_resident(dev: int, steps: int = 20) -> dict:
@@ -934,6 +967,8 @@ def run_gpu(args, rank, world):
             "adjoint_cost_ratio": round(a["cost_ratio"], 3),
             "adjoint_cost_ratio_vs_graph_forward": round(a["cost_ratio_vs_graph_forward"], 3),
             "dipolar_spin_updates_per_s": d["value"],
+            "dipolar_padded_grid_spin_updates_per_s": d["padded_grid"]["value"],
+            "dipolar_eval_roofline_frac": round(d["reference_grid"]["dipolar_eval"]["frac"], 4),
             "hbm_resident_4096_step_roofline_frac": round(extras["hbm_resident_4096"]["step_roofline"]["frac"], 4)})
     if cpu:
         summ["cpu_baseline_spin_updates_per_s"] = cpu["value"]

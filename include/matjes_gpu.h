@@ -69,7 +69,13 @@ typedef struct {
     double c_H_J, c_H_D, c_H_ani, c_zeeman; /* reference defaults: -1, -1, +1, -1 */
     double B_ext[3];                        /* H_ext (Tesla) */
     int32_t zeeman_on;                      /* enable_H; also on when |H_ext| >= 1e-8 */
-    int32_t dip_on;                         /* mag_dip_use (FFT route) */
+    int32_t dip_on;                         /* mag_dip_use (FFT route): 1 = the reference's grid
+                                               (Hamiltonian_type/fft_ham_base.f90:204-214: open axes
+                                               doubled, periodic axes kept, images folded in); 2 = every
+                                               axis longer than one cell zero-padded to 2 L (a linear
+                                               convolution, images summed over -cut..cut for every pair
+                                               as in the explicit route dipolar_magnetic.f90:181-273;
+                                               no counterpart flag in the reference) */
     int32_t dip_period_cut[3];              /* mag_dip_period_cut, default 1 1 1 */
 } mj_hamiltonian_desc;
 

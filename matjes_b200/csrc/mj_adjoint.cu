@@ -198,8 +198,7 @@ __global__ void __launch_bounds__(256) k_adj_f1(const __grid_constant__ StencilP
     const int64_t N = static_cast<int64_t>(P.L[0]) * P.L[1] * P.L[2];
     const double3 m0 = ld3(m, i, N);
     const double3 H = add3(add3(w_apply(P, m, N, x, y, z, m0), zeeman(P, bmap, i, N)), noise(C, step, i, N));
-    const double3 yv = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
-    st3(mb, i, N, make_double3(0.5 * (m0.x + yv.x), 0.5 * (m0.y + yv.y), 0.5 * (m0.z + yv.z)));
+    st3(mb, i, N, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
 }
 
 __global__ void __launch_bounds__(256) k_adj_f2(const __grid_constant__ StencilParams P, const DynCoef C, uint32_t step,

@@ -186,8 +186,7 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
                     st3(A.aux, i, Nt, b);
                     H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
                 }
-                const double3 yv = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
-                st3(A.out, i, Nt, make_double3(0.5 * (m0.x + yv.x), 0.5 * (m0.y + yv.y), 0.5 * (m0.z + yv.z)));
+                st3(A.out, i, Nt, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
             } else {
                 double3 H = f.B;
                 if (thermal) H = make_double3(H.x + pre[r].b.x, H.y + pre[r].b.y, H.z + pre[r].b.z);

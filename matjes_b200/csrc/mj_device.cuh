@@ -210,6 +210,8 @@ __device__ __forceinline__ double3 project(double3 t, double3 m) {
 // y = m + ((m + y)/2) x a,  h = a/2 = hc (H + alpha p^ x H), hc = -dt/(2 hbar (1+alpha^2)).
 // Closed form (the Cayley transform of the rotation): y = m + 2/(1+|h|^2) (u + u x h),
 // u = m x h  (|y| = |m|).
+// MID: the predictor's midpoint (m + y)/2 = m + c/2 (u + u x h) instead of y.
+template <bool MID = false>
 __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, double alpha, double hc) {
     const double inv = inv_norm(dot(p, p));
     const double3 pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
@@ -217,7 +219,8 @@ __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, do
     const double3 h = make_double3(hc * (H.x + alpha * pxh.x), hc * (H.y + alpha * pxh.y), hc * (H.z + alpha * pxh.z));
     const double3 u = cross(m, h);
     const double3 w = cross(u, h);
-    const double c = cayley_scale(dot(h, h));
+    double c = cayley_scale(dot(h, h));
+    if constexpr (MID) c = 0.5 * c;
     return make_double3(fma(c, u.x + w.x, m.x), fma(c, u.y + w.y, m.y), fma(c, u.z + w.z, m.z));
 }
 

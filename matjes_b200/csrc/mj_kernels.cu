@@ -285,8 +285,7 @@ __global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, cons
             const double3 b = thermal_field(C, step, i, N);
             H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
         }
-        const double3 yv = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
-        st3(mid, i, N, make_double3(0.5 * (m0.x + yv.x), 0.5 * (m0.y + yv.y), 0.5 * (m0.z + yv.z)));
+        st3(mid, i, N, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
     }
     if (R.out) {
         double v[1] = {e};

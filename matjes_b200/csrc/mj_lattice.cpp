@@ -335,11 +335,17 @@ bool build_dipolar_kernel(const Geometry& g, const mj_hamiltonian_desc& h, int n
         err = "the FFT dipolar kernel supports one magnetic atom per cell";
         return false;
     }
+    // grid rule: dip_on 1 is the reference's (Hamiltonian_type/fft_ham_base.f90:204-214,
+    // open axes doubled, periodic axes kept with their images folded in circularly);
+    // dip_on 2 zero-pads every axis longer than one cell to 2 L, so that the
+    // convolution is linear and each pair's image sum runs over the symmetric
+    // window -cut..cut (the explicit route of Energy/dipolar_magnetic.f90:181-273)
+    const bool full = h.dip_on == 2;
     int kb0[3], kb1[3];
     for (int d = 0; d < 3; ++d) {
-        const bool per = g.d.periodic[d] || g.d.L[d] == 1;
-        nrep[d] = per ? g.d.L[d] : 2 * g.d.L[d];
-        kb0[d] = per ? 0 : -g.d.L[d] + 1;
+        const bool keep = g.d.L[d] == 1 || (g.d.periodic[d] && !full);
+        nrep[d] = keep ? g.d.L[d] : 2 * g.d.L[d];
+        kb0[d] = keep ? 0 : -g.d.L[d] + 1;
         kb1[d] = g.d.L[d] - 1;
     }
     const int64_t nk = static_cast<int64_t>(nrep[0]) * nrep[1] * nrep[2];

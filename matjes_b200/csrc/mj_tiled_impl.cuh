@@ -242,8 +242,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
             if (A.aux) st3(A.aux, i, N, b);  // the corrector reuses this step's draw
             H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
         }
-        const double3 y = sib_solve(m0, m0, H, C.alpha, C.sib_hc);
-        st3(A.out, i, N, make_double3(0.5 * (m0.x + y.x), 0.5 * (m0.y + y.y), 0.5 * (m0.z + y.z)));
+        st3(A.out, i, N, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
         return energy_part<HD>(Brs, Bzee, m0, hd);
     } else {  // PASS_SIB2: m0 is the midpoint, the corrector starts from m_n
         double3 H = B;

@@ -42,7 +42,7 @@ class Deck:
     K: List[Tuple[int, Vec3, float]] = field(default_factory=list)
     B_ext: Vec3 = (0.0, 0.0, 0.0)
     zeeman_on: bool = False
-    dip: bool = False
+    dip: int = 0  # FFT dipolar term: 0 off, 1 the reference's grid rule, 2 zero-padded to 2 L on every axis
     dip_cut: Tuple[int, int, int] = (1, 1, 1)
     c_H_J: float = -1.0
     c_H_D: float = -1.0
@@ -111,7 +111,7 @@ class Deck:
             h.B_ext[k] = float(self.B_ext[k])
             h.dip_period_cut[k] = int(self.dip_cut[k])
         h.zeeman_on = int(bool(self.zeeman_on))
-        h.dip_on = int(bool(self.dip))
+        h.dip_on = int(self.dip)
         return lat, h, (J, D, K)
 
 

@@ -42,7 +42,12 @@ struct orc_model {
     int nrep[3];
     int64_t nk;
     double* K; /* [nk][3nmag][3nmag], K[k][r][c] = Karr(r,c,k) */
+    double* KF;   /* FFT route: [9][nk] complex (re, im) transforms of K / nk, or NULL */
+    int dip_direct; /* 1: the direct circular sum even where the FFT route exists */
 };
+
+static int is_pow2(int n);
+static void build_dip_fft(orc_model* M);
 
 /* ------------------------------------------------------------------ */
 /* small vector helpers                                                 */
@@ -322,9 +327,12 @@ static void build_dipolar(orc_model* M) {
     const orc_lattice* L = &M->in.lat;
     int nm = M->nmag, dm = 3 * nm;
     int period[3], kb[2][3];
-    /* init_shape (fft_ham_base.f90:191-220): open axes are doubled */
+    /* init_shape (fft_ham_base.f90:191-220): open axes are doubled (dip_on 1);
+     * dip_on 2 doubles every axis longer than one cell (linear convolution, the
+     * image sums over the symmetric window of the explicit route) */
+    const int full = M->in.dip_on == 2;
     for (int d = 0; d < 3; d++) {
-        period[d] = L->periodic[d] || L->L[d] == 1;
+        period[d] = L->L[d] == 1 || (L->periodic[d] && !full);
         M->nrep[d] = L->L[d];
         kb[0][d] = 0; kb[1][d] = L->L[d] - 1;
         if (!period[d]) { M->nrep[d] = 2 * L->L[d]; kb[0][d] = -L->L[d] + 1; kb[1][d] = L->L[d] - 1; }
@@ -497,7 +505,10 @@ int orc_model_build(const orc_input* in, orc_model** out) {
     M->bfield = (double*)malloc(sizeof(double) * 3 * M->ncell);
     for (int64_t c = 0; c < M->ncell; c++)
         for (int k = 0; k < 3; k++) M->bfield[3 * c + k] = in->B_ext[k];
-    if (in->dip_on) build_dipolar(M);
+    if (in->dip_on) {
+        build_dipolar(M);
+        if (M->nmag == 1 && is_pow2(M->nrep[0]) && is_pow2(M->nrep[1]) && is_pow2(M->nrep[2])) build_dip_fft(M);
+    }
     *out = M;
     return 0;
 }
@@ -506,7 +517,7 @@ void orc_model_free(orc_model* M) {
     if (!M) return;
     free(M->rowptr); free(M->col); free(M->val);
     free(M->trowptr); free(M->tcol); free(M->tval);
-    free(M->bfield); free(M->K);
+    free(M->bfield); free(M->K); free(M->KF);
     free(M);
 }
 
@@ -535,10 +546,134 @@ int orc_set_bfield(orc_model* M, const double* b) {
 }
 
 /* ------------------------------------------------------------------ */
+/* FFT route of the dipolar convolution on power-of-two grids (one magnetic
+ * atom per cell): our own iterative radix-2 transform (bit reversal, then
+ * butterflies with twiddles from long-double sin/cos), applied along each axis
+ * of the N_rep grid; H = IFFT(sum_j K_F(j,i) M_F(j)) with K_F = FFT(K)/prod(N_rep)
+ * (fft_ham_fftw.f90:134-178,239-262).  Complex numbers as (re, im) pairs. */
+static int is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static void fft_line(double* a, int n, const double* w) {
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t0 = a[2 * i], t1 = a[2 * i + 1];
+            a[2 * i] = a[2 * j]; a[2 * i + 1] = a[2 * j + 1];
+            a[2 * j] = t0; a[2 * j + 1] = t1;
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        int half = len >> 1, step = n / len;
+        for (int i = 0; i < n; i += len)
+            for (int k = 0; k < half; k++) {
+                const double* wk = w + 2 * (k * step);
+                double* u = a + 2 * (i + k);
+                double* v = a + 2 * (i + k + half);
+                double vr = v[0] * wk[0] - v[1] * wk[1], vi = v[0] * wk[1] + v[1] * wk[0];
+                v[0] = u[0] - vr; v[1] = u[1] - vi;
+                u[0] = u[0] + vr; u[1] = u[1] + vi;
+            }
+    }
+}
+
+/* in-place transform of g (x fastest, n[0] x n[1] x n[2] complex), sign -1 forward, +1 inverse */
+static void fft3(double* g, const int n[3], int sign) {
+    const int64_t tot = (int64_t)n[0] * n[1] * n[2];
+    for (int ax = 0; ax < 3; ax++) {
+        const int len = n[ax];
+        if (len == 1) continue;
+        double* w = (double*)malloc(sizeof(double) * len);
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        for (int k = 0; k < len / 2; k++) {
+            long double a = two_pi * (long double)k / (long double)len;
+            w[2 * k] = (double)cosl(a);
+            w[2 * k + 1] = (double)(sign * sinl(a));
+        }
+        const int64_t stride = ax == 0 ? 1 : (ax == 1 ? n[0] : (int64_t)n[0] * n[1]);
+        const int64_t nlines = tot / len;
+#pragma omp parallel
+        {
+            double* line = (double*)malloc(sizeof(double) * 2 * len);
+#pragma omp for schedule(static)
+            for (int64_t l = 0; l < nlines; l++) {
+                /* line l: all points sharing the other two coordinates */
+                const int64_t lo = l % stride, hi = l / stride;
+                const int64_t base = lo + hi * stride * len;
+                for (int q = 0; q < len; q++) {
+                    line[2 * q] = g[2 * (base + q * stride)];
+                    line[2 * q + 1] = g[2 * (base + q * stride) + 1];
+                }
+                fft_line(line, len, w);
+                for (int q = 0; q < len; q++) {
+                    g[2 * (base + q * stride)] = line[2 * q];
+                    g[2 * (base + q * stride) + 1] = line[2 * q + 1];
+                }
+            }
+            free(line);
+        }
+        free(w);
+    }
+}
+
+/* K_F of the nine components, scaled by 1/prod(N_rep) (once per model) */
+static void build_dip_fft(orc_model* M) {
+    const int64_t nk = M->nk;
+    M->KF = (double*)malloc(sizeof(double) * 2 * 9 * nk);
+    for (int c = 0; c < 9; c++) {
+        double* g = M->KF + 2 * c * nk;
+        for (int64_t k = 0; k < nk; k++) { g[2 * k] = M->K[k * 9 + c]; g[2 * k + 1] = 0.0; }
+        fft3(g, M->nrep, -1);
+        for (int64_t k = 0; k < 2 * nk; k++) g[k] = g[k] / (double)nk;
+    }
+}
+
+static void dip_H_fft(const orc_model* M, const double* m, double* H) {
+    const orc_lattice* L = &M->in.lat;
+    const int64_t nk = M->nk;
+    const int* nr = M->nrep;
+    double* g = (double*)calloc((size_t)(2 * 3 * nk), sizeof(double));
+    for (int64_t x = 0; x < M->ncell; x++) {
+        int64_t xx = x % L->L[0], xy = (x / L->L[0]) % L->L[1], xz = x / ((int64_t)L->L[0] * L->L[1]);
+        int64_t q = xx + (int64_t)nr[0] * (xy + (int64_t)nr[1] * xz);
+        for (int c = 0; c < 3; c++) g[2 * (c * nk + q)] = m[3 * x + c];
+    }
+    for (int c = 0; c < 3; c++) fft3(g + 2 * c * nk, nr, -1);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nk; k++) {
+        double mr[3], mi[3], hr[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        for (int j = 0; j < 3; j++) { mr[j] = g[2 * (j * nk + k)]; mi[j] = g[2 * (j * nk + k) + 1]; }
+        /* H_F(i) = sum_j K_F(j,i) M_F(j)  (fft_ham_fftw.f90:249-253) */
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                const double* kf = M->KF + 2 * ((j * 3 + i) * nk + k);
+                hr[i] += kf[0] * mr[j] - kf[1] * mi[j];
+                hi[i] += kf[0] * mi[j] + kf[1] * mr[j];
+            }
+        for (int i = 0; i < 3; i++) { g[2 * (i * nk + k)] = hr[i]; g[2 * (i * nk + k) + 1] = hi[i]; }
+    }
+    for (int c = 0; c < 3; c++) fft3(g + 2 * c * nk, nr, +1);
+    for (int64_t x = 0; x < M->ncell; x++) {
+        int64_t xx = x % L->L[0], xy = (x / L->L[0]) % L->L[1], xz = x / ((int64_t)L->L[0] * L->L[1]);
+        int64_t q = xx + (int64_t)nr[0] * (xy + (int64_t)nr[1] * xz);
+        for (int c = 0; c < 3; c++) H[3 * x + c] = g[2 * (c * nk + q)];
+    }
+    free(g);
+}
+
 /* dipolar field H = K * M as the direct circular convolution over the
  * N_rep grid (identical in exact arithmetic to the FFT route of
- * fft_ham_fftw.f90:239-262 with the 1/prod(N_rep) normalised K_F). */
+ * fft_ham_fftw.f90:239-262 with the 1/prod(N_rep) normalised K_F); the FFT
+ * route above replaces it on power-of-two grids unless dip_direct is set. */
+static void dip_H_direct(const orc_model* M, const double* m, double* H);
 static void dip_H(const orc_model* M, const double* m, double* H) {
+    if (M->KF && !M->dip_direct) dip_H_fft(M, m, H);
+    else dip_H_direct(M, m, H);
+}
+void orc_dip_direct(orc_model* M, int direct) { M->dip_direct = direct; }
+
+static void dip_H_direct(const orc_model* M, const double* m, double* H) {
     const orc_lattice* L = &M->in.lat;
     int nm = M->nmag, dm = 3 * nm;
     int64_t nc = M->ncell;

@@ -91,7 +91,8 @@ typedef struct {
     double c_H_J, c_H_D, c_H_ani, c_zeeman;   /* -1, -1, +1, -1 in the reference */
     double B_ext[3];                          /* H_ext in Tesla */
     int zeeman_on;
-    int dip_on;
+    int dip_on;                               /* 1: the reference's grid rule; 2: every axis
+                                                 longer than one cell zero-padded to 2 L */
     int dip_period_cut[3];                    /* mag_dip_period_cut, default 1 1 1 */
 } orc_input;
 
@@ -175,6 +176,9 @@ int orc_mc_random(const orc_model* M, double* m, orc_mc* p, int nsweeps, double*
                   int64_t* accepted);
 /* Field contributions split: MM only, Zeeman only, dipolar only (for tests). */
 void orc_field_terms(const orc_model* m, const double* mvec, double* B_mm, double* B_zee, double* B_dip);
+/* Route of the model's dipolar convolution: 1 = the direct circular sum,
+ * 0 = the FFT route where the grid is a power of two in every axis (default). */
+void orc_dip_direct(orc_model* m, int direct);
 /* Explicit O(N^2) dipolar field (get_dipolar, mag_dip_fft F). */
 void orc_dipolar_explicit_field(const orc_model* m, const double* mvec, double* B);
 

@@ -141,7 +141,7 @@ class Model:
             inp.B_ext[k] = float(deck.B_ext[k])
             inp.dip_period_cut[k] = int(deck.dip_cut[k])
         inp.zeeman_on = int(bool(deck.zeeman_on))
-        inp.dip_on = int(bool(deck.dip))
+        inp.dip_on = int(deck.dip)
         h = C.c_void_p()
         rc = lib.orc_model_build(C.byref(inp), C.byref(h))
         if rc != 0:
@@ -174,6 +174,12 @@ class Model:
 
     def energy(self, m) -> float:
         return float(lib.orc_energy(self.h, _p(np.ascontiguousarray(m, np.float64))))
+
+    def dip_direct(self, direct: bool = True) -> None:
+        """Dipolar convolution by the direct circular sum (True) or, on
+        power-of-two grids, by the oracle's own FFT (False, the default)."""
+        lib.orc_dip_direct.argtypes = [C.c_void_p, C.c_int]
+        lib.orc_dip_direct(self.h, int(bool(direct)))
 
     def dipolar_explicit(self, m):
         m = np.ascontiguousarray(m, np.float64)

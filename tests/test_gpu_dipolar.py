@@ -53,3 +53,54 @@ def test_dipolar_trajectory(integrator):
     mo = m0.copy()
     O.Model(deck).run(mo, 100, **dyn)
     assert np.abs(m - mo).max() < 1e-9
+
+
+def test_zero_padded_grid_matches_the_explicit_pair_sum():
+    """dip = 2 (every axis longer than one cell zero-padded to 2 L) on a film
+    periodic in plane: the device field equals the oracle's explicit pair sum,
+    and the whole field (all terms) the oracle's to 1e-12."""
+    import matjes_b200 as mj
+
+    deck = mj.square_film((8, 6, 3), Jv=0.0, Dv=0.0, Kv=0.0, Bz=0.0, periodic=(1, 1, 0), a=0.25, dip=2)
+    m = mj.random_sphere(deck.nsites, 9)
+    B = mj.Hamiltonian(deck).get_eff_field(m)
+    Bx = O.Model(deck).dipolar_explicit(m)
+    assert np.abs(B - Bx).max() < 1e-12 * np.abs(Bx).max()
+    full = mj.square_film((16, 16, 4), Jv=1e-3, Dv=0.15e-3, Kv=-0.02e-3, Bz=0.2, periodic=(1, 1, 0), a=0.25,
+                          med_z=-0.3, dip=2)
+    m = mj.random_sphere(full.nsites, 10)
+    B, e = mj.Hamiltonian(full).get_eff_field(m, with_energy=True)
+    Bo, eo = O.Model(full).field(m)
+    assert site_rel_err(B, Bo) < 1e-12
+    assert scalar_rel_err(e, eo) < 1e-12
+
+
+@pytest.mark.parametrize("dip", [1, 2])
+def test_full_size_film_field_and_sib_steps(dip):
+    """The dipolar workload at its full size (128 x 128 x 16 simple cubic, a =
+    0.25 nm, periodic in plane, open along z; J + D + K + Bz = 0.2 T + FFT
+    dipolar, mu_s = 2): on the reference's grid (dip = 1, 128 x 128 x 32) and
+    on the fully zero-padded one (dip = 2, 256 x 256 x 32) the field and the
+    per-site energies equal the oracle's to 1e-12, and 20 SIB steps with
+    Philox noise at 5 K stay within 1e-9 of the oracle's."""
+    import matjes_b200 as mj
+
+    w = mj.workload("film128x16_dipolar")
+    deck = w["deck"]
+    deck.dip = dip
+    ham = mj.Hamiltonian(deck)
+    M = O.Model(deck)
+    assert M.nrep() == ((128, 128, 32) if dip == 1 else (256, 256, 32))
+    m0 = w["m0"]
+    B, e = ham.get_eff_field(m0, with_energy=True)
+    Bo, eo = M.field(m0)
+    assert site_rel_err(B, Bo) < 1e-12
+    assert scalar_rel_err(e, eo) < 1e-12
+    dyn = dict(w["dyn"])
+    dyn.pop("steps")
+    m = m0.copy()
+    mj.SpinDynamics(ham, **dyn).run(m, 20)
+    mo = m0.copy()
+    M.run(mo, 20, **dyn)
+    assert np.abs(m - mo).max() < 1e-9
+    assert np.abs(np.linalg.norm(m, axis=1) - 1.0).max() < 1e-13

@@ -97,6 +97,32 @@ def test_plan_and_replica_paths_agree():
     assert np.abs(a.images - b.images).max() < 1e-6
 
 
+def test_plan_and_replica_paths_agree_with_many_images_and_tma_staging():
+    """14 images of a 64 x 64 DMI film: more images than the plan path's 8
+    forked streams (several images queued on one stream) and a lattice whose
+    interior tiles the plan's field kernels stage by TMA (the default).  After 60
+    iterations the plan's path equals the batch's (the fused GNEB field pass) to
+    1e-10, reaction coordinates and energies included."""
+    from matjes_b200 import Hamiltonian
+    from matjes_b200._abi import lib
+    from matjes_b200.deck import square_film
+    from matjes_b200.gneb import GNEBInput, find_path, find_path_plan
+
+    deck = square_film((64, 64, 1), Jv=1e-3, Dv=0.4e-3, Kv=-0.2e-3, Bz=0.3, mu_s=2.0, periodic=(1, 1, 0))
+    path = _path(deck, 14, seed=6)
+    inp = GNEBInput(spring=0.3, dt=0.02, mass=1.0, mepftol=0.0, itrmax=60, en_zero="I")
+    a = find_path(deck, path, inp)
+    ham = Hamiltonian(deck)
+    variant, shape = C.c_int32(), C.c_int32()
+    assert lib.mj_plan_get_variant(ham.plan, C.byref(variant), C.byref(shape)) == 0
+    assert variant.value >= 0 and shape.value != 0  # tiled kernels, TMA staging on by default
+    b = find_path_plan(ham, path, inp)
+    assert a.iterations == b.iterations == 60
+    assert np.abs(a.images - b.images).max() < 1e-10
+    np.testing.assert_allclose(a.rx, b.rx, rtol=1e-10)
+    assert np.abs(a.ene - b.ene).max() <= 1e-10 * np.abs(a.ene).max()
+
+
 def test_plan_path_arguments_are_checked():
     import torch
 

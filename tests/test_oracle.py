@@ -131,6 +131,39 @@ def test_dipolar_periodic_grid_rule():
     assert O.Model(deck).nrep() == (8, 8, 8)
 
 
+@pytest.mark.parametrize("dip,nrep", [(1, (8, 8, 8)), (2, (16, 16, 8))])
+def test_dipolar_fft_route_equals_direct_circular_sum(dip, nrep):
+    """The oracle's own FFT of the N_rep grid and the direct circular sum over it
+    give the same dipolar field (reference grid rule and the zero-padded grid)."""
+    deck = square_film((8, 8, 4), Jv=0.0, Dv=0.0, Kv=0.0, Bz=0.0, periodic=(1, 1, 0), a=0.25, dip=dip)
+    M = O.Model(deck)
+    assert M.nrep() == nrep
+    m = np.random.default_rng(2).normal(size=(deck.nsites, 3))
+    B_fft = M.field(m)[0]
+    M.dip_direct(True)
+    B_dir = M.field(m)[0]
+    assert np.abs(B_fft - B_dir).max() < 1e-13 * np.abs(B_dir).max()
+    assert M.energy(m) != 0.0
+
+
+def test_zero_padded_grid_equals_the_explicit_pair_sum():
+    """dip = 2 (every axis zero-padded to 2 L, BASELINE's 256 x 256 x 32 for the
+    128 x 128 x 16 film): a linear convolution whose kernel sums the periodic
+    images over -cut..cut for every pair, which is the explicit route
+    (Energy/dipolar_magnetic.f90:181-273).  The reference's grid (periodic axes
+    kept at L, images folded in circularly) sums a window shifted by one period
+    for pairs at negative offsets, so it differs from the explicit sum by far
+    more than rounding."""
+    kw = dict(Jv=0.0, Dv=0.0, Kv=0.0, Bz=0.0, periodic=(1, 1, 0), a=0.25)
+    m = np.random.default_rng(3).normal(size=(8 * 6 * 3, 3))
+    padded = O.Model(square_film((8, 6, 3), dip=2, **kw))
+    assert padded.nrep() == (16, 12, 6)
+    Bx = padded.dipolar_explicit(m)
+    assert np.abs(padded.field(m)[0] - Bx).max() < 1e-12 * np.abs(Bx).max()
+    ref_rule = O.Model(square_film((8, 6, 3), dip=1, **kw))
+    assert np.abs(ref_rule.field(m)[0] - Bx).max() > 1e-6 * np.abs(Bx).max()
+
+
 def test_dipolar_shape_anisotropy_sign():
     deck = square_film((8, 8, 2), Jv=0.0, Dv=0.0, Kv=0.0, Bz=0.0, periodic=(1, 1, 0), a=0.25, dip=True)
     M = O.Model(deck)
