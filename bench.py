@@ -524,8 +524,11 @@ def run_hbm_resident(dev: int, steps: int = 20) -> dict:
     best, best_tma = _abi.C.c_int32(), _abi.C.c_int32()
     _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 3, _abi.C.byref(best),
                                     _abi.C.byref(best_tma), None))
-    E = torch.zeros(steps + 8, dtype=torch.float64, device=m.device)
+    E = torch.zeros(steps + 64, dtype=torch.float64, device=m.device)
     stream = torch.cuda.current_stream().cuda_stream
+    # the fields (403 MB each) exceed L2: no flush between the tuning steps
+    cfg, _ = tune_kernels(lib, _abi, ham.plan, m, p, lambda: None, E, stream, variants=False)
+    cfg.update(variant=int(best.value), tma=int(best_tma.value))
     for k in range(3):
         p.step0 = k
         _abi.check(lib.mj_step_dev(ham.plan, m.data_ptr(), _abi.C.byref(p), 1, E.data_ptr(), stream))
@@ -544,14 +547,14 @@ def run_hbm_resident(dev: int, steps: int = 20) -> dict:
     _abi.check(lib.mj_profile_enable(ham.plan, 0))
     pk = peaks()
     kern = {}
-    for name, b in (("k_sib1", 48.0), ("k_sib2", 72.0)):
+    for name, b in (("k_sib1", 48.0), ("k_sib2", 72.0), ("k_sib_fused", 120.0)):
         if name in prof:
             tot, cnt = prof[name]
             avg = tot / max(cnt, 1)
             gbs = b * N / (avg / 1e3) / 1e9
             kern[name] = {"avg_us": 1e3 * avg, "achieved_gbs": gbs, "frac": gbs / pk["hbm_gbs"]}
-    return {"workload": "triangular4096_thermal", "sites": N, "steps": steps, "kernel_variant": int(best.value),
-            "tma_halo": bool(best_tma.value), "value": N / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+    return {"workload": "triangular4096_thermal", "sites": N, "steps": steps, "kernels_config": cfg,
+            "value": N / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
             "step_roofline": {"alg_bytes_per_site": 120.0, "achieved_gbs": 120.0 * N / (ms / 1e3) / 1e9,
                               "frac": 120.0 * N / (ms / 1e3) / 1e9 / pk["hbm_gbs"]},
             "kernels": kern}
@@ -745,6 +748,49 @@ def timed_steps(lib, _abi, plan, m, p, first_step, K, flush, E, stream):
     return sum(a.elapsed_time(b) for a, b in ev)
 
 
+OPTION_NAMES = {"fused": 1, "pdl": 2, "store_draw": 3}  # mj_plan_set_option ids
+
+
+def tune_kernels(lib, _abi, plan, m, p, flush, E, stream, variants=True):
+    """The plan's kernel configuration timed under the bench's own conditions
+    (L2 flushed before every step, per-step CUDA events, median of 8): first the
+    variant and its halo staging (two launches per step), then, one at a time on
+    top of the best, the fused one-launch step, no programmatic dependent launch
+    and the redrawn (not stored) Philox draw.  Returns the chosen configuration
+    and the table of medians (ms per step)."""
+    def med(k0):
+        timed_steps(lib, _abi, plan, m, p, k0, 2, flush, E, stream)
+        return sorted(timed_steps(lib, _abi, plan, m, p, k0 + 2 + k, 1, flush, E, stream) for k in range(8))[4]
+
+    table = {}
+    best = {"variant": None, "tma": None, "fused": 0, "pdl": 1, "store_draw": 1}
+    for name, val in (("fused", 0), ("pdl", 1), ("store_draw", 1)):
+        _abi.check(lib.mj_plan_set_option(plan, OPTION_NAMES[name], val))
+    if variants:
+        configs = [(-1, 0)] + [(v, t) for t in (0, 1) for v in range(6)]
+        for v, t in configs:
+            _abi.check(lib.mj_plan_set_variant(plan, v))
+            _abi.check(lib.mj_plan_set_tma(plan, t))
+            table["generic" if v < 0 else f"tile{v}" + ("_tma" if t else "")] = med(1000)
+        key = min(table, key=table.get)
+        bv = -1 if key == "generic" else int(key[4])
+        bt = 1 if key.endswith("_tma") else 0
+        _abi.check(lib.mj_plan_set_variant(plan, bv))
+        _abi.check(lib.mj_plan_set_tma(plan, bt))
+        best.update(variant=bv, tma=bt)
+    base = min(table.values()) if table else med(1000)
+    for name, val in (("fused", 1), ("pdl", 0), ("store_draw", 0)):
+        _abi.check(lib.mj_plan_set_option(plan, OPTION_NAMES[name], val))
+        t = med(2000)
+        table[f"{name}={val}"] = t
+        if t < base:
+            base = t
+            best[name] = val
+        else:
+            _abi.check(lib.mj_plan_set_option(plan, OPTION_NAMES[name], best[name]))
+    return best, {k: round(float(v), 5) for k, v in table.items()}
+
+
 def kernel_table(prof, bytes_site, N):
     """Per-kernel launches, average time and achieved algorithmic GB/s."""
     out = {}
@@ -787,12 +833,10 @@ def run_integrator_key(dev, wname, integrator, K, W, noise=None, inject_steps=0)
     p.energy_mode = _abi.MJ_ENERGY_BEFORE
     m = torch.tensor(w["m0"].T.copy(), device=f"cuda:{dev}")
     lib = _abi.lib
-    best, best_tma = _abi.C.c_int32(), _abi.C.c_int32()
-    _abi.check(lib.mj_plan_autotune(ham.plan, m.data_ptr(), _abi.C.byref(p), 3, _abi.C.byref(best),
-                                    _abi.C.byref(best_tma), None))
     flush = L2Flush(m.device)
     E = torch.zeros(K + W + 8, dtype=torch.float64, device=m.device)
     stream = torch.cuda.current_stream().cuda_stream
+    cfg, _ = tune_kernels(lib, _abi, ham.plan, m, p, flush, E, stream)
     timed_steps(lib, _abi, ham.plan, m, p, 0, W, flush, E, stream)
     ms = timed_steps(lib, _abi, ham.plan, m, p, W, K, flush, E, stream)
     _abi.check(lib.mj_profile_enable(ham.plan, 1))
@@ -803,14 +847,14 @@ def run_integrator_key(dev, wname, integrator, K, W, noise=None, inject_steps=0)
     pk = peaks()
     thermal = dyn.get("temperature", 0.0) > 0
     if integrator == "sib":
-        extra = 24.0 if thermal else 0.0
-        bytes_site = {"k_sib1": 48.0 + extra, "k_sib2": 72.0 + extra}
+        extra = 24.0 if (thermal and noise == "inject") else 0.0
+        bytes_site = {"k_sib1": 48.0 + extra, "k_sib2": 72.0 + extra, "k_sib_fused": 120.0 + 2 * extra}
+        step_b = 120.0 + 2 * extra
     else:
         bytes_site = {"k_heun1": 72.0 + (24.0 if thermal else 0.0), "k_heun2": 72.0 + (24.0 if thermal else 0.0)}
-    step_b = sum(bytes_site.values())
+        step_b = sum(bytes_site.values())
     sec = ms / K / 1e3
-    return {"workload": wname, "integrator": integrator, "noise": dyn.get("noise", "off"),
-            "kernel_variant": int(best.value), "tma_halo": bool(best_tma.value),
+    return {"workload": wname, "integrator": integrator, "noise": dyn.get("noise", "off"), "kernels_config": cfg,
             "value": N / sec, "unit": UNIT, "ms_per_step": ms / K,
             "step_roofline": {"alg_bytes_per_site": step_b, "achieved_gbs": step_b * N / sec / 1e9,
                               "frac": step_b * N / sec / 1e9 / pk["hbm_gbs"]},
@@ -847,25 +891,19 @@ def run_gpu(args, rank, world):
     stream = torch.cuda.current_stream().cuda_stream
     lib = _abi.lib
 
-    # kernel variant (tile shape, TMA halo staging) timed under the conditions of
-    # the timed loop below (L2 flushed before every step, per-step events); the
-    # library's own mj_plan_autotune times back-to-back steps, the right choice
-    # when the fields stay in L2 between steps
-    # (--variant skips the sweep: a run under a profiler, whose timing would pick
-    # another variant than a live run)
-    configs = [(-1, 0)] + [(v, t) for t in (0, 1) for v in range(6)]
-    if args.variant is not None:
-        configs = [(args.variant, args.tma)]
-    tune = np.zeros(len(configs))
-    for ci, (v, t) in enumerate(configs if args.variant is None else []):
-        _abi.check(lib.mj_plan_set_variant(ham.plan, v))
-        _abi.check(lib.mj_plan_set_tma(ham.plan, t))
-        timed_steps(lib, _abi, ham.plan, m, p, 1000, 2, flush, E, stream)
-        evs = [timed_steps(lib, _abi, ham.plan, m, p, 1002 + k, 1, flush, E, stream) for k in range(8)]
-        tune[ci] = sorted(evs)[len(evs) // 2]
-    bv, bt = configs[int(np.argmin(tune))]
-    _abi.check(lib.mj_plan_set_variant(ham.plan, bv))
-    _abi.check(lib.mj_plan_set_tma(ham.plan, bt))
+    # kernel configuration timed under the conditions of the timed loop below
+    # (L2 flushed before every step, per-step events); the library's own
+    # mj_plan_autotune times back-to-back steps, the right choice when the fields
+    # stay in L2 between steps.  --variant fixes it instead (a run under a
+    # profiler, whose timing would pick another configuration than a live run).
+    if args.variant is None:
+        best, tune = tune_kernels(lib, _abi, ham.plan, m, p, flush, E, stream)
+    else:
+        best = {"variant": args.variant, "tma": args.tma, "fused": args.fused, "pdl": 1, "store_draw": 1}
+        _abi.check(lib.mj_plan_set_variant(ham.plan, args.variant))
+        _abi.check(lib.mj_plan_set_tma(ham.plan, args.tma))
+        _abi.check(lib.mj_plan_set_option(ham.plan, OPTION_NAMES["fused"], args.fused))
+        tune = {}
 
     timed_steps(lib, _abi, ham.plan, m, p, 0, W, flush, E, stream)
     if dist:
@@ -906,9 +944,11 @@ def run_gpu(args, rank, world):
         return
     pk = peaks()
     thermal = dyn.get("temperature", 0.0) > 0 and dyn.get("noise") == "philox"
-    # algorithmic bytes per site of the two SIB passes (the stored draw counted
-    # separately: written by pass 1, read by pass 2 at T > 0)
-    bytes_site = {"k_sib1": 48.0, "k_sib2": 72.0}
+    # algorithmic bytes per site of the SIB step's kernels: the two passes (read
+    # m, write the midpoint; read the midpoint and m, write m) or the one fused
+    # launch doing both; the stored draw (written by the predictor, read by the
+    # corrector at T > 0) is not counted
+    bytes_site = {"k_sib1": 48.0, "k_sib2": 72.0, "k_sib_fused": 120.0}
     kernels = kernel_table(prof, bytes_site, N)
     dom = max((k for k in kernels if k in bytes_site), key=lambda k: kernels[k]["avg_us"])
     ach = kernels[dom]["achieved_gbs"]
@@ -925,8 +965,7 @@ def run_gpu(args, rank, world):
         extras["hbm_resident_4096"] = run_hbm_resident(dev)
         extras["gneb"] = run_gneb(dev)
     # bulky tables go to stderr, not into the bench line
-    verbose = {"variant_sweep_ms_per_step": {("generic" if v < 0 else f"tile{v}" + ("_tma" if t else "")):
-                                             round(float(x), 5) for (v, t), x in zip(configs, tune)}}
+    verbose = {"kernel_tuning_ms_per_step": tune}
     for k, v in extras.items():
         if isinstance(v, dict) and "autotune_ms_per_step" in v:
             verbose[f"{k}_autotune_ms_per_step"] = v.pop("autotune_ms_per_step")
@@ -939,7 +978,7 @@ def run_gpu(args, rank, world):
                                                        {"parallelism": f"replicas x{world}" if world > 1 else "single",
                                                         "energy_per_step": "energy of the incoming state, fused "
                                                                            "into the first field pass",
-                                                        "kernel_variant": int(bv), "tma_halo": bool(bt)}),
+                                                        "kernels": best}),
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
                      "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},
@@ -950,7 +989,7 @@ def run_gpu(args, rank, world):
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 24 * N + 8,
                 "path": "mj_step_host: pinned host AoS in and out, one step, energy to the host; copies, "
                         "transposes and passes overlapped in 12 stripes of tile rows"},
-        "gpu_launches": 2 * K,
+        "gpu_launches": int(sum(c for _, c in prof.values())),
         "cpu_baseline": cpu,
         **extras,
     }
@@ -1015,6 +1054,7 @@ def _prof_main(argv=None):
     ap.add_argument("--integrator", default="sib")
     ap.add_argument("--variant", default="auto")
     ap.add_argument("--tma", type=int, default=1, help="halo staging of the tiled kernels: 1 TMA, 0 plain loads")
+    ap.add_argument("--fused", type=int, default=1, help="SIB steps: 1 one fused launch, 0 two launches")
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--adjoint", action="store_true", help="one forward + backward sweep of the SIB adjoint")
     ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
@@ -1064,6 +1104,8 @@ def _prof_main(argv=None):
     elif ham.noffsets:
         _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, int(a.variant)))
         _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, int(a.tma)))
+    if ham.noffsets:
+        _abi.check(_abi.lib.mj_plan_set_fused(ham.plan, int(a.fused)))
     E = torch.zeros(a.steps + 1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     for k in range(a.steps):
@@ -1144,6 +1186,7 @@ def main():
     ap.add_argument("--variant", type=int, default=None,
                     help="kernel variant (-1 generic, 0..5 tiled) instead of the timed sweep")
     ap.add_argument("--tma", type=int, default=0, help="halo staging with --variant: 1 TMA, 0 plain loads")
+    ap.add_argument("--fused", type=int, default=1, help="with --variant: 1 one launch per SIB step, 0 two")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batch, adjoint, dipolar and Monte Carlo measurements")
     args = ap.parse_args()

@@ -28,6 +28,7 @@ MJ_NOISE_OFF = 0
 MJ_NOISE_PHILOX = 1
 MJ_NOISE_INJECT = 2
 MJ_MAX_ATOMS = 16
+MJ_OPT_TMA, MJ_OPT_FUSED, MJ_OPT_PDL, MJ_OPT_STORE_DRAW = 0, 1, 2, 3
 
 INTEGRATORS = {"euler": MJ_EULER, "heun": MJ_HEUN_MATJES, "heun_matjes": MJ_HEUN_MATJES, "sib": MJ_SIB}
 NOISES = {"off": MJ_NOISE_OFF, "philox": MJ_NOISE_PHILOX, "inject": MJ_NOISE_INJECT}
@@ -139,6 +140,8 @@ SIGNATURES = {
     "mj_plan_autotune": (C.c_int32, [P, P, C.POINTER(DynParams), C.c_int32, C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), P]),
     "mj_plan_set_tma": (C.c_int32, [P, C.c_int32]),
+    "mj_plan_set_fused": (C.c_int32, [P, C.c_int32]),
+    "mj_plan_set_option": (C.c_int32, [P, C.c_int32, C.c_int32]),
     "mj_plan_check_status": (C.c_int32, [P]),
     "mj_plan_selftest_timeout": (C.c_int32, [P, C.c_uint32, P]),
     "mj_plan_set_bfield": (C.c_int32, [P, P]),

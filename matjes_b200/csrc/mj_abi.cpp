@@ -274,6 +274,12 @@ mj_status alloc_scratch(mj_plan* p) {
     if ((st = dalloc(&p->d_partials, static_cast<size_t>(p->partial_cap), "partials")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_counter, 4, "counter")) != MJ_OK) return st;
     if ((st = cuda_status(cudaMemset(p->d_counter, 0, 4 * sizeof(unsigned int)), "counter init")) != MJ_OK) return st;
+    if (p->is_stencil) {
+        const int64_t words = sched_words(p);
+        if ((st = dalloc(&p->d_sched, words, "fused-step scheduler")) != MJ_OK) return st;
+        if ((st = cuda_status(cudaMemset(p->d_sched, 0, sizeof(unsigned int) * words), "scheduler init")) != MJ_OK)
+            return st;
+    }
     if ((st = dalloc(&p->d_scalar, 8, "scalar")) != MJ_OK) return st;
     if ((st = dalloc(&p->d_status, 4, "status")) != MJ_OK) return st;
     if ((st = cuda_status(cudaMemset(p->d_status, 0, 4 * sizeof(int)), "status init")) != MJ_OK) return st;
@@ -307,6 +313,7 @@ void free_plan(mj_plan* p) {
     cudaFree(p->d_counter);
     cudaFree(p->d_scalar);
     cudaFree(p->d_status);
+    cudaFree(p->d_sched);
     if (p->h_status) cudaFreeHost(p->h_status);
     cudaFree(p->d_noise_tab);
     cudaFree(p->d_stage);
@@ -921,6 +928,26 @@ mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable) {
         plan->graph_exec = nullptr;
         plan->graph_key.clear();
     }
+    return MJ_OK;
+}
+
+mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    switch (option) {
+        case MJ_OPT_TMA: plan->use_tma = value != 0; break;
+        case MJ_OPT_FUSED: plan->fused_sib = value != 0; break;
+        case MJ_OPT_PDL: plan->use_pdl = value != 0; break;
+        case MJ_OPT_STORE_DRAW: plan->store_draw = value != 0; break;
+        default: return set_error(MJ_ERR_ARG, "unknown plan option " + std::to_string(option));
+    }
+    drop_graph(plan);
+    return MJ_OK;
+}
+
+mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable) {
+    if (!plan) return set_error(MJ_ERR_ARG, "null plan");
+    plan->fused_sib = enable != 0;
+    drop_graph(plan);
     return MJ_OK;
 }
 

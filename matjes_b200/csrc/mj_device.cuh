@@ -213,10 +213,10 @@ __device__ __forceinline__ double3 project(double3 t, double3 m) {
 // MID: the predictor's midpoint (m + y)/2 = m + c/2 (u + u x h) instead of y.
 template <bool MID = false>
 __device__ __forceinline__ double3 sib_solve(double3 m, double3 p, double3 H, double alpha, double hc) {
-    const double inv = inv_norm(dot(p, p));
-    const double3 pn = make_double3(p.x * inv, p.y * inv, p.z * inv);
-    const double3 pxh = cross(pn, H);
-    const double3 h = make_double3(hc * (H.x + alpha * pxh.x), hc * (H.y + alpha * pxh.y), hc * (H.z + alpha * pxh.z));
+    // h = hc H + (hc alpha / |p|) p x H: the normalisation folded into one scalar
+    const double sa = hc * alpha * inv_norm(dot(p, p));
+    const double3 pxh = cross(p, H);
+    const double3 h = make_double3(fma(sa, pxh.x, hc * H.x), fma(sa, pxh.y, hc * H.y), fma(sa, pxh.z, hc * H.z));
     const double3 u = cross(m, h);
     const double3 w = cross(u, h);
     double c = cayley_scale(dot(h, h));

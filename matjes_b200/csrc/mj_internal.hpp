@@ -107,6 +107,10 @@ struct mj_plan {
     int tile_variant = 0;            // tiled-kernel shape (threads in y x sites per thread), see mj_tiled.cu
     int tiled_shape = 0;             // matched compile-time shape (sp.shape is 0 while the generic path is forced)
     bool use_tma = true;             // tiled kernels stage tile + halo with one TMA copy per block
+    bool fused_sib = false;          // SIB steps of tiled plans without the dipolar term in one launch
+    bool use_pdl = true;             // tiled passes launched as programmatic dependents of the kernel before
+    bool store_draw = true;          // SIB: the predictor stores its Philox draw for the corrector (else recomputed)
+    unsigned int* d_sched = nullptr; // fused step scheduler: work counter, exit ticket, done tiles per row
     int num_sms = 148;
     int* d_status = nullptr;         // device status word: kStatusTimeout | kStatusNonFinite
     int* h_status = nullptr;         // pinned host copy of it (host-array step calls)
@@ -227,6 +231,17 @@ mj_status launch_tiled(mj_plan* p, int pass, const DynCoef& C, const double* ms,
     mj_status fn(mj_plan* p, int pass, const DynCoef& C, const double* ms, const double* mn, double* out,         \
                  double* aux, double* aux2, DipView Hd, double* E_out, uint32_t step, cudaStream_t s, int emode,  \
                  int ty0, int nty);
+// one SIB step in one launch (k_sib_fused): tiled plans without the dipolar term
+mj_status launch_sib_fused(mj_plan* p, const DynCoef& C, double* m, double* draw, double* E_out, uint32_t step,
+                           cudaStream_t s);
+#define MJ_FUSED_SHAPE_DECL(fn) \
+    mj_status fn(mj_plan* p, const DynCoef& C, double* m, double* draw, double* E_out, uint32_t step, cudaStream_t s);
+MJ_FUSED_SHAPE_DECL(launch_sib_fused_square_nn)
+MJ_FUSED_SHAPE_DECL(launch_sib_fused_square2)
+MJ_FUSED_SHAPE_DECL(launch_sib_fused_tri_nn)
+MJ_FUSED_SHAPE_DECL(launch_sib_fused_tri3)
+// scheduler words of the fused step: 2 + tile rows at the smallest tile height
+int64_t sched_words(const mj_plan* p);
 MJ_TILED_SHAPE_DECL(launch_tiled_square_nn)
 MJ_TILED_SHAPE_DECL(launch_tiled_square2)
 MJ_TILED_SHAPE_DECL(launch_tiled_tri_nn)

@@ -559,7 +559,13 @@ mj_status tiled_step(mj_plan* p, double* m, double* m_out, const DynCoef& c, uin
                               E_prev ? 2 : 0);
         case MJ_SIB: {
             // Philox draws are made once per step in pass 1 and kept for the corrector
-            double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX) ? p->d_aux : nullptr;
+            double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX && p->store_draw) ? p->d_aux : nullptr;
+            if (p->fused_sib && !p->dip_on && p->d_sched) {  // predictor and corrector in one launch
+                const int rec = prof_begin(p, "k_sib_fused", s);
+                st = launch_sib_fused(p, c, m, bstore, E_prev, step, s);
+                prof_end(p, rec, s);
+                return st;
+            }
             if ((st = tiled_call(p, "k_sib1", 4, c, m, nullptr, p->d_mid, bstore, nullptr, Hd, nullptr, step, s,
                                  E_prev ? 1 : 0)) != MJ_OK)
                 return st;

@@ -34,6 +34,24 @@ int64_t tiled_energy_blocks(const mj_plan* p) {
     return static_cast<int64_t>((p->sp.L[0] + 31) / 32) * ((p->sp.L[1] + ty - 1) / ty) * p->sp.L[2];
 }
 
+int64_t sched_words(const mj_plan* p) {
+    int min_ty = kTiledVariantTY[0];
+    for (int v = 1; v < kTiledVariants; ++v) min_ty = std::min(min_ty, kTiledVariantTY[v]);
+    return 2 + static_cast<int64_t>((p->sp.L[1] + min_ty - 1) / min_ty) * p->sp.L[2];
+}
+
+mj_status launch_sib_fused(mj_plan* p, const DynCoef& C, double* m, double* draw, double* E_out, uint32_t step,
+                           cudaStream_t s) {
+    if (!p->d_sched) return set_error(MJ_ERR_ARG, "plan has no fused-step scheduler");
+    switch (p->sp.shape) {
+        case kShapeSquareNN: return launch_sib_fused_square_nn(p, C, m, draw, E_out, step, s);
+        case kShapeSquare2: return launch_sib_fused_square2(p, C, m, draw, E_out, step, s);
+        case kShapeTriNN: return launch_sib_fused_tri_nn(p, C, m, draw, E_out, step, s);
+        case kShapeTri3: return launch_sib_fused_tri3(p, C, m, draw, E_out, step, s);
+        default: return set_error(MJ_ERR_ARG, "no tiled kernel for this stencil shape");
+    }
+}
+
 int tiled_tile_rows(const mj_plan* p) {
     const int v = (p->tile_variant >= 0 && p->tile_variant < kTiledVariants) ? p->tile_variant : 0;
     const int ty = kTiledVariantTY[v];

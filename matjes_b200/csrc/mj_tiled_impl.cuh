@@ -70,7 +70,16 @@ struct TiledArgs {
     int nty_all;        // tile rows of the whole lattice (0: the launch covers all of them)
     int ty_count;       // tile rows of this launch (host side: its grid height)
     int tma;            // 1: tile + halo staged by TMA through the kernel's tensor map
+    int pdl;            // 1: launched as a programmatic dependent of the previous kernel
 };
+
+// Programmatic dependent launch: a kernel lets the next one in its stream launch
+// once all of its own blocks are resident (launch_dependents at its start), and
+// reads what the previous kernel wrote only after griddepcontrol.wait, which
+// returns once that kernel has completed with its memory visible.  Both are
+// no-ops for a launch without the programmatic attribute.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prev() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <class S, int BYT, int RY>
 struct TileGeom {
@@ -147,6 +156,15 @@ __device__ __forceinline__ void all_columns(const StencilParams& P, const double
         ...);
 }
 
+// Global loads of the staging and prefetch: CG = false takes the read-only
+// path (data no block of the launch writes); CG = true caches at L2 only, for
+// data written earlier in the same launch by other blocks (the fused step).
+template <bool CG>
+__device__ __forceinline__ double ldg_or_cg(const double* p) {
+    if constexpr (CG) return __ldcg(p);
+    return __ldg(p);
+}
+
 // per-site epilogue inputs that live in global memory, loaded before the
 // stencil so that their latency overlaps it
 struct Pre {
@@ -157,14 +175,17 @@ struct Pre {
 // The thermal draw of the passes that make one (Euler, Heun predictor, SIB
 // predictor) is part of the prefetch: it depends on neither the tile nor the
 // stencil, so it can run while the tile's halo loads are in flight.
-template <int PASS>
+template <int PASS, bool CG = false>
 __device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N) {
     Pre p;
     p.a = make_double3(0.0, 0.0, 0.0);
     p.b = p.a;
     if constexpr (PASS == PASS_SIB2) {
         p.a = make_double3(A.mn[i], A.mn[N + i], A.mn[2 * N + i]);
-        if (C.thermal) p.b = A.aux ? ld3(A.aux, i, N) : thermal_field(C, A.step, i, N);
+        if (C.thermal)
+            p.b = A.aux ? make_double3(ldg_or_cg<CG>(A.aux + i), ldg_or_cg<CG>(A.aux + N + i),
+                                       ldg_or_cg<CG>(A.aux + 2 * N + i))
+                        : thermal_field(C, A.step, i, N);
     } else if constexpr (PASS == PASS_HEUN2) {
         p.a = ld3(A.aux, i, N);
         if (C.thermal) p.b = ld3(A.aux2, i, N);
@@ -176,9 +197,12 @@ __device__ __forceinline__ Pre prefetch(const DynCoef& C, const TiledArgs& A, in
 
 // Contribution of one site to H%energy: -m.Bmm/2 - m.Bzee (+ m.Hd with the dipolar
 // term, counted once; fft_ham_base.f90:258-267), B = Bmm + Bzee the real-space field.
-template <bool HD>
+// ZAX: the Zeeman part points along z (its x, y parts are not added: IEEE
+// arithmetic keeps x + 0 and x * 0 as operations).
+template <bool HD, bool ZAX = false>
 __device__ __forceinline__ double energy_part(double3 B, double3 Bzee, double3 m, double3 hd) {
-    const double e = -0.5 * (dot(m, B) + dot(m, Bzee));
+    const double mz = ZAX ? m.z * Bzee.z : dot(m, Bzee);
+    const double e = -0.5 * (dot(m, B) + mz);
     if constexpr (HD) return e + dot(m, hd);
     return e;
 }
@@ -186,7 +210,7 @@ __device__ __forceinline__ double energy_part(double3 B, double3 Bzee, double3 m
 // The pass's update of one site.  B = the real-space field (MM + Zeeman), Bzee
 // its Zeeman part, hd the dipolar H (HD); returns the site's energy part where
 // the pass computes one.
-template <int PASS, bool HD>
+template <int PASS, bool HD, bool ZAX = false>
 __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A, int64_t i, int64_t N, double3 m0,
                                            double3 Brs, double3 Bzee, double3 hd, const Pre& pre) {
     double3 B = Brs;
@@ -196,11 +220,11 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         // per-site energy (energy_distrib, left-assigned; hamiltonian_collection.f90:332-363):
         // the dipolar term doubled as in fft_ham_base.f90:247-256
         if (A.aux) {
-            double es = -0.5 * (dot(m0, Brs) + dot(m0, Bzee));
+            double es = -0.5 * (dot(m0, Brs) + (ZAX ? m0.z * Bzee.z : dot(m0, Bzee)));
             if constexpr (HD) es += 2.0 * dot(m0, hd);
             A.aux[i] = es;
         }
-        return energy_part<HD>(Brs, Bzee, m0, hd);
+        return energy_part<HD, ZAX>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_EULER) {
         const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double c = C.h_over_hbar;
@@ -212,7 +236,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         const double3 mo = project(t, m0);
         flag_nonfinite(A.status, mo);
         st3(A.out, i, N, mo);
-        return energy_part<HD>(Brs, Bzee, m0, hd);
+        return energy_part<HD, ZAX>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_HEUN1) {
         const double3 D = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double c = C.h_over_hbar;
@@ -220,7 +244,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
         st3(A.out, i, N, project(t, m0));
         st3(A.aux, i, N, D);
         if (C.thermal) st3(A.aux2, i, N, llg_rhs(pre.b, m0, C.alpha, C.inv_den));
-        return energy_part<HD>(Brs, Bzee, m0, hd);
+        return energy_part<HD, ZAX>(Brs, Bzee, m0, hd);
     } else if constexpr (PASS == PASS_HEUN2) {
         const double3 D2 = llg_rhs(B, m0, C.alpha, C.inv_den);
         const double3 d1 = pre.a;
@@ -243,7 +267,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
             H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
         }
         st3(A.out, i, N, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
-        return energy_part<HD>(Brs, Bzee, m0, hd);
+        return energy_part<HD, ZAX>(Brs, Bzee, m0, hd);
     } else {  // PASS_SIB2: m0 is the midpoint, the corrector starts from m_n
         double3 H = B;
         if (C.thermal) H = make_double3(H.x + pre.b.x, H.y + pre.b.y, H.z + pre.b.z);
@@ -255,7 +279,7 @@ __device__ __forceinline__ double epilogue(const DynCoef& C, const TiledArgs& A,
 }
 
 // plain staging of tile + halo; periodic wrap per element, zeros off open edges
-template <class S, int BYT, int RY>
+template <class S, int BYT, int RY, bool CG = false>
 __device__ __forceinline__ void load_tile(const StencilParams& P, const double* ms, int x0, int y0, int z, double* sm) {
     using G = TileGeom<S, BYT, RY>;
     const int Lx = P.L[0], Ly = P.L[1];
@@ -279,9 +303,9 @@ __device__ __forceinline__ void load_tile(const StencilParams& P, const double* 
         double vx = 0.0, vy = 0.0, vz = 0.0;
         if (ok) {
             const int64_t j = gx + static_cast<int64_t>(Lx) * gy;
-            vx = __ldg(mx + j);
-            vy = __ldg(mx + N + j);
-            vz = __ldg(mx + 2 * N + j);
+            vx = ldg_or_cg<CG>(mx + j);
+            vy = ldg_or_cg<CG>(mx + N + j);
+            vz = ldg_or_cg<CG>(mx + 2 * N + j);
         }
         sm[idx] = vx;
         sm[G::NS + idx] = vy;
@@ -292,7 +316,7 @@ __device__ __forceinline__ void load_tile(const StencilParams& P, const double* 
 // After a TMA box landed with zeros outside the lattice: rewrite the halo cells
 // that lie across a periodic edge with the wrapped spins (cells across an open
 // edge keep the zeros).
-template <class S, int BYT, int RY>
+template <class S, int BYT, int RY, bool CG = false>
 __device__ __forceinline__ void patch_periodic_halo(const StencilParams& P, const double* ms, int x0, int y0, int z,
                                                     double* sm) {
     using G = TileGeom<S, BYT, RY>;
@@ -311,9 +335,9 @@ __device__ __forceinline__ void patch_periodic_halo(const StencilParams& P, cons
         if (outx) gx = ((gx % Lx) + Lx) % Lx;
         if (outy) gy = ((gy % Ly) + Ly) % Ly;
         const int64_t j = gx + static_cast<int64_t>(Lx) * gy;
-        sm[idx] = __ldg(mx + j);
-        sm[G::NS + idx] = __ldg(mx + N + j);
-        sm[2 * G::NS + idx] = __ldg(mx + 2 * N + j);
+        sm[idx] = ldg_or_cg<CG>(mx + j);
+        sm[G::NS + idx] = ldg_or_cg<CG>(mx + N + j);
+        sm[2 * G::NS + idx] = ldg_or_cg<CG>(mx + 2 * N + j);
     }
 }
 
@@ -385,7 +409,7 @@ __device__ __forceinline__ void load_tile_commit(const Staged<S, BYT, RY>& st, d
 }
 
 // epilogue inputs of the thread's RY sites (see prefetch)
-template <class S, int BYT, int RY, int PASS>
+template <class S, int BYT, int RY, int PASS, bool CG = false>
 __device__ __forceinline__ void prefetch_sites(const StencilParams& P, const DynCoef& C, const TiledArgs& A, int x0,
                                                int y0, int z, Pre* pre) {
     const int Lx = P.L[0], Ly = P.L[1];
@@ -395,7 +419,7 @@ __device__ __forceinline__ void prefetch_sites(const StencilParams& P, const Dyn
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
         const int y = y0 + threadIdx.y * RY + r;
-        if (x < Lx && y < Ly) pre[r] = prefetch<PASS>(C, A, layer * z + x + static_cast<int64_t>(Lx) * y, N);
+        if (x < Lx && y < Ly) pre[r] = prefetch<PASS, CG>(C, A, layer * z + x + static_cast<int64_t>(Lx) * y, N);
     }
 }
 
@@ -442,10 +466,12 @@ __device__ __forceinline__ double sites_epilogue(const StencilParams& P, const D
                     Bzee = make_double3(P.zc * P.bext[0], P.zc * P.bext[1], P.zc * P.bext[2]);
                 }
             }
-            const double3 Brs = make_double3(b0 + Bzee.x, b1 + Bzee.y, b2 + Bzee.z);
+            constexpr bool ZAX = SP == SP_AXIAL && !ZMAP;
+            const double3 Brs =
+                ZAX ? make_double3(b0, b1, b2 + Bzee.z) : make_double3(b0 + Bzee.x, b1 + Bzee.y, b2 + Bzee.z);
             double3 hd = make_double3(0.0, 0.0, 0.0);
             if constexpr (HD) hd = ld_dip(A.Hd, x, y, z);
-            e += epilogue<PASS, HD>(C, A, i, N, m0, Brs, Bzee, hd, pre[r]);
+            e += epilogue<PASS, HD, ZAX>(C, A, i, N, m0, Brs, Bzee, hd, pre[r]);
         }
     }
     return e;
@@ -527,6 +553,14 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
     const int x0 = blockIdx.x * G::TX, y0 = by * G::TY, z = blockIdx.z;
     const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
     const int tid = threadIdx.x + 32 * threadIdx.y;
+    // the epilogue inputs of the passes that draw the thermal field depend on no
+    // earlier kernel (an injected buffer is the caller's): computed before the
+    // wait for the previous kernel, the others after it
+    constexpr bool kPurePre = PASS == PASS_SIB1 || PASS == PASS_EULER || PASS == PASS_HEUN1 || PASS == PASS_FIELD;
+    if (A.pdl) {
+        pdl_allow_next();
+        if constexpr (!kPurePre) pdl_wait_prev();
+    }
     if (A.R.mode == 2 && bid == 0) ordered_sum<1>(A.R.partials, A.R.nblocks, A.R.out);
     Pre pre[RY];
     bool ok = true;
@@ -536,11 +570,13 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
         if (tid == 0) {
             mbar_init(&bar, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            if (A.pdl) pdl_wait_prev();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&bar, static_cast<uint32_t>(G::buf_bytes));
             tma_load_4d(&tmap, &bar, smem_t, x0 - G::RX, y0 - G::R, z, 0);
         }
         prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
+        if (A.pdl) pdl_wait_prev();
         __syncthreads();  // the barrier's initialisation is visible to every waiting thread
         ok = mbar_wait_bounded(&bar, 0u, kTmaWaitPolls);
         if (__syncthreads_or(!ok)) {
@@ -560,11 +596,13 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
     } else if constexpr (Staged<S, BYT, RY>::NPT <= kMaxStagedPerThread) {
         // halo loads in flight while the epilogue inputs (the thermal draw) are computed
         Staged<S, BYT, RY> st;
+        if (A.pdl) pdl_wait_prev();
         load_tile_issue<S, BYT, RY>(P, A.ms, x0, y0, z, st);
         prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
         load_tile_commit<S, BYT, RY>(st, smem_t);
         __syncthreads();
     } else {
+        if (A.pdl) pdl_wait_prev();
         load_tile<S, BYT, RY>(P, A.ms, x0, y0, z, smem_t);
         prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
         __syncthreads();
@@ -576,6 +614,246 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
     } else if (A.R.mode == 0 && A.R.out) {
         double v[1] = {e};
         grid_reduce<1>(v, A.R.partials, A.R.counter, A.R.out, A.R.nblocks);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One SIB step in one launch (k_sib_fused).  The work items are tile rows of
+// the predictor (P1) and of the corrector (P2) in a wavefront order per layer
+// with a lag of L rows (L about the tile rows in flight at once, so that a
+// corrector rarely finds its rows unfinished): P1 rows 0 .. L, then P1 row r
+// followed by P2 row r-L for r = L+1 .. nty-1, then P2 rows nty-L .. nty-1 and
+// 0 (each entry ntx tiles; one row: P1 then P2).  A corrector row r needs the
+// predictor rows r-1, r, r+1 (across a periodic edge the row on the other
+// side): all of them come earlier in the order.  Blocks take items from an
+// atomic counter; a predictor tile counts itself into its row once its
+// midpoint and draw are stored, and a corrector tile starts once its rows are
+// complete.  Every row a corrector waits for was handed out before it, to a
+// block that is running, so the waits end (they are bounded all the same), and
+// the midpoint and draw are read back soon after they were written, from L2.
+// No corrector tile's write of m overlaps a predictor tile still reading it (a
+// corrector writes row r only after the predictor rows r-1 .. r+1 are done).
+// The results equal the two-pass launches' bit for bit: the same tile code, the
+// energy partials per predictor tile summed in tile order by the last block to
+// finish, which also re-arms the scheduler words for the next launch.
+struct FusedArgs {
+    double* m;              // m_n in, m_{n+1} out
+    double* mid;            // midpoint buffer
+    double* draw;           // stored Philox draw (T > 0) or null
+    const double* bmap;
+    double* partials;       // energy partial per predictor tile
+    double* E_out;          // energy of m_n or null
+    unsigned int* sched;    // [0] work counter, [1] exit ticket, [2 ..) completed tiles per predictor row
+    int* status;
+    uint32_t step;
+    int tma;                // stage by TMA through map_m / map_mid
+    int lag;                // rows the corrector trails the predictor by (>= 1)
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+constexpr uint32_t kRowWaitPolls = 1u << 22;
+
+// entry e (0 .. 2 nty - 1) of a layer's wavefront order: (corrector?, tile row)
+__device__ __forceinline__ void wavefront_entry(int e, int nty, int lag_req, bool& corr, int& row) {
+    if (nty == 1) {
+        corr = e == 1;
+        row = 0;
+        return;
+    }
+    const int lag = lag_req < 1 ? 1 : (lag_req > nty - 1 ? nty - 1 : lag_req);
+    const int a = lag + 1, b = 2 * (nty - 1 - lag);
+    if (e < a) {  // P1 rows 0 .. lag
+        corr = false;
+        row = e;
+    } else if (e < a + b) {  // P1 row r, then P2 row r - lag
+        const int k = e - a;
+        const int r = lag + 1 + (k >> 1);
+        corr = (k & 1) != 0;
+        row = corr ? r - lag : r;
+    } else {  // P2 rows nty - lag .. nty - 1, then 0
+        const int j = e - a - b;
+        corr = true;
+        row = j < lag ? nty - lag + j : 0;
+    }
+}
+
+// Stage one tile (+ halo) of `src` into shared memory by TMA (with the
+// periodic patch) or plain loads, computing the epilogue inputs meanwhile.
+// Returns false when the copy's bounded wait gave up.
+template <class S, int BYT, int RY, int PASS, bool CG>
+__device__ __forceinline__ bool fused_stage(const CUtensorMap* map, const StencilParams& P, const DynCoef& C,
+                                            const TiledArgs& A, bool tma, double* sm, uint64_t* bar, uint32_t& phase,
+                                            int x0, int y0, int z, Pre* pre) {
+    using G = TileGeom<S, BYT, RY>;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    if (tma) {
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, static_cast<uint32_t>(G::buf_bytes));
+            tma_load_4d(map, bar, sm, x0 - G::RX, y0 - G::R, z, 0);
+        }
+        prefetch_sites<S, BYT, RY, PASS, CG>(P, C, A, x0, y0, z, pre);
+        const bool ok = mbar_wait_bounded(bar, phase, kTmaWaitPolls);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            mbar_wait_bounded(bar, phase ^ 1u, 1u << 16);  // let the copy land before leaving
+            return false;
+        }
+        const bool wraps = (P.periodic[0] && (x0 - G::RX < 0 || x0 + G::TX + G::RX > P.L[0])) ||
+                           (P.periodic[1] && (y0 - G::R < 0 || y0 + G::TY + G::R > P.L[1]));
+        if (wraps) {
+            patch_periodic_halo<S, BYT, RY, CG>(P, A.ms, x0, y0, z, sm);
+            __syncthreads();
+        }
+        return true;
+    }
+    load_tile<S, BYT, RY, CG>(P, A.ms, x0, y0, z, sm);
+    prefetch_sites<S, BYT, RY, PASS, CG>(P, C, A, x0, y0, z, pre);
+    __syncthreads();
+    return true;
+}
+
+// predictor tile t = (tx, ty, z): midpoint, draw and energy partial stored, row counted
+template <class S, int BYT, int RY, int SP>
+__device__ __forceinline__ bool fused_predictor(const CUtensorMap* map, const StencilParams& P, const DynCoef& C,
+                                             const FusedArgs& F, double* sm, uint64_t* bar, uint32_t& phase, int tx,
+                                             int ty, int z, int t, int T, unsigned int* row_done) {
+    using G = TileGeom<S, BYT, RY>;
+    TiledArgs A = {};
+    A.bmap = F.bmap;
+    A.step = F.step;
+    A.status = F.status;
+    A.ms = F.m;
+    A.out = F.mid;
+    A.aux = F.draw;
+    const int x0 = tx * G::TX, y0 = ty * G::TY;
+    Pre pre[RY];
+    if (!fused_stage<S, BYT, RY, PASS_SIB1, false>(map, P, C, A, F.tma, sm, bar, phase, x0, y0, z, pre)) return false;
+    const double e = compute_tile<S, BYT, RY, PASS_SIB1, SP>(P, C, A, sm, x0, y0, z, pre);
+    double v[1] = {e};
+    block_partials<1>(v, F.partials, T, t);  // after the tile's stores
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        atomicAdd(row_done, 1u);
+    }
+    return true;
+}
+
+// corrector tile (tx, ty, z): m_{n+1} of the tile's sites, in place
+template <class S, int BYT, int RY, int SP>
+__device__ __forceinline__ bool fused_corrector(const CUtensorMap* map, const StencilParams& P, const DynCoef& C,
+                                             const FusedArgs& F, double* sm, uint64_t* bar, uint32_t& phase, int tx,
+                                             int ty, int z) {
+    using G = TileGeom<S, BYT, RY>;
+    TiledArgs A = {};
+    A.bmap = F.bmap;
+    A.step = F.step;
+    A.status = F.status;
+    A.ms = F.mid;
+    A.mn = F.m;
+    A.out = F.m;
+    A.aux = F.draw;
+    const int x0 = tx * G::TX, y0 = ty * G::TY;
+    Pre pre[RY];
+    if (!fused_stage<S, BYT, RY, PASS_SIB2, true>(map, P, C, A, F.tma, sm, bar, phase, x0, y0, z, pre)) return false;
+    compute_tile<S, BYT, RY, PASS_SIB2, SP>(P, C, A, sm, x0, y0, z, pre);
+    return true;
+}
+
+template <class S, int BYT, int RY, int MINB, int SP>
+__global__ void __launch_bounds__(32 * BYT, MINB) k_sib_fused(const __grid_constant__ CUtensorMap map_m,
+                                                         const __grid_constant__ CUtensorMap map_mid,
+                                                         const __grid_constant__ StencilParams P,
+                                                         const __grid_constant__ DynCoef C,
+                                                         const __grid_constant__ FusedArgs F) {
+    using G = TileGeom<S, BYT, RY>;
+    extern __shared__ __align__(128) double smem_t[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int s_item;
+    __shared__ int s_ok;
+    __shared__ bool s_last;
+    const int tid = threadIdx.x + 32 * threadIdx.y;
+    const int ntx = (P.L[0] + G::TX - 1) / G::TX, nty = (P.L[1] + G::TY - 1) / G::TY;
+    const int T = ntx * nty * P.L[2];
+    unsigned int* work = F.sched;
+    unsigned int* ticket = F.sched + 1;
+    unsigned int* rows = F.sched + 2;
+    if (F.tma && tid == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0u;
+    for (;;) {
+        if (tid == 0) s_item = static_cast<int>(atomicAdd(work, 1u));
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= 2 * T) break;
+        const int tx = item % ntx;
+        const int ent = item / ntx;
+        const int z = ent / (2 * nty);
+        bool corr;
+        int ty;
+        wavefront_entry(ent - z * 2 * nty, nty, F.lag, corr, ty);
+        bool ok;
+        if (!corr) {
+            ok = fused_predictor<S, BYT, RY, SP>(&map_m, P, C, F, smem_t, &bar, phase, tx, ty, z,
+                                                 tx + ntx * (ty + nty * z), T, rows + z * nty + ty);
+        } else {
+            // wait for the predictor rows the corrector's stencil reaches
+            if (tid == 0) {
+                int okw = 1;
+                for (int d = -1; d <= 1 && okw; ++d) {
+                    int r = ty + d;
+                    if (r < 0 || r >= nty) {
+                        if (!P.periodic[1] || nty < 2) continue;
+                        r = (r + nty) % nty;
+                    }
+                    const unsigned int* w = rows + z * nty + r;
+                    uint32_t it = 0;
+                    while (ld_acquire_u32(w) < static_cast<unsigned int>(ntx)) {
+                        if (++it > kRowWaitPolls) {
+                            okw = 0;
+                            break;
+                        }
+                        if (it > 32) __nanosleep(128);
+                    }
+                }
+                __threadfence();
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                s_ok = okw;
+            }
+            __syncthreads();
+            ok = s_ok != 0;
+            if (ok) ok = fused_corrector<S, BYT, RY, SP>(&map_mid, P, C, F, smem_t, &bar, phase, tx, ty, z);
+        }
+        if (!ok) {
+            if (tid == 0 && F.status) atomicOr(F.status, kStatusTimeout);
+            break;
+        }
+        __syncthreads();  // the staging buffer is reused by the next item
+    }
+    // the last block to leave sums the energy partials and re-arms the scheduler
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (F.E_out) ordered_sum<1>(F.partials, T, F.E_out);
+    const int nrows = nty * P.L[2];
+    for (int r = tid; r < nrows; r += 32 * BYT) rows[r] = 0u;
+    if (tid == 0) {
+        *work = 0u;
+        *ticket = 0u;
     }
 }
 
@@ -594,8 +872,37 @@ struct TiledLauncher {
         auto kern = k_tiled<S, BYT, RY, PASS, MINB, SP>;
         dim3 g = grid(P);
         if (A.nty_all) g.y = static_cast<unsigned>(A.ty_count);  // a range of tile rows
-        kern<<<g, dim3(32, BYT), G::buf_bytes, s>>>(map, P, C, A);
-        return cuda_status(cudaGetLastError(), "k_tiled");
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = g;
+        cfg.blockDim = dim3(32, BYT);
+        cfg.dynamicSmemBytes = G::buf_bytes;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = A.pdl ? 1 : 0;
+        return cuda_status(cudaLaunchKernelEx(&cfg, kern, map, P, C, A), "k_tiled");
+    }
+    // the fused kernel holds both passes' code: a register cap of its own
+    static constexpr int FMINB = RY <= 2 ? 768 / (32 * BYT) : 1;
+    template <int SP>
+    static mj_status launch_fused(const CUtensorMap& map_m, const CUtensorMap& map_mid, const StencilParams& P,
+                                  const DynCoef& C, const FusedArgs& F, int num_sms, cudaStream_t s) {
+        auto kern = k_sib_fused<S, BYT, RY, FMINB, SP>;
+        static int per_sm = 0;  // resident blocks per SM (once per instantiation)
+        if (per_sm <= 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * BYT, G::buf_bytes) != cudaSuccess ||
+                per_sm <= 0)
+                per_sm = 1;
+        }
+        const dim3 g = grid(P);
+        const int64_t items = 2 * static_cast<int64_t>(g.x) * g.y * g.z;
+        const int nb = static_cast<int>(std::min<int64_t>(items, static_cast<int64_t>(per_sm) * num_sms));
+        FusedArgs Fl = F;
+        Fl.lag = static_cast<int>((nb + g.x - 1) / g.x) + 1;  // tile rows in flight, plus one
+        kern<<<nb, dim3(32, BYT), G::buf_bytes, s>>>(map_m, map_mid, P, C, Fl);
+        return cuda_status(cudaGetLastError(), "k_sib_fused");
     }
 };
 
@@ -717,12 +1024,44 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
             A.nty_all = static_cast<int>(Launcher::grid(p->sp).y);
             A.ty_count = nty;
             if (nty == 0) return MJ_OK;
-        } else if (p->use_tma && make_map(&map, ms, p->sp, G::PX, G::PY)) {
-            A.tma = 1;
+        } else {
+            if (p->use_tma && make_map(&map, ms, p->sp, G::PX, G::PY)) A.tma = 1;
+            A.pdl = p->use_pdl ? 1 : 0;
         }
         if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
         return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, axial, map,
                                                                                                    p->sp, C, A, s);
+    });
+}
+
+// One fused SIB step (predictor and corrector in one launch) of a 2D or layered
+// lattice without the dipolar term; E_out receives the energy of m_n (or null).
+template <class S>
+mj_status launch_sib_fused_shape(mj_plan* p, const DynCoef& C, double* m, double* draw, double* E_out, uint32_t step,
+                                 cudaStream_t s) {
+    FusedArgs F;
+    std::memset(&F, 0, sizeof(F));
+    F.m = m;
+    F.mid = p->d_mid;
+    F.draw = draw;
+    F.bmap = p->d_bmap;
+    F.partials = p->d_partials;
+    F.E_out = E_out;
+    F.sched = p->d_sched;
+    F.status = p->d_status;
+    F.step = step;
+    const bool axial = stencil_axial<S>(p->sp, p->d_bmap != nullptr);
+    return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
+        using Launcher = decltype(L);
+        using G = typename Launcher::G;
+        CUtensorMap map_m, map_mid;
+        std::memset(&map_m, 0, sizeof(map_m));
+        std::memset(&map_mid, 0, sizeof(map_mid));
+        if (p->use_tma && make_map(&map_m, m, p->sp, G::PX, G::PY) && make_map(&map_mid, p->d_mid, p->sp, G::PX, G::PY))
+            F.tma = 1;
+        p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
+        if (axial) return Launcher::template launch_fused<SP_AXIAL>(map_m, map_mid, p->sp, C, F, p->num_sms, s);
+        return Launcher::template launch_fused<SP_FULL>(map_m, map_mid, p->sp, C, F, p->num_sms, s);
     });
 }
 

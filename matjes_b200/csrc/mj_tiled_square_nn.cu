@@ -7,4 +7,8 @@ mj_status launch_tiled_square_nn(mj_plan* p, int pass, const DynCoef& C, const d
                          int emode, int ty0, int nty) {
     return launch_tiled_shape<ShapeSquareNN>(p, pass, C, ms, mn, out, aux, aux2, Hd, E_out, step, s, emode, ty0, nty);
 }
+mj_status launch_sib_fused_square_nn(mj_plan* p, const DynCoef& C, double* m, double* draw, double* E_out, uint32_t step,
+                         cudaStream_t s) {
+    return launch_sib_fused_shape<ShapeSquareNN>(p, C, m, draw, E_out, step, s);
+}
 }  // namespace mj

@@ -285,3 +285,78 @@ def test_full_size_injected_noise_200_steps(integrator):
     assert np.abs(m - mo).max() < 1e-9
     drift = np.abs(np.linalg.norm(m, axis=1) - 1.0).max()
     assert drift < (1e-13 if integrator == "sib" else 3e-13)
+
+
+@pytest.mark.parametrize("lattice", ["tri3_periodic", "square_open", "tri_nn_odd"])
+@pytest.mark.parametrize("thermal", [False, True])
+@pytest.mark.parametrize("variant,tma", [(5, 1), (4, 0), (1, 1)])
+def test_fused_sib_step_equals_two_launches(lattice, thermal, variant, tma):
+    """One SIB step in one launch (k_sib_fused: predictor and corrector tiles
+    from one work counter, a corrector tile waiting for the predictor rows it
+    reads) gives the two-launch result bit for bit: spins after 25 steps and the
+    energies of every step's incoming state.  Periodic and open edges, a lattice
+    whose sides are no multiple of the tile (and an odd Lx, plain staging),
+    Philox noise stored for the corrector."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    if lattice == "tri3_periodic":
+        deck = mj.triangular((96, 80))
+    elif lattice == "square_open":
+        deck = mj.square_film((70, 45, 1), periodic=(0, 0, 0))
+    else:
+        deck = mj.triangular((37, 53), J=(1.0e-3,))
+    m0 = torch.tensor(mj.random_sphere(deck.nsites, 12).T.copy(), device="cuda")
+    out = []
+    for fused in (1, 0):
+        ham = mj.Hamiltonian(deck)
+        _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, variant))
+        _abi.check(_abi.lib.mj_plan_set_tma(ham.plan, tma))
+        _abi.check(_abi.lib.mj_plan_set_fused(ham.plan, fused))
+        sd = mj.SpinDynamics(ham, integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0 if thermal else 0.0,
+                             noise="philox" if thermal else "off", seed=5)
+        sd.p.energy_mode = _abi.MJ_ENERGY_BEFORE
+        m = m0.clone()
+        E = sd.run(m, 25, energies=True)
+        torch.cuda.synchronize()
+        assert _abi.lib.mj_plan_check_status(ham.plan) == _abi.MJ_OK
+        out.append((m.cpu(), E.cpu()))
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("option,value", [("pdl", 0), ("store_draw", 0), ("fused_store", (1, 0))])
+def test_kernel_options_change_no_result(option, value):
+    """The plan's kernel options change how a step is computed, not its result:
+    without programmatic dependent launch, with the Philox draw redrawn by the
+    corrector instead of stored, and the fused step with the redrawn draw, 30
+    thermal SIB steps and their energies equal the default configuration's bit
+    for bit."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    deck = mj.triangular((96, 64))
+    m0 = torch.tensor(mj.random_sphere(deck.nsites, 13).T.copy(), device="cuda")
+    out = []
+    for changed in (False, True):
+        ham = mj.Hamiltonian(deck)
+        _abi.check(_abi.lib.mj_plan_set_variant(ham.plan, 5))
+        if changed:
+            if option == "fused_store":
+                _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_FUSED, value[0]))
+                _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_STORE_DRAW, value[1]))
+            else:
+                opt = {"pdl": _abi.MJ_OPT_PDL, "store_draw": _abi.MJ_OPT_STORE_DRAW}[option]
+                _abi.check(_abi.lib.mj_plan_set_option(ham.plan, opt, value))
+        sd = mj.SpinDynamics(ham, integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=8)
+        sd.p.energy_mode = _abi.MJ_ENERGY_BEFORE
+        m = m0.clone()
+        E = sd.run(m, 30, energies=True)
+        torch.cuda.synchronize()
+        out.append((m.cpu(), E.cpu()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    assert _abi.lib.mj_plan_set_option(ham.plan, 99, 1) == _abi.MJ_ERR_ARG
