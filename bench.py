@@ -1054,7 +1054,7 @@ def _prof_main(argv=None):
     ap.add_argument("--integrator", default="sib")
     ap.add_argument("--variant", default="auto")
     ap.add_argument("--tma", type=int, default=1, help="halo staging of the tiled kernels: 1 TMA, 0 plain loads")
-    ap.add_argument("--fused", type=int, default=1, help="SIB steps: 1 one fused launch, 0 two launches")
+    ap.add_argument("--fused", type=int, default=0, help="SIB steps: 1 one fused launch, 0 two launches")
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--adjoint", action="store_true", help="one forward + backward sweep of the SIB adjoint")
     ap.add_argument("--every", type=int, default=50, help="adjoint checkpoint spacing")
@@ -1186,7 +1186,7 @@ def main():
     ap.add_argument("--variant", type=int, default=None,
                     help="kernel variant (-1 generic, 0..5 tiled) instead of the timed sweep")
     ap.add_argument("--tma", type=int, default=0, help="halo staging with --variant: 1 TMA, 0 plain loads")
-    ap.add_argument("--fused", type=int, default=1, help="with --variant: 1 one launch per SIB step, 0 two")
+    ap.add_argument("--fused", type=int, default=0, help="with --variant: 1 one launch per SIB step, 0 two")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batch, adjoint, dipolar and Monte Carlo measurements")
     args = ap.parse_args()

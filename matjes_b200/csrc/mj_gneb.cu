@@ -7,8 +7,11 @@
 // :154-157).  The path is nimg images of the plan's N spins in one device
 // array, image r the SoA block x[N] | y[N] | z[N] at 3 N r.
 //
-// Per image one field launch (launch_field), the images side by side on forked
-// streams unless the dipolar term's FFT grid is shared; then k_gneb_sums
+// The images' fields: on a tiled plan without the dipolar term one launch over
+// all images (launch_field_images: blockIdx.z runs over image and layer, a 5D
+// TMA map over the path); otherwise per image one field launch (launch_field),
+// the images side by side on forked streams unless the dipolar term's FFT grid
+// is shared; then k_gneb_sums
 // (projection, the six path sums and, for side-by-side images, the energy of
 // every image) or, for the dipolar term's one-by-one launches that reduce
 // their energies themselves, k_gneb_project outside the iterations.  The rest of
@@ -74,6 +77,13 @@ struct PlanFields {
                 if (e != MJ_OK) return e;
             }
             return MJ_OK;
+        }
+        if (p->is_stencil && p->sp.shape != 0) {
+            // tiled plans: one launch over all images (image r = blockIdx.z's image)
+            const int rec = prof_begin(p, "k_field_images", s);
+            mj_status e = launch_field_images(p, m, F, esite, nrep, s);
+            prof_end(p, rec, s);
+            return e;
         }
         const int nside = std::min(kSide, nrep);
         mj_status e = cuda_status(cudaEventRecord(fork, s), "GNEB fork");

@@ -52,6 +52,16 @@ mj_status launch_sib_fused(mj_plan* p, const DynCoef& C, double* m, double* draw
     }
 }
 
+mj_status launch_field_images(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s) {
+    switch (p->sp.shape) {
+        case kShapeSquareNN: return launch_field_images_square_nn(p, m, B, e_site, nimg, s);
+        case kShapeSquare2: return launch_field_images_square2(p, m, B, e_site, nimg, s);
+        case kShapeTriNN: return launch_field_images_tri_nn(p, m, B, e_site, nimg, s);
+        case kShapeTri3: return launch_field_images_tri3(p, m, B, e_site, nimg, s);
+        default: return set_error(MJ_ERR_ARG, "no tiled kernel for this stencil shape");
+    }
+}
+
 int tiled_tile_rows(const mj_plan* p) {
     const int v = (p->tile_variant >= 0 && p->tile_variant < kTiledVariants) ? p->tile_variant : 0;
     const int ty = kTiledVariantTY[v];

@@ -71,6 +71,8 @@ struct TiledArgs {
     int ty_count;       // tile rows of this launch (host side: its grid height)
     int tma;            // 1: tile + halo staged by TMA through the kernel's tensor map
     int pdl;            // 1: launched as a programmatic dependent of the previous kernel
+    int nimg;           // > 1: blockIdx.z runs over (image, layer) of nimg lattices stored
+                        // back to back (3N doubles apart in ms / out, N in aux)
 };
 
 // Programmatic dependent launch: a kernel lets the next one in its stream launch
@@ -526,6 +528,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     }
     return false;
 }
+__device__ __forceinline__ void tma_load_5d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y, int z,
+                                            int c, int img) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+        "[%7];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(c), "r"(img), "r"(smem_u32(bar))
+        : "memory");
+}
 __device__ __forceinline__ void tma_load_4d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y, int z,
                                             int c) {
     asm volatile(
@@ -542,15 +552,25 @@ constexpr uint32_t kTmaWaitPolls = 1u << 22;
 template <class S, int BYT, int RY, int PASS, int MINB, int SP>
 __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant__ CUtensorMap tmap,
                                                      const __grid_constant__ StencilParams P, const DynCoef C,
-                                                     const TiledArgs A) {
+                                                     const TiledArgs A0) {
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_t[];
     __shared__ __align__(8) uint64_t bar;
     // a launch may cover the tile rows [ty0, ty0 + gridDim.y) of nty_all; block ids
     // (energy partials) are those of the launch over the whole lattice
-    const int by = static_cast<int>(blockIdx.y) + A.ty0;
-    const int nty = A.nty_all ? A.nty_all : static_cast<int>(gridDim.y);
-    const int x0 = blockIdx.x * G::TX, y0 = by * G::TY, z = blockIdx.z;
+    const int by = static_cast<int>(blockIdx.y) + A0.ty0;
+    const int nty = A0.nty_all ? A0.nty_all : static_cast<int>(gridDim.y);
+    int z = blockIdx.z, img = 0;
+    TiledArgs A = A0;
+    if (A0.nimg > 1) {  // image img of a launch over several lattices
+        img = z / P.L[2];
+        z -= img * P.L[2];
+        const int64_t n = static_cast<int64_t>(P.L[0]) * P.L[1] * P.L[2];
+        A.ms += 3 * n * img;
+        if (A.out) A.out += 3 * n * img;
+        if (A.aux) A.aux += n * img;
+    }
+    const int x0 = blockIdx.x * G::TX, y0 = by * G::TY;
     const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
     const int tid = threadIdx.x + 32 * threadIdx.y;
     // the epilogue inputs of the passes that draw the thermal field depend on no
@@ -573,7 +593,8 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
             if (A.pdl) pdl_wait_prev();
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&bar, static_cast<uint32_t>(G::buf_bytes));
-            tma_load_4d(&tmap, &bar, smem_t, x0 - G::RX, y0 - G::R, z, 0);
+            if (A.nimg > 1) tma_load_5d(&tmap, &bar, smem_t, x0 - G::RX, y0 - G::R, z, 0, img);
+            else tma_load_4d(&tmap, &bar, smem_t, x0 - G::RX, y0 - G::R, z, 0);
         }
         prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
         if (A.pdl) pdl_wait_prev();
@@ -872,6 +893,7 @@ struct TiledLauncher {
         auto kern = k_tiled<S, BYT, RY, PASS, MINB, SP>;
         dim3 g = grid(P);
         if (A.nty_all) g.y = static_cast<unsigned>(A.ty_count);  // a range of tile rows
+        if (A.nimg > 1) g.z *= static_cast<unsigned>(A.nimg);    // (image, layer)
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = g;
         cfg.blockDim = dim3(32, BYT);
@@ -990,6 +1012,24 @@ bool make_map(CUtensorMap* map, const double* base, const StencilParams& P, int 
     return r == CUDA_SUCCESS;
 }
 
+// 5D map over nimg lattices stored back to back: (x, y, z, component, image)
+bool make_map_images(CUtensorMap* map, const double* base, const StencilParams& P, int nimg, int box_x, int box_y) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    if ((reinterpret_cast<uintptr_t>(base) & 15u) != 0 || (P.L[0] & 1) != 0) return false;
+    const cuuint64_t layer = static_cast<cuuint64_t>(P.L[0]) * P.L[1];
+    const cuuint64_t n = layer * P.L[2];
+    const cuuint64_t dims[5] = {static_cast<cuuint64_t>(P.L[0]), static_cast<cuuint64_t>(P.L[1]),
+                                static_cast<cuuint64_t>(P.L[2]), 3, static_cast<cuuint64_t>(nimg)};
+    const cuuint64_t strides[4] = {static_cast<cuuint64_t>(P.L[0]) * 8, layer * 8, n * 8, 3 * n * 8};
+    const cuuint32_t box[5] = {static_cast<cuuint32_t>(box_x), static_cast<cuuint32_t>(box_y), 1, 3, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 // All passes of one compile-time shape (one translation unit per shape keeps
 // the build parallel).  pass: 0 field, 1 euler, 2 heun1, 3 heun2, 4 sib1, 5 sib2
 template <class S>
@@ -1062,6 +1102,34 @@ mj_status launch_sib_fused_shape(mj_plan* p, const DynCoef& C, double* m, double
         p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
         if (axial) return Launcher::template launch_fused<SP_AXIAL>(map_m, map_mid, p->sp, C, F, p->num_sms, s);
         return Launcher::template launch_fused<SP_FULL>(map_m, map_mid, p->sp, C, F, p->num_sms, s);
+    });
+}
+
+// The field and per-site energies (PASS_FIELD) of nimg lattices stored back to
+// back (m and B: 3N doubles apart; e_site: N apart) in one launch; no total
+// energy.  The GNEB on a plan evaluates its images this way.
+template <class S>
+mj_status launch_field_images_shape(mj_plan* p, const double* m, double* B, double* e_site, int nimg,
+                                    cudaStream_t s) {
+    TiledArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.ms = m;
+    A.out = B;
+    A.aux = e_site;
+    A.bmap = p->d_bmap;
+    A.status = p->d_status;
+    A.nimg = nimg;
+    A.pdl = p->use_pdl ? 1 : 0;
+    DynCoef C{};
+    const bool axial = stencil_axial<S>(p->sp, p->d_bmap != nullptr);
+    return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
+        using Launcher = decltype(L);
+        using G = typename Launcher::G;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        if (p->use_tma && make_map_images(&map, m, p->sp, nimg, G::PX, G::PY)) A.tma = 1;
+        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(PASS_FIELD, axial,
+                                                                                                   map, p->sp, C, A, s);
     });
 }
 

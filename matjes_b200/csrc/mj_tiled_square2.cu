@@ -11,4 +11,7 @@ mj_status launch_sib_fused_square2(mj_plan* p, const DynCoef& C, double* m, doub
                          cudaStream_t s) {
     return launch_sib_fused_shape<ShapeSquare2>(p, C, m, draw, E_out, step, s);
 }
+mj_status launch_field_images_square2(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s) {
+    return launch_field_images_shape<ShapeSquare2>(p, m, B, e_site, nimg, s);
+}
 }  // namespace mj
