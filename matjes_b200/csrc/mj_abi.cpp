@@ -296,6 +296,7 @@ void free_plan(mj_plan* p) {
     if (p->dip) dipolar_destroy(p);
     prof_clear(p);
     if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+    if (p->host_graph_exec) cudaGraphExecDestroy(p->host_graph_exec);
     if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
     for (cudaStream_t& ps : p->pipe_stream)
         if (ps) cudaStreamDestroy(ps);
@@ -334,15 +335,16 @@ mj_status ensure_host_scratch(mj_plan* p) {
     if (!p->d_tmp_b && (st = dalloc(&p->d_tmp_b, 3 * N, "tmp b")) != MJ_OK) return st;
     if (!p->d_tmp_e && (st = dalloc(&p->d_tmp_e, N + 8, "tmp e")) != MJ_OK) return st;
     if (!p->h_status) {
-        if ((st = cuda_status(cudaHostAlloc(&p->h_status, sizeof(int), cudaHostAllocDefault), "status mirror")) != MJ_OK)
+        if ((st = cuda_status(cudaHostAlloc(&p->h_status, 32, cudaHostAllocDefault), "status mirror")) != MJ_OK)
             return st;
-        *p->h_status = 0;
+        std::memset(p->h_status, 0, 32);
     }
     return MJ_OK;
 }
 
 mj_status dyn_coef(const mj_dyn_params* d, const mj_plan* plan, DynCoef& c) {
     if (!d) return set_error(MJ_ERR_ARG, "null dynamics parameters");
+    std::memset(&c, 0, sizeof(c));  // padding too: graphs are keyed by these bytes
     if (d->integrator != MJ_EULER && d->integrator != MJ_HEUN_MATJES && d->integrator != MJ_SIB)
         return set_error(MJ_ERR_ARG, "integrator must be MJ_EULER, MJ_HEUN_MATJES or MJ_SIB");
     if (!(d->timestep > 0.0) || !std::isfinite(d->timestep)) return set_error(MJ_ERR_ARG, "timestep must be > 0");
@@ -415,6 +417,9 @@ void drop_graph(mj_plan* p) {
     if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
     p->graph_exec = nullptr;
     p->graph_key.clear();
+    if (p->host_graph_exec) cudaGraphExecDestroy(p->host_graph_exec);
+    p->host_graph_exec = nullptr;
+    p->host_graph_key.clear();
 }
 
 void match_shape(StencilParams& sp) {
@@ -444,23 +449,20 @@ namespace {
 // 1.07 ms unstriped) beat more stripes or more compute streams.
 constexpr int kPipeStripes = 12;
 constexpr int kPipeCompute = 1;
-mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm, double* E_host, bool& used) {
-    used = false;
-    if (!p->is_stencil || p->sp.shape == 0 || p->sp.L[2] != 1 || p->dip_on) return MJ_OK;
-    cudaPointerAttributes pa;
-    if (cudaPointerGetAttributes(&pa, m_host) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
-        cudaGetLastError();  // a pageable pointer is not an error here
-        return MJ_OK;
-    }
+constexpr int kPipeStreams = 2 + kPipeCompute;
+constexpr int kPipeLevels = 5;  // at most transpose in, two passes, an energy pass, transpose out
+// The pinned mirror of the plan's status word (int at [0]) and of one energy
+// (double at byte 8), written by the host-array step's last copies.
+double* host_energy(mj_plan* p) { return reinterpret_cast<double*>(p->h_status + 2); }
+
+// The striped step's work, forked from and joined back into pipe_stream[0]
+// (captured once as a graph and replayed; the step index comes from the
+// plan's device step counter).
+mj_status striped_enqueue(mj_plan* p, double* m_host, const DynCoef& c, int energy_mode, bool E_wanted) {
+    const bool before = energy_mode == MJ_ENERGY_BEFORE;
+    const int64_t N = p->N, Lx = p->sp.L[0], Ly = p->sp.L[1];
     const int nty = tiled_tile_rows(p);
     const int K = std::min(kPipeStripes, nty);
-    if (K < 3) return MJ_OK;
-    DynCoef c;
-    mj_status st = dyn_coef(prm, p, c);
-    if (st != MJ_OK) return st;
-    if ((st = ensure_host_scratch(p)) != MJ_OK) return st;
-    used = true;
-    const int64_t N = p->N, Lx = p->sp.L[0], Ly = p->sp.L[1];
     const int TY = kTiledVariantTY[p->tile_variant];
     // passes of the step: (pass id, stencil input, own-site m_n, output, aux, aux2, energy partials)
     struct Pass {
@@ -474,40 +476,32 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
     };
     double* m = p->d_tmp_m;
     double* result = m;
-    const bool before = prm->energy_mode == MJ_ENERGY_BEFORE;
     std::vector<Pass> passes;
     if (c.integrator == MJ_EULER) {
-        passes.push_back({1, m, nullptr, p->d_mid, nullptr, nullptr, E_host && before});
+        passes.push_back({1, m, nullptr, p->d_mid, nullptr, nullptr, E_wanted && before});
         result = p->d_mid;
     } else if (c.integrator == MJ_HEUN_MATJES) {
-        passes.push_back({2, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, E_host && before});
+        passes.push_back({2, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, E_wanted && before});
         passes.push_back({3, p->d_mid, nullptr, m, p->d_aux, p->d_aux2, false});
     } else {
         double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX) ? p->d_aux : nullptr;
-        passes.push_back({4, m, nullptr, p->d_mid, bstore, nullptr, E_host && before});
+        passes.push_back({4, m, nullptr, p->d_mid, bstore, nullptr, E_wanted && before});
         passes.push_back({5, p->d_mid, m, m, bstore, nullptr, false});
     }
-    if (E_host && !before) passes.push_back({0, result, nullptr, nullptr, nullptr, nullptr, true});
+    if (E_wanted && !before) passes.push_back({0, result, nullptr, nullptr, nullptr, nullptr, true});
     const int Q = static_cast<int>(passes.size());
     const int nlev = Q + 2;  // 0 transpose in, 1..Q passes, Q + 1 transpose out
-    // streams: [0] uploads, [1] downloads, [2 ..] compute; events: uploads, tasks, start
-    for (cudaStream_t& ps : p->pipe_stream)
-        if (!ps && (st = cuda_status(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking), "pipeline stream")) != MJ_OK)
-            return st;
-    const int nev = K + nlev * K + 1;
-    while (static_cast<int>(p->pipe_events.size()) < nev) {
-        cudaEvent_t e;
-        if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pipeline event")) != MJ_OK) return st;
-        p->pipe_events.push_back(e);
-    }
+    // streams: [0] uploads (the origin), [1] downloads, [2 ..] compute; events:
+    // uploads, tasks, the fork, the joins
+    mj_status st;
     cudaStream_t sin = p->pipe_stream[0], sout = p->pipe_stream[1];
     cudaStream_t* sc = p->pipe_stream + 2;
     cudaEvent_t* ev_in = p->pipe_events.data();
     cudaEvent_t* ev_task = ev_in + K;  // [lvl * K + k]
-    cudaEvent_t ev_start = p->pipe_events[K + nlev * K];
-    // order after the work already queued on the legacy stream
-    cudaEventRecord(ev_start, 0);
-    for (cudaStream_t ps : p->pipe_stream) cudaStreamWaitEvent(ps, ev_start, 0);
+    cudaEvent_t ev_fork = p->pipe_events[K + kPipeLevels * K];
+    cudaEvent_t* ev_join = p->pipe_events.data() + K + kPipeLevels * K + 1;
+    cudaEventRecord(ev_fork, sin);
+    for (int q = 1; q < kPipeStreams; ++q) cudaStreamWaitEvent(p->pipe_stream[q], ev_fork, 0);
     // stripe k: tile rows [t0[k], t0[k + 1]), sites [s0[k], s0[k + 1])
     std::vector<int64_t> s0(K + 1);
     std::vector<int> t0(K + 1);
@@ -585,7 +579,7 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
             st = aos_to_soa_range(p->d_stage, m, a, cnt, N, cs);
         } else if (lvl <= Q) {
             const Pass& P = passes[lvl - 1];
-            st = launch_tiled(p, P.id, c, P.ms, P.mn, P.out, P.aux, P.aux2, Hd, nullptr, prm->step0, cs,
+            st = launch_tiled(p, P.id, c, P.ms, P.mn, P.out, P.aux, P.aux2, Hd, nullptr, 0u, cs,
                               P.energy ? 1 : 0, t0[kk], t0[kk + 1] - t0[kk]);
         } else {
             st = soa_to_aos_range(result, p->d_stage, a, cnt, N, cs);
@@ -608,15 +602,88 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
     if ((st = cuda_status(cudaMemcpyAsync(p->h_status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, sc[0]),
                           "status mirror")) != MJ_OK)
         return st;
-    if (E_host) {
+    if (E_wanted) {
         const int nthr = 32 * kTiledVariantBYT[p->tile_variant];
         if ((st = launch_ordered_sum(p->d_partials, static_cast<int>(tiled_energy_blocks(p)), nthr, p->d_scalar, sc[0])) != MJ_OK)
             return st;
+        if ((st = cuda_status(cudaMemcpyAsync(host_energy(p), p->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, sc[0]),
+                              "energy mirror")) != MJ_OK)
+            return st;
     }
-    for (cudaStream_t ps : p->pipe_stream)
-        if ((st = cuda_status(cudaStreamSynchronize(ps), "striped step")) != MJ_OK) return st;
+    // join every stream back into the origin
+    for (int q = 1; q < kPipeStreams; ++q) {
+        cudaEventRecord(ev_join[q], p->pipe_stream[q]);
+        cudaStreamWaitEvent(sin, ev_join[q], 0);
+    }
+    return MJ_OK;
+}
+
+mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm, double* E_host, bool& used) {
+    used = false;
+    if (!p->is_stencil || p->sp.shape == 0 || p->sp.L[2] != 1 || p->dip_on) return MJ_OK;
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, m_host) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+        cudaGetLastError();  // a pageable pointer is not an error here
+        return MJ_OK;
+    }
+    const int nty = tiled_tile_rows(p);
+    const int K = std::min(kPipeStripes, nty);
+    if (K < 3) return MJ_OK;
+    DynCoef c;
+    mj_status st = dyn_coef(prm, p, c);
+    if (st != MJ_OK) return st;
+    if ((st = ensure_host_scratch(p)) != MJ_OK) return st;
+    if (!p->d_stepctr && (st = dalloc(&p->d_stepctr, 4, "step counter")) != MJ_OK) return st;
+    used = true;
+    c.step_base = p->d_stepctr;
+    for (cudaStream_t& ps : p->pipe_stream)
+        if (!ps && (st = cuda_status(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking), "pipeline stream")) != MJ_OK)
+            return st;
+    // uploads, tasks, the fork, the joins, the start
+    const int nev = K + kPipeLevels * K + 1 + kPipeStreams + 1;
+    while (static_cast<int>(p->pipe_events.size()) < nev) {
+        cudaEvent_t e;
+        if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pipeline event")) != MJ_OK) return st;
+        p->pipe_events.push_back(e);
+    }
+    cudaStream_t sin = p->pipe_stream[0];
+    // the graph holds the host pointer, the coefficients, the stencil and the kernel configuration
+    std::string key(reinterpret_cast<const char*>(&c), sizeof(c));
+    key += std::string(reinterpret_cast<const char*>(&p->sp), sizeof(p->sp));
+    key += std::string(reinterpret_cast<const char*>(&m_host), sizeof(m_host));
+    key += std::string(reinterpret_cast<const char*>(&p->d_bmap), sizeof(p->d_bmap));
+    key += "/" + std::to_string(E_host != nullptr) + "/" + std::to_string(prm->energy_mode) + "/" +
+           std::to_string(p->tile_variant) + "/" + std::to_string(p->store_draw);
+    if (!p->host_graph_exec || p->host_graph_key != key) {
+        if (p->host_graph_exec) cudaGraphExecDestroy(p->host_graph_exec);
+        p->host_graph_exec = nullptr;
+        if ((st = cuda_status(cudaStreamBeginCapture(sin, cudaStreamCaptureModeThreadLocal), "begin capture")) != MJ_OK)
+            return st;
+        const mj_status inner = striped_enqueue(p, m_host, c, prm->energy_mode, E_host != nullptr);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(sin, &graph);
+        if (inner != MJ_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return inner;
+        }
+        if ((st = cuda_status(e, "end capture")) != MJ_OK) return st;
+        const cudaError_t ei = cudaGraphInstantiate(&p->host_graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if ((st = cuda_status(ei, "graph instantiate")) != MJ_OK) {
+            p->host_graph_exec = nullptr;
+            return st;
+        }
+        p->host_graph_key = key;
+    }
+    // after the work already queued on the legacy stream: the step index, then the step
+    cudaEvent_t ev_start = p->pipe_events[K + kPipeLevels * K + 1 + kPipeStreams];
+    cudaEventRecord(ev_start, 0);
+    cudaStreamWaitEvent(sin, ev_start, 0);
+    if ((st = step_counter(p->d_stepctr, prm->step0, false, sin)) != MJ_OK) return st;
+    if ((st = cuda_status(cudaGraphLaunch(p->host_graph_exec, sin), "graph launch")) != MJ_OK) return st;
+    if ((st = cuda_status(cudaStreamSynchronize(sin), "striped step")) != MJ_OK) return st;
     if ((st = status_from_word(p, *p->h_status)) != MJ_OK) return st;
-    if (E_host) return cuda_status(cudaMemcpy(E_host, p->d_scalar, sizeof(double), cudaMemcpyDeviceToHost), "energy");
+    if (E_host) *E_host = *host_energy(p);
     return MJ_OK;
 }
 

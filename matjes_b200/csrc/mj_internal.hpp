@@ -150,6 +150,9 @@ struct mj_plan {
     std::vector<cudaEvent_t> pipe_events;
     cudaGraphExec_t graph_exec = nullptr;
     std::string graph_key;
+    // the striped host-array step captured as a graph (mj_step_host), with its key
+    cudaGraphExec_t host_graph_exec = nullptr;
+    std::string host_graph_key;
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;
     struct ProfRec {

@@ -96,3 +96,25 @@ def test_striped_host_steps_chain_and_skip_energy():
     dev = torch.tensor(m0.T.copy(), device="cuda")
     mj.SpinDynamics(ham, **kw).run(dev, 5)
     np.testing.assert_allclose(host.numpy(), dev.cpu().numpy().T, rtol=0, atol=1e-15)
+
+
+def test_replayed_host_step_follows_buffer_and_parameter_changes():
+    """The striped step is captured once per host buffer, coefficients and kernel
+    configuration and replayed: alternating two pinned buffers and two
+    temperatures, each call equals the device step of the same input, step
+    index and parameters."""
+    import matjes_b200 as mj
+
+    deck = mj.triangular((96, 200))
+    ham = mj.Hamiltonian(deck)
+    bufs = [_pinned(mj.random_sphere(deck.nsites, s)) for s in (11, 12)]
+    for call in range(6):
+        kw = dict(integrator="sib", temperature=(5.0, 30.0)[call % 2], noise="philox", alpha=0.1, seed=7)
+        host = bufs[(call // 2) % 2]
+        m_in = host.numpy().copy()
+        want_m, want_E = _device_step(ham, m_in, kw, 0, 100 + call)
+        sd = mj.SpinDynamics(ham, **kw)
+        sd.p.energy_mode = 0
+        E = sd.run(host.numpy(), 1, energies=True, step0=100 + call)
+        assert np.array_equal(host.numpy(), want_m), call
+        assert E[0] == want_E, call
