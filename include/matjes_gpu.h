@@ -147,11 +147,11 @@ mj_status mj_plan_get_variant(const mj_plan* plan, int32_t* variant, int32_t* sh
  * the open boundary); 0 = plain loads with the periodic wrap per element.
  * Lattices with an odd Lx or a spin array not 16-byte aligned use plain loads. */
 mj_status mj_plan_set_tma(mj_plan* plan, int32_t enable);
-/* SIB steps of tiled plans without the dipolar term: enable = 1 (default) runs
+/* SIB steps of tiled plans without the dipolar term: enable = 1 runs
  * predictor and corrector in one launch (k_sib_fused: blocks take tiles from a
  * work counter, a corrector tile starts as soon as the predictor rows its
- * stencil reaches are done); 0 = two launches.  The results are the same bit
- * for bit.  No counterpart in the reference. */
+ * stencil reaches are done); 0 (default) = two launches.  The results are the
+ * same bit for bit.  No counterpart in the reference. */
 mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable);
 /* Kernel options of a stencil plan (none changes a result, every one only how
  * it is computed; no counterpart in the reference):
@@ -164,8 +164,12 @@ mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable);
  *   MJ_OPT_STORE_DRAW (default 1)  SIB with Philox noise: the predictor stores
  *                              its draw for the corrector (24 B per site written
  *                              and read back) instead of the corrector drawing
- *                              it again (the same numbers either way). */
-enum { MJ_OPT_TMA = 0, MJ_OPT_FUSED = 1, MJ_OPT_PDL = 2, MJ_OPT_STORE_DRAW = 3 };
+ *                              it again (the same numbers either way);
+ *   MJ_OPT_HOST_STRIPES (0 = default 4, at most 64)  stripes of tile rows that
+ *                              mj_step_host cuts a one-step call with pinned
+ *                              host spins into (fewer when the lattice has
+ *                              fewer than 5 tile rows per stripe). */
+enum { MJ_OPT_TMA = 0, MJ_OPT_FUSED = 1, MJ_OPT_PDL = 2, MJ_OPT_STORE_DRAW = 3, MJ_OPT_HOST_STRIPES = 4 };
 mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value);
 /* Autotuner: times `steps` steps of `p` for every kernel configuration of the
  * plan on a scratch copy of the device spins m_dev_soa (left untouched), keeps

@@ -433,27 +433,52 @@ void match_shape(StencilParams& sp) {
 namespace {
 
 // One step of host spins to host spins with the copies, the transposes and the
-// passes cut into K stripes of tile rows, so that the copies of one stripe run
-// while other stripes compute and the download of early stripes overlaps the
-// upload of late ones (full duplex).  Pass q of stripe k needs pass q - 1 of
-// stripes k - 1, k, k + 1 (stripes are at least one tile, 8 rows, deep; the
-// stencil reaches 2), the first pass needs the uploaded rows of those stripes;
-// stripe k's tasks run on compute stream k mod kPipeCompute with events for the
-// dependencies between streams, the copies on two more streams.  The
-// arithmetic, block ids and energy partials are those of the unstriped step, so
-// spins and energy are bit for bit the same.  Applies to tiled 2D plans without
-// the dipolar term, one step, pinned host memory; `used` is false otherwise.
-// The counts are measured (1024^2 triangular, B200 over PCIe): the copies bound
-// the step, and the copy engines overlap striped copies of opposite directions
-// only in part, so 12 stripes on one compute stream (0.95 ms per step against
-// 1.07 ms unstriped) beat more stripes or more compute streams.
-constexpr int kPipeStripes = 12;
-constexpr int kPipeCompute = 1;
-constexpr int kPipeStreams = 2 + kPipeCompute;
-constexpr int kPipeLevels = 5;  // at most transpose in, two passes, an energy pass, transpose out
+// passes cut into K stripes of tile rows, so that the upload of late stripes
+// runs while early ones compute and download (the host link is full duplex).
+// The passes of a step form a chain: each reads the previous one's output
+// through the stencil, which reaches ry <= TY rows, so at most one tile row
+// away.  Pass q of Q therefore runs over its stripe's tile rows shifted up by
+// Q - 1 - q: stripe k's passes then need only the output of stripes <= k, and
+// its first pass only the rows below 8 (t_{k+1} + Q - 1) + ry, which is what
+// upload chunk k holds.  Every stripe waits for its own upload alone, one
+// compute stream runs the stripes in order, and the copies stay few and large:
+// a copy engine overlaps opposite copies of >= 6 MB almost fully, of 2 MB only
+// in part (measured on a B200 over PCIe: 0.54 ms for 4 + 4 chunks of 24 MB
+// each way, 0.70 ms for 12 + 12).  With a periodic y, stripe 0 also runs each
+// shifted pass over the tile rows that the shift moves past the last row, and
+// upload chunk 0 carries the rows they read.  The arithmetic, block ids and
+// energy partials are those of the unstriped step, so spins and energy are bit
+// for bit the same.  Applies to tiled 2D plans without the dipolar term, one
+// step, pinned host memory; `used` is false otherwise.
+constexpr int kPipeStripesDefault = 4;
+constexpr int kPipeStreams = 3;  // uploads (the origin), downloads, compute
+
 // The pinned mirror of the plan's status word (int at [0]) and of one energy
 // (double at byte 8), written by the host-array step's last copies.
 double* host_energy(mj_plan* p) { return reinterpret_cast<double*>(p->h_status + 2); }
+
+// The y reach of the plan's stencil in rows.
+int stencil_reach_y(const mj_plan* p) {
+    int ry = 0;
+    for (int o = 0; o < p->sp.n_off; ++o) ry = std::max(ry, std::abs(p->sp.off[o][1]));
+    return ry;
+}
+
+// Stripes of the host-array step for this plan: 0 when it does not stripe.
+// Each stripe is at least 2 (Q - 1) + 1 = 5 tile rows deep, so that the
+// shifted ranges of every pass stay ordered.  The stencil must reach at most
+// one tile row, also across a periodic y edge (a last tile row shorter than
+// the reach would put two tile rows in reach of row 0).
+int host_stripes(const mj_plan* p) {
+    const int nty = tiled_tile_rows(p);
+    const int TY = kTiledVariantTY[p->tile_variant];
+    const int ry = stencil_reach_y(p);
+    if (ry > TY) return 0;
+    if (p->sp.periodic[1] && p->sp.L[1] - TY * (nty - 1) < ry) return 0;
+    const int want = p->host_stripes > 0 ? p->host_stripes : kPipeStripesDefault;
+    const int K = std::min(want, nty / 5);
+    return K >= 2 ? K : 0;
+}
 
 // The striped step's work, forked from and joined back into pipe_stream[0]
 // (captured once as a graph and replayed; the step index comes from the
@@ -462,8 +487,10 @@ mj_status striped_enqueue(mj_plan* p, double* m_host, const DynCoef& c, int ener
     const bool before = energy_mode == MJ_ENERGY_BEFORE;
     const int64_t N = p->N, Lx = p->sp.L[0], Ly = p->sp.L[1];
     const int nty = tiled_tile_rows(p);
-    const int K = std::min(kPipeStripes, nty);
+    const int K = host_stripes(p);
     const int TY = kTiledVariantTY[p->tile_variant];
+    const int ry = stencil_reach_y(p);
+    const bool per_y = p->sp.periodic[1] != 0;
     // passes of the step: (pass id, stencil input, own-site m_n, output, aux, aux2, energy partials)
     struct Pass {
         int id;
@@ -484,129 +511,111 @@ mj_status striped_enqueue(mj_plan* p, double* m_host, const DynCoef& c, int ener
         passes.push_back({2, m, nullptr, p->d_mid, p->d_aux, p->d_aux2, E_wanted && before});
         passes.push_back({3, p->d_mid, nullptr, m, p->d_aux, p->d_aux2, false});
     } else {
-        double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX) ? p->d_aux : nullptr;
+        double* bstore = (c.thermal && c.noise == MJ_NOISE_PHILOX && p->store_draw) ? p->d_aux : nullptr;
         passes.push_back({4, m, nullptr, p->d_mid, bstore, nullptr, E_wanted && before});
         passes.push_back({5, p->d_mid, m, m, bstore, nullptr, false});
     }
+    const int r = static_cast<int>(passes.size()) - 1;  // the pass that writes `result`
     if (E_wanted && !before) passes.push_back({0, result, nullptr, nullptr, nullptr, nullptr, true});
     const int Q = static_cast<int>(passes.size());
-    const int nlev = Q + 2;  // 0 transpose in, 1..Q passes, Q + 1 transpose out
-    // streams: [0] uploads (the origin), [1] downloads, [2 ..] compute; events:
-    // uploads, tasks, the fork, the joins
-    mj_status st;
-    cudaStream_t sin = p->pipe_stream[0], sout = p->pipe_stream[1];
-    cudaStream_t* sc = p->pipe_stream + 2;
-    cudaEvent_t* ev_in = p->pipe_events.data();
-    cudaEvent_t* ev_task = ev_in + K;  // [lvl * K + k]
-    cudaEvent_t ev_fork = p->pipe_events[K + kPipeLevels * K];
-    cudaEvent_t* ev_join = p->pipe_events.data() + K + kPipeLevels * K + 1;
-    cudaEventRecord(ev_fork, sin);
-    for (int q = 1; q < kPipeStreams; ++q) cudaStreamWaitEvent(p->pipe_stream[q], ev_fork, 0);
-    // stripe k: tile rows [t0[k], t0[k + 1]), sites [s0[k], s0[k + 1])
-    std::vector<int64_t> s0(K + 1);
-    std::vector<int> t0(K + 1);
-    for (int k = 0; k <= K; ++k) {
-        t0[k] = static_cast<int>(static_cast<int64_t>(k) * nty / K);
-        s0[k] = std::min<int64_t>(static_cast<int64_t>(t0[k]) * TY, Ly) * Lx;
-    }
-    const bool per_y = p->sp.periodic[1] != 0;
-    // uploads in the order the first pass needs them: with a periodic y the last
-    // stripe is a neighbour of the first
-    std::vector<int> order;
-    if (per_y) order.push_back(K - 1);
-    for (int k = 0; k < K - (per_y ? 1 : 0); ++k) order.push_back(k);
-    for (int k : order) {
-        const size_t off = static_cast<size_t>(3 * s0[k]), cnt = static_cast<size_t>(3 * (s0[k + 1] - s0[k]));
-        if ((st = cuda_status(cudaMemcpyAsync(p->d_stage + off, m_host + off, sizeof(double) * cnt,
-                                              cudaMemcpyHostToDevice, sin), "striped upload")) != MJ_OK)
-            return st;
-        cudaEventRecord(ev_in[k], sin);
-    }
-    // the stripes a task of stripe k at level lvl >= 1 reads from level lvl - 1
-    auto nbrs = [&](int lvl, int k, int out[3]) {
+    // stripe k: tile rows [t[k], t[k + 1])
+    std::vector<int> t(K + 1);
+    for (int k = 0; k <= K; ++k) t[k] = static_cast<int>(static_cast<int64_t>(k) * nty / K);
+    // the tile-row ranges of pass q in stripe k (two with a periodic wrap)
+    auto ranges = [&](int q, int k, int out[2][2]) {
+        const int sh = Q - 1 - q;
         int n = 0;
-        if (lvl == nlev - 1) {
-            out[n++] = k;
-            return n;
-        }
-        for (int d = -1; d <= 1; ++d) {
-            int j = k + d;
-            if (j < 0 || j >= K) {
-                if (!per_y) continue;
-                j = (j + K) % K;
-            }
-            if (n == 0 || out[n - 1] != j) out[n++] = j;
+        const int lo = k == 0 ? 0 : t[k] + sh;
+        const int hi = k == K - 1 ? nty - (per_y ? sh : 0) : t[k + 1] + sh;
+        out[n][0] = lo;
+        out[n++][1] = hi;
+        if (k == 0 && per_y && sh > 0) {
+            out[n][0] = nty - sh;
+            out[n++][1] = nty;
         }
         return n;
     };
-    // issue order: the deepest task whose inputs are issued, else the next upload's
-    // transpose (every event is recorded before a stream waits on it)
-    std::vector<std::vector<char>> done(nlev, std::vector<char>(K, 0));
-    size_t next_in = 0;
-    int remaining = nlev * K;
-    DipView Hd{};
-    while (remaining > 0) {
-        int lvl = -1, kk = -1;
-        for (int l = nlev - 1; l >= 1 && lvl < 0; --l)
-            for (int k = 0; k < K; ++k) {
-                if (done[l][k]) continue;
-                int nb[3];
-                const int n = nbrs(l, k, nb);
-                bool ready = true;
-                for (int q = 0; q < n && ready; ++q) ready = done[l - 1][nb[q]] != 0;
-                if (ready) {
-                    lvl = l;
-                    kk = k;
-                    break;
+    auto row_of = [&](int tile_row) { return std::min<int64_t>(static_cast<int64_t>(tile_row) * TY, Ly); };
+    // upload chunks in rows: chunk k = [u[k], u[k + 1]); with a periodic y chunk 0 also
+    // holds the wrap rows [w, Ly) that the shifted first pass reads
+    const int sh0 = Q - 1;
+    const int64_t w = per_y ? std::max<int64_t>(0, (sh0 > 0 ? row_of(nty - sh0) : Ly) - ry) : Ly;
+    std::vector<int64_t> u(K + 1);
+    u[0] = 0;
+    for (int k = 0; k < K; ++k) {
+        int rg[2][2];
+        ranges(0, k, rg);
+        u[k + 1] = k == K - 1 ? w : std::min(w, std::max(u[k], row_of(rg[0][1]) + ry));
+    }
+    mj_status st;
+    cudaStream_t sin = p->pipe_stream[0], sout = p->pipe_stream[1], sc = p->pipe_stream[2];
+    cudaEvent_t* ev_in = p->pipe_events.data();
+    cudaEvent_t* ev_out = ev_in + K;
+    cudaEvent_t ev_fork = ev_out[K];
+    cudaEvent_t* ev_join = ev_out + K + 1;
+    cudaEventRecord(ev_fork, sin);
+    for (int q = 1; q < kPipeStreams; ++q) cudaStreamWaitEvent(p->pipe_stream[q], ev_fork, 0);
+    auto upload = [&](int64_t r0, int64_t r1) -> mj_status {
+        if (r1 <= r0) return MJ_OK;
+        const size_t off = static_cast<size_t>(3 * Lx * r0), cnt = static_cast<size_t>(3 * Lx * (r1 - r0));
+        return cuda_status(cudaMemcpyAsync(p->d_stage + off, m_host + off, sizeof(double) * cnt, cudaMemcpyHostToDevice,
+                                           sin), "striped upload");
+    };
+    for (int k = 0; k < K; ++k) {
+        if (k == 0 && (st = upload(w, Ly)) != MJ_OK) return st;
+        if ((st = upload(u[k], u[k + 1])) != MJ_OK) return st;
+        cudaEventRecord(ev_in[k], sin);
+    }
+    for (int k = 0; k < K; ++k) {
+        cudaStreamWaitEvent(sc, ev_in[k], 0);
+        if (k == 0 && w < Ly && (st = aos_to_soa_range(p->d_stage, m, Lx * w, Lx * (Ly - w), N, sc)) != MJ_OK) return st;
+        if (u[k + 1] > u[k] && (st = aos_to_soa_range(p->d_stage, m, Lx * u[k], Lx * (u[k + 1] - u[k]), N, sc)) != MJ_OK)
+            return st;
+        int down[2][2];
+        int ndown = 0;
+        for (int q = 0; q < Q; ++q) {
+            const Pass& P = passes[q];
+            int rg[2][2];
+            const int n = ranges(q, k, rg);
+            for (int i = 0; i < n; ++i) {
+                if (rg[i][1] <= rg[i][0]) continue;
+                st = launch_tiled(p, P.id, c, P.ms, P.mn, P.out, P.aux, P.aux2, DipView{}, nullptr, 0u, sc,
+                                  P.energy ? 1 : 0, rg[i][0], rg[i][1] - rg[i][0]);
+                if (st != MJ_OK) return st;
+            }
+            if (q == r) {
+                ndown = n;
+                for (int i = 0; i < n; ++i) {
+                    down[i][0] = rg[i][0];
+                    down[i][1] = rg[i][1];
                 }
             }
-        if (lvl < 0) {
-            if (next_in >= order.size()) return set_error(MJ_ERR_ARG, "striped step: no task to issue");
-            lvl = 0;
-            kk = order[next_in++];
         }
-        cudaStream_t cs = sc[kk % kPipeCompute];
-        if (lvl == 0) {
-            cudaStreamWaitEvent(cs, ev_in[kk], 0);
-        } else {
-            int nb[3];
-            const int n = nbrs(lvl, kk, nb);
-            for (int q = 0; q < n; ++q)
-                if (nb[q] % kPipeCompute != kk % kPipeCompute) cudaStreamWaitEvent(cs, ev_task[(lvl - 1) * K + nb[q]], 0);
+        for (int i = 0; i < ndown; ++i) {
+            const int64_t r0 = row_of(down[i][0]), r1 = row_of(down[i][1]);
+            if (r1 > r0 && (st = soa_to_aos_range(result, p->d_stage, Lx * r0, Lx * (r1 - r0), N, sc)) != MJ_OK) return st;
         }
-        const int64_t a = s0[kk], cnt = s0[kk + 1] - s0[kk];
-        if (lvl == 0) {
-            st = aos_to_soa_range(p->d_stage, m, a, cnt, N, cs);
-        } else if (lvl <= Q) {
-            const Pass& P = passes[lvl - 1];
-            st = launch_tiled(p, P.id, c, P.ms, P.mn, P.out, P.aux, P.aux2, Hd, nullptr, 0u, cs,
-                              P.energy ? 1 : 0, t0[kk], t0[kk + 1] - t0[kk]);
-        } else {
-            st = soa_to_aos_range(result, p->d_stage, a, cnt, N, cs);
-        }
-        if (st != MJ_OK) return st;
-        cudaEventRecord(ev_task[lvl * K + kk], cs);
-        if (lvl == nlev - 1) {
-            cudaStreamWaitEvent(sout, ev_task[lvl * K + kk], 0);
-            if ((st = cuda_status(cudaMemcpyAsync(m_host + 3 * a, p->d_stage + 3 * a, sizeof(double) * 3 * cnt,
+        cudaEventRecord(ev_out[k], sc);
+        cudaStreamWaitEvent(sout, ev_out[k], 0);
+        for (int i = 0; i < ndown; ++i) {
+            const int64_t r0 = row_of(down[i][0]), r1 = row_of(down[i][1]);
+            if (r1 <= r0) continue;
+            const size_t off = static_cast<size_t>(3 * Lx * r0), cnt = static_cast<size_t>(3 * Lx * (r1 - r0));
+            if ((st = cuda_status(cudaMemcpyAsync(m_host + off, p->d_stage + off, sizeof(double) * cnt,
                                                   cudaMemcpyDeviceToHost, sout), "striped download")) != MJ_OK)
                 return st;
         }
-        done[lvl][kk] = 1;
-        --remaining;
     }
-    // every stripe's last task (its passes, energy partials included) has
-    // finished before sc[0] reads the status word and sums the energy
-    for (int k = 0; k < K; ++k)
-        if (k % kPipeCompute != 0) cudaStreamWaitEvent(sc[0], ev_task[(nlev - 1) * K + k], 0);
-    if ((st = cuda_status(cudaMemcpyAsync(p->h_status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, sc[0]),
+    // every stripe's passes (energy partials included) have run on sc before it
+    // reads the status word and sums the energy
+    if ((st = cuda_status(cudaMemcpyAsync(p->h_status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, sc),
                           "status mirror")) != MJ_OK)
         return st;
     if (E_wanted) {
         const int nthr = 32 * kTiledVariantBYT[p->tile_variant];
-        if ((st = launch_ordered_sum(p->d_partials, static_cast<int>(tiled_energy_blocks(p)), nthr, p->d_scalar, sc[0])) != MJ_OK)
+        if ((st = launch_ordered_sum(p->d_partials, static_cast<int>(tiled_energy_blocks(p)), nthr, p->d_scalar, sc)) != MJ_OK)
             return st;
-        if ((st = cuda_status(cudaMemcpyAsync(host_energy(p), p->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, sc[0]),
+        if ((st = cuda_status(cudaMemcpyAsync(host_energy(p), p->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, sc),
                               "energy mirror")) != MJ_OK)
             return st;
     }
@@ -626,9 +635,8 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
         cudaGetLastError();  // a pageable pointer is not an error here
         return MJ_OK;
     }
-    const int nty = tiled_tile_rows(p);
-    const int K = std::min(kPipeStripes, nty);
-    if (K < 3) return MJ_OK;
+    const int K = host_stripes(p);
+    if (K == 0) return MJ_OK;
     DynCoef c;
     mj_status st = dyn_coef(prm, p, c);
     if (st != MJ_OK) return st;
@@ -636,11 +644,12 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
     if (!p->d_stepctr && (st = dalloc(&p->d_stepctr, 4, "step counter")) != MJ_OK) return st;
     used = true;
     c.step_base = p->d_stepctr;
-    for (cudaStream_t& ps : p->pipe_stream)
-        if (!ps && (st = cuda_status(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking), "pipeline stream")) != MJ_OK)
+    for (int q = 0; q < kPipeStreams; ++q)
+        if (!p->pipe_stream[q] &&
+            (st = cuda_status(cudaStreamCreateWithFlags(&p->pipe_stream[q], cudaStreamNonBlocking), "pipeline stream")) != MJ_OK)
             return st;
-    // uploads, tasks, the fork, the joins, the start
-    const int nev = K + kPipeLevels * K + 1 + kPipeStreams + 1;
+    // uploads, downloads, the fork, the joins, the start
+    const int nev = 2 * K + 1 + kPipeStreams + 1;
     while (static_cast<int>(p->pipe_events.size()) < nev) {
         cudaEvent_t e;
         if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "pipeline event")) != MJ_OK) return st;
@@ -653,7 +662,7 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
     key += std::string(reinterpret_cast<const char*>(&m_host), sizeof(m_host));
     key += std::string(reinterpret_cast<const char*>(&p->d_bmap), sizeof(p->d_bmap));
     key += "/" + std::to_string(E_host != nullptr) + "/" + std::to_string(prm->energy_mode) + "/" +
-           std::to_string(p->tile_variant) + "/" + std::to_string(p->store_draw);
+           std::to_string(p->tile_variant) + "/" + std::to_string(p->store_draw) + "/" + std::to_string(K);
     if (!p->host_graph_exec || p->host_graph_key != key) {
         if (p->host_graph_exec) cudaGraphExecDestroy(p->host_graph_exec);
         p->host_graph_exec = nullptr;
@@ -676,7 +685,7 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
         p->host_graph_key = key;
     }
     // after the work already queued on the legacy stream: the step index, then the step
-    cudaEvent_t ev_start = p->pipe_events[K + kPipeLevels * K + 1 + kPipeStreams];
+    cudaEvent_t ev_start = p->pipe_events[nev - 1];
     cudaEventRecord(ev_start, 0);
     cudaStreamWaitEvent(sin, ev_start, 0);
     if ((st = step_counter(p->d_stepctr, prm->step0, false, sin)) != MJ_OK) return st;
@@ -1005,6 +1014,10 @@ mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value) {
         case MJ_OPT_FUSED: plan->fused_sib = value != 0; break;
         case MJ_OPT_PDL: plan->use_pdl = value != 0; break;
         case MJ_OPT_STORE_DRAW: plan->store_draw = value != 0; break;
+        case MJ_OPT_HOST_STRIPES:
+            if (value < 0 || value > 64) return set_error(MJ_ERR_ARG, "host stripes must be in [0, 64]");
+            plan->host_stripes = value;
+            break;
         default: return set_error(MJ_ERR_ARG, "unknown plan option " + std::to_string(option));
     }
     drop_graph(plan);

@@ -153,6 +153,7 @@ struct mj_plan {
     // the striped host-array step captured as a graph (mj_step_host), with its key
     cudaGraphExec_t host_graph_exec = nullptr;
     std::string host_graph_key;
+    int host_stripes = 0;  // stripes of mj_step_host (0: the default)
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;
     struct ProfRec {

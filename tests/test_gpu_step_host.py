@@ -118,3 +118,26 @@ def test_replayed_host_step_follows_buffer_and_parameter_changes():
         E = sd.run(host.numpy(), 1, energies=True, step0=100 + call)
         assert np.array_equal(host.numpy(), want_m), call
         assert E[0] == want_E, call
+
+
+@pytest.mark.parametrize("stripes", [2, 3, 5, 9, 64])
+def test_any_stripe_count_equals_the_device_step(stripes):
+    """Every stripe count (64 is clamped to 5 tile rows per stripe) gives the
+    device step bit for bit: SIB at 10 K with the energy after the step (three
+    chained passes, the first shifted by two tile rows) and before it."""
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    deck = mj.triangular((96, 1000))
+    ham = mj.Hamiltonian(deck)
+    _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_STRIPES, stripes))
+    kw = dict(integrator="sib", temperature=10.0, noise="philox", alpha=0.1, timestep=0.1, seed=5)
+    m0 = mj.random_sphere(deck.nsites, 21)
+    for energy_mode in (1, 0):
+        want_m, want_E = _device_step(ham, m0, kw, energy_mode, 7)
+        host = _pinned(m0)
+        sd = mj.SpinDynamics(ham, **kw)
+        sd.p.energy_mode = energy_mode
+        E = sd.run(host.numpy(), 1, energies=True, step0=7)
+        assert np.array_equal(host.numpy(), want_m), (stripes, energy_mode)
+        assert E[0] == want_E, (stripes, energy_mode)
