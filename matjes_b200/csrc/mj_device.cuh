@@ -34,19 +34,46 @@ __device__ __forceinline__ void philox10(uint32_t c[4], uint32_t k0, uint32_t k1
     }
 }
 
-// Philox4x32-10 with the ten round keys precomputed (keys[2r], keys[2r+1]).
+// Philox4x32-10 with the ten round keys precomputed (keys[2r], keys[2r+1]);
+// each round's two products as one 32 x 32 -> 64-bit multiply (low and high
+// words of the same product).
 __device__ __forceinline__ void philox10k(uint32_t c[4], const uint32_t* keys) {
     const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = M0 * c[0], hi0 = __umulhi(M0, c[0]);
-        const uint32_t lo1 = M1 * c[2], hi1 = __umulhi(M1, c[2]);
+        const uint64_t p0 = static_cast<uint64_t>(M0) * c[0], p1 = static_cast<uint64_t>(M1) * c[2];
+        const uint32_t lo0 = static_cast<uint32_t>(p0), hi0 = static_cast<uint32_t>(p0 >> 32);
+        const uint32_t lo1 = static_cast<uint32_t>(p1), hi1 = static_cast<uint32_t>(p1 >> 32);
         const uint32_t n0 = hi1 ^ c[1] ^ keys[2 * r];
         const uint32_t n2 = hi0 ^ c[3] ^ keys[2 * r + 1];
         c[0] = n0;
         c[1] = lo1;
         c[2] = n2;
         c[3] = lo0;
+    }
+}
+
+// Two independent blocks through the same rounds (the round keys read once,
+// the two dependency chains interleaved): the same words as two philox10k calls.
+__device__ __forceinline__ void philox10k_x2(uint32_t a[4], uint32_t b[4], const uint32_t* keys) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t k0 = keys[2 * r], k1 = keys[2 * r + 1];
+        const uint64_t pa0 = static_cast<uint64_t>(M0) * a[0], pa1 = static_cast<uint64_t>(M1) * a[2];
+        const uint64_t pb0 = static_cast<uint64_t>(M0) * b[0], pb1 = static_cast<uint64_t>(M1) * b[2];
+        const uint32_t na0 = static_cast<uint32_t>(pa1 >> 32) ^ a[1] ^ k0;
+        const uint32_t na2 = static_cast<uint32_t>(pa0 >> 32) ^ a[3] ^ k1;
+        const uint32_t nb0 = static_cast<uint32_t>(pb1 >> 32) ^ b[1] ^ k0;
+        const uint32_t nb2 = static_cast<uint32_t>(pb0 >> 32) ^ b[3] ^ k1;
+        a[0] = na0;
+        a[1] = static_cast<uint32_t>(pa1);
+        a[2] = na2;
+        a[3] = static_cast<uint32_t>(pa0);
+        b[0] = nb0;
+        b[1] = static_cast<uint32_t>(pb1);
+        b[2] = nb2;
+        b[3] = static_cast<uint32_t>(pb0);
     }
 }
 
@@ -99,12 +126,8 @@ __device__ __forceinline__ void sincos2pi_word(uint32_t w, const double* __restr
     *c = t.y + fma(t.y, cm, -(t.x * sx));
 }
 
-// N(0,1) triple of one site and step from one Philox block, counter = (site,
-// step, stream, 0)
-__device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, const double* __restrict__ tab,
-                                                      uint32_t step, uint32_t stream, uint32_t site) {
-    uint32_t c[4] = {site, step, stream, 0u};
-    philox10k(c, keys);
+// The three normals of one Philox block's words: (r1 cos t1, r1 sin t1, r2 cos t2)
+__device__ __forceinline__ double3 normals_of_block(const uint32_t c[4], const double* __restrict__ tab) {
     const double r1 = sqrt(-2.0 * tab_log(u32_half(c[0]), tab));
     const double r2 = sqrt(-2.0 * tab_log(u32_half(c[2]), tab));
     double s1, c1, s2, c2;
@@ -113,6 +136,16 @@ __device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, cons
     return make_double3(r1 * c1, r1 * s1, r2 * c2);
 }
 
+// N(0,1) triple of one site and step from one Philox block, counter = (site,
+// step, stream, 0)
+__device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, const double* __restrict__ tab,
+                                                      uint32_t step, uint32_t stream, uint32_t site) {
+    uint32_t c[4] = {site, step, stream, 0u};
+    philox10k(c, keys);
+    return normals_of_block(c, tab);
+}
+
+// The same from the 64-bit seed (round keys derived here)
 __device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site,
                                                   const double* __restrict__ tab) {
     uint32_t keys[20];
@@ -136,6 +169,19 @@ __device__ __forceinline__ double3 thermal_field(const DynCoef& C, uint32_t step
     }
     const double* buf = C.inject + static_cast<int64_t>(step % static_cast<uint32_t>(C.inject_nbuf)) * 3 * N;
     return make_double3(C.sigma * __ldg(buf + i), C.sigma * __ldg(buf + N + i), C.sigma * __ldg(buf + 2 * N + i));
+}
+
+// The Philox thermal fields of two sites of one step together (the words and
+// normals of two thermal_field calls).
+__device__ __forceinline__ void thermal_field_x2(const DynCoef& C, uint32_t step, int64_t i0, int64_t i1, double3& b0,
+                                                 double3& b1) {
+    if (C.step_base) step += *C.step_base;
+    uint32_t a[4] = {static_cast<uint32_t>(i0), step, C.stream_id, 0u};
+    uint32_t b[4] = {static_cast<uint32_t>(i1), step, C.stream_id, 0u};
+    philox10k_x2(a, b, C.keys);
+    const double3 za = normals_of_block(a, C.noise_tab), zb = normals_of_block(b, C.noise_tab);
+    b0 = make_double3(C.sigma * za.x, C.sigma * za.y, C.sigma * za.z);
+    b1 = make_double3(C.sigma * zb.x, C.sigma * zb.y, C.sigma * zb.z);
 }
 
 // ---------------------------------------------------------------------------

@@ -418,6 +418,20 @@ __device__ __forceinline__ void prefetch_sites(const StencilParams& P, const Dyn
     const int64_t layer = static_cast<int64_t>(Lx) * Ly;
     const int64_t N = layer * P.L[2];
     const int x = x0 + threadIdx.x;
+    if constexpr (RY % 2 == 0 && (PASS == PASS_SIB1 || PASS == PASS_EULER || PASS == PASS_HEUN1)) {
+        if (C.thermal && C.noise == MJ_NOISE_PHILOX) {
+            // the draws of the thread's sites two at a time (a site past the
+            // lattice's edge draws too and is not used)
+#pragma unroll
+            for (int r = 0; r < RY; r += 2) {
+                const int y = y0 + threadIdx.y * RY + r;
+                const int64_t i = layer * z + x + static_cast<int64_t>(Lx) * y;
+                pre[r].a = pre[r + 1].a = make_double3(0.0, 0.0, 0.0);
+                thermal_field_x2(C, A.step, i, i + Lx, pre[r].b, pre[r + 1].b);
+            }
+            return;
+        }
+    }
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
         const int y = y0 + threadIdx.y * RY + r;
