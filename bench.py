@@ -667,12 +667,14 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
     ach = bpsite * n * nim / per_it / 1e9
     del batch
     # the same path held on the deck's plan (mj_gneb_path: one field launch of
-    # the plan per image, then the path sums): 312 algorithmic bytes per image
-    # site and iteration (the field pass 48, the sums m and F in, F out 72, the
-    # step 120, the move 72)
+    # the plan over all images, then the path sums): 312 algorithmic bytes per
+    # image site and iteration (the field pass 48, the sums m and F in, F out 72,
+    # the step 120, the move 72); the plan's tile variant autotuned first
     from matjes_b200.gneb import PlanPath
 
-    holder = PlanPath(mj.Hamiltonian(deck, device=dev), path)
+    ham_p = mj.Hamiltonian(deck, device=dev)
+    holder = PlanPath(ham_p, path)
+    tv = plan_variant_tuned(ham_p, holder.m[0])
 
     def call_plan(its):
         holder.m.copy_(torch.tensor(path.transpose(0, 2, 1).copy(), device=holder.m.device))
@@ -685,7 +687,7 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
 
     call_plan(40)
     per_it_plan = (min(call_plan(600) for _ in range(3)) - min(call_plan(100) for _ in range(3))) / 500
-    del holder
+    del holder, ham_p
     plan_bpsite = 312.0
     plan_ach = plan_bpsite * n * nim / per_it_plan / 1e9
     mod = O.Model(deck)
@@ -701,9 +703,10 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
             "launches_per_iteration": 4,
             "roofline": {"bound": "hbm", "alg_bytes_per_site": bpsite, "achieved": ach, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"]},
-            "on_plan": {"path": "mj_gneb_path: the images held on the deck's plan, one tiled field launch per image",
+            "on_plan": {"path": "mj_gneb_path: the images held on the deck's plan, one tiled field launch over all "
+                                "images (5D tensor map with an image index), then the GNEB sums, step and move",
                         "value": n * nim / per_it_plan, "us_per_iteration": 1e6 * per_it_plan,
-                        "launches_per_iteration": nim + 3,
+                        "launches_per_iteration": 4, "tile_variant": tv,
                         "roofline": {"bound": "hbm", "alg_bytes_per_site": plan_bpsite, "achieved": plan_ach,
                                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": plan_ach / pk["hbm_gbs"],
                                      "peak_source": pk["source"]}},
@@ -748,7 +751,7 @@ def timed_steps(lib, _abi, plan, m, p, first_step, K, flush, E, stream):
     return sum(a.elapsed_time(b) for a, b in ev)
 
 
-OPTION_NAMES = {"fused": 1, "pdl": 2, "store_draw": 3}  # mj_plan_set_option ids
+OPTION_NAMES = {"fused": 1, "pdl": 2, "store_draw": 3, "blocks_per_sm": 5}  # mj_plan_set_option ids
 
 
 def tune_kernels(lib, _abi, plan, m, p, flush, E, stream, variants=True):
@@ -763,8 +766,8 @@ def tune_kernels(lib, _abi, plan, m, p, flush, E, stream, variants=True):
         return sorted(timed_steps(lib, _abi, plan, m, p, k0 + 2 + k, 1, flush, E, stream) for k in range(8))[4]
 
     table = {}
-    best = {"variant": None, "tma": None, "fused": 0, "pdl": 1, "store_draw": 1}
-    for name, val in (("fused", 0), ("pdl", 1), ("store_draw", 1)):
+    best = {"variant": None, "tma": None, "fused": 0, "pdl": 1, "store_draw": 1, "blocks_per_sm": 0}
+    for name, val in (("fused", 0), ("pdl", 1), ("store_draw", 1), ("blocks_per_sm", 0)):
         _abi.check(lib.mj_plan_set_option(plan, OPTION_NAMES[name], val))
     if variants:
         configs = [(-1, 0)] + [(v, t) for t in (0, 1) for v in range(6)]
@@ -779,7 +782,8 @@ def tune_kernels(lib, _abi, plan, m, p, flush, E, stream, variants=True):
         _abi.check(lib.mj_plan_set_tma(plan, bt))
         best.update(variant=bv, tma=bt)
     base = min(table.values()) if table else med(1000)
-    for name, val in (("fused", 1), ("pdl", 0), ("store_draw", 0)):
+    for name, val in (("fused", 1), ("pdl", 0), ("store_draw", 0), ("blocks_per_sm", 7), ("blocks_per_sm", 6),
+                      ("blocks_per_sm", 5)):
         _abi.check(lib.mj_plan_set_option(plan, OPTION_NAMES[name], val))
         t = med(2000)
         table[f"{name}={val}"] = t
@@ -1148,6 +1152,20 @@ def _prof_adjoint(a):
     print("ok", gt.tolist(), float(g0.abs().sum()), float(gb.abs().sum()))
 
 
+def plan_variant_tuned(ham, m_soa) -> int:
+    """The plan's tile variant autotuned on SIB steps of the spins m_soa (a (3,
+    N) device tensor, left untouched); -1 for a plan without tiled kernels."""
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    tv = _abi.C.c_int32(-1)
+    if ham.noffsets:
+        sd = mj.SpinDynamics(ham, integrator="sib", timestep=0.1, alpha=0.1)
+        _abi.check(_abi.lib.mj_plan_autotune(ham.plan, m_soa.data_ptr(), _abi.C.byref(sd.p), 3, _abi.C.byref(tv),
+                                             None, None))
+    return int(tv.value)
+
+
 def _prof_gneb(a):
     import matjes_b200 as mj
     from matjes_b200.gneb import geodesic_path
@@ -1160,7 +1178,9 @@ def _prof_gneb(a):
     if a.plan:
         from matjes_b200.gneb import PlanPath
 
-        bt = PlanPath(mj.Hamiltonian(deck), path)
+        ham = mj.Hamiltonian(deck)
+        bt = PlanPath(ham, path)
+        plan_variant_tuned(ham, bt.m[0])
     else:
         bt = mj.ReplicaBatch(deck, [(a.L, a.L)] * a.nim, np.tile(deck.B_ext, (a.nim, 1)), [0.0] * a.nim)
         bt.upload(path.reshape(-1, 3))

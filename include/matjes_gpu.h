@@ -168,8 +168,20 @@ mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable);
  *   MJ_OPT_HOST_STRIPES (0 = default 4, at most 64)  stripes of tile rows that
  *                              mj_step_host cuts a one-step call with pinned
  *                              host spins into (fewer when the lattice has
- *                              fewer than 5 tile rows per stripe). */
-enum { MJ_OPT_TMA = 0, MJ_OPT_FUSED = 1, MJ_OPT_PDL = 2, MJ_OPT_STORE_DRAW = 3, MJ_OPT_HOST_STRIPES = 4 };
+ *                              fewer than 5 tile rows per stripe);
+ *   MJ_OPT_BLOCKS_PER_SM (0 = default: no cap, else 4..32)  at most this many
+ *                              blocks of a tiled pass resident per SM (each
+ *                              launch asks for enough shared memory), so that
+ *                              the tiles of a lattice fill the last wave of
+ *                              the GPU better. */
+enum {
+    MJ_OPT_TMA = 0,
+    MJ_OPT_FUSED = 1,
+    MJ_OPT_PDL = 2,
+    MJ_OPT_STORE_DRAW = 3,
+    MJ_OPT_HOST_STRIPES = 4,
+    MJ_OPT_BLOCKS_PER_SM = 5
+};
 mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value);
 /* Autotuner: times `steps` steps of `p` for every kernel configuration of the
  * plan on a scratch copy of the device spins m_dev_soa (left untouched), keeps

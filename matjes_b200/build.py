@@ -75,7 +75,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int = 0) -> str:
     text = "\n".join(report)
     if verbose:
         sys.stderr.write(text)
-    with open(os.path.join(HERE, "ptxas_report.txt"), "w") as f:
+    with open(os.path.join(os.path.dirname(OBJDIR), "ptxas_report.txt"), "w") as f:
         f.write(text)
     return OUT
 

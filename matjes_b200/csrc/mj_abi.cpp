@@ -1018,6 +1018,26 @@ mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value) {
             if (value < 0 || value > 64) return set_error(MJ_ERR_ARG, "host stripes must be in [0, 64]");
             plan->host_stripes = value;
             break;
+        case MJ_OPT_BLOCKS_PER_SM: {
+            if (value != 0 && (value < 4 || value > 32))
+                return set_error(MJ_ERR_ARG, "blocks per SM must be 0 or in [4, 32]");
+            plan->blocks_per_sm = value;
+            plan->smem_cap_bytes = 0;
+            if (value > 0) {
+                // enough shared memory per block that value + 1 blocks do not fit
+                // on an SM and value blocks do (below the 48 KB default limit)
+                cudaDeviceProp prop;
+                mj_status st = cuda_status(cudaGetDeviceProperties(&prop, plan->device), "device properties");
+                if (st != MJ_OK) return st;
+                const size_t per_sm = prop.sharedMemPerMultiprocessor, rsv = prop.reservedSharedMemPerBlock;
+                size_t b = per_sm / static_cast<size_t>(value + 1) - rsv + 128;
+                b = (b + 127) / 128 * 128;
+                if (b > 48 * 1024 || static_cast<size_t>(value) * (b + rsv + 1024) > per_sm)
+                    return set_error(MJ_ERR_ARG, "blocks per SM: no shared memory size gives this cap");
+                plan->smem_cap_bytes = static_cast<int>(b);
+            }
+            break;
+        }
         default: return set_error(MJ_ERR_ARG, "unknown plan option " + std::to_string(option));
     }
     drop_graph(plan);

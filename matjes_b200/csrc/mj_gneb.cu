@@ -101,9 +101,10 @@ struct PlanFields {
         return e;
     }
     mj_status sums(double* F, double* m, double* E, double* img, const GnebCtl* ctl) {
-        const int nblk = static_cast<int>((X.n + 255) / 256);
-        k_gneb_sums<<<dim3(nrep, nblk), 256, 0, s>>>(m, F, X, nrep, concurrent ? esite : nullptr, E, part, cnt, img,
-                                                     ctl);
+        constexpr int kSpt = 4;  // sites per thread
+        const int nblk = static_cast<int>((X.n + 256 * kSpt - 1) / (256 * kSpt));
+        k_gneb_sums<kSpt><<<dim3(nrep, nblk), 256, 0, s>>>(m, F, X, nrep, concurrent ? esite : nullptr, E, part, cnt,
+                                                           img, ctl);
         return cuda_status(cudaGetLastError(), "k_gneb_sums");
     }
     mj_status field(double* F, double* m, double* E) {

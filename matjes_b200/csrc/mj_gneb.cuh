@@ -302,29 +302,34 @@ __device__ __forceinline__ void gneb_path_terms(double3 m0, double3 mp, double3 
 // last block of an image sums the partials in block order into img[q nrep + r].
 // With esite (per-site energies, image r at esite[r n, (r + 1) n)) also their
 // sum into E[r].  For fields that come without them (a plan's field kernels);
-// ctl may be null (always runs).
+// ctl may be null (always runs).  SPT sites per thread, 256 apart (coalesced),
+// so that the seven block reductions are paid once per SPT sites.
+template <int SPT>
 __global__ void __launch_bounds__(256) k_gneb_sums(const double* __restrict__ m, double* F, GnebIdx X, int nrep,
                                                    const double* __restrict__ esite, double* E, double* part,
                                                    unsigned int* cnt, double* img, const GnebCtl* ctl) {
     if (ctl && ctl->done) return;
     const int r = blockIdx.x;
     const int nblk = gridDim.y;
-    const int64_t li = blockIdx.y * static_cast<int64_t>(blockDim.x) + threadIdx.x;
     double g[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (li < X.n) {
-        const int64_t i = r * X.is + li;
-        const double3 m0 = ld3(m, i, X.cs);
-        const bool up = r + 1 < nrep;
-        const double3 mp = up ? ld3(m, i + X.is, X.cs) : m0;
-        const double3 mm = r > 0 ? ld3(m, i - X.is, X.cs) : m0;
-        double3 f = ld3(F, i, X.cs);
-        const double d = dot(f, m0);
-        f = make_double3(f.x - d * m0.x, f.y - d * m0.y, f.z - d * m0.z);
-        st3(F, i, X.cs, f);
-        double g6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        gneb_path_terms(m0, mp, mm, up, f, g6);
-        for (int q = 0; q < 6; ++q) g[q] = g6[q];
-        if (esite) g[6] = esite[r * X.n + li];
+    const bool up = r + 1 < nrep;
+#pragma unroll
+    for (int q = 0; q < SPT; ++q) {
+        const int64_t li = (blockIdx.y * static_cast<int64_t>(SPT) + q) * blockDim.x + threadIdx.x;
+        if (li < X.n) {
+            const int64_t i = r * X.is + li;
+            const double3 m0 = ld3(m, i, X.cs);
+            const double3 mp = up ? ld3(m, i + X.is, X.cs) : m0;
+            const double3 mm = r > 0 ? ld3(m, i - X.is, X.cs) : m0;
+            double3 f = ld3(F, i, X.cs);
+            const double d = dot(f, m0);
+            f = make_double3(f.x - d * m0.x, f.y - d * m0.y, f.z - d * m0.z);
+            st3(F, i, X.cs, f);
+            double g6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            gneb_path_terms(m0, mp, mm, up, f, g6);
+            for (int k = 0; k < 6; ++k) g[k] += g6[k];
+            if (esite) g[6] += esite[r * X.n + li];
+        }
     }
     double* pr = part + static_cast<int64_t>(r) * 7 * nblk;
     block_partials<7>(g, pr, nblk, blockIdx.y);

@@ -154,6 +154,8 @@ struct mj_plan {
     cudaGraphExec_t host_graph_exec = nullptr;
     std::string host_graph_key;
     int host_stripes = 0;  // stripes of mj_step_host (0: the default)
+    int blocks_per_sm = 0;    // cap on resident tiled-pass blocks per SM (0: none)
+    int smem_cap_bytes = 0;   // the dynamic shared memory per block that makes the cap
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;
     struct ProfRec {

@@ -73,6 +73,8 @@ struct TiledArgs {
     int pdl;            // 1: launched as a programmatic dependent of the previous kernel
     int nimg;           // > 1: blockIdx.z runs over (image, layer) of nimg lattices stored
                         // back to back (3N doubles apart in ms / out, N in aux)
+    int smem_bytes;     // host side: dynamic shared memory of the launch when above the
+                        // tile's (caps the resident blocks per SM; the excess is unused)
 };
 
 // Programmatic dependent launch: a kernel lets the next one in its stream launch
@@ -911,7 +913,7 @@ struct TiledLauncher {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = g;
         cfg.blockDim = dim3(32, BYT);
-        cfg.dynamicSmemBytes = G::buf_bytes;
+        cfg.dynamicSmemBytes = std::max<size_t>(G::buf_bytes, static_cast<size_t>(A.smem_bytes));
         cfg.stream = s;
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1083,6 +1085,7 @@ mj_status launch_tiled_shape(mj_plan* p, int pass, const DynCoef& C, const doubl
             A.pdl = p->use_pdl ? 1 : 0;
         }
         if (emode == 1) p->defer_nblocks = static_cast<int>(tiled_energy_blocks(p));
+        A.smem_bytes = p->smem_cap_bytes;
         return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(pass, axial, map,
                                                                                                    p->sp, C, A, s);
     });

@@ -327,11 +327,12 @@ def test_fused_sib_step_equals_two_launches(lattice, thermal, variant, tma):
     assert torch.equal(out[0][1], out[1][1])
 
 
-@pytest.mark.parametrize("option,value", [("pdl", 0), ("store_draw", 0), ("fused_store", (1, 0))])
+@pytest.mark.parametrize("option,value", [("pdl", 0), ("store_draw", 0), ("blocks_per_sm", 5), ("fused_store", (1, 0))])
 def test_kernel_options_change_no_result(option, value):
     """The plan's kernel options change how a step is computed, not its result:
     without programmatic dependent launch, with the Philox draw redrawn by the
-    corrector instead of stored, and the fused step with the redrawn draw, 30
+    corrector instead of stored, with at most 5 resident blocks per SM, and the
+    fused step with the redrawn draw, 30
     thermal SIB steps and their energies equal the default configuration's bit
     for bit."""
     import torch
@@ -350,7 +351,8 @@ def test_kernel_options_change_no_result(option, value):
                 _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_FUSED, value[0]))
                 _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_STORE_DRAW, value[1]))
             else:
-                opt = {"pdl": _abi.MJ_OPT_PDL, "store_draw": _abi.MJ_OPT_STORE_DRAW}[option]
+                opt = {"pdl": _abi.MJ_OPT_PDL, "store_draw": _abi.MJ_OPT_STORE_DRAW,
+                       "blocks_per_sm": _abi.MJ_OPT_BLOCKS_PER_SM}[option]
                 _abi.check(_abi.lib.mj_plan_set_option(ham.plan, opt, value))
         sd = mj.SpinDynamics(ham, integrator="sib", timestep=0.1, alpha=0.1, temperature=10.0, noise="philox", seed=8)
         sd.p.energy_mode = _abi.MJ_ENERGY_BEFORE
@@ -360,3 +362,4 @@ def test_kernel_options_change_no_result(option, value):
         out.append((m.cpu(), E.cpu()))
     assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
     assert _abi.lib.mj_plan_set_option(ham.plan, 99, 1) == _abi.MJ_ERR_ARG
+    assert _abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_BLOCKS_PER_SM, 2) == _abi.MJ_ERR_ARG
