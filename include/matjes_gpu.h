@@ -510,10 +510,12 @@ mj_status mj_gneb_path(mj_plan* plan, double* m_dev_images, int32_t nimg, const 
                        double* ene, double* dene, int64_t* iterations, double* max_force, int32_t* climbing,
                        void* stream);
 /* Tile variant (0: 32x16 tiles, 4 sites per thread; 1: 32x16, 2 per thread;
- * 2: 32x32, 4 per thread) and persistent blocks per SM (1..64). */
+ * 2: 32x32, 4 per thread; 3: 32x8, 2 per thread, registers capped for 8
+ * resident blocks of 4 warps; 4: 32x16, 2 per thread, capped for 4 blocks of 8
+ * warps) and persistent blocks per SM (1..64). */
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm);
 /* Times `steps` steps of every (variant, blocks per SM in {2,4,8,16,32}) on the
- * current state (restored afterwards), keeps the fastest; ms_table (15 doubles,
+ * current state (restored afterwards), keeps the fastest; ms_table (25 doubles,
  * may be NULL) gets ms per step in variant-major order. */
 mj_status mj_batch_autotune(mj_batch* b, const mj_dyn_params* p, int32_t steps, int32_t* best_variant,
                             int32_t* best_blocks_per_sm, double* ms_table);

@@ -21,7 +21,7 @@ from . import _abi
 from ._abi import check, lib, ptr
 from .deck import Deck
 
-N_BATCH_VARIANTS = 3
+N_BATCH_VARIANTS = 5
 BATCH_BLOCKS_PER_SM = (2, 4, 8, 16, 32)
 
 

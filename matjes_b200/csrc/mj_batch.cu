@@ -99,7 +99,9 @@ __device__ __forceinline__ void load_tile_b(const StencilParams& P, const BatchR
     }
 }
 
-template <class S, int BYT, int RY, int PASS>
+// SP_AXIAL: the stencil's and the on-site term's zeros of the axial form (as
+// the single-lattice tiled kernels; every replica's field then points along z).
+template <class S, int BYT, int RY, int PASS, int SP = SP_FULL>
 __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const DynCoef& C, const BatchArgs& A,
                                                  const BatchRep& R, int rep, const double* sm, int x0, int y0,
                                                  double (&gs)[6]) {
@@ -121,12 +123,26 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
                 pre[r].b = thermal ? ld3(A.aux, i, Nt) : make_double3(0.0, 0.0, 0.0);
             }
         }
+    } else if constexpr (PASS == BPASS_SIB1 && RY % 2 == 0) {
+        // the thermal draws of the thread's sites, two at a time (a site past the
+        // replica's edge draws too and is not used)
+        if (thermal) {
+#pragma unroll
+            for (int r = 0; r < RY; r += 2) {
+                const int64_t li = x + static_cast<int64_t>(R.Lx) * (y0 + ty * RY + r);
+                double3 z0, z1;
+                philox_normals_x2(C.keys, C.noise_tab, A.step, C.stream_id + R.stream, static_cast<uint32_t>(li),
+                                  static_cast<uint32_t>(li + R.Lx), z0, z1);
+                pre[r].b = make_double3(sigma * z0.x, sigma * z0.y, sigma * z0.z);
+                pre[r + 1].b = make_double3(sigma * z1.x, sigma * z1.y, sigma * z1.z);
+            }
+        }
     }
     double bx[RY], by[RY], bz[RY];
 #pragma unroll
     for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
     const int base = (ty * RY) * G::PX + tx;
-    all_columns<S, BYT, RY>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
+    all_columns<S, BYT, RY, SP>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
     double e = 0.0;
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
@@ -139,9 +155,13 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
             double b0 = bx[r], b1 = by[r], b2 = bz[r];
             if (P.has_onsite) {
                 const double* W = P.W0;
-                b0 = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, b0)));
-                b1 = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, b1)));
-                b2 = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, b2)));
+                if constexpr (SP == SP_AXIAL) {
+                    b2 = fma(W[8], m0.z, b2);
+                } else {
+                    b0 = fma(W[0], m0.x, fma(W[1], m0.y, fma(W[2], m0.z, b0)));
+                    b1 = fma(W[3], m0.x, fma(W[4], m0.y, fma(W[5], m0.z, b1)));
+                    b2 = fma(W[6], m0.x, fma(W[7], m0.y, fma(W[8], m0.z, b2)));
+                }
             }
             FieldOut f;
             f.Bzee = make_double3(R.zb[0], R.zb[1], R.zb[2]);
@@ -181,8 +201,14 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
                 e += total_energy_part(f, m0, zero);
                 double3 H = f.B;
                 if (thermal) {
-                    const double3 z = philox_normals_tab(C.keys, C.noise_tab, A.step, C.stream_id + R.stream, static_cast<uint32_t>(li));
-                    const double3 b = make_double3(sigma * z.x, sigma * z.y, sigma * z.z);
+                    double3 b;
+                    if constexpr (RY % 2 == 0) {
+                        b = pre[r].b;
+                    } else {
+                        const double3 z = philox_normals_tab(C.keys, C.noise_tab, A.step, C.stream_id + R.stream,
+                                                             static_cast<uint32_t>(li));
+                        b = make_double3(sigma * z.x, sigma * z.y, sigma * z.z);
+                    }
                     st3(A.aux, i, Nt, b);
                     H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
                 }
@@ -197,9 +223,9 @@ __device__ __forceinline__ double compute_tile_b(const StencilParams& P, const D
     return e;
 }
 
-template <class S, int BYT, int RY, int PASS>
-__global__ void __launch_bounds__(32 * BYT) k_batch(const __grid_constant__ StencilParams P, const DynCoef C,
-                                                     const BatchArgs A) {
+template <class S, int BYT, int RY, int MINB, int PASS, int SP>
+__global__ void __launch_bounds__(32 * BYT, MINB) k_batch(const __grid_constant__ StencilParams P, const DynCoef C,
+                                                           const BatchArgs A) {
     using G = TileGeom<S, BYT, RY>;
     extern __shared__ __align__(128) double smem_b[];
     // per tile: the energy, and for the GNEB pass its six path sums
@@ -215,7 +241,7 @@ __global__ void __launch_bounds__(32 * BYT) k_batch(const __grid_constant__ Sten
         __syncthreads();
         double v[NV];
         double gs[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        v[0] = compute_tile_b<S, BYT, RY, PASS>(P, C, Ar, R, tl.x, smem_b, tl.y, tl.z, gs);
+        v[0] = compute_tile_b<S, BYT, RY, PASS, SP>(P, C, Ar, R, tl.x, smem_b, tl.y, tl.z, gs);
 #pragma unroll
         for (int q = 1; q < NV; ++q) v[q] = gs[q - 1];
         if (A.tile_e) {
@@ -415,48 +441,60 @@ __global__ void __launch_bounds__(256) k_gneb_img(const BatchRep* reps, int nrep
     }
 }
 
-template <class S, int BYT, int RY>
+template <class S, int BYT, int RY, int MINB>
 struct BatchLauncher {
     using G = TileGeom<S, BYT, RY>;
     static constexpr int TY = G::TY;
-    template <int PASS>
+    template <int PASS, int SP>
     static mj_status launch(const StencilParams& P, const DynCoef& C, const BatchArgs& A, int nblocks, cudaStream_t s) {
-        k_batch<S, BYT, RY, PASS><<<nblocks, dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
+        k_batch<S, BYT, RY, MINB, PASS, SP><<<nblocks, dim3(32, BYT), G::buf_bytes, s>>>(P, C, A);
         return cuda_status(cudaGetLastError(), "k_batch");
     }
-    static mj_status pass(int ps, const StencilParams& P, const DynCoef& C, const BatchArgs& A, int nblocks,
-                          cudaStream_t s) {
+    // the dynamics and energy passes in the axial form where it holds; the
+    // field and GNEB passes in the full form
+    static mj_status pass(int ps, bool axial, const StencilParams& P, const DynCoef& C, const BatchArgs& A,
+                          int nblocks, cudaStream_t s) {
         switch (ps) {
-            case BPASS_SIB1: return launch<BPASS_SIB1>(P, C, A, nblocks, s);
-            case BPASS_SIB2: return launch<BPASS_SIB2>(P, C, A, nblocks, s);
-            case BPASS_FIELD: return launch<BPASS_FIELD>(P, C, A, nblocks, s);
-            case BPASS_GNEB: return launch<BPASS_GNEB>(P, C, A, nblocks, s);
-            default: return launch<BPASS_ENERGY>(P, C, A, nblocks, s);
+            case BPASS_SIB1:
+                return axial ? launch<BPASS_SIB1, SP_AXIAL>(P, C, A, nblocks, s)
+                             : launch<BPASS_SIB1, SP_FULL>(P, C, A, nblocks, s);
+            case BPASS_SIB2:
+                return axial ? launch<BPASS_SIB2, SP_AXIAL>(P, C, A, nblocks, s)
+                             : launch<BPASS_SIB2, SP_FULL>(P, C, A, nblocks, s);
+            case BPASS_FIELD: return launch<BPASS_FIELD, SP_FULL>(P, C, A, nblocks, s);
+            case BPASS_GNEB: return launch<BPASS_GNEB, SP_FULL>(P, C, A, nblocks, s);
+            default:
+                return axial ? launch<BPASS_ENERGY, SP_AXIAL>(P, C, A, nblocks, s)
+                             : launch<BPASS_ENERGY, SP_FULL>(P, C, A, nblocks, s);
         }
     }
 };
 
-// batch tile variants: (threads in y, sites per thread)
-constexpr int kBatchVariants = 3;
-constexpr int kBatchTY[kBatchVariants] = {16, 16, 32};
+// batch tile variants: (threads in y, sites per thread, min resident blocks per SM)
+constexpr int kBatchVariants = 5;
+constexpr int kBatchTY[kBatchVariants] = {16, 16, 32, 8, 16};
 
 template <class S>
-mj_status batch_pass_shape(int variant, int ps, const StencilParams& P, const DynCoef& C, const BatchArgs& A,
-                           int nblocks, cudaStream_t s) {
+mj_status batch_pass_shape(int variant, int ps, bool zaxial, const StencilParams& P, const DynCoef& C,
+                           const BatchArgs& A, int nblocks, cudaStream_t s) {
+    // axial: the stencil's zeros hold and every replica's field points along z
+    const bool axial = zaxial && stencil_axial<S>(P, true);
     switch (variant) {
-        case 1: return BatchLauncher<S, 8, 2>::pass(ps, P, C, A, nblocks, s);
-        case 2: return BatchLauncher<S, 8, 4>::pass(ps, P, C, A, nblocks, s);
-        default: return BatchLauncher<S, 4, 4>::pass(ps, P, C, A, nblocks, s);
+        case 1: return BatchLauncher<S, 8, 2, 1>::pass(ps, axial, P, C, A, nblocks, s);
+        case 2: return BatchLauncher<S, 8, 4, 1>::pass(ps, axial, P, C, A, nblocks, s);
+        case 3: return BatchLauncher<S, 4, 2, 8>::pass(ps, axial, P, C, A, nblocks, s);
+        case 4: return BatchLauncher<S, 8, 2, 4>::pass(ps, axial, P, C, A, nblocks, s);
+        default: return BatchLauncher<S, 4, 4, 1>::pass(ps, axial, P, C, A, nblocks, s);
     }
 }
 
-mj_status batch_pass(int shape, int variant, int ps, const StencilParams& P, const DynCoef& C, const BatchArgs& A,
-                     int nblocks, cudaStream_t s) {
+mj_status batch_pass(int shape, int variant, int ps, bool zaxial, const StencilParams& P, const DynCoef& C,
+                     const BatchArgs& A, int nblocks, cudaStream_t s) {
     switch (shape) {
-        case kShapeSquareNN: return batch_pass_shape<ShapeSquareNN>(variant, ps, P, C, A, nblocks, s);
-        case kShapeSquare2: return batch_pass_shape<ShapeSquare2>(variant, ps, P, C, A, nblocks, s);
-        case kShapeTriNN: return batch_pass_shape<ShapeTriNN>(variant, ps, P, C, A, nblocks, s);
-        case kShapeTri3: return batch_pass_shape<ShapeTri3>(variant, ps, P, C, A, nblocks, s);
+        case kShapeSquareNN: return batch_pass_shape<ShapeSquareNN>(variant, ps, zaxial, P, C, A, nblocks, s);
+        case kShapeSquare2: return batch_pass_shape<ShapeSquare2>(variant, ps, zaxial, P, C, A, nblocks, s);
+        case kShapeTriNN: return batch_pass_shape<ShapeTriNN>(variant, ps, zaxial, P, C, A, nblocks, s);
+        case kShapeTri3: return batch_pass_shape<ShapeTri3>(variant, ps, zaxial, P, C, A, nblocks, s);
         default: return set_error(MJ_ERR_UNSUPPORTED, "batches need a tiled lattice shape");
     }
 }
@@ -473,6 +511,7 @@ struct mj_batch {
     int shape = 0;
     int variant = 0;
     int blocks_per_sm = 8;
+    bool zaxial = false;              // every replica's Zeeman field along z
     int num_sms = 148;
     std::vector<mj::BatchRep> reps;   // host copy (initial table)
     std::vector<int> L;               // 2*nrep
@@ -627,7 +666,7 @@ BatchArgs batch_args(mj_batch* b, uint32_t step, double dt) {
 mj_status batch_energy(mj_batch* b, const DynCoef& c, double* E, cudaStream_t s) {
     BatchArgs A = batch_args(b, 0, 0.0);
     A.tile_e = b->d_tile_e;
-    mj_status st = batch_pass(b->shape, b->variant, BPASS_ENERGY, b->sp, c, A, batch_blocks(b), s);
+    mj_status st = batch_pass(b->shape, b->variant, BPASS_ENERGY, b->zaxial, b->sp, c, A, batch_blocks(b), s);
     if (st != MJ_OK) return st;
     k_batch_energy<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, E);
     return cuda_status(cudaGetLastError(), "k_batch_energy");
@@ -643,10 +682,10 @@ mj_status batch_sequence(mj_batch* b, const DynCoef& c0, double dt, uint32_t ste
     for (int32_t k = 0; k < nsteps; ++k) {
         const uint32_t step = step0 + static_cast<uint32_t>(k);
         BatchArgs A = batch_args(b, step, dt);
-        if ((st = batch_pass(b->shape, b->variant, BPASS_SIB1, b->sp, c, A, nb, s)) != MJ_OK) return st;
+        if ((st = batch_pass(b->shape, b->variant, BPASS_SIB1, b->zaxial, b->sp, c, A, nb, s)) != MJ_OK) return st;
         A.ms = b->d_mid;
         A.out = b->d_m;
-        if ((st = batch_pass(b->shape, b->variant, BPASS_SIB2, b->sp, c, A, nb, s)) != MJ_OK) return st;
+        if ((st = batch_pass(b->shape, b->variant, BPASS_SIB2, b->zaxial, b->sp, c, A, nb, s)) != MJ_OK) return st;
         if (swap_every > 0 && ((step + 1) % static_cast<uint32_t>(swap_every)) == 0) {
             if ((st = batch_energy(b, c, b->d_E, s)) != MJ_OK) return st;
             // round index (step + 1) / swap_every; in a graph the device counter (a multiple of
@@ -676,7 +715,7 @@ struct BatchFields {
         A.out = F;
         A.project = 1;
         A.tile_e = b->d_tile_e;
-        mj_status e = batch_pass(b->shape, b->variant, BPASS_FIELD, b->sp, c, A, batch_blocks(b), s);
+        mj_status e = batch_pass(b->shape, b->variant, BPASS_FIELD, b->zaxial, b->sp, c, A, batch_blocks(b), s);
         if (e != MJ_OK) return e;
         k_batch_energy<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, E);
         return cuda_status(cudaGetLastError(), "k_batch_energy");
@@ -689,7 +728,7 @@ struct BatchFields {
         A.tile_g = tile_g;
         A.gneb_n = b->Ntot / b->nrep;
         A.gneb_nimg = b->nrep;
-        mj_status e = batch_pass(b->shape, b->variant, BPASS_GNEB, b->sp, c, A, batch_blocks(b), s);
+        mj_status e = batch_pass(b->shape, b->variant, BPASS_GNEB, b->zaxial, b->sp, c, A, batch_blocks(b), s);
         if (e != MJ_OK) return e;
         k_gneb_img<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, tile_g, b->ntile, E, img, ctl);
         return cuda_status(cudaGetLastError(), "k_gneb_img");
@@ -755,6 +794,7 @@ mj_status mj_batch_create(const mj_lattice_desc* cell, const mj_hamiltonian_desc
     b->slot_kT.resize(nrep);
     std::vector<int> image(nrep);
     int64_t off = 0;
+    bool zax = true;
     for (int r = 0; r < nrep; ++r) {
         BatchRep& R = b->reps[r];
         R.off = off;
@@ -765,9 +805,11 @@ mj_status mj_batch_create(const mj_lattice_desc* cell, const mj_hamiltonian_desc
         const double* Br = B_ext + 3 * r;
         const bool zee = ham->zeeman_on || std::sqrt(Br[0] * Br[0] + Br[1] * Br[1] + Br[2] * Br[2]) >= 1e-8;
         for (int k = 0; k < 3; ++k) R.zb[k] = zee ? zc * Br[k] : 0.0;
+        if (R.zb[0] != 0.0 || R.zb[1] != 0.0) zax = false;
         R.kT = temperature[r] * kKB;
         R.stream = static_cast<uint32_t>(r);
     }
+    b->zaxial = zax;
     for (int l = 0; l < nrep; ++l) {
         b->slot_kT[l] = temperature[order[l]] * kKB;
         image[l] = order[l];
@@ -955,7 +997,7 @@ mj_status mj_batch_field(mj_batch* b, double* B_dev, double* E_dev, int32_t proj
     A.out = B_dev;
     A.project = project ? 1 : 0;
     A.tile_e = b->d_tile_e;
-    mj_status st = batch_pass(b->shape, b->variant, B_dev ? BPASS_FIELD : BPASS_ENERGY, b->sp, c, A, batch_blocks(b), s);
+    mj_status st = batch_pass(b->shape, b->variant, B_dev ? BPASS_FIELD : BPASS_ENERGY, b->zaxial, b->sp, c, A, batch_blocks(b), s);
     if (st != MJ_OK) return st;
     if (E_dev) {
         k_batch_energy<<<b->nrep, 256, 0, s>>>(b->d_reps, b->nrep, b->d_tile_e, E_dev);
@@ -987,7 +1029,7 @@ mj_status mj_batch_gneb_tangent(mj_batch* b, const double* E_dev, int32_t mode, 
 
 mj_status mj_batch_set_config(mj_batch* b, int32_t variant, int32_t blocks_per_sm) {
     if (!b || variant < 0 || variant >= kBatchVariants || blocks_per_sm < 1 || blocks_per_sm > 64)
-        return set_error(MJ_ERR_ARG, "variant 0..2 and blocks_per_sm 1..64");
+        return set_error(MJ_ERR_ARG, "variant 0..4 and blocks_per_sm 1..64");
     cudaSetDevice(b->device);
     const bool retile = variant != b->variant;
     b->variant = variant;

@@ -145,6 +145,18 @@ __device__ __forceinline__ double3 philox_normals_tab(const uint32_t* keys, cons
     return normals_of_block(c, tab);
 }
 
+// The normals of two sites of one step and stream together (the words and
+// normals of two philox_normals_tab calls).
+__device__ __forceinline__ void philox_normals_x2(const uint32_t* keys, const double* __restrict__ tab, uint32_t step,
+                                                  uint32_t stream, uint32_t site0, uint32_t site1, double3& z0,
+                                                  double3& z1) {
+    uint32_t a[4] = {site0, step, stream, 0u};
+    uint32_t b[4] = {site1, step, stream, 0u};
+    philox10k_x2(a, b, keys);
+    z0 = normals_of_block(a, tab);
+    z1 = normals_of_block(b, tab);
+}
+
 // The same from the 64-bit seed (round keys derived here)
 __device__ __forceinline__ double3 philox_normals(uint64_t seed, uint32_t step, uint32_t stream, uint32_t site,
                                                   const double* __restrict__ tab) {
@@ -176,10 +188,9 @@ __device__ __forceinline__ double3 thermal_field(const DynCoef& C, uint32_t step
 __device__ __forceinline__ void thermal_field_x2(const DynCoef& C, uint32_t step, int64_t i0, int64_t i1, double3& b0,
                                                  double3& b1) {
     if (C.step_base) step += *C.step_base;
-    uint32_t a[4] = {static_cast<uint32_t>(i0), step, C.stream_id, 0u};
-    uint32_t b[4] = {static_cast<uint32_t>(i1), step, C.stream_id, 0u};
-    philox10k_x2(a, b, C.keys);
-    const double3 za = normals_of_block(a, C.noise_tab), zb = normals_of_block(b, C.noise_tab);
+    double3 za, zb;
+    philox_normals_x2(C.keys, C.noise_tab, step, C.stream_id, static_cast<uint32_t>(i0), static_cast<uint32_t>(i1), za,
+                      zb);
     b0 = make_double3(C.sigma * za.x, C.sigma * za.y, C.sigma * za.z);
     b1 = make_double3(C.sigma * zb.x, C.sigma * zb.y, C.sigma * zb.z);
 }

@@ -96,7 +96,7 @@ def test_batch_variants_and_grids_bitwise_equal():
     cell, B, decks = CASES["square_mixed"]()
     m0 = np.concatenate(_initial(decks, 5))
     ref = None
-    for v in range(3):
+    for v in range(5):
         for bps in (1, 3, 8, 32):
             batch = mj.ReplicaBatch(cell, [d.L[:2] for d in decks], B, TEMPS["square_mixed"])
             batch.set_config(v, bps)
@@ -200,7 +200,7 @@ def test_batch_rejects_what_it_cannot_run():
     assert _abi.lib.mj_batch_step(batch.handle, C.byref(p), 1, 0, None, None) == _abi.MJ_ERR_UNSUPPORTED
     p = batch.params()
     assert _abi.lib.mj_batch_graph_run(batch.handle, C.byref(p), 15, 1, 10, None, None) == _abi.MJ_ERR_ARG
-    assert _abi.lib.mj_batch_set_config(batch.handle, 3, 8) == _abi.MJ_ERR_ARG
+    assert _abi.lib.mj_batch_set_config(batch.handle, 5, 8) == _abi.MJ_ERR_ARG
     dip = mj.square_film((8, 8, 2), a=0.25, med_z=-0.3, dip=True)
     with pytest.raises(mj.MatjesError):
         mj.ReplicaBatch(dip, [(8, 8)], B, [1.0])
