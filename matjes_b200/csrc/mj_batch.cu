@@ -1102,8 +1102,8 @@ static mj_status batch_mc_setup(mj_batch* b, double cone0, cudaStream_t s) {
         L3[3 * r + 2] = 1;
     }
     if (!mc_colouring(b->sp, L3.data(), b->nrep, b->mc_col))
-        return set_error(MJ_ERR_UNSUPPORTED, "no linear colouring of at most 16 colours and no product colouring of "
-                                             "at most 4 x 4 x 4 fits the stencil and every replica's sizes");
+        return set_error(MJ_ERR_UNSUPPORTED, "no linear or product colouring fits the stencil and every "
+                                             "replica's sizes");
     const McClass K0 = mc_classes(b->mc_col)[0];
     std::vector<int4> tiles;
     for (int r = 0; r < b->nrep; ++r) {

@@ -113,8 +113,8 @@ mj_status mj_mc_sweeps(mj_plan* plan, double* m, mj_mc_params* p, int32_t nsweep
     if (!(p->temperature >= 0.0) || !(p->cone > 0.0)) return set_error(MJ_ERR_ARG, "temperature >= 0 and cone > 0");
     int col[4] = {0, 0, 0, 0};
     if (!mc_colouring(plan->sp, plan->sp.L, 1, col))
-        return set_error(MJ_ERR_UNSUPPORTED, "no linear colouring of at most 16 colours and no product colouring of "
-                                             "at most 4 x 4 x 4 fits the stencil and the periodic sizes");
+        return set_error(MJ_ERR_UNSUPPORTED, "no linear or product colouring fits the stencil and the periodic "
+                                             "sizes");
     if (colors)
         for (int d = 0; d < 4; ++d) colors[d] = col[d];
     const std::vector<McClass> classes = mc_classes(col);

@@ -176,22 +176,50 @@ __device__ __forceinline__ int mc_class_x(const McClass& K, int y, int z, int t)
 
 // The colouring with the fewest colours (at least 2) in which no stencil offset
 // joins two sites of one colour, on every lattice of sizes L[3 l .. 3 l + 2]:
-// out = {q, b, c, 1} for the linear colour (x + b y + c z) mod q, q <= 16, or
-// {cx, cy, cz, 0} for the product colour, counts <= 4.  A periodic direction
-// must map its wrapped images to the same colour (q divides Lx, b Ly and c Lz;
-// cx, cy, cz divide the sizes).
+// out = {q, b, c, 1} for the linear colour (x + b y + c z) mod q, or {cx, cy,
+// cz, 0} for the product colour (x mod cx, y mod cy, z mod cz).  A periodic
+// direction must map its wrapped images to the same colour (q divides every
+// Lx, q divides b Ly and c Lz; cx divides every Lx, ...), so along a periodic
+// direction the counts are the divisors of the sizes' greatest common divisor
+// (a prime size p gives p colours), along an open one 2 .. 64.  Linear
+// colourings up to 4096 colours, product ones up to 4096 in all.
 inline bool mc_colouring(const StencilParams& sp, const int* L, int nlat, int out[4]) {
+    auto gcd = [](int a, int b) {
+        while (b) {
+            const int t = a % b;
+            a = b;
+            b = t;
+        }
+        return a;
+    };
+    // counts allowed along direction d (ascending), from `lo`
+    auto counts = [&](int d, int lo, int open_max) {
+        std::vector<int> v;
+        if (sp.periodic[d]) {
+            int g = 0;
+            for (int l = 0; l < nlat; ++l) g = gcd(g, L[3 * l + d]);
+            for (int q = lo; q <= g; ++q)
+                if (g % q == 0) v.push_back(q);
+        } else {
+            for (int q = lo; q <= open_max; ++q) v.push_back(q);
+        }
+        return v;
+    };
     auto wraps_ok = [&](int d, int mult, int q) {
         if (!sp.periodic[d]) return true;
         for (int l = 0; l < nlat; ++l)
-            if ((mult * L[3 * l + d]) % q) return false;
+            if ((static_cast<int64_t>(mult) * L[3 * l + d]) % q) return false;
         return true;
     };
+    bool zoff = false;  // any offset along z
+    for (int k = 0; k < sp.n_off; ++k) zoff = zoff || sp.off[k][2] != 0;
     int best = 1 << 30;
-    for (int q = 2; q <= 16 && q < best; ++q)
-        for (int c = 0; c < q && q < best; ++c)
+    for (int q : counts(0, 2, 64)) {
+        if (q >= best || q > 4096) break;
+        const int cmax = zoff ? q : 1;  // without z offsets c = 0 serves every lattice
+        for (int c = 0; c < cmax && q < best; ++c)
             for (int b = 0; b < q && q < best; ++b) {
-                bool ok = wraps_ok(0, 1, q) && wraps_ok(1, b, q) && wraps_ok(2, c, q);
+                bool ok = wraps_ok(1, b, q) && wraps_ok(2, c, q);
                 for (int k = 0; k < sp.n_off && ok; ++k)
                     ok = (((sp.off[k][0] + b * sp.off[k][1] + c * sp.off[k][2]) % q) + q) % q != 0;
                 if (ok) {
@@ -202,19 +230,22 @@ inline bool mc_colouring(const StencilParams& sp, const int* L, int nlat, int ou
                     out[3] = 1;
                 }
             }
-    for (int cz = 1; cz <= 4; ++cz)
-        for (int cy = 1; cy <= 4; ++cy)
-            for (int cx = 1; cx <= 4; ++cx) {
+    }
+    const std::vector<int> cxs = counts(0, 1, 8), cys = counts(1, 1, 8), czs = counts(2, 1, 8);
+    for (int cz : czs)
+        for (int cy : cys)
+            for (int cx : cxs) {
+                const int64_t n = static_cast<int64_t>(cx) * cy * cz;
+                if (n >= best || n <= 1 || n > 4096) continue;
                 const int cc[3] = {cx, cy, cz};
-                bool ok = cx * cy * cz < best && cx * cy * cz > 1;
-                for (int d = 0; d < 3 && ok; ++d) ok = wraps_ok(d, 1, cc[d]);
+                bool ok = true;
                 for (int k = 0; k < sp.n_off && ok; ++k) {
                     bool differs = false;
                     for (int d = 0; d < 3; ++d) differs = differs || (((sp.off[k][d] % cc[d]) + cc[d]) % cc[d]) != 0;
                     ok = differs;
                 }
                 if (ok) {
-                    best = cx * cy * cz;
+                    best = static_cast<int>(n);
                     out[0] = cx;
                     out[1] = cy;
                     out[2] = cz;

@@ -213,14 +213,15 @@ def test_unsupported_plans_and_bad_arguments():
     with pytest.raises(mj.MatjesError) as e:
         MetropolisMC(ham, "sphere").sweeps(m, 1, 10.0)
     assert e.value.status == _abi.MJ_ERR_UNSUPPORTED
-    # a colouring needs the periodic sizes to keep the colours of their images (17 is prime)
-    odd = mj.square_film((17, 17, 1), Jv=1e-3, Dv=0.0, Kv=0.0, Bz=0.0)
+    # periodic sizes 17 and 16 admit no linear colouring of the square stencil
+    # (q must divide 17 and b 16 must be a multiple of q): the product one
+    odd = mj.square_film((17, 16, 1), Jv=1e-3, Dv=0.0, Kv=0.0, Bz=0.0)
     ham2 = mj.Hamiltonian(odd)
     m2 = torch.zeros((3, odd.nsites), dtype=torch.float64, device="cuda")
     m2[2] = 1.0
-    with pytest.raises(mj.MatjesError) as e:
-        MetropolisMC(ham2, "sphere").sweeps(m2, 1, 10.0)
-    assert e.value.status == _abi.MJ_ERR_UNSUPPORTED
+    ch2 = MetropolisMC(ham2, "sphere")
+    ch2.sweeps(m2, 1, 10.0)
+    assert list(ch2.colors) == [17, 2, 1, 0]  # product colouring (x mod 17, y mod 2)
     sq = mj.square_film((8, 8, 1))
     ham3 = mj.Hamiltonian(sq)
     m3 = torch.zeros((3, sq.nsites), dtype=torch.float64, device="cuda")
@@ -290,3 +291,28 @@ Total_MC_Steps 600
 cone 1.0
 ising .T.
 """
+
+
+@pytest.mark.parametrize("L,colors", [((17, 17), [17, 1, 0, 1]), ((13, 26), [13, 1, 0, 1])])
+def test_prime_periodic_sizes_take_as_many_colours(L, colors):
+    """A periodic size p prime admits only colourings of p colours along it:
+    the chain then moves colour by colour as the oracle does, move by move."""
+    import torch
+
+    import matjes_b200 as mj
+    from matjes_b200.montecarlo import SAMPLING, MetropolisMC
+
+    deck = mj.square_film((L[0], L[1], 1), Jv=1e-3, Dv=0.3e-3, Kv=-0.1e-3, Bz=0.5)
+    ham = mj.Hamiltonian(deck)
+    m0 = mj.random_sphere(deck.nsites, 3)
+    m = torch.tensor(m0.T.copy(), device="cuda")
+    chain = MetropolisMC(ham, "sphere", cone=0.6, seed=11, stream_id=2, adapt_cone=False)
+    E, Mg, acc = chain.sweeps(m, 6, 30.0)
+    torch.cuda.synchronize()
+    assert list(chain.colors) == colors
+    mo = m0.copy()
+    st = O.MC(temperature=30.0, cone=0.6, proposal=SAMPLING["sphere"], adapt_cone=0, seed=11, stream_id=2, sweep0=0)
+    Eo, Mgo, acco = O.mc_sweeps(O.Model(deck), mo, st, 6, chain.colors, deck.L)
+    assert acc == acco > 0
+    assert np.abs(m.cpu().numpy().T - mo).max() < 1e-11
+    assert np.abs(E.cpu().numpy() - Eo).max() <= 1e-11 * np.abs(Eo).max()
