@@ -173,14 +173,19 @@ mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable);
  *                              blocks of a tiled pass resident per SM (each
  *                              launch asks for enough shared memory), so that
  *                              the tiles of a lattice fill the last wave of
- *                              the GPU better. */
+ *                              the GPU better;
+ *   MJ_OPT_DIP_ZCONV (default 1)  FFT dipolar term with a z grid of a power
+ *                              of two up to 32: the z transforms and the
+ *                              product with K_F as one kernel (0: cuFFT z
+ *                              transforms and a separate product). */
 enum {
     MJ_OPT_TMA = 0,
     MJ_OPT_FUSED = 1,
     MJ_OPT_PDL = 2,
     MJ_OPT_STORE_DRAW = 3,
     MJ_OPT_HOST_STRIPES = 4,
-    MJ_OPT_BLOCKS_PER_SM = 5
+    MJ_OPT_BLOCKS_PER_SM = 5,
+    MJ_OPT_DIP_ZCONV = 6
 };
 mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value);
 /* Autotuner: times `steps` steps of `p` for every kernel configuration of the

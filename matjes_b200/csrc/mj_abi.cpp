@@ -1018,6 +1018,7 @@ mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value) {
             if (value < 0 || value > 64) return set_error(MJ_ERR_ARG, "host stripes must be in [0, 64]");
             plan->host_stripes = value;
             break;
+        case MJ_OPT_DIP_ZCONV: plan->dip_zconv = value != 0; break;
         case MJ_OPT_BLOCKS_PER_SM: {
             if (value != 0 && (value < 4 || value > 32))
                 return set_error(MJ_ERR_ARG, "blocks per SM must be 0 or in [4, 32]");

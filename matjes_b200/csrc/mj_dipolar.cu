@@ -20,10 +20,19 @@
 // slightly uneven (imaginary parts of K_F ~1e-7 of its scale), and the complex
 // product is kept whenever they exceed 1e-13.  The unpack is fused into the consumers: the field and
 // step kernels read H on the padded (y, x) grid of the lattice planes.
+//
+// When N_rep,z is a power of two up to 32 the z transforms and the pointwise
+// product are one kernel (k_zconv): one warp per (ky, kx) column, lane = z,
+// a radix-2 FFT across the lanes by shuffles (forward in decimation in
+// frequency, which leaves the spectrum in bit-reversed order, K_F stored per
+// column in that order, inverse in decimation in time back to natural order).
+// It reads only the Lz lattice planes of the 2D spectra (the others are the
+// zero padding) and writes only the Lz planes the inverse 2D transform reads.
 #include <cufft.h>
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "mj_internal.hpp"
@@ -45,6 +54,12 @@ struct DipolarPlan {
     cufftDoubleComplex* d_kfc = nullptr;   // complex K_F when it is not real
     cufftHandle f2d = 0, fz = 0, b2d = 0;
     bool have_f2d = false, have_fz = false, have_b2d = false;
+    // the fused z convolution: K_F per column [pc][nz][6] (kz in bit-reversed
+    // order), real or complex, and the twiddles exp(-2 pi i m / nz), m < nz / 2
+    bool zconv = false;
+    double* d_kzr = nullptr;
+    cufftDoubleComplex* d_kzc = nullptr;
+    double tw[32] = {};
 };
 
 __global__ void k_pad(const double* __restrict__ m, double* __restrict__ pad, int Lx, int Ly, int Lz, int px,
@@ -109,6 +124,125 @@ __global__ void k_scale(cufftDoubleComplex* __restrict__ a, int64_t n, double s)
     a[k].y *= s;
 }
 
+// Twiddles of a length-NZ transform: (cos, sin) of -2 pi m / NZ, m < NZ/2
+struct ZTwiddle {
+    double c[16], s[16];
+};
+
+__device__ __forceinline__ double2 shfl_xor_c(double2 v, int h) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, h), __shfl_xor_sync(0xffffffffu, v.y, h));
+}
+__device__ __forceinline__ double2 cmul_d(double2 a, double c, double s) {  // a (c + i s)
+    return make_double2(fma(a.x, c, -(a.y * s)), fma(a.x, s, a.y * c));
+}
+
+// The forward transform of the lanes' values (lane l of a group of NZ holds
+// element l): decimation in frequency, lane l ends with X(bitrev(l)).
+template <int NZ>
+__device__ __forceinline__ double2 zfft_forward(double2 x, int l, const double2* __restrict__ tw) {
+#pragma unroll
+    for (int h = NZ / 2; h >= 1; h >>= 1) {
+        const double2 p = shfl_xor_c(x, h);
+        if (l & h) {
+            const double2 w = tw[(l & (h - 1)) * (NZ / (2 * h))];
+            x = cmul_d(make_double2(p.x - x.x, p.y - x.y), w.x, w.y);
+        } else {
+            x = make_double2(x.x + p.x, x.y + p.y);
+        }
+    }
+    return x;
+}
+
+// The inverse (exp(+2 pi i ...), unscaled) of bit-reversed lanes: decimation
+// in time, lane l ends with y(l).
+template <int NZ>
+__device__ __forceinline__ double2 zfft_inverse(double2 x, int l, const double2* __restrict__ tw) {
+#pragma unroll
+    for (int h = 1; h < NZ; h <<= 1) {
+        const double2 w = tw[(l & (h - 1)) * (NZ / (2 * h))];
+        const double2 t = (l & h) ? cmul_d(x, w.x, -w.y) : x;
+        const double2 p = shfl_xor_c(t, h);
+        x = (l & h) ? make_double2(p.x - t.x, p.y - t.y) : make_double2(t.x + p.x, t.y + p.y);
+    }
+    return x;
+}
+
+// z transforms and the product H_F = K_F M_F in one pass: spec_in [z][c][col]
+// (planes z < lz), out [z][c][col] (planes z < lz), K_F [col][6][l] with l the
+// lane (bit-reversed kz); REAL: K_F real.  A block of 8 warps takes C = 256/NZ
+// consecutive columns, one column per NZ lanes (every lane one z): the rows
+// (z, c) of its columns are read and written whole through shared memory,
+// [z][c * C + column] with rows of 3 C + 1 16-byte slots, so that the lanes of
+// one column hit distinct banks.
+template <int NZ>
+struct ZcGeom {
+    static constexpr int C = 256 / NZ;   // columns per block
+    static constexpr int ROW = 3 * C + 1;
+    static constexpr size_t smem = sizeof(double2) * NZ * ROW;
+};
+
+template <int NZ, bool REAL>
+__global__ void __launch_bounds__(256) k_zconv(const double2* __restrict__ in, double2* __restrict__ out,
+                                               const double* __restrict__ kr, const double2* __restrict__ kc,
+                                               int64_t pc, int lz, const ZTwiddle W) {
+    using Z = ZcGeom<NZ>;
+    extern __shared__ double2 zs[];  // [NZ][ROW]
+    // the twiddles in shared memory (the lanes index them differently)
+    __shared__ double2 tw[16];
+    if (threadIdx.x < NZ / 2) tw[threadIdx.x] = make_double2(W.c[threadIdx.x], W.s[threadIdx.x]);
+    const int64_t col0 = static_cast<int64_t>(blockIdx.x) * Z::C;
+    const int ncol = pc - col0 < Z::C ? static_cast<int>(pc - col0) : Z::C;
+    // rows (z, c), z < lz: consecutive threads on consecutive columns of a row
+    for (int idx = threadIdx.x; idx < 3 * lz * Z::C; idx += blockDim.x) {
+        const int row = idx / Z::C, q = idx - row * Z::C;
+        const int z = row / 3, c = row - 3 * z;
+        zs[z * Z::ROW + c * Z::C + q] =
+            q < ncol ? in[(static_cast<int64_t>(z) * 3 + c) * pc + col0 + q] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const int l = threadIdx.x % NZ, q = threadIdx.x / NZ;  // this lane's z and column
+    const int64_t col = col0 + (q < ncol ? q : 0);
+    double2 v[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        v[c] = l < lz ? zs[l * Z::ROW + c * Z::C + q] : make_double2(0.0, 0.0);
+        v[c] = zfft_forward<NZ>(v[c], l, tw);
+    }
+    double2 h[3];
+    if constexpr (REAL) {
+        const double* k = kr + col * 6 * NZ + l;
+        const double kxx = __ldg(k), kxy = __ldg(k + NZ), kxz = __ldg(k + 2 * NZ), kyy = __ldg(k + 3 * NZ),
+                     kyz = __ldg(k + 4 * NZ), kzz = __ldg(k + 5 * NZ);
+        h[0] = make_double2(fma(kxx, v[0].x, fma(kxy, v[1].x, kxz * v[2].x)),
+                            fma(kxx, v[0].y, fma(kxy, v[1].y, kxz * v[2].y)));
+        h[1] = make_double2(fma(kxy, v[0].x, fma(kyy, v[1].x, kyz * v[2].x)),
+                            fma(kxy, v[0].y, fma(kyy, v[1].y, kyz * v[2].y)));
+        h[2] = make_double2(fma(kxz, v[0].x, fma(kyz, v[1].x, kzz * v[2].x)),
+                            fma(kxz, v[0].y, fma(kyz, v[1].y, kzz * v[2].y)));
+    } else {
+        const double2* k = kc + col * 6 * NZ + l;
+        const double2 kxx = k[0], kxy = k[NZ], kxz = k[2 * NZ], kyy = k[3 * NZ], kyz = k[4 * NZ], kzz = k[5 * NZ];
+        auto mac = [](double2 a, double2 b, double2 acc) {
+            return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+        };
+        const double2 z0 = make_double2(0.0, 0.0);
+        h[0] = mac(kxx, v[0], mac(kxy, v[1], mac(kxz, v[2], z0)));
+        h[1] = mac(kxy, v[0], mac(kyy, v[1], mac(kyz, v[2], z0)));
+        h[2] = mac(kxz, v[0], mac(kyz, v[1], mac(kzz, v[2], z0)));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double2 y = zfft_inverse<NZ>(h[c], l, tw);
+        if (l < lz) zs[l * Z::ROW + c * Z::C + q] = y;  // this lane's own slot, read above by it alone
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 3 * lz * Z::C; idx += blockDim.x) {
+        const int row = idx / Z::C, q2 = idx - row * Z::C;
+        const int z = row / 3, c = row - 3 * z;
+        if (q2 < ncol) out[(static_cast<int64_t>(z) * 3 + c) * pc + col0 + q2] = zs[z * Z::ROW + c * Z::C + q2];
+    }
+}
+
 mj_status cufft_status(cufftResult r, const char* where) {
     if (r == CUFFT_SUCCESS) return MJ_OK;
     return set_error(MJ_ERR_CUDA, std::string("cuFFT error ") + std::to_string(static_cast<int>(r)) + " in " + where);
@@ -125,6 +259,8 @@ void free_plan(DipolarPlan* d) {
     cudaFree(d->d_cz);
     cudaFree(d->d_kfr);
     cudaFree(d->d_kfc);
+    cudaFree(d->d_kzr);
+    cudaFree(d->d_kzc);
     delete d;
 }
 
@@ -205,6 +341,53 @@ mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t 
             im = std::max(im, std::fabs(c.y));
         }
         d->real_kf = im <= 1e-13 * re;
+        // the fused z convolution's K_F: per column, kz in the lanes' bit-reversed order
+        if (nz >= 2 && nz <= 32 && (nz & (nz - 1)) == 0) {
+            int bits = 0;
+            while ((1 << bits) < nz) ++bits;
+            auto bitrev = [&](int l) {
+                int r = 0;
+                for (int b = 0; b < bits; ++b) r |= ((l >> b) & 1) << (bits - 1 - b);
+                return r;
+            };
+            const size_t ncol = static_cast<size_t>(d->pc);
+            if (d->real_kf) {
+                std::vector<double> kz(ncol * nz * 6);
+                for (size_t col = 0; col < ncol; ++col)
+                    for (int c = 0; c < 6; ++c)
+                        for (int l = 0; l < nz; ++l)
+                            kz[(col * 6 + c) * nz + l] =
+                                h[static_cast<size_t>(c) * nkc + static_cast<size_t>(bitrev(l)) * ncol + col].x;
+                st = al(&d->d_kzr, sizeof(double) * kz.size(), "dipolar K_F columns");
+                if (st == MJ_OK)
+                    st = cuda_status(cudaMemcpy(d->d_kzr, kz.data(), sizeof(double) * kz.size(), cudaMemcpyHostToDevice),
+                                     "K_F columns upload");
+            } else {
+                std::vector<cufftDoubleComplex> kz(ncol * nz * 6);
+                for (size_t col = 0; col < ncol; ++col)
+                    for (int c = 0; c < 6; ++c)
+                        for (int l = 0; l < nz; ++l)
+                            kz[(col * 6 + c) * nz + l] =
+                                h[static_cast<size_t>(c) * nkc + static_cast<size_t>(bitrev(l)) * ncol + col];
+                st = al(&d->d_kzc, sizeof(cufftDoubleComplex) * kz.size(), "dipolar K_F columns");
+                if (st == MJ_OK)
+                    st = cuda_status(cudaMemcpy(d->d_kzc, kz.data(), sizeof(cufftDoubleComplex) * kz.size(),
+                                                cudaMemcpyHostToDevice),
+                                     "K_F columns upload");
+            }
+            if (st != MJ_OK) {
+                cudaFree(kf);
+                return fail(st);
+            }
+            // exp(-2 pi i m / nz), m < nz / 2, rounded once from long double
+            const long double pi = 3.141592653589793238462643383279502884L;
+            for (int m = 0; m < nz / 2; ++m) {
+                const long double a = 2.0L * pi * static_cast<long double>(m) / static_cast<long double>(nz);
+                d->tw[m] = static_cast<double>(std::cos(a));
+                d->tw[16 + m] = static_cast<double>(-std::sin(a));
+            }
+            d->zconv = true;
+        }
         if (d->real_kf) {
             std::vector<double> r(h.size());
             for (size_t q = 0; q < h.size(); ++q) r[q] = h[q].x;
@@ -263,6 +446,34 @@ mj_status dipolar_apply(mj_plan* p, const double* m, double* /*H unused: consume
     if (d->have_fz) cufftSetStream(d->fz, s);
     // planes z < Lz of d_cx; the rest of it stays zero
     if ((st = cufft_status(cufftExecD2Z(d->f2d, d->d_pad, d->d_cx), "2D D2Z")) != MJ_OK) return st;
+    if (d->zconv && p->dip_zconv) {
+        // z transforms and product in one pass, into the planes z < Lz of d_cz
+        ZTwiddle W;
+        for (int m = 0; m < 16; ++m) {
+            W.c[m] = d->tw[m];
+            W.s[m] = d->tw[16 + m];
+        }
+        const int nz = d->nrep[2];
+        const double2* in = reinterpret_cast<const double2*>(d->d_cx);
+        double2* out = reinterpret_cast<double2*>(d->d_cz);
+        const double2* kc = reinterpret_cast<const double2*>(d->d_kzc);
+        auto go = [&](auto nzc) {
+            constexpr int NZ = decltype(nzc)::value;
+            using Z = ZcGeom<NZ>;
+            const unsigned nb = static_cast<unsigned>((d->pc + Z::C - 1) / Z::C);
+            if (d->real_kf) k_zconv<NZ, true><<<nb, 256, Z::smem, s>>>(in, out, d->d_kzr, kc, d->pc, d->lz, W);
+            else k_zconv<NZ, false><<<nb, 256, Z::smem, s>>>(in, out, d->d_kzr, kc, d->pc, d->lz, W);
+        };
+        switch (nz) {
+            case 2: go(std::integral_constant<int, 2>{}); break;
+            case 4: go(std::integral_constant<int, 4>{}); break;
+            case 8: go(std::integral_constant<int, 8>{}); break;
+            case 16: go(std::integral_constant<int, 16>{}); break;
+            default: go(std::integral_constant<int, 32>{}); break;
+        }
+        if ((st = cuda_status(cudaGetLastError(), "k_zconv")) != MJ_OK) return st;
+        return cufft_status(cufftExecZ2D(d->b2d, d->d_cz, d->d_h), "2D Z2D");
+    }
     cufftDoubleComplex* spec = d->d_cx;
     if (d->have_fz) {
         if ((st = cufft_status(cufftExecZ2Z(d->fz, d->d_cx, d->d_cz, CUFFT_FORWARD), "z forward")) != MJ_OK) return st;

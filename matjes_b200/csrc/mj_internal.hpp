@@ -155,6 +155,7 @@ struct mj_plan {
     std::string host_graph_key;
     int host_stripes = 0;  // stripes of mj_step_host (0: the default)
     int blocks_per_sm = 0;    // cap on resident tiled-pass blocks per SM (0: none)
+    bool dip_zconv = true;    // FFT dipolar: the fused z convolution where the grid allows it
     int smem_cap_bytes = 0;   // the dynamic shared memory per block that makes the cap
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;

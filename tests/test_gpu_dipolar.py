@@ -104,3 +104,26 @@ def test_full_size_film_field_and_sib_steps(dip):
     M.run(mo, 20, **dyn)
     assert np.abs(m - mo).max() < 1e-9
     assert np.abs(np.linalg.norm(m, axis=1) - 1.0).max() < 1e-13
+
+
+@pytest.mark.parametrize("L,periodic,dip", [((16, 16, 4), (1, 1, 0), 1), ((8, 8, 8), (1, 1, 1), 1),
+                                            ((6, 5, 4), (0, 0, 0), 1), ((16, 16, 4), (1, 1, 0), 2),
+                                            ((12, 10, 2), (1, 0, 0), 1)])
+def test_fused_z_convolution_equals_the_cufft_route(L, periodic, dip):
+    """z grids of 16, 8, 8, 8 and 4 planes: the fused z transforms and product
+    (lane FFTs, K_F per column) give the field and energies of the cuFFT z
+    transforms with the separate product to 1e-13."""
+    import matjes_b200 as mj
+    from matjes_b200 import _abi
+
+    deck = _film(L, periodic, Jv=1e-3, Dv=0.15e-3, Kv=-0.02e-3, Bz=0.2)
+    deck.dip = dip
+    m = mj.random_sphere(deck.nsites, 12)
+    out = []
+    for zconv in (1, 0):
+        ham = mj.Hamiltonian(deck)
+        _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_DIP_ZCONV, zconv))
+        out.append(ham.get_eff_field(m, with_energy=True))
+    (B1, e1), (B0, e0) = out
+    assert site_rel_err(B1, B0) < 1e-13
+    assert scalar_rel_err(e1, e0) < 1e-13
