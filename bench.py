@@ -952,11 +952,16 @@ def run_gpu(args, rank, world):
         return ts
 
     stripe_ms = {}
-    for hs in (2, 3, 4, 6, 8):
-        _abi.check(lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_STRIPES, hs))
-        stripe_ms[hs] = round(1e3 * float(np.median(host_steps(10, 20_000 + 100 * hs)[2:])), 4)
-    host_stripes = min(stripe_ms, key=stripe_ms.get)
+    for zc in (1, 0):
+        _abi.check(lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_ZEROCOPY, zc))
+        for hs in (2, 3, 4, 6, 8):
+            _abi.check(lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_STRIPES, hs))
+            stripe_ms[f"{hs}{'_zerocopy' if zc else ''}"] = round(
+                1e3 * float(np.median(host_steps(10, 20_000 + 100 * hs + 1000 * zc)[2:])), 4)
+    best_host = min(stripe_ms, key=stripe_ms.get)
+    host_stripes, host_zc = int(best_host.split("_")[0]), int(best_host.endswith("_zerocopy"))
     _abi.check(lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_STRIPES, host_stripes))
+    _abi.check(lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_ZEROCOPY, host_zc))
     host.copy_(torch.from_numpy(w["m0"]))
     ke = max(3, min(K, 20))
     times = host_steps(ke + 2, 10_000)[2:]
@@ -1009,8 +1014,9 @@ def run_gpu(args, rank, world):
         "clocks": ck,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 24 * N, "d2h_bytes_per_step": 24 * N + 8,
                 "path": "mj_step_host: pinned host AoS in and out, one step, energy to the host; copies, "
-                        f"transposes and passes overlapped in {host_stripes} stripes of tile rows",
-                "host_stripes": host_stripes},
+                        f"transposes and passes overlapped in {host_stripes} stripes of tile rows"
+                        + (", the stepped spins written by kernels into the mapped buffer" if host_zc else ""),
+                "host_stripes": host_stripes, "host_zerocopy": host_zc},
         "gpu_launches": int(sum(c for _, c in prof.values())),
         "cpu_baseline": cpu,
         **extras,

@@ -27,7 +27,8 @@ module m_matjes_gpu
   integer(c_int32_t), parameter :: MJ_MAX_ATOMS = 16
   integer(c_int32_t), parameter :: MJ_MC_CONE = 0, MJ_MC_ISING = 1, MJ_MC_UNDERRELAX = 2, MJ_MC_OVERRELAX = 3
   integer(c_int32_t), parameter :: MJ_OPT_TMA = 0, MJ_OPT_FUSED = 1, MJ_OPT_PDL = 2, MJ_OPT_STORE_DRAW = 3, &
-                                   MJ_OPT_HOST_STRIPES = 4, MJ_OPT_BLOCKS_PER_SM = 5, MJ_OPT_DIP_ZCONV = 6
+                                   MJ_OPT_HOST_STRIPES = 4, MJ_OPT_BLOCKS_PER_SM = 5, MJ_OPT_DIP_ZCONV = 6, &
+                                   MJ_OPT_HOST_ZEROCOPY = 7
 
   ! ---- descriptors ----
   ! Nsize, Periodic_log, lattice (areal(:, j) = lattice vector j in nm, alat

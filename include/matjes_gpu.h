@@ -177,7 +177,10 @@ mj_status mj_plan_set_fused(mj_plan* plan, int32_t enable);
  *   MJ_OPT_DIP_ZCONV (default 1)  FFT dipolar term with a z grid of a power
  *                              of two up to 32: the z transforms and the
  *                              product with K_F as one kernel (0: cuFFT z
- *                              transforms and a separate product). */
+ *                              transforms and a separate product);
+ *   MJ_OPT_HOST_ZEROCOPY (default 1)  striped mj_step_host with a mapped pinned
+ *                              buffer: kernels write the stepped spins into it
+ *                              directly (0: device transposes and copies). */
 enum {
     MJ_OPT_TMA = 0,
     MJ_OPT_FUSED = 1,
@@ -185,7 +188,8 @@ enum {
     MJ_OPT_STORE_DRAW = 3,
     MJ_OPT_HOST_STRIPES = 4,
     MJ_OPT_BLOCKS_PER_SM = 5,
-    MJ_OPT_DIP_ZCONV = 6
+    MJ_OPT_DIP_ZCONV = 6,
+    MJ_OPT_HOST_ZEROCOPY = 7
 };
 mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value);
 /* Autotuner: times `steps` steps of `p` for every kernel configuration of the

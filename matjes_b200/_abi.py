@@ -29,7 +29,7 @@ MJ_NOISE_PHILOX = 1
 MJ_NOISE_INJECT = 2
 MJ_MAX_ATOMS = 16
 MJ_OPT_TMA, MJ_OPT_FUSED, MJ_OPT_PDL, MJ_OPT_STORE_DRAW, MJ_OPT_HOST_STRIPES, MJ_OPT_BLOCKS_PER_SM = 0, 1, 2, 3, 4, 5
-MJ_OPT_DIP_ZCONV = 6
+MJ_OPT_DIP_ZCONV, MJ_OPT_HOST_ZEROCOPY = 6, 7
 
 INTEGRATORS = {"euler": MJ_EULER, "heun": MJ_HEUN_MATJES, "heun_matjes": MJ_HEUN_MATJES, "sib": MJ_SIB}
 NOISES = {"off": MJ_NOISE_OFF, "philox": MJ_NOISE_PHILOX, "inject": MJ_NOISE_INJECT}

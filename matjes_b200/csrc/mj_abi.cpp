@@ -483,7 +483,8 @@ int host_stripes(const mj_plan* p) {
 // The striped step's work, forked from and joined back into pipe_stream[0]
 // (captured once as a graph and replayed; the step index comes from the
 // plan's device step counter).
-mj_status striped_enqueue(mj_plan* p, double* m_host, const DynCoef& c, int energy_mode, bool E_wanted) {
+mj_status striped_enqueue(mj_plan* p, double* m_host, double* m_mapped, const DynCoef& c, int energy_mode,
+                          bool E_wanted) {
     const bool before = energy_mode == MJ_ENERGY_BEFORE;
     const int64_t N = p->N, Lx = p->sp.L[0], Ly = p->sp.L[1];
     const int nty = tiled_tile_rows(p);
@@ -591,6 +592,18 @@ mj_status striped_enqueue(mj_plan* p, double* m_host, const DynCoef& c, int ener
                 }
             }
         }
+        if (m_mapped) {
+            // the download stream writes the stripe's rows straight into the
+            // mapped host buffer (later stripes only write other rows of `result`)
+            cudaEventRecord(ev_out[k], sc);
+            cudaStreamWaitEvent(sout, ev_out[k], 0);
+            for (int i = 0; i < ndown; ++i) {
+                const int64_t r0 = row_of(down[i][0]), r1 = row_of(down[i][1]);
+                if (r1 > r0 && (st = soa_to_aos_stream(result, m_mapped, Lx * r0, Lx * (r1 - r0), N, sout)) != MJ_OK)
+                    return st;
+            }
+            continue;
+        }
         for (int i = 0; i < ndown; ++i) {
             const int64_t r0 = row_of(down[i][0]), r1 = row_of(down[i][1]);
             if (r1 > r0 && (st = soa_to_aos_range(result, p->d_stage, Lx * r0, Lx * (r1 - r0), N, sc)) != MJ_OK) return st;
@@ -635,6 +648,8 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
         cudaGetLastError();  // a pageable pointer is not an error here
         return MJ_OK;
     }
+    // the buffer's device address when it is mapped (kernels then write the result into it)
+    double* m_mapped = p->host_zerocopy ? static_cast<double*>(pa.devicePointer) : nullptr;
     const int K = host_stripes(p);
     if (K == 0) return MJ_OK;
     DynCoef c;
@@ -660,6 +675,7 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
     std::string key(reinterpret_cast<const char*>(&c), sizeof(c));
     key += std::string(reinterpret_cast<const char*>(&p->sp), sizeof(p->sp));
     key += std::string(reinterpret_cast<const char*>(&m_host), sizeof(m_host));
+    key += std::string(reinterpret_cast<const char*>(&m_mapped), sizeof(m_mapped));
     key += std::string(reinterpret_cast<const char*>(&p->d_bmap), sizeof(p->d_bmap));
     key += "/" + std::to_string(E_host != nullptr) + "/" + std::to_string(prm->energy_mode) + "/" +
            std::to_string(p->tile_variant) + "/" + std::to_string(p->store_draw) + "/" + std::to_string(K);
@@ -668,7 +684,7 @@ mj_status step_host_striped(mj_plan* p, double* m_host, const mj_dyn_params* prm
         p->host_graph_exec = nullptr;
         if ((st = cuda_status(cudaStreamBeginCapture(sin, cudaStreamCaptureModeThreadLocal), "begin capture")) != MJ_OK)
             return st;
-        const mj_status inner = striped_enqueue(p, m_host, c, prm->energy_mode, E_host != nullptr);
+        const mj_status inner = striped_enqueue(p, m_host, m_mapped, c, prm->energy_mode, E_host != nullptr);
         cudaGraph_t graph = nullptr;
         const cudaError_t e = cudaStreamEndCapture(sin, &graph);
         if (inner != MJ_OK) {
@@ -1019,6 +1035,7 @@ mj_status mj_plan_set_option(mj_plan* plan, int32_t option, int32_t value) {
             plan->host_stripes = value;
             break;
         case MJ_OPT_DIP_ZCONV: plan->dip_zconv = value != 0; break;
+        case MJ_OPT_HOST_ZEROCOPY: plan->host_zerocopy = value != 0; break;
         case MJ_OPT_BLOCKS_PER_SM: {
             if (value != 0 && (value < 4 || value > 32))
                 return set_error(MJ_ERR_ARG, "blocks per SM must be 0 or in [4, 32]");

@@ -156,6 +156,7 @@ struct mj_plan {
     int host_stripes = 0;  // stripes of mj_step_host (0: the default)
     int blocks_per_sm = 0;    // cap on resident tiled-pass blocks per SM (0: none)
     bool dip_zconv = true;    // FFT dipolar: the fused z convolution where the grid allows it
+    bool host_zerocopy = true;  // striped mj_step_host: downloads written by kernels into the mapped host buffer
     int smem_cap_bytes = 0;   // the dynamic shared memory per block that makes the cap
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;
@@ -216,6 +217,8 @@ mj_status soa_to_aos(const double* src_soa, double* dst_aos, int64_t n, cudaStre
 // the transposes restricted to the sites [i0, i0 + cnt) of n
 mj_status aos_to_soa_range(const double* src_aos, double* dst_soa, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s);
 mj_status soa_to_aos_range(const double* src_soa, double* dst_aos, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s);
+// the same into a mapped host buffer (sites staged per block, contiguous writes)
+mj_status soa_to_aos_stream(const double* src_soa, double* dst_aos, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s);
 // one block of nthreads sums nblocks energy partials in ordered_sum's fixed order
 mj_status launch_ordered_sum(const double* partials, int nblocks, int nthreads, double* out, cudaStream_t s);
 int64_t energy_blocks(const mj_plan* p);

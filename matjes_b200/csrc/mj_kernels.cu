@@ -376,6 +376,26 @@ __global__ void k_soa_to_aos_range(const double* __restrict__ s, double* __restr
     a[3 * i + 1] = s[n + i];
     a[3 * i + 2] = s[2 * n + i];
 }
+// The same into memory across the host link (a mapped pinned host buffer): a
+// block's 256 sites staged in shared memory as AoS, then written as contiguous
+// doubles (consecutive threads on consecutive addresses).
+__global__ void __launch_bounds__(256) k_soa_to_aos_stream(const double* __restrict__ s, double* __restrict__ a,
+                                                           int64_t i0, int64_t cnt, int64_t n) {
+    __shared__ double buf[3 * 256];
+    const int64_t base = i0 + blockIdx.x * static_cast<int64_t>(256);
+    const int64_t end = i0 + cnt;
+    const int t = threadIdx.x;
+    const int64_t i = base + t;
+    if (i < end) {
+        buf[3 * t] = s[i];
+        buf[3 * t + 1] = s[n + i];
+        buf[3 * t + 2] = s[2 * n + i];
+    }
+    __syncthreads();
+    const int nd = 3 * static_cast<int>(end - base < 256 ? end - base : 256);
+    double* dst = a + 3 * base;
+    for (int k = t; k < nd; k += 256) dst[k] = buf[k];
+}
 // energy partials summed in the fixed order of ordered_sum (one block)
 __global__ void k_ordered_sum1(const double* partials, int nblocks, double* out) { ordered_sum<1>(partials, nblocks, out); }
 
@@ -641,6 +661,11 @@ mj_status soa_to_aos_range(const double* so, double* a, int64_t i0, int64_t cnt,
     if (cnt <= 0) return MJ_OK;
     k_soa_to_aos_range<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(so, a, i0, cnt, n);
     return cuda_status(cudaGetLastError(), "soa_to_aos_range");
+}
+mj_status soa_to_aos_stream(const double* so, double* a, int64_t i0, int64_t cnt, int64_t n, cudaStream_t s) {
+    if (cnt <= 0) return MJ_OK;
+    k_soa_to_aos_stream<<<static_cast<unsigned>((cnt + 255) / 256), 256, 0, s>>>(so, a, i0, cnt, n);
+    return cuda_status(cudaGetLastError(), "soa_to_aos_stream");
 }
 mj_status launch_ordered_sum(const double* partials, int nblocks, int nthreads, double* out, cudaStream_t s) {
     k_ordered_sum1<<<1, nthreads, 0, s>>>(partials, nblocks, out);

@@ -120,17 +120,20 @@ def test_replayed_host_step_follows_buffer_and_parameter_changes():
         assert E[0] == want_E, call
 
 
-@pytest.mark.parametrize("stripes", [2, 3, 5, 9, 64])
-def test_any_stripe_count_equals_the_device_step(stripes):
+@pytest.mark.parametrize("stripes,zerocopy", [(2, 1), (3, 1), (5, 1), (9, 1), (64, 1), (3, 0), (9, 0)])
+def test_any_stripe_count_equals_the_device_step(stripes, zerocopy):
     """Every stripe count (64 is clamped to 5 tile rows per stripe) gives the
     device step bit for bit: SIB at 10 K with the energy after the step (three
-    chained passes, the first shifted by two tile rows) and before it."""
+    chained passes, the first shifted by two tile rows) and before it; the
+    stepped spins written by kernels into the mapped host buffer (zerocopy 1)
+    or transposed on the device and copied (0)."""
     import matjes_b200 as mj
     from matjes_b200 import _abi
 
     deck = mj.triangular((96, 1000))
     ham = mj.Hamiltonian(deck)
     _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_STRIPES, stripes))
+    _abi.check(_abi.lib.mj_plan_set_option(ham.plan, _abi.MJ_OPT_HOST_ZEROCOPY, zerocopy))
     kw = dict(integrator="sib", temperature=10.0, noise="philox", alpha=0.1, timestep=0.1, seed=5)
     m0 = mj.random_sphere(deck.nsites, 21)
     for energy_mode in (1, 0):
