@@ -377,11 +377,12 @@ __global__ void k_soa_to_aos_range(const double* __restrict__ s, double* __restr
     a[3 * i + 2] = s[2 * n + i];
 }
 // The same into memory across the host link (a mapped pinned host buffer): a
-// block's 256 sites staged in shared memory as AoS, then written as contiguous
-// doubles (consecutive threads on consecutive addresses).
+// block's 256 sites staged in shared memory as AoS, then written contiguously
+// (consecutive threads on consecutive addresses), 16 bytes a thread where the
+// block's span starts on a 16-byte boundary, else 8.
 __global__ void __launch_bounds__(256) k_soa_to_aos_stream(const double* __restrict__ s, double* __restrict__ a,
                                                            int64_t i0, int64_t cnt, int64_t n) {
-    __shared__ double buf[3 * 256];
+    __shared__ __align__(16) double buf[3 * 256];
     const int64_t base = i0 + blockIdx.x * static_cast<int64_t>(256);
     const int64_t end = i0 + cnt;
     const int t = threadIdx.x;
@@ -394,7 +395,15 @@ __global__ void __launch_bounds__(256) k_soa_to_aos_stream(const double* __restr
     __syncthreads();
     const int nd = 3 * static_cast<int>(end - base < 256 ? end - base : 256);
     double* dst = a + 3 * base;
-    for (int k = t; k < nd; k += 256) dst[k] = buf[k];
+    if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+        const int np = nd / 2;  // whole 16-byte pairs, then an odd last double
+        double2* d2 = reinterpret_cast<double2*>(dst);
+        const double2* b2 = reinterpret_cast<const double2*>(buf);
+        for (int k = t; k < np; k += 256) d2[k] = b2[k];
+        if ((nd & 1) && t == 0) dst[nd - 1] = buf[nd - 1];
+    } else {
+        for (int k = t; k < nd; k += 256) dst[k] = buf[k];
+    }
 }
 // energy partials summed in the fixed order of ordered_sum (one block)
 __global__ void k_ordered_sum1(const double* partials, int nblocks, double* out) { ordered_sum<1>(partials, nblocks, out); }
