@@ -386,9 +386,22 @@ mj_status dyn_coef(const mj_dyn_params* d, const mj_plan* plan, DynCoef& c) {
 // Euler alternates between m and the plan's midpoint buffer.
 mj_status step_sequence(mj_plan* p, double* m, const DynCoef& c, int energy_mode, uint32_t step0, int32_t nsteps,
                         double* E_dev, cudaStream_t s) {
-    mj_status st;
+    mj_status st = MJ_OK;
     double* cur = m;
     double* other = p->d_mid;
+    // the step kernels keep the dipolar pad grid current for the next
+    // evaluation only within this sequence (the caller may change m between calls)
+    struct PadScope {
+        mj_plan* p;
+        explicit PadScope(mj_plan* q) : p(q) {
+            p->dip_fuse_pad = true;
+            p->dip_pad_holds = nullptr;
+        }
+        ~PadScope() {
+            p->dip_fuse_pad = false;
+            p->dip_pad_holds = nullptr;
+        }
+    } pad_scope(p);
     for (int32_t k = 0; k < nsteps; ++k) {
         double* E = nullptr;
         if (E_dev) {

@@ -216,6 +216,12 @@ __device__ __forceinline__ void st3(double* m, int64_t i, int64_t N, double3 v) 
     m[2 * N + i] = v.z;
 }
 
+__device__ __forceinline__ void st_pad(const DipPad& d, int x, int y, int z, double3 v) {
+    const int64_t q = x + static_cast<int64_t>(d.px) * y + d.zs * z;
+    d.p[q] = v.x;
+    d.p[d.cs + q] = v.y;
+    d.p[2 * d.cs + q] = v.z;
+}
 __device__ __forceinline__ double3 ld_dip(const DipView& v, int x, int y, int z) {
     const int64_t q = x + static_cast<int64_t>(v.px) * y + v.zs * z;
     return make_double3(__ldg(v.h + q), __ldg(v.h + v.cs + q), __ldg(v.h + 2 * v.cs + q));

@@ -437,10 +437,14 @@ mj_status dipolar_apply(mj_plan* p, const double* m, double* /*H unused: consume
     if (!d) return set_error(MJ_ERR_ARG, "dipolar plan missing");
     const int64_t N = p->N;
     const int64_t nkc = d->pc * d->nrep[2];
-    k_pad<<<static_cast<unsigned>((N + 255) / 256), 256, 0, s>>>(m, d->d_pad, p->sp.L[0], p->sp.L[1], p->sp.L[2],
-                                                                  d->nrep[0], d->pr);
-    mj_status st = cuda_status(cudaGetLastError(), "k_pad");
-    if (st != MJ_OK) return st;
+    mj_status st = MJ_OK;
+    // the pass that wrote m may have written the padded grid as well
+    if (p->dip_pad_holds != m) {
+        k_pad<<<static_cast<unsigned>((N + 255) / 256), 256, 0, s>>>(m, d->d_pad, p->sp.L[0], p->sp.L[1], p->sp.L[2],
+                                                                      d->nrep[0], d->pr);
+        if ((st = cuda_status(cudaGetLastError(), "k_pad")) != MJ_OK) return st;
+    }
+    p->dip_pad_holds = nullptr;
     cufftSetStream(d->f2d, s);
     cufftSetStream(d->b2d, s);
     if (d->have_fz) cufftSetStream(d->fz, s);
@@ -488,6 +492,12 @@ mj_status dipolar_apply(mj_plan* p, const double* m, double* /*H unused: consume
         return st;
     // H of the lattice planes: the first 3 Lz complex planes of the spectrum
     return cufft_status(cufftExecZ2D(d->b2d, spec, d->d_h), "2D Z2D");
+}
+
+DipPad dipolar_pad(const mj_plan* p) {
+    const DipolarPlan* d = static_cast<const DipolarPlan*>(p->dip);
+    if (!p->dip_on || !d) return DipPad{nullptr, 0, 0, 0};
+    return DipPad{d->d_pad, d->pr, 3 * d->pr, d->nrep[0]};
 }
 
 DipView dipolar_view(const mj_plan* p) {

@@ -70,6 +70,16 @@ struct DipView {
     int px;       // padded x extent (row stride)
 };
 
+// The dipolar term's padded input grid (the layout of DipView): a step kernel
+// given one stores every spin it writes there too, so that the next dipolar
+// evaluation of those spins needs no pad launch.  p = null: none.
+struct DipPad {
+    double* p;
+    int64_t cs;
+    int64_t zs;
+    int px;
+};
+
 // Dynamics coefficients computed once per call on the host.
 struct DynCoef {
     int integrator;
@@ -157,6 +167,10 @@ struct mj_plan {
     int blocks_per_sm = 0;    // cap on resident tiled-pass blocks per SM (0: none)
     bool dip_zconv = true;    // FFT dipolar: the fused z convolution where the grid allows it
     bool host_zerocopy = true;  // striped mj_step_host: downloads written by kernels into the mapped host buffer
+    // FFT dipolar inside a step sequence: the step kernels also write their spins
+    // into the padded grid, which then holds dip_pad_holds (null: unknown)
+    bool dip_fuse_pad = false;
+    const double* dip_pad_holds = nullptr;
     int smem_cap_bytes = 0;   // the dynamic shared memory per block that makes the cap
     // per-kernel event timing (mj_profile_enable / mj_profile_read)
     bool prof_on = false;
@@ -282,5 +296,6 @@ mj_status dipolar_create(mj_plan* p, const std::vector<double>& K, cudaStream_t 
 void dipolar_destroy(mj_plan* p);
 // H = K * m on the padded grid; consumers read it through dipolar_view and fold B -= 2H.
 mj_status dipolar_apply(mj_plan* p, const double* m, double* H_unused, cudaStream_t s);
+DipPad dipolar_pad(const mj_plan* p);
 DipView dipolar_view(const mj_plan* p);
 }  // namespace mj

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) k_field(const __grid_constant__ F fp, con
 template <class F>
 __global__ void __launch_bounds__(256) k_euler(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
                                                const double* __restrict__ m, double* __restrict__ mout,
-                                               const DipView Hd, Reduce R, int* status) {
+                                               const DipView Hd, Reduce R, int* status, const DipPad pad) {
     int64_t i;
     int x, y, z;
     const bool act = fp.site(i, x, y, z);
@@ -202,6 +202,7 @@ __global__ void __launch_bounds__(256) k_euler(const __grid_constant__ F fp, con
         const double3 mo = project(t, m0);
         flag_nonfinite(status, mo);
         st3(mout, i, N, mo);
+        if (pad.p) st_pad(pad, x, y, z, mo);
     }
     if (R.out) {
         double v[1] = {e};
@@ -214,7 +215,7 @@ template <class F>
 __global__ void __launch_bounds__(256) k_heun1(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
                                                const double* __restrict__ m, double* __restrict__ mid,
                                                double* __restrict__ D1, double* __restrict__ DTo,
-                                               const DipView Hd, Reduce R) {
+                                               const DipView Hd, Reduce R, const DipPad pad) {
     int64_t i;
     int x, y, z;
     const bool act = fp.site(i, x, y, z);
@@ -228,7 +229,9 @@ __global__ void __launch_bounds__(256) k_heun1(const __grid_constant__ F fp, con
         const double3 D = llg_rhs(minus2(f.B, hd), m0, C.alpha, C.inv_den);
         const double c = C.h_over_hbar;
         const double3 t = make_double3(m0.x + D.x * c, m0.y + D.y * c, m0.z + D.z * c);
-        st3(mid, i, N, project(t, m0));
+        const double3 mt = project(t, m0);
+        st3(mid, i, N, mt);
+        if (pad.p) st_pad(pad, x, y, z, mt);
         st3(D1, i, N, D);
         if (C.thermal) st3(DTo, i, N, llg_rhs(thermal_field(C, step, i, N), m0, C.alpha, C.inv_den));
     }
@@ -243,7 +246,7 @@ template <class F>
 __global__ void __launch_bounds__(256) k_heun2(const __grid_constant__ F fp, const DynCoef C,
                                                const double* __restrict__ mid, const double* __restrict__ D1,
                                                const double* __restrict__ DTi, double* __restrict__ mout,
-                                               const DipView Hd, int* status) {
+                                               const DipView Hd, int* status, const DipPad pad) {
     int64_t i;
     int x, y, z;
     if (!fp.site(i, x, y, z)) return;
@@ -263,13 +266,14 @@ __global__ void __launch_bounds__(256) k_heun2(const __grid_constant__ F fp, con
     const double3 mo = project(t, mt);
     flag_nonfinite(status, mo);
     st3(mout, i, N, mo);
+    if (pad.p) st_pad(pad, x, y, z, mo);
 }
 
 // SIB pass 1: Cayley predictor from m_n with A(m_n); writes the midpoint (m_n + m~)/2.
 template <class F>
 __global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
                                               const double* __restrict__ m, double* __restrict__ mid,
-                                              const DipView Hd, Reduce R) {
+                                              const DipView Hd, Reduce R, const DipPad pad) {
     int64_t i;
     int x, y, z;
     const bool act = fp.site(i, x, y, z);
@@ -285,7 +289,9 @@ __global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, cons
             const double3 b = thermal_field(C, step, i, N);
             H = make_double3(H.x + b.x, H.y + b.y, H.z + b.z);
         }
-        st3(mid, i, N, sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc));
+        const double3 mb = sib_solve<true>(m0, m0, H, C.alpha, C.sib_hc);
+        st3(mid, i, N, mb);
+        if (pad.p) st_pad(pad, x, y, z, mb);
     }
     if (R.out) {
         double v[1] = {e};
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(256) k_sib1(const __grid_constant__ F fp, cons
 template <class F>
 __global__ void __launch_bounds__(256) k_sib2(const __grid_constant__ F fp, const DynCoef C, uint32_t step,
                                               const double* __restrict__ mid, double* m, const DipView Hd,
-                                              int* status) {
+                                              int* status, const DipPad pad) {
     int64_t i;
     int x, y, z;
     if (!fp.site(i, x, y, z)) return;
@@ -314,6 +320,7 @@ __global__ void __launch_bounds__(256) k_sib2(const __grid_constant__ F fp, cons
     const double3 mo = sib_solve(m0, mb, H, C.alpha, C.sib_hc);
     flag_nonfinite(status, mo);
     st3(m, i, N, mo);
+    if (pad.p) st_pad(pad, x, y, z, mo);
 }
 
 // Reference temperature estimator (dynamics/measure_temp.f90:21-43): sum |m x B|^2, sum m.B.
@@ -491,29 +498,38 @@ template <class F>
 mj_status step_impl(mj_plan* p, const Launch<F>& L, double* m, double* m_out, const DynCoef& c, uint32_t step,
                     double* E_prev, cudaStream_t s) {
     mj_status st;
+    // inside a step sequence with the dipolar term: every pass also writes its
+    // spins into the padded grid of the next dipolar evaluation
+    const DipPad pd = (p->dip_on && p->dip_fuse_pad) ? dipolar_pad(p) : DipPad{nullptr, 0, 0, 0};
     switch (c.integrator) {
         case MJ_EULER: {
             DipView Hd = dip_field(p, m, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_euler", k_euler<F>, L.fp, c, step, m, m_out, Hd, make_reduce(p, E_prev), p->d_status);
+            MJ_LAUNCH("k_euler", k_euler<F>, L.fp, c, step, m, m_out, Hd, make_reduce(p, E_prev), p->d_status, pd);
+            if (pd.p) p->dip_pad_holds = m_out;
             return MJ_OK;
         }
         case MJ_HEUN_MATJES: {
             DipView Hd = dip_field(p, m, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_heun1", k_heun1<F>, L.fp, c, step, m, p->d_mid, p->d_aux, p->d_aux2, Hd, make_reduce(p, E_prev));
+            MJ_LAUNCH("k_heun1", k_heun1<F>, L.fp, c, step, m, p->d_mid, p->d_aux, p->d_aux2, Hd, make_reduce(p, E_prev),
+                      pd);
+            if (pd.p) p->dip_pad_holds = p->d_mid;
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_heun2", k_heun2<F>, L.fp, c, p->d_mid, p->d_aux, p->d_aux2, m, Hd, p->d_status);
+            MJ_LAUNCH("k_heun2", k_heun2<F>, L.fp, c, p->d_mid, p->d_aux, p->d_aux2, m, Hd, p->d_status, pd);
+            if (pd.p) p->dip_pad_holds = m;
             return MJ_OK;
         }
         case MJ_SIB: {
             DipView Hd = dip_field(p, m, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_sib1", k_sib1<F>, L.fp, c, step, m, p->d_mid, Hd, make_reduce(p, E_prev));
+            MJ_LAUNCH("k_sib1", k_sib1<F>, L.fp, c, step, m, p->d_mid, Hd, make_reduce(p, E_prev), pd);
+            if (pd.p) p->dip_pad_holds = p->d_mid;
             Hd = dip_field(p, p->d_mid, s, st);
             if (st != MJ_OK) return st;
-            MJ_LAUNCH("k_sib2", k_sib2<F>, L.fp, c, step, p->d_mid, m, Hd, p->d_status);
+            MJ_LAUNCH("k_sib2", k_sib2<F>, L.fp, c, step, p->d_mid, m, Hd, p->d_status, pd);
+            if (pd.p) p->dip_pad_holds = m;
             return MJ_OK;
         }
         default:

@@ -127,3 +127,35 @@ def test_fused_z_convolution_equals_the_cufft_route(L, periodic, dip):
     (B1, e1), (B0, e0) = out
     assert site_rel_err(B1, B0) < 1e-13
     assert scalar_rel_err(e1, e0) < 1e-13
+
+
+@pytest.mark.parametrize("integrator", ["sib", "heun", "euler"])
+def test_pad_written_by_the_steps_is_never_stale(integrator):
+    """Within a step sequence the step kernels also write the dipolar term's
+    padded input grid; a call that follows, after the caller replaced the
+    spins, must see the new spins: 6 steps, new spins, 6 more steps, each part
+    against the oracle (and a field evaluation in between)."""
+    import torch
+
+    import matjes_b200 as mj
+
+    deck = _film((16, 16, 4), (1, 1, 0), Jv=1e-3, Dv=0.15e-3, Kv=-0.02e-3, Bz=0.2)
+    ham = mj.Hamiltonian(deck)
+    M = O.Model(deck)
+    dyn = dict(integrator=integrator, timestep=0.1, alpha=0.1, temperature=0.0)
+    sd = mj.SpinDynamics(ham, **dyn)
+    m0 = mj.random_sphere(deck.nsites, 31)
+    m = torch.tensor(m0.T.copy(), device="cuda")
+    sd.run(m, 6)
+    mo = m0.copy()
+    M.run(mo, 6, **dyn)
+    assert np.abs(m.cpu().numpy().T - mo).max() < 1e-11
+    m1 = mj.random_sphere(deck.nsites, 32)
+    m.copy_(torch.tensor(m1.T.copy(), device="cuda"))
+    B = ham.get_eff_field(m1)
+    Bo, _ = M.field(m1)
+    assert site_rel_err(B, Bo) < 1e-12
+    sd.run(m, 6)
+    mo = m1.copy()
+    M.run(mo, 6, **dyn)
+    assert np.abs(m.cpu().numpy().T - mo).max() < 1e-11
