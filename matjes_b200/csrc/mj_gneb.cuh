@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) k_gneb_sums(const double* __restrict__ m,
 // blockIdx.x: the images of one site range run side by side, so the
 // neighbouring images' spins come from L2.
 template <int SPT>
-__global__ void __launch_bounds__(256) k_gneb_step(const double* __restrict__ m, const double* __restrict__ mo,
+__global__ void __launch_bounds__(256, 4) k_gneb_step(const double* __restrict__ m, const double* __restrict__ mo,
                                                    const double* __restrict__ Fo, double* Fn,
                                                    const double* __restrict__ E, const double* __restrict__ img,
                                                    GnebIdx X, int nrep, double spring, double dt, double mass,
