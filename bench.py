@@ -34,12 +34,12 @@ UNIT = "spin-updates/s"
 FLUSH_BYTES = 256 << 20  # larger than the 126 MB L2
 
 
+# the benchmark's metric, as the reference's headline figure names it
+METRIC = "LLG spin-updates/s & HBM GB/s at 1e-12 field err; batched/adjoint vs plain, 1 B200"
+
+
 def metric_name() -> str:
-    try:
-        with open(os.path.join(ROOT, "BASELINE.json")) as f:
-            return json.load(f)["metric"]
-    except Exception:
-        return "LLG spin-updates/s & HBM GB/s"
+    return METRIC
 
 
 def peaks() -> dict:
@@ -431,7 +431,7 @@ def run_dipolar(dev: int, steps: int = 50) -> dict:
     """The dipolar film (128 x 128 x 16 simple cubic, a = 0.25 nm, periodic in-plane,
     open along z, J + D + K + Zeeman + FFT dipolar, SIB alpha = 0.1, T = 5 K
     Philox) on the reference's grid (128 x 128 x 32) and on the fully zero-padded
-    one (256 x 256 x 32, the grid BASELINE's configuration names): one system
+    one (256 x 256 x 32, every axis padded to twice the lattice): one system
     each, and on the reference's grid 8 systems with their own initial states
     (seeds 4..11) advanced concurrently on 8 CUDA streams.  Each grid's dipolar
     evaluation (pad, transforms, pointwise product; the unpack is fused into the

@@ -147,7 +147,7 @@ def test_dipolar_fft_route_equals_direct_circular_sum(dip, nrep):
 
 
 def test_zero_padded_grid_equals_the_explicit_pair_sum():
-    """dip = 2 (every axis zero-padded to 2 L, BASELINE's 256 x 256 x 32 for the
+    """dip = 2 (every axis zero-padded to 2 L, 256 x 256 x 32 for the
     128 x 128 x 16 film): a linear convolution whose kernel sums the periodic
     images over -cut..cut for every pair, which is the explicit route
     (Energy/dipolar_magnetic.f90:181-273).  The reference's grid (periodic axes
