@@ -222,7 +222,7 @@ def deck_module():
 
 def oracle_native():
     """The oracle built -O3 -march=native on this machine (the CPU legs' timed
-    build; the tests' checker is the portable -O2 build of the same source)."""
+    build; the tests use the portable -O2 build of the same source)."""
     os.environ["ORACLE_NATIVE"] = "1"
     from oracle import oracle as O
 

@@ -107,7 +107,7 @@ class MetropolisMC:
 
 @dataclass
 class ThermVal:
-    """therm_val (Metropolis-MC/thermo_val.f90:16-33), the columns this build fills."""
+    """therm_val (Metropolis-MC/thermo_val.f90:16-33), the columns this library fills."""
     T: float
     E: float
     E_err: float

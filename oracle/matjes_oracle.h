@@ -1,7 +1,8 @@
 /*
  * matjes_oracle.h -- CPU restatement of the Matjes spin-dynamics hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: only tests/,
+ * TEST INFRASTRUCTURE ONLY.  The tests compare the CUDA path against this
+ * library: only tests/,
  * __graft_entry__.smoke() and bench.py's cpu_baseline / reference leg may
  * load it.  The product (matjes_b200) never calls into it.
  *

@@ -1,6 +1,6 @@
 """ctypes wrapper of the CPU oracle (liboracle.so).
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA path.  Only tests/,
+TEST INFRASTRUCTURE ONLY: what the tests compare the CUDA path against.  Only tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs may use
 it; the product (matjes_b200) never imports it.  See matjes_oracle.h for the
 reference routines it restates and for its pinning status.
