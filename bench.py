@@ -132,15 +132,20 @@ class Clocks:
                 "samples": len(self.samples), "source": "nvml"}
 
 
-def ncu_traffic(kernel: str, summary: str = "k_tiled_sib_triangular2048.md"):
-    """DRAM bytes (read + write) per site of one launch of `kernel`, from the committed
-    ncu summary of the same kernels on a 2048^2 lattice; None if there is none.  The
-    passes stream their fields once, so the traffic scales with the site count."""
+def ncu_figure(name: str, kernel: str, summary: str = "k_tiled_sib_triangular2048.md"):
+    """A per-kernel figure (`<name> <kernel>: value`) of the committed ncu summary
+    of the SIB passes on a 2048^2 lattice; None if there is none."""
     fn = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(fn):
         return None
-    m = re.search(r"dram_bytes_per_site %s:\s*([0-9.eE+-]+)" % re.escape(kernel), open(fn).read())
+    m = re.search(r"%s %s:\s*([0-9.eE+-]+)" % (re.escape(name), re.escape(kernel)), open(fn).read())
     return float(m.group(1)) if m else None
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes (read + write) per site of one launch of `kernel` (the passes
+    stream their fields once, so the traffic scales with the site count)."""
+    return ncu_figure("dram_bytes_per_site", kernel)
 
 
 # ----------------------------------------------------------------------
@@ -1007,6 +1012,10 @@ def run_gpu(args, rank, world):
         "kernel_config": best,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": ach / pk["hbm_gbs"], "traffic": None if tr is None else tr * N,
+                     # DRAM bytes of the ncu capture over the live launch time, and the
+                     # capture's FP64-pipe utilisation of the same kernel
+                     "dram_gbs": None if tr is None else round(tr * N / (kernels[dom]["avg_us"] * 1e3), 1),
+                     "fp64_pipe_pct": ncu_figure("fp64_pipe_pct", dom),
                      "kernel": dom, "alg_bytes_per_site": bytes_site[dom], "peak_source": pk["source"]},
         "step_roofline": {"alg_bytes_per_site": 120.0, "achieved_gbs": 120.0 * N / (ms_max / K / 1e3) / 1e9,
                           "frac": step_frac, "draw_bytes_per_site": 48.0 if thermal else 0.0},
