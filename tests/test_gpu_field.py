@@ -38,12 +38,12 @@ DECK_NAMES = ["square64_cfg", "triangular64_3shells", "film16x16x6_open_z", "odd
 
 
 def variants(ham):
-    """Kernel variants of a plan: -1 generic, 0..3 tiled (when a shape matched)."""
+    """Kernel variants of a plan: -1 generic, 0..5 tiled (when a shape matched)."""
     from matjes_b200 import _abi
 
     v, s = _abi.C.c_int32(), _abi.C.c_int32()
     _abi.check(_abi.lib.mj_plan_get_variant(ham.plan, _abi.C.byref(v), _abi.C.byref(s)))
-    return [-1, 0, 1, 2, 3] if s.value else [-1]
+    return [-1, 0, 1, 2, 3, 4, 5] if s.value else [-1]
 
 
 def set_variant(ham, v):
