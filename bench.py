@@ -1059,15 +1059,16 @@ PROFILE_RUN_DOC = """Run a few LLG steps of a synthetic workload, for profilers 
     python bench.py --profile-run --lattice triangular --L 4096 --T 10 \
         --integrator sib --variant 2 --steps 3
 
---variant: -1 generic kernel, 0..3 tiled tile shapes, "auto" = the autotuner's pick.
+--variant: -1 generic kernel, 0..5 tiled tile shapes, "auto" = the autotuner's pick.
 
     python bench.py --profile-run --adjoint --L 256 --steps 20 --every 10
 
 runs one forward + backward sweep of the reverse-mode SIB trajectory instead;
 
-    python bench.py --profile-run --batch --steps 3
+    python bench.py --profile-run --batch --steps 3 [--variant 3 --bps 8]
 
-steps the 256-replica batch workload;
+steps the 256-replica batch workload (its configuration autotuned, or the
+batch tile variant 0..4 with --bps blocks per SM);
 
     python bench.py --profile-run --mc --lattice square --L 2048 --steps 3
 
@@ -1090,6 +1091,7 @@ def _prof_main(argv=None):
     ap.add_argument("--T", type=float, default=10.0)
     ap.add_argument("--integrator", default="sib")
     ap.add_argument("--variant", default="auto")
+    ap.add_argument("--bps", type=int, default=8, help="with --batch and a --variant: blocks per SM")
     ap.add_argument("--tma", type=int, default=1, help="halo staging of the tiled kernels: 1 TMA, 0 plain loads")
     ap.add_argument("--fused", type=int, default=0, help="SIB steps: 1 one fused launch, 0 two launches")
     ap.add_argument("--steps", type=int, default=3)
@@ -1217,7 +1219,10 @@ def _prof_batch(a):
     bt.upload(w["m0"])
     d = w["dyn"]
     p = bt.params(timestep=d["timestep"], alpha=d["alpha"], noise="philox", seed=d["seed"])
-    bt.autotune(p, steps=5)  # the configuration the bench's batch key runs
+    if a.variant == "auto":
+        bt.autotune(p, steps=5)  # the configuration the bench's batch key runs
+    else:  # a fixed configuration (the autotuner's timing under a profiler picks another)
+        bt.set_config(int(a.variant), a.bps)
     bt.upload(w["m0"])
     bt.step(p, a.steps)
     torch.cuda.synchronize()
