@@ -676,10 +676,11 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
     bpsite = 240.0
     ach = bpsite * n * nim / per_it / 1e9
     del batch
-    # the same path held on the deck's plan (mj_gneb_path: one field launch of
-    # the plan over all images, then the path sums): 312 algorithmic bytes per
-    # image site and iteration (the field pass 48, the sums m and F in, F out 72,
-    # the step 120, the move 72); the plan's tile variant autotuned first
+    # the same path held on the deck's plan (mj_gneb_path: one launch of the
+    # plan's tiled kernel over all images with the projection and the path sums,
+    # then the per-image sums): 240 algorithmic bytes per image site and
+    # iteration, as the batch (the GNEB pass 48, the step 120, the move 72); the
+    # plan's tile variant autotuned first
     from matjes_b200.gneb import PlanPath
 
     ham_p = mj.Hamiltonian(deck, device=dev)
@@ -698,7 +699,7 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
     call_plan(40)
     per_it_plan = (min(call_plan(600) for _ in range(3)) - min(call_plan(100) for _ in range(3))) / 500
     del holder, ham_p
-    plan_bpsite = 312.0
+    plan_bpsite = 240.0
     plan_ach = plan_bpsite * n * nim / per_it_plan / 1e9
     mod = O.Model(deck)
     O.set_threads(1)
@@ -713,8 +714,9 @@ def run_gneb(dev: int, nim: int = 16, side: int = 256) -> dict:
             "launches_per_iteration": 4,
             "roofline": {"bound": "hbm", "alg_bytes_per_site": bpsite, "achieved": ach, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "peak_source": pk["source"]},
-            "on_plan": {"path": "mj_gneb_path: the images held on the deck's plan, one tiled field launch over all "
-                                "images (5D tensor map with an image index), then the GNEB sums, step and move",
+            "on_plan": {"path": "mj_gneb_path: the images held on the deck's plan, one tiled launch over all "
+                                "images (5D tensor map with an image index) with the projection and the path sums, "
+                                "then the per-image sums, step and move",
                         "value": n * nim / per_it_plan, "us_per_iteration": 1e6 * per_it_plan,
                         "launches_per_iteration": 4, "tile_variant": tv,
                         "roofline": {"bound": "hbm", "alg_bytes_per_site": plan_bpsite, "achieved": plan_ach,

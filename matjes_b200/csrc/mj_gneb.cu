@@ -8,10 +8,12 @@
 // array, image r the SoA block x[N] | y[N] | z[N] at 3 N r.
 //
 // The images' fields: on a tiled plan without the dipolar term one launch over
-// all images (launch_field_images: blockIdx.z runs over image and layer, a 5D
-// TMA map over the path); otherwise per image one field launch (launch_field),
-// the images side by side on forked streams unless the dipolar term's FFT grid
-// is shared; then k_gneb_sums
+// all images (launch_gneb_images: blockIdx.z runs over image and layer, a 5D
+// TMA map over the path) that also projects the field on each spin's tangent
+// plane and leaves per tile the six path sums and the energy, then
+// k_gneb_tile_sums adds the tiles of every image in tile order; otherwise per
+// image one field launch (launch_field), the images side by side on forked
+// streams unless the dipolar term's FFT grid is shared, then k_gneb_sums
 // (projection, the six path sums and, for side-by-side images, the energy of
 // every image) or, for the dipolar term's one-by-one launches that reduce
 // their energies themselves, k_gneb_project outside the iterations.  The rest of
@@ -24,6 +26,25 @@
 
 namespace mj {
 namespace {
+
+// Per image (r = blockIdx.x): its T tile partials of the fused GNEB image pass
+// (partials[q nb + r T + t], q = the six path sums, then the energy) added in
+// tile order, warp q for quantity q, into img[q nrep + r] and E[r].
+__global__ void __launch_bounds__(256) k_gneb_tile_sums(const double* __restrict__ part, int T, int64_t nb, int nrep,
+                                                        double* img, double* E, const GnebCtl* ctl) {
+    if (ctl && ctl->done) return;
+    const int r = blockIdx.x;
+    const int lane = threadIdx.x & 31, q = threadIdx.x >> 5;
+    if (q >= 7) return;
+    const double* pq = part + q * nb + static_cast<int64_t>(r) * T;
+    double v = 0.0;
+    for (int t = lane; t < T; t += 32) v += pq[t];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+        if (q < 6) img[q * nrep + r] = v;
+        else E[r] = v;
+    }
+}
 
 // The field of the images for gneb_relax.  Without the dipolar term the images'
 // field launches share no scratch (no total energy asked, per-site energies
@@ -38,7 +59,9 @@ struct PlanFields {
     GnebIdx X;
     cudaStream_t s;
     bool concurrent;
-    double* part = nullptr;       // partials: 7 per (image, block)
+    bool tiled = false;           // the fused GNEB image pass of a tiled plan (set by setup)
+    int64_t tiles = 0;            // its tiles per image
+    double* part = nullptr;       // partials: 7 per (image, block or tile)
     unsigned int* cnt = nullptr;  // last-block counters, one per image
     double* esite = nullptr;      // per-site energies, image r at [r N, (r + 1) N) (concurrent form)
     double* img0 = nullptr;       // path sums of the calls outside the iterations (unused)
@@ -47,11 +70,13 @@ struct PlanFields {
     cudaEvent_t join[kSide] = {};
 
     mj_status setup(int64_t nblk) {
-        mj_status st = cuda_status(cudaMalloc(&part, sizeof(double) * 7 * nblk * nrep), "GNEB buffers");
+        tiled = concurrent && p->is_stencil && p->sp.shape != 0;
+        const int64_t nper = tiled ? std::max(nblk, tiled_energy_blocks(p)) : nblk;
+        mj_status st = cuda_status(cudaMalloc(&part, sizeof(double) * 7 * nper * nrep), "GNEB buffers");
         if (st == MJ_OK) st = cuda_status(cudaMalloc(&cnt, sizeof(unsigned int) * nrep), "GNEB buffers");
         if (st == MJ_OK) st = cuda_status(cudaMalloc(&img0, sizeof(double) * 6 * nrep), "GNEB buffers");
         if (st == MJ_OK) st = cuda_status(cudaMemsetAsync(cnt, 0, sizeof(unsigned int) * nrep, s), "GNEB buffers");
-        if (st != MJ_OK || !concurrent) return st;
+        if (st != MJ_OK || !concurrent || tiled) return st;
         st = cuda_status(cudaMalloc(&esite, sizeof(double) * X.n * nrep), "GNEB buffers");
         if (st == MJ_OK) st = cuda_status(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "GNEB events");
         for (int k = 0; k < kSide && st == MJ_OK; ++k) {
@@ -78,13 +103,6 @@ struct PlanFields {
             }
             return MJ_OK;
         }
-        if (p->is_stencil && p->sp.shape != 0) {
-            // tiled plans: one launch over all images (image r = blockIdx.z's image)
-            const int rec = prof_begin(p, "k_field_images", s);
-            mj_status e = launch_field_images(p, m, F, esite, nrep, s);
-            prof_end(p, rec, s);
-            return e;
-        }
         const int nside = std::min(kSide, nrep);
         mj_status e = cuda_status(cudaEventRecord(fork, s), "GNEB fork");
         for (int k = 0; k < nside && e == MJ_OK; ++k) e = cuda_status(cudaStreamWaitEvent(side[k], fork, 0), "GNEB fork");
@@ -107,7 +125,18 @@ struct PlanFields {
                                                            img, ctl);
         return cuda_status(cudaGetLastError(), "k_gneb_sums");
     }
+    // tiled plans: one launch over all images (image r = blockIdx.z's image) with
+    // the projection and the tiles' path sums, then the sums of every image
+    mj_status gneb_tiled(double* F, const double* m, double* E, double* img, const GnebCtl* ctl) {
+        const int rec = prof_begin(p, "k_gneb_images", s);
+        mj_status e = launch_gneb_images(p, m, F, part, nrep, &tiles, s);
+        prof_end(p, rec, s);
+        if (e != MJ_OK) return e;
+        k_gneb_tile_sums<<<nrep, 7 * 32, 0, s>>>(part, static_cast<int>(tiles), tiles * nrep, nrep, img, E, ctl);
+        return cuda_status(cudaGetLastError(), "k_gneb_tile_sums");
+    }
     mj_status field(double* F, double* m, double* E) {
+        if (tiled) return gneb_tiled(F, m, E, img0, nullptr);
         mj_status e = images(F, m, E);
         if (e != MJ_OK) return e;
         if (concurrent) return sums(F, m, E, img0, nullptr);
@@ -116,6 +145,7 @@ struct PlanFields {
         return cuda_status(cudaGetLastError(), "k_gneb_project");
     }
     mj_status iterate(double* F, double* m, double* E, double* img, const GnebCtl* ctl) {
+        if (tiled) return gneb_tiled(F, m, E, img, ctl);
         mj_status e = images(F, m, E);
         if (e != MJ_OK) return e;
         return sums(F, m, E, img, ctl);

@@ -277,26 +277,6 @@ __device__ __forceinline__ double3 gneb_tangent_site(const double* __restrict__ 
     return make_double3(t.x - d * m0.x, t.y - d * m0.y, t.z - d * m0.z);
 }
 
-// The six path sums of one site (see the header): A = P(m_{r+1} - m), B =
-// P(m - m_{r-1}) (zero at the ends), |A|^2, A.B, |B|^2, F.A, F.B, squared angle
-// to image r + 1.  The same arithmetic as the batch's GNEB field pass.
-__device__ __forceinline__ void gneb_path_terms(double3 m0, double3 mp, double3 mm, bool up, double3 F, double (&g)[6]) {
-    double3 u = make_double3(mp.x - m0.x, mp.y - m0.y, mp.z - m0.z);
-    double3 w = make_double3(m0.x - mm.x, m0.y - mm.y, m0.z - mm.z);
-    const double du = dot(u, m0), dw = dot(w, m0);
-    u = make_double3(u.x - du * m0.x, u.y - du * m0.y, u.z - du * m0.z);
-    w = make_double3(w.x - dw * m0.x, w.y - dw * m0.y, w.z - dw * m0.z);
-    g[0] += dot(u, u);
-    g[1] += dot(u, w);
-    g[2] += dot(w, w);
-    g[3] += dot(F, u);
-    g[4] += dot(F, w);
-    if (up) {
-        const double3 c = cross(m0, mp);
-        const double l = atan2(sqrt(dot(c, c)), dot(m0, mp));
-        g[5] += l * l;
-    }
-}
 
 // Per image (r = blockIdx.x): F projected in place and the six path sums; the
 // last block of an image sums the partials in block order into img[q nrep + r].

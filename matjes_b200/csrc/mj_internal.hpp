@@ -264,15 +264,18 @@ MJ_FUSED_SHAPE_DECL(launch_sib_fused_square_nn)
 MJ_FUSED_SHAPE_DECL(launch_sib_fused_square2)
 MJ_FUSED_SHAPE_DECL(launch_sib_fused_tri_nn)
 MJ_FUSED_SHAPE_DECL(launch_sib_fused_tri3)
-// field and per-site energies of nimg lattices stored back to back, one launch
-// (tiled plans without the dipolar term; the GNEB images on a plan)
-mj_status launch_field_images(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s);
-#define MJ_IMAGES_SHAPE_DECL(fn) \
-    mj_status fn(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s);
-MJ_IMAGES_SHAPE_DECL(launch_field_images_square_nn)
-MJ_IMAGES_SHAPE_DECL(launch_field_images_square2)
-MJ_IMAGES_SHAPE_DECL(launch_field_images_tri_nn)
-MJ_IMAGES_SHAPE_DECL(launch_field_images_tri3)
+// The GNEB images of a path on a tiled plan without the dipolar term: the
+// projected field into F and per tile the six path sums and the energy
+// (partials[q nblocks + tile], tiles image-major, *tiles_per_image of them).
+mj_status launch_gneb_images(mj_plan* p, const double* m, double* F, double* partials, int nimg,
+                             int64_t* tiles_per_image, cudaStream_t s);
+#define MJ_GNEB_SHAPE_DECL(name)                                                                       \
+    mj_status name(mj_plan* p, const double* m, double* F, double* partials, int nimg, int64_t* tiles, \
+                   cudaStream_t s);
+MJ_GNEB_SHAPE_DECL(launch_gneb_images_square_nn)
+MJ_GNEB_SHAPE_DECL(launch_gneb_images_square2)
+MJ_GNEB_SHAPE_DECL(launch_gneb_images_tri_nn)
+MJ_GNEB_SHAPE_DECL(launch_gneb_images_tri3)
 // scheduler words of the fused step: 2 + tile rows at the smallest tile height
 int64_t sched_words(const mj_plan* p);
 MJ_TILED_SHAPE_DECL(launch_tiled_square_nn)

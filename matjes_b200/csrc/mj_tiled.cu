@@ -52,12 +52,13 @@ mj_status launch_sib_fused(mj_plan* p, const DynCoef& C, double* m, double* draw
     }
 }
 
-mj_status launch_field_images(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s) {
+mj_status launch_gneb_images(mj_plan* p, const double* m, double* F, double* partials, int nimg,
+                             int64_t* tiles_per_image, cudaStream_t s) {
     switch (p->sp.shape) {
-        case kShapeSquareNN: return launch_field_images_square_nn(p, m, B, e_site, nimg, s);
-        case kShapeSquare2: return launch_field_images_square2(p, m, B, e_site, nimg, s);
-        case kShapeTriNN: return launch_field_images_tri_nn(p, m, B, e_site, nimg, s);
-        case kShapeTri3: return launch_field_images_tri3(p, m, B, e_site, nimg, s);
+        case kShapeSquareNN: return launch_gneb_images_square_nn(p, m, F, partials, nimg, tiles_per_image, s);
+        case kShapeSquare2: return launch_gneb_images_square2(p, m, F, partials, nimg, tiles_per_image, s);
+        case kShapeTriNN: return launch_gneb_images_tri_nn(p, m, F, partials, nimg, tiles_per_image, s);
+        case kShapeTri3: return launch_gneb_images_tri3(p, m, F, partials, nimg, tiles_per_image, s);
         default: return set_error(MJ_ERR_ARG, "no tiled kernel for this stencil shape");
     }
 }

@@ -41,7 +41,10 @@
 namespace mj {
 namespace {
 
-enum { PASS_FIELD = 0, PASS_EULER = 1, PASS_HEUN1 = 2, PASS_HEUN2 = 3, PASS_SIB1 = 4, PASS_SIB2 = 5 };
+// PASS_GNEB: the field of GNEB images (a launch over nimg images), projected
+// on each spin's tangent plane and stored, with each tile's six path sums and
+// energy as block partials
+enum { PASS_FIELD = 0, PASS_EULER = 1, PASS_HEUN1 = 2, PASS_HEUN2 = 3, PASS_SIB1 = 4, PASS_SIB2 = 5, PASS_GNEB = 6 };
 enum { SP_FULL = 0, SP_AXIAL = 1 };
 
 // Energy reduction of a launch.  mode 0: grid_reduce into `out` (if set);
@@ -75,6 +78,7 @@ struct TiledArgs {
                         // back to back (3N doubles apart in ms / out, N in aux)
     int smem_bytes;     // host side: dynamic shared memory of the launch when above the
                         // tile's (caps the resident blocks per SM; the excess is unused)
+    int img_up, img_dn; // PASS_GNEB, set per block: the image has a next / a previous one
 };
 
 // Programmatic dependent launch: a kernel lets the next one in its stream launch
@@ -446,7 +450,8 @@ __device__ __forceinline__ void prefetch_sites(const StencilParams& P, const Dyn
 template <class S, int BYT, int RY, int PASS, int SP, bool ZMAP, bool HD>
 __device__ __forceinline__ double sites_epilogue(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
                                                  const double* sm, int x0, int y0, int z, const Pre* pre,
-                                                 const double* bx, const double* by, const double* bz) {
+                                                 const double* bx, const double* by, const double* bz,
+                                                 double (&g6)[6]) {
     using G = TileGeom<S, BYT, RY>;
     const int Lx = P.L[0], Ly = P.L[1];
     const int64_t layer = static_cast<int64_t>(Lx) * Ly;
@@ -487,9 +492,21 @@ __device__ __forceinline__ double sites_epilogue(const StencilParams& P, const D
             constexpr bool ZAX = SP == SP_AXIAL && !ZMAP;
             const double3 Brs =
                 ZAX ? make_double3(b0, b1, b2 + Bzee.z) : make_double3(b0 + Bzee.x, b1 + Bzee.y, b2 + Bzee.z);
-            double3 hd = make_double3(0.0, 0.0, 0.0);
-            if constexpr (HD) hd = ld_dip(A.Hd, x, y, z);
-            e += epilogue<PASS, HD, ZAX>(C, A, i, N, m0, Brs, Bzee, hd, pre[r]);
+            if constexpr (PASS == PASS_GNEB) {
+                // the image's site energy (energy_distrib, as the field pass stores
+                // it), the field projected on the tangent plane, the path sums
+                e += -0.5 * (dot(m0, Brs) + (ZAX ? m0.z * Bzee.z : dot(m0, Bzee)));
+                const double d = dot(Brs, m0);
+                const double3 f = make_double3(Brs.x - d * m0.x, Brs.y - d * m0.y, Brs.z - d * m0.z);
+                st3(A.out, i, N, f);
+                const double3 mp = A.img_up ? ld3(A.ms + 3 * N, i, N) : m0;
+                const double3 mm = A.img_dn ? ld3(A.ms - 3 * N, i, N) : m0;
+                gneb_path_terms(m0, mp, mm, A.img_up != 0, f, g6);
+            } else {
+                double3 hd = make_double3(0.0, 0.0, 0.0);
+                if constexpr (HD) hd = ld_dip(A.Hd, x, y, z);
+                e += epilogue<PASS, HD, ZAX>(C, A, i, N, m0, Brs, Bzee, hd, pre[r]);
+            }
         }
     }
     return e;
@@ -498,20 +515,25 @@ __device__ __forceinline__ double sites_epilogue(const StencilParams& P, const D
 // stencil + epilogue of one staged tile; returns the energy of its sites
 template <class S, int BYT, int RY, int PASS, int SP>
 __device__ __forceinline__ double compute_tile(const StencilParams& P, const DynCoef& C, const TiledArgs& A,
-                                               const double* sm, int x0, int y0, int z, const Pre* pre) {
+                                               const double* sm, int x0, int y0, int z, const Pre* pre,
+                                               double (&g6)[6]) {
     using G = TileGeom<S, BYT, RY>;
     double bx[RY], by[RY], bz[RY];
 #pragma unroll
     for (int r = 0; r < RY; ++r) bx[r] = by[r] = bz[r] = 0.0;
     const int base = (threadIdx.y * RY) * G::PX + threadIdx.x;
     all_columns<S, BYT, RY, SP>(P, sm, base, bx, by, bz, std::make_integer_sequence<int, 2 * S::R + 1>{});
-    // the branches are uniform over the launch
+    // the branches are uniform over the launch; the GNEB images have no dipolar term
     if (A.bmap) {
-        if (A.Hd.h) return sites_epilogue<S, BYT, RY, PASS, SP, true, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
-        return sites_epilogue<S, BYT, RY, PASS, SP, true, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
+        if constexpr (PASS != PASS_GNEB)
+            if (A.Hd.h)
+                return sites_epilogue<S, BYT, RY, PASS, SP, true, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz, g6);
+        return sites_epilogue<S, BYT, RY, PASS, SP, true, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz, g6);
     }
-    if (A.Hd.h) return sites_epilogue<S, BYT, RY, PASS, SP, false, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
-    return sites_epilogue<S, BYT, RY, PASS, SP, false, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz);
+    if constexpr (PASS != PASS_GNEB)
+        if (A.Hd.h)
+            return sites_epilogue<S, BYT, RY, PASS, SP, false, true>(P, C, A, sm, x0, y0, z, pre, bx, by, bz, g6);
+    return sites_epilogue<S, BYT, RY, PASS, SP, false, false>(P, C, A, sm, x0, y0, z, pre, bx, by, bz, g6);
 }
 
 // ---------------------------------------------------------------------------
@@ -586,6 +608,8 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
         if (A.out) A.out += 3 * n * img;
         if (A.aux) A.aux += n * img;
     }
+    A.img_up = img + 1 < A0.nimg ? 1 : 0;
+    A.img_dn = img > 0 ? 1 : 0;
     const int x0 = blockIdx.x * G::TX, y0 = by * G::TY;
     const int bid = blockIdx.x + gridDim.x * (by + nty * blockIdx.z);
     const int tid = threadIdx.x + 32 * threadIdx.y;
@@ -644,7 +668,13 @@ __global__ void __launch_bounds__(32 * BYT, MINB) k_tiled(const __grid_constant_
         prefetch_sites<S, BYT, RY, PASS>(P, C, A, x0, y0, z, pre);
         __syncthreads();
     }
-    const double e = ok ? compute_tile<S, BYT, RY, PASS, SP>(P, C, A, smem_t, x0, y0, z, pre) : 0.0;
+    double g6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double e = ok ? compute_tile<S, BYT, RY, PASS, SP>(P, C, A, smem_t, x0, y0, z, pre, g6) : 0.0;
+    if constexpr (PASS == PASS_GNEB) {  // the tile's path sums and energy, image-major
+        double v[7] = {g6[0], g6[1], g6[2], g6[3], g6[4], g6[5], e};
+        block_partials<7>(v, A.R.partials, A.R.nblocks, bid);
+        return;
+    }
     if (A.R.mode == 1) {
         double v[1] = {e};
         block_partials<1>(v, A.R.partials, A.R.nblocks, bid);
@@ -771,7 +801,8 @@ __device__ __forceinline__ bool fused_predictor(const CUtensorMap* map, const St
     const int x0 = tx * G::TX, y0 = ty * G::TY;
     Pre pre[RY];
     if (!fused_stage<S, BYT, RY, PASS_SIB1, false>(map, P, C, A, F.tma, sm, bar, phase, x0, y0, z, pre)) return false;
-    const double e = compute_tile<S, BYT, RY, PASS_SIB1, SP>(P, C, A, sm, x0, y0, z, pre);
+    double g6[6];
+    const double e = compute_tile<S, BYT, RY, PASS_SIB1, SP>(P, C, A, sm, x0, y0, z, pre, g6);
     double v[1] = {e};
     block_partials<1>(v, F.partials, T, t);  // after the tile's stores
     __syncthreads();
@@ -799,7 +830,8 @@ __device__ __forceinline__ bool fused_corrector(const CUtensorMap* map, const St
     const int x0 = tx * G::TX, y0 = ty * G::TY;
     Pre pre[RY];
     if (!fused_stage<S, BYT, RY, PASS_SIB2, true>(map, P, C, A, F.tma, sm, bar, phase, x0, y0, z, pre)) return false;
-    compute_tile<S, BYT, RY, PASS_SIB2, SP>(P, C, A, sm, x0, y0, z, pre);
+    double g6[6];
+    compute_tile<S, BYT, RY, PASS_SIB2, SP>(P, C, A, sm, x0, y0, z, pre, g6);
     return true;
 }
 
@@ -950,6 +982,7 @@ mj_status tiled_pass_sp(int pass, const CUtensorMap& map, const StencilParams& P
     using L = TiledLauncher<S, BYT, RY, MINB>;
     switch (pass) {
         case PASS_FIELD: return L::template launch<PASS_FIELD, SP>(map, P, C, A, s);
+        case PASS_GNEB: return L::template launch<PASS_GNEB, SP>(map, P, C, A, s);
         case PASS_EULER: return L::template launch<PASS_EULER, SP>(map, P, C, A, s);
         case PASS_HEUN1: return L::template launch<PASS_HEUN1, SP>(map, P, C, A, s);
         case PASS_HEUN2: return L::template launch<PASS_HEUN2, SP>(map, P, C, A, s);
@@ -1122,17 +1155,17 @@ mj_status launch_sib_fused_shape(mj_plan* p, const DynCoef& C, double* m, double
     });
 }
 
-// The field and per-site energies (PASS_FIELD) of nimg lattices stored back to
-// back (m and B: 3N doubles apart; e_site: N apart) in one launch; no total
-// energy.  The GNEB on a plan evaluates its images this way.
+// The GNEB images of a path held on the plan (nimg lattices back to back in m):
+// per site the field projected on the spin's tangent plane into F, per tile the
+// six path sums and the energy into partials[q nblocks + tile] (tiles image-major;
+// *tiles_per_image receives the count).  No dipolar term.
 template <class S>
-mj_status launch_field_images_shape(mj_plan* p, const double* m, double* B, double* e_site, int nimg,
-                                    cudaStream_t s) {
+mj_status launch_gneb_images_shape(mj_plan* p, const double* m, double* F, double* partials, int nimg,
+                                   int64_t* tiles_per_image, cudaStream_t s) {
     TiledArgs A;
     std::memset(&A, 0, sizeof(A));
     A.ms = m;
-    A.out = B;
-    A.aux = e_site;
+    A.out = F;
     A.bmap = p->d_bmap;
     A.status = p->d_status;
     A.nimg = nimg;
@@ -1142,10 +1175,14 @@ mj_status launch_field_images_shape(mj_plan* p, const double* m, double* B, doub
     return with_variant<S>(p->tile_variant, [&](auto L) -> mj_status {
         using Launcher = decltype(L);
         using G = typename Launcher::G;
+        const dim3 g = Launcher::grid(p->sp);
+        *tiles_per_image = static_cast<int64_t>(g.x) * g.y * g.z;
+        A.R.partials = partials;
+        A.R.nblocks = static_cast<int>(*tiles_per_image * nimg);
         CUtensorMap map;
         std::memset(&map, 0, sizeof(map));
         if (p->use_tma && make_map_images(&map, m, p->sp, nimg, G::PX, G::PY)) A.tma = 1;
-        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(PASS_FIELD, axial,
+        return tiled_pass<typename Launcher::Shape, Launcher::BYT_, Launcher::RY_, Launcher::MINB_>(PASS_GNEB, axial,
                                                                                                    map, p->sp, C, A, s);
     });
 }

@@ -11,7 +11,8 @@ mj_status launch_sib_fused_tri_nn(mj_plan* p, const DynCoef& C, double* m, doubl
                          cudaStream_t s) {
     return launch_sib_fused_shape<ShapeTriNN>(p, C, m, draw, E_out, step, s);
 }
-mj_status launch_field_images_tri_nn(mj_plan* p, const double* m, double* B, double* e_site, int nimg, cudaStream_t s) {
-    return launch_field_images_shape<ShapeTriNN>(p, m, B, e_site, nimg, s);
+mj_status launch_gneb_images_tri_nn(mj_plan* p, const double* m, double* F, double* partials, int nimg,
+                         int64_t* tiles, cudaStream_t s) {
+    return launch_gneb_images_shape<ShapeTriNN>(p, m, F, partials, nimg, tiles, s);
 }
 }  // namespace mj
