@@ -35,12 +35,16 @@ struct McCoef {
     uint32_t stream;
 };
 
+// blocks of 32 x kMcBY threads: 52 registers a thread hold nine blocks of 128
+// threads per SM (36 warps) where blocks of 256 held four (32 warps)
+constexpr int kMcBY = 4;
+
 // S: the plan's compile-time stencil shape, void for runtime offsets
 template <class S>
-__global__ void __launch_bounds__(256, 4) k_mc_color(const __grid_constant__ StencilParams P, const double* __restrict__ bmap,
+__global__ void __launch_bounds__(32 * kMcBY, 8) k_mc_color(const __grid_constant__ StencilParams P, const double* __restrict__ bmap,
                                                   double* m, const McCoef C, const McClass K,
                                                   unsigned long long* accepted) {
-    const int y = K.ry + K.sy * static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    const int y = K.ry + K.sy * static_cast<int>(blockIdx.y * kMcBY + threadIdx.y);
     const int z = K.rz + K.sz * static_cast<int>(blockIdx.z);
     const int x = mc_class_x(K, y, z, static_cast<int>(blockIdx.x * 32 + threadIdx.x));
     bool acc = false;
@@ -125,7 +129,7 @@ mj_status mj_mc_sweeps(mj_plan* plan, double* m, mj_mc_params* p, int32_t nsweep
     const McClass& K0 = classes[0];
     const int sub[3] = {(plan->sp.L[0] + K0.qx - 1) / K0.qx, (plan->sp.L[1] + K0.sy - 1) / K0.sy,
                         (plan->sp.L[2] + K0.sz - 1) / K0.sz};
-    const dim3 grid((sub[0] + 31) / 32, (sub[1] + 7) / 8, sub[2]), blk(32, 8);
+    const dim3 grid((sub[0] + 31) / 32, (sub[1] + kMcBY - 1) / kMcBY, sub[2]), blk(32, kMcBY);
     const int nbc = static_cast<int>(grid.x * grid.y * grid.z);  // blocks of one colour pass
     const int ncol = static_cast<int>(classes.size());
     const bool track = p->track_totals && (E_dev || M_dev);
