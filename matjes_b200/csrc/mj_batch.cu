@@ -317,7 +317,7 @@ __global__ void k_pt_swap(BatchRep* reps, int* image, const double* slot_kT, int
 // replica is a chain of its own (its own cone and counts, Philox stream
 // stream_id + r, its site index within the replica), moved colour by colour at
 // the temperature its ladder slot holds; the moves are mj_mc.cuh's.  MC tiles
-// are (replica, tx block, ty block) of 32 x 8 threads over a colour class.
+// are (replica, tx block, ty block) of 32 x kMcBY threads over a colour class.
 struct BatchMcArgs {
     const double* tab;          // sin/cos tables
     const BatchRep* reps;
@@ -334,12 +334,12 @@ struct BatchMcArgs {
 };
 
 template <class S>
-__global__ void __launch_bounds__(256) k_batch_mc(const __grid_constant__ StencilParams P,
+__global__ void __launch_bounds__(32 * kMcBY, 8) k_batch_mc(const __grid_constant__ StencilParams P,
                                                   const __grid_constant__ BatchMcArgs A) {
     const int4 tl = A.tiles[blockIdx.x];
     const BatchRep R = A.reps[tl.x];
     const McClass& K = A.K;
-    const int y = K.ry + K.sy * (tl.z * 8 + static_cast<int>(threadIdx.y));
+    const int y = K.ry + K.sy * (tl.z * kMcBY + static_cast<int>(threadIdx.y));
     const int z = K.rz;  // replicas are one layer thick
     const int x = mc_class_x(K, y, z, tl.y * 32 + static_cast<int>(threadIdx.x));
     bool acc = false;
@@ -1108,7 +1108,7 @@ static mj_status batch_mc_setup(mj_batch* b, double cone0, cudaStream_t s) {
     std::vector<int4> tiles;
     for (int r = 0; r < b->nrep; ++r) {
         const int nx = (b->reps[r].Lx + K0.qx - 1) / K0.qx, ny = (b->reps[r].Ly + K0.sy - 1) / K0.sy;
-        for (int by = 0; by < (ny + 7) / 8; ++by)
+        for (int by = 0; by < (ny + kMcBY - 1) / kMcBY; ++by)
             for (int bx = 0; bx < (nx + 31) / 32; ++bx) tiles.push_back(make_int4(r, bx, by, 0));
     }
     b->mc_ntile = static_cast<int>(tiles.size());
@@ -1177,11 +1177,11 @@ mj_status mj_batch_mc(mj_batch* b, mj_mc_params* p, int32_t nrounds, int32_t swe
             for (const McClass& K : classes) {
                 A.K = K;
                 switch (b->shape) {
-                    case kShapeSquareNN: k_batch_mc<ShapeSquareNN><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
-                    case kShapeSquare2: k_batch_mc<ShapeSquare2><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
-                    case kShapeTriNN: k_batch_mc<ShapeTriNN><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
-                    case kShapeTri3: k_batch_mc<ShapeTri3><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A); break;
-                    default: k_batch_mc<void><<<b->mc_ntile, dim3(32, 8), 0, s>>>(b->sp, A);
+                    case kShapeSquareNN: k_batch_mc<ShapeSquareNN><<<b->mc_ntile, dim3(32, kMcBY), 0, s>>>(b->sp, A); break;
+                    case kShapeSquare2: k_batch_mc<ShapeSquare2><<<b->mc_ntile, dim3(32, kMcBY), 0, s>>>(b->sp, A); break;
+                    case kShapeTriNN: k_batch_mc<ShapeTriNN><<<b->mc_ntile, dim3(32, kMcBY), 0, s>>>(b->sp, A); break;
+                    case kShapeTri3: k_batch_mc<ShapeTri3><<<b->mc_ntile, dim3(32, kMcBY), 0, s>>>(b->sp, A); break;
+                    default: k_batch_mc<void><<<b->mc_ntile, dim3(32, kMcBY), 0, s>>>(b->sp, A);
                 }
             }
             k_batch_mc_cone<<<(nrep + 127) / 128, 128, 0, s>>>(b->d_reps, nrep, b->d_mc_acc, b->d_mc_prop,

@@ -35,10 +35,6 @@ struct McCoef {
     uint32_t stream;
 };
 
-// blocks of 32 x kMcBY threads: 52 registers a thread hold nine blocks of 128
-// threads per SM (36 warps) where blocks of 256 held four (32 warps)
-constexpr int kMcBY = 4;
-
 // S: the plan's compile-time stencil shape, void for runtime offsets
 template <class S>
 __global__ void __launch_bounds__(32 * kMcBY, 8) k_mc_color(const __grid_constant__ StencilParams P, const double* __restrict__ bmap,

@@ -162,6 +162,11 @@ __device__ __forceinline__ bool mc_move(const StencilParams& P, const uint32_t* 
     return acc;
 }
 
+// Colour-pass blocks of 32 x kMcBY threads: at 52-56 registers a thread, nine
+// blocks of 128 threads fit an SM (36 warps) where blocks of 256 held four
+// (32 warps).
+constexpr int kMcBY = 4;
+
 // One colour class of a sweep: the sites y = ry + sy ty, z = rz + sz tz,
 // x = ((k - b y - c z) mod qx) + qx tx.  A linear colouring (q, b, c) has
 // qx = q, sy = sz = 1, colour k; a product colouring (cx, cy, cz) has qx = cx,
